@@ -1,0 +1,331 @@
+"""Generate the golden fixtures that pin the oracle to the reference.
+
+Runs the UNMODIFIED dsa110-rt reference (``src/dsart``, imported from a
+local checkout given by ``--reference`` / ``$DSART_REFERENCE``) on seeded
+inputs at its native geometry (96 antennas, 16 x 384 channels) and writes
+small ``.npz`` fixtures next to this script.  Large inputs are not stored:
+they are regenerated from the recorded seed with numpy's PCG64 (bit-stable
+across platforms) and the fixture stores exact fingerprints (hashes, exact
+integer sums, sampled elements).
+
+Usage (in a container where the reference checkout exists):
+
+    python tests/golden/make_golden.py --reference <dsa110-rt>/src
+
+The GPU box never runs this script; tests only read the ``.npz`` files.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# ---------------------------------------------------------------------------
+# Shared seeded-input recipes (the tests import these to regenerate inputs)
+# ---------------------------------------------------------------------------
+
+UNPACK_SEED = 20261203
+CORR_SEED = 7301
+STAGE1_SEED = 4242
+
+
+def t_layout_antpos(nants: int, seed: int, ew_m: float = 2600.0, ns_m: float = 1600.0):
+    """Seeded T layout: ~60% of antennas on the EW arm, the rest on the NS arm."""
+    rng = np.random.default_rng(seed)
+    n_ew = int(round(nants * 0.6))
+    e = np.empty(nants)
+    n = np.empty(nants)
+    e[:n_ew] = np.sort(rng.uniform(-ew_m / 2, ew_m / 2, n_ew))
+    n[:n_ew] = rng.normal(0.0, 2.0, n_ew)
+    n[n_ew:] = -np.sort(rng.uniform(5.0, ns_m, nants - n_ew))
+    e[n_ew:] = rng.normal(0.0, 2.0, nants - n_ew)
+    return e.astype(np.float64), n.astype(np.float64)
+
+
+def unpack_raw(seed: int = UNPACK_SEED) -> np.ndarray:
+    """Full reference fada page: 2048 x 96 x 384 x 2 x 2 bytes."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 256, size=2048 * 96 * 384 * 4, dtype=np.uint8)
+
+
+def corr_raw(npkt: int, nant: int, nchan: int, seed: int = CORR_SEED) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 256, size=npkt * nant * nchan * 4, dtype=np.uint8)
+
+
+def stage1_vis(n_fv: int, nbase: int, nchan_eff: int, seed: int) -> np.ndarray:
+    """Integer-valued complex64 visibilities in ``[-50, 50]``."""
+    rng = np.random.default_rng(seed)
+    re = rng.integers(-50, 51, size=(n_fv, nbase, nchan_eff)).astype(np.float32)
+    im = rng.integers(-50, 51, size=(n_fv, nbase, nchan_eff)).astype(np.float32)
+    return (re + 1j * im).astype(np.complex64)
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+# ---------------------------------------------------------------------------
+# Fixture builders
+# ---------------------------------------------------------------------------
+
+
+def make_unpack():
+    import torch
+    from dsart.services.slow_corr_kernel import unpack_int4_split
+    raw = unpack_raw()
+    re, im = unpack_int4_split(raw, device="cpu", scale=1.0, out_dtype=torch.float32)
+    re8 = re.numpy().astype(np.int8)
+    im8 = im.numpy().astype(np.int8)
+    rng = np.random.default_rng(1)
+    idx = rng.integers(0, re8.size, 4096)
+    np.savez_compressed(
+        os.path.join(HERE, "unpack.npz"),
+        seed=UNPACK_SEED, shape=np.asarray(re8.shape),
+        sha_re=sha(re8), sha_im=sha(im8),
+        idx=idx, re_s=re8.reshape(-1)[idx], im_s=im8.reshape(-1)[idx],
+    )
+
+
+def make_corr():
+    import torch
+    from dsart.services.corr_fast_kernel import FastCorrKernel
+    out = {}
+    # (a) fused Stokes-I + chan-sum at 96 antennas
+    npkt, nant, nchan, t_int, csf = 8, 96, 16, 8, 4
+    raw = corr_raw(npkt, nant, nchan).reshape(npkt, nant, nchan, 2, 2)
+    r8 = torch.from_numpy(raw.view(np.int8).copy())
+    re = ((r8 << 4) >> 4).permute(2, 3, 4, 0, 1).contiguous().to(torch.float32)
+    im = (r8 >> 4).permute(2, 3, 4, 0, 1).contiguous().to(torch.float32)
+    k = FastCorrKernel(device="cpu", t_int_fast_native=t_int, nants=nant, nchan=nchan)
+    vis = k.compute_split(re, im, fuse_stokes_i=True, chan_sum_factor=csf).numpy()
+    out.update(si_npkt=npkt, si_nant=nant, si_nchan=nchan, si_t_int=t_int, si_csf=csf,
+               si_re=vis.real.astype(np.float32), si_im=vis.imag.astype(np.float32))
+    # (b) legacy 2-pol output, small array, n_fv chunking exercised
+    npkt, nant, nchan, t_int = 16, 10, 6, 4
+    raw = corr_raw(npkt, nant, nchan, seed=CORR_SEED + 1).reshape(npkt, nant, nchan, 2, 2)
+    r8 = torch.from_numpy(raw.view(np.int8).copy())
+    re = ((r8 << 4) >> 4).permute(2, 3, 4, 0, 1).contiguous().to(torch.float32)
+    im = (r8 >> 4).permute(2, 3, 4, 0, 1).contiguous().to(torch.float32)
+    k = FastCorrKernel(device="cpu", t_int_fast_native=t_int, nants=nant, nchan=nchan)
+    vis = k.compute_split(re, im, n_fv_chunk=3).numpy()
+    out.update(p2_npkt=npkt, p2_nant=nant, p2_nchan=nchan, p2_t_int=t_int,
+               p2_re=vis.real.astype(np.float32), p2_im=vis.imag.astype(np.float32))
+    np.savez_compressed(os.path.join(HERE, "corr.npz"), **out)
+
+
+def make_grid_and_plan():
+    import torch
+    from dsart.grid.sparsity_pattern import (build_pattern, compute_top_of_band_cell_lambda)
+    from dsart.grid.kernel import FastVisGridder
+    from dsart.coarse_dm.synthetic_plan import build_synthetic_summed_plan
+    from dsart.coarse_dm.stage2_shifts import compute_stage2_shifts
+    from dsart.fine_dm.combiner import compute_time_shift_search
+    e, n = t_layout_antpos(96, seed=11)
+    n_grid, csf = 256, 8
+    cell = compute_top_of_band_cell_lambda(e, n, n_grid=n_grid)
+    out = dict(antpos_e=e, antpos_n=n, n_grid=n_grid, csf=csf, cell_lambda=cell)
+    for g in (0, 15):
+        pat = build_pattern(e, n, chgroup=g, dec_deg=37.0, n_grid=n_grid,
+                            chan_sum_factor=csf, cell_lambda=cell)
+        grd = FastVisGridder.from_pattern(pat, e, n, device="cpu")
+        cim = grd.cell_index_map.numpy().reshape(4656, 384 // csf)
+        out[f"ix_row_{g}"] = pat.ix_row
+        out[f"ix_col_{g}"] = pat.ix_col
+        out[f"cim_{g}"] = cim.astype(np.int32)
+        out[f"cellw_{g}"] = grd.cell_weights.numpy()
+        if g == 15:
+            vis = stage1_vis(2, 4656, 384 // csf, seed=55)
+            gv = grd.compute(torch.from_numpy(vis)).numpy()
+            out["grid_in_seed"] = 55
+            out["grid_out"] = gv
+    # DM plan delay bins (all chgroups)
+    coarse = np.linspace(0.0, 3000.0, 16)
+    plan = build_synthetic_summed_plan(n_coarse=16, dm_max=3000.0, chan_sum_factor=csf,
+                                       t_int_fast_us=8 * 32.768)
+    out["plan_coarse"] = coarse
+    out["plan_bins"] = np.stack([plan.delay_bins_per_chgroup(g) for g in range(16)])
+    out["plan_nat"] = np.stack([plan.delay_native_samples_per_chgroup(g) for g in range(16)])
+    # stage-2 shifts, all chgroups
+    cd = np.asarray([0.0, 50.0, 258.0, 581.5, 1312.0, 2962.0])
+    out["s2_coarse"] = cd
+    out["s2_shifts"] = np.stack([
+        compute_stage2_shifts(chgroup=g, coarse_dm_pc_cm3=cd, t_int_corr_us=262.144).shifts_samples
+        for g in range(16)])
+    # fine-DM shift table, merged rounding + plain
+    coarse8 = np.linspace(100.0, 1500.0, 8)
+    fine = np.linspace(60.0, 1540.0, 64)
+    f2c = np.clip(np.searchsorted(coarse8, fine) , 0, 7).astype(np.int64)
+    t_int = 262.144
+    tab_m = compute_time_shift_search(coarse_dm_pc_cm3=coarse8, fine_dm_pc_cm3=fine,
+                                      fine_to_coarse=f2c, t_int_search_us=t_int,
+                                      merge_coarse_rounding=True, t_int_corr_us=t_int)
+    tab_p = compute_time_shift_search(coarse_dm_pc_cm3=coarse8, fine_dm_pc_cm3=fine,
+                                      fine_to_coarse=f2c, t_int_search_us=t_int)
+    out.update(fs_coarse=coarse8, fs_fine=fine, fs_f2c=f2c, fs_t_int=t_int,
+               fs_merged=tab_m.shifts, fs_plain=tab_p.shifts)
+    np.savez_compressed(os.path.join(HERE, "grid_plan.npz"), **out)
+
+
+def make_stage1():
+    import torch
+    from dsart.grid.sparsity_pattern import build_pattern, compute_top_of_band_cell_lambda
+    from dsart.grid.kernel import FastVisGridder
+    from dsart.coarse_dm.synthetic_plan import build_synthetic_summed_plan
+    from dsart.services.corr_fast_integration import Stage1MultiDMCoarseDM
+    e, n = t_layout_antpos(96, seed=11)
+    n_grid, csf, g = 256, 8, 15
+    cell = compute_top_of_band_cell_lambda(e, n, n_grid=n_grid)
+    pat = build_pattern(e, n, chgroup=g, dec_deg=37.0, n_grid=n_grid,
+                        chan_sum_factor=csf, cell_lambda=cell)
+    grd = FastVisGridder.from_pattern(pat, e, n, device="cpu")
+    plan = build_synthetic_summed_plan(n_coarse=6, dm_max=150.0, chan_sum_factor=csf,
+                                       t_int_fast_us=8 * 32.768)
+    st = Stage1MultiDMCoarseDM(plan=plan, gridder=grd, chgroup=g, sliding_window=True)
+    n_fv = 32
+    outs = {}
+    for blk in range(3):
+        vis = stage1_vis(n_fv, 4656, 384 // csf, seed=STAGE1_SEED + blk)
+        o = st.dedisperse_from_vis(torch.from_numpy(vis), block_n=blk).numpy()
+        re = np.rint(o.real).astype(np.int64)
+        im = np.rint(o.imag).astype(np.int64)
+        assert np.array_equal(re, o.real) and np.array_equal(im, o.imag)
+        outs[f"b{blk}_sum_t_re"] = re.sum(axis=1)
+        outs[f"b{blk}_sum_t_im"] = im.sum(axis=1)
+        outs[f"b{blk}_sum_c_re"] = re.sum(axis=2)
+        outs[f"b{blk}_sum_c_im"] = im.sum(axis=2)
+        rng = np.random.default_rng(blk)
+        idx = rng.integers(0, o.size, 2048)
+        outs[f"b{blk}_idx"] = idx
+        outs[f"b{blk}_re_s"] = o.real.reshape(-1)[idx]
+        outs[f"b{blk}_im_s"] = o.imag.reshape(-1)[idx]
+        outs[f"b{blk}_shape"] = np.asarray(o.shape)
+    # non-sliding single window
+    st2 = Stage1MultiDMCoarseDM(plan=plan, gridder=grd, chgroup=g, sliding_window=False)
+    vis = stage1_vis(n_fv, 4656, 384 // csf, seed=STAGE1_SEED + 9)
+    o = st2.dedisperse_from_vis(torch.from_numpy(vis), block_n=0).numpy()
+    outs["ns_shape"] = np.asarray(o.shape)
+    outs["ns_sum_t_re"] = np.rint(o.real).astype(np.int64).sum(axis=1)
+    outs["ns_sum_c_im"] = np.rint(o.imag).astype(np.int64).sum(axis=2)
+    outs["bins"] = plan.delay_bins_per_chgroup(g)
+    outs.update(seed=STAGE1_SEED, n_fv=n_fv, chgroup=g, csf=csf, n_grid=n_grid,
+                dm_max=150.0, n_coarse=6)
+    np.savez_compressed(os.path.join(HERE, "stage1.npz"), **outs)
+
+
+def make_fifos_and_sky():
+    import torch
+    from dsart.services.corr_fast_integration import StaticSkyMean
+    from dsart.coarse_dm.stage2_chgroup_alignment import Stage2InterChgroupShiftFifo
+    from dsart.coarse_dm.stage2_per_dm_fifo import PerCoarseDmStage2FIFO
+    from dsart.coarse_dm.stage2_shifts import compute_stage2_shifts
+    out = {}
+    rng = np.random.default_rng(77)
+    # static sky
+    sky = StaticSkyMean(window_blocks=3, warmup_cubes=2, n_dm=2)
+    ins, outs = [], []
+    for i in range(9):
+        x = (rng.integers(-20, 21, (4, 40)) + 1j * rng.integers(-20, 21, (4, 40))).astype(np.complex64)
+        ins.append(x)
+        outs.append(sky.apply(torch.from_numpy(x), dm_slot=i % 2).numpy())
+    out.update(sky_in=np.stack(ins), sky_out=np.stack(outs))
+    # inter-chgroup shift FIFO
+    cd = np.asarray([0.0, 300.0, 900.0, 1600.0, 2500.0])
+    tab = compute_stage2_shifts(chgroup=2, coarse_dm_pc_cm3=cd, t_int_corr_us=262.144 * 32)
+    fifo = Stage2InterChgroupShiftFifo(chgroup=2, coarse_dm_pc_cm3=cd, t_dedisp=16,
+                                       t_int_corr_us=262.144 * 32, shift_table=tab)
+    ins, outs, emitted = [], [], []
+    for i in range(12):
+        x = (rng.integers(-9, 10, (5, 16, 3)) + 1j * rng.integers(-9, 10, (5, 16, 3))).astype(np.complex64)
+        ins.append(x)
+        r = fifo.push(torch.from_numpy(x), block_n=i)
+        emitted.append(len(r))
+        outs.append(r[0].numpy() if r else np.zeros_like(x))
+    out.update(ics_shifts=tab.shifts_samples, ics_in=np.stack(ins), ics_out=np.stack(outs),
+               ics_emitted=np.asarray(emitted))
+    # per-coarse-DM FIFO
+    pf = PerCoarseDmStage2FIFO([0, 1, 3])
+    seq = []
+    for i in range(6):
+        for c in range(3):
+            r = pf.push(c, torch.full((2,), float(10 * i + c)))
+            seq.append(-1 if r is None else int(r[0].item()))
+    out["pdf_seq"] = np.asarray(seq)
+    np.savez_compressed(os.path.join(HERE, "fifo_sky.npz"), **out)
+
+
+def make_image_detector():
+    import torch
+    from dsart.image.imager import compute_edge_mask, dirty_image_from_uv_grid, apply_edge_mask
+    from dsart.fine_dm.combiner import combine_chgroups
+    from dsart.detector.forward import precompute_padded_cumsum, boxcar_from_padded_cumsum
+    from dsart.detector.decoder import decode_topk_argmax_lowmem
+    from dsart.noise_norm.layer1 import sigma_clipped_std_batched
+    out = {}
+    rng = np.random.default_rng(99)
+    # combine_chgroups on dense streams
+    N, Ts = 16, 10
+    streams = (rng.integers(-5, 6, (16, Ts, N, N)) + 1j * rng.integers(-5, 6, (16, Ts, N, N))).astype(np.complex64)
+    shifts = rng.integers(-4, 5, 16).astype(np.int32)
+    comb = combine_chgroups(per_chgroup_streams={g: streams[g] for g in range(16)},
+                            time_shift_per_chgroup=shifts, t_window=(2, 9))
+    out.update(cmb_streams=streams, cmb_shifts=shifts, cmb_out=comb)
+    # dirty image + edge mask
+    N = 32
+    uv = (rng.normal(size=(3, N, N)) + 1j * rng.normal(size=(3, N, N))).astype(np.complex64)
+    img = dirty_image_from_uv_grid(uv)
+    mask = compute_edge_mask(n_grid=N)
+    out.update(img_uv=uv, img_out=img, img_mask=mask, img_masked=apply_edge_mask(img, mask))
+    # padded cumsum + boxcars
+    cube = rng.normal(size=(40, 2, 5, 6)).astype(np.float32)
+    widths = [1, 2, 4, 8, 16]
+    cs = precompute_padded_cumsum(torch.from_numpy(cube), axis=0, max_width=16)
+    bx = [boxcar_from_padded_cumsum(cs, axis=0, width=w, max_width=16, n_out=24, t_base=8).numpy()
+          for w in widths]
+    out.update(bc_cube=cube, bc_cs=cs.numpy(), bc_box=np.stack(bx))
+    # decode
+    score = rng.normal(size=(12, 3, 8, 8)).astype(np.float32)
+    score[3, 1, 4, 4] = 9.5
+    score[4, 1, 4, 5] = 9.0       # suppressed by merge radius
+    score[10, 0, 1, 1] = 8.0
+    winner = rng.integers(0, 5, score.shape).astype(np.int16)
+    cands = decode_topk_argmax_lowmem(
+        torch.from_numpy(score), torch.from_numpy(winner), threshold=3.5,
+        kernel_ids=[f"unit_d1_b{w}" for w in widths], kernel_time_widths=widths,
+        merge_radius_lm=3, merge_radius_fdm=5, merge_radius_t=128 // 32, n_top=64)
+    out.update(dec_score=score, dec_winner=winner,
+               dec_out=np.asarray([[c.event_specnum, c.dm_idx, c.l, c.m, c.width_samples, c.snr]
+                                   for c in cands], np.float64))
+    # Layer-1 clipped std
+    s = rng.normal(0, 2.0, (4, 3001)).astype(np.float32)
+    s[0, :40] = 50.0
+    s[2, 7] = np.nan
+    out.update(l1_in=s, l1_out=sigma_clipped_std_batched(torch.from_numpy(s)).numpy())
+    np.savez_compressed(os.path.join(HERE, "image_detector.npz"), **out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("DSART_REFERENCE", ""))
+    ap.add_argument("--only", default="")
+    a = ap.parse_args()
+    if not a.reference or not os.path.isdir(a.reference):
+        sys.exit("need --reference <dsa110-rt>/src")
+    sys.path.insert(0, a.reference)
+    todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
+            make_image_detector]
+    for fn in todo:
+        if a.only and a.only not in fn.__name__:
+            continue
+        print("building", fn.__name__, flush=True)
+        fn()
+
+
+if __name__ == "__main__":
+    main()
