@@ -1,0 +1,588 @@
+// 4-bit unpack and X-engine correlator kernels (sm_100a).
+//
+//  * dsb_unpack_int4   : on-wire (npkt, nant, nchan, 2t, 2p) int4 pairs ->
+//                        GEMM layout (nchan, 2t, 2p, npkt, nant) int8/fp16/fp32.
+//  * dsb_corr_split    : correlator on GEMM-layout voltages (any of the three
+//                        dtypes), Stokes-I + channel sum or 2-pol output.
+//  * dsb_corr_tc       : fused unpack + correlate from raw on-wire bytes on the
+//                        5th-generation tensor cores (tcgen05.mma kind::i8,
+//                        int32 accumulators in tensor memory), Stokes-I and
+//                        channel sum folded into the contraction dimension.
+//                        Epilogue writes strided complex64 visibilities, or
+//                        grids them per subband into time-major rows.
+#include "dsb_common.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <type_traits>
+
+namespace {
+
+// ===========================================================================
+// unpack
+// ===========================================================================
+template <typename T>
+DSB_DEV T from_code(int v, float scale);
+template <>
+DSB_DEV int8_t from_code<int8_t>(int v, float) { return (int8_t)v; }
+template <>
+DSB_DEV __half from_code<__half>(int v, float scale) {
+  return __float2half_rn((float)v * scale);
+}
+template <>
+DSB_DEV float from_code<float>(int v, float scale) { return (float)v * scale; }
+
+// Tile: 32 (pkt*nant) rows x 32 channels; smem transpose so that the
+// 4-byte raw words are read along channels and the outputs are written
+// along (pkt, ant).
+template <typename T>
+__global__ void unpack_kernel(const uint32_t* __restrict__ raw, int rows, int nchan, float scale,
+                              T* __restrict__ ore, T* __restrict__ oim) {
+  __shared__ uint32_t tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int i = ty; i < 32; i += 8) {
+    int r = r0 + i, c = c0 + tx;
+    tile[i][tx] = (r < rows && c < nchan) ? raw[(size_t)r * nchan + c] : 0u;
+  }
+  __syncthreads();
+  const size_t plane = (size_t)rows;  // elements per (c, t, pol) plane
+  for (int i = ty; i < 32; i += 8) {
+    int c = c0 + i, r = r0 + tx;
+    if (c >= nchan || r >= rows) continue;
+    uint32_t w = tile[tx][i];
+#pragma unroll
+    for (int tp = 0; tp < 4; ++tp) {  // byte tp = (t, pol)
+      int b = (w >> (8 * tp)) & 0xFF;
+      int re = (b & 8) ? (b & 0xF) - 16 : (b & 0xF);
+      int hi = b >> 4;
+      int im = (hi & 8) ? hi - 16 : hi;
+      size_t o = ((size_t)c * 4 + tp) * plane + r;
+      ore[o] = from_code<T>(re, scale);
+      oim[o] = from_code<T>(im, scale);
+    }
+  }
+}
+
+// ===========================================================================
+// generic (CUDA-core) correlator on GEMM-layout voltages
+// ===========================================================================
+DSB_DEV void bls_to_ab(int j, int& a, int& b) {
+  int aa = (int)((sqrtf(8.f * (float)j + 1.f) - 1.f) * 0.5f);
+  while (aa * (aa + 1) / 2 > j) --aa;
+  while ((aa + 1) * (aa + 2) / 2 <= j) ++aa;
+  a = aa;
+  b = j - aa * (aa + 1) / 2;
+}
+
+template <typename T>
+DSB_DEV float to_f(T v);
+template <>
+DSB_DEV float to_f<int8_t>(int8_t v) { return (float)v; }
+template <>
+DSB_DEV float to_f<__half>(__half v) { return __half2float(v); }
+template <>
+DSB_DEV float to_f<float>(float v) { return v; }
+
+constexpr int GEN_THREADS = 256;
+constexpr int GEN_KCH = 32;   // samples staged per pass
+constexpr int GEN_MAXB = 24;  // baselines per thread (nbase <= 6144)
+
+// One block per output unit. Stokes-I unit = (fv, summed channel): K runs
+// over (ch in group, pol, t-sub, packet). 2-pol unit = (fv, ch, pol).
+template <typename T, typename Acc>
+__global__ void __launch_bounds__(GEN_THREADS) corr_generic_kernel(
+    const T* __restrict__ re, const T* __restrict__ im, int nchan, int npkt, int nant,
+    int ppfv, int fuse, int csf, float2* __restrict__ out) {
+  __shared__ float sR[GEN_KCH][128];
+  __shared__ float sI[GEN_KCH][128];
+  const int nbase = nant * (nant + 1) / 2;
+  const int n_fv = npkt / ppfv;
+  const int unit = blockIdx.x;
+  int fv, ch0, nch_u, pol0, npol_u;
+  if (fuse) {
+    const int ceff = nchan / csf;
+    fv = unit / ceff;
+    ch0 = (unit % ceff) * csf;
+    nch_u = csf;
+    pol0 = 0;
+    npol_u = 2;
+  } else {
+    fv = unit / (nchan * 2);
+    ch0 = (unit / 2) % nchan;
+    nch_u = 1;
+    pol0 = unit % 2;
+    npol_u = 1;
+  }
+  if (fv >= n_fv) return;
+  const int ksz = nch_u * npol_u * 2 * ppfv;  // samples per antenna
+  Acc accr[GEN_MAXB], acci[GEN_MAXB];
+  int aa[GEN_MAXB], bb[GEN_MAXB];
+  int nmine = 0;
+  for (int j = threadIdx.x; j < nbase && nmine < GEN_MAXB; j += GEN_THREADS) {
+    bls_to_ab(j, aa[nmine], bb[nmine]);
+    accr[nmine] = 0;
+    acci[nmine] = 0;
+    ++nmine;
+  }
+  const size_t plane = (size_t)npkt * nant;
+  for (int k0 = 0; k0 < ksz; k0 += GEN_KCH) {
+    const int kn = min(GEN_KCH, ksz - k0);
+    for (int idx = threadIdx.x; idx < kn * nant; idx += GEN_THREADS) {
+      const int kk = idx / nant, a = idx % nant;
+      int k = k0 + kk;
+      // k -> (ch, pol, t, p)
+      const int p = k % ppfv;
+      k /= ppfv;
+      const int t = k % 2;
+      k /= 2;
+      const int pol = pol0 + (k % npol_u);
+      const int ch = ch0 + k / npol_u;
+      const size_t o = (((size_t)ch * 2 + t) * 2 + pol) * plane + (size_t)(fv * ppfv + p) * nant + a;
+      sR[kk][a] = to_f<T>(re[o]);
+      sI[kk][a] = to_f<T>(im[o]);
+    }
+    __syncthreads();
+    for (int m = 0; m < nmine; ++m) {
+      const int a = aa[m], b = bb[m];
+      Acc sr = 0, si = 0;
+      for (int kk = 0; kk < kn; ++kk) {
+        const float rb = sR[kk][b], ib = sI[kk][b], ra = sR[kk][a], ia = sI[kk][a];
+        if constexpr (std::is_integral<Acc>::value) {
+          sr += (int)rb * (int)ra + (int)ib * (int)ia;
+          si += (int)rb * (int)ia - (int)ib * (int)ra;
+        } else {
+          sr = fmaf(rb, ra, fmaf(ib, ia, sr));
+          si = fmaf(rb, ia, fmaf(-ib, ra, si));
+        }
+      }
+      accr[m] += sr;
+      acci[m] += si;
+    }
+    __syncthreads();
+  }
+  for (int m = 0; m < nmine; ++m) {
+    const int j = upper_bls(aa[m], bb[m]);
+    size_t o;
+    if (fuse)
+      o = ((size_t)fv * nbase + j) * (nchan / csf) + ch0 / csf;
+    else
+      o = (((size_t)fv * nbase + j) * nchan + ch0) * 2 + pol0;
+    out[o] = make_float2((float)accr[m], (float)acci[m]);
+  }
+}
+
+// ===========================================================================
+// tensor-core correlator (tcgen05, kind::i8)
+// ===========================================================================
+constexpr int TC_THREADS = 128;
+constexpr int TC_TMEM_COLS = 512;   // two accumulators of <= 256 columns
+constexpr int TC_SMEM_BUDGET = 200 * 1024;
+// Every CTA requests more than half an SM's shared memory so that exactly
+// one CTA (and one 512-column tensor-memory allocation) lives on each SM.
+constexpr int TC_MIN_SMEM = 120 * 1024;
+
+struct TcArgs {
+  const uint8_t* raw;
+  long long raw_g_stride;  // bytes
+  int n_chgroup, npkt, nant, nchan, t_int, csf;
+  int ceff, ppfv, n_fv, rows, kc, n_chunks, nkblk, stage_bytes, nstage, n_mma;
+  int unit_order;  // 0: fast-vis tile fastest, 1: summed channel fastest
+  // mode 0
+  float2* out;
+  long long o_g, o_f, o_b, o_s;
+  // mode 1
+  const int* ycell;   // (n_chgroup*ceff, nbase) local row or -1
+  const int* yoff;    // (n_chgroup*ceff) first global row of the group
+  const int* ycnt;    // (n_chgroup*ceff) rows in the group
+  int ymax;           // max rows over groups (shared accumulator size)
+  float2* yout;
+  long long y_t_stride;
+  long long t_base;
+  long long t_mask;
+  int* status;
+};
+
+DSB_DEV void tc_unit_coords(const TcArgs& A, int u, int& g, int& f, int& s) {
+  const int per_g = A.n_fv * A.ceff;
+  g = u / per_g;
+  const int r = u % per_g;
+  if (A.unit_order == 0) {
+    f = r % A.n_fv;
+    s = r / A.n_fv;
+  } else {
+    s = r % A.ceff;
+    f = r / A.ceff;
+  }
+}
+
+// Convert one K chunk of one unit from packed int4 into the operand stage:
+// rows [0, nant) = [R | I], rows [nant, 2 nant) = [I | -R] (K-major, SW128).
+DSB_DEV void tc_fill(const TcArgs& A, uint8_t* st, int g, int f, int s, int q) {
+  const int nw = A.kc / 4;  // 32-bit words (4 complex samples) per antenna per chunk
+  const int kc = A.kc;
+  const uint32_t region = (uint32_t)A.rows * 128u;
+  const uint8_t* base = A.raw + (size_t)g * A.raw_g_stride;
+  const int nant = A.nant;
+  if ((A.csf & 3) == 0 && (A.nchan & 3) == 0) {
+    const int nv = nw / 4;
+    for (int idx = threadIdx.x; idx < nant * nv; idx += TC_THREADS) {
+      const int a = idx / nv, v = idx % nv;
+      const int j = q * nw + v * 4;
+      const int p = j / A.csf, c = j % A.csf;
+      const uint4 w = __ldg(reinterpret_cast<const uint4*>(
+          base + ((((size_t)(f * A.ppfv + p) * nant + a) * A.nchan + (size_t)s * A.csf + c) * 4)));
+      uint4 R, I, N;
+      R.x = nib_lo_s8x4(w.x); R.y = nib_lo_s8x4(w.y); R.z = nib_lo_s8x4(w.z); R.w = nib_lo_s8x4(w.w);
+      I.x = nib_hi_s8x4(w.x); I.y = nib_hi_s8x4(w.y); I.z = nib_hi_s8x4(w.z); I.w = nib_hi_s8x4(w.w);
+      N.x = neg_s8x4(R.x); N.y = neg_s8x4(R.y); N.z = neg_s8x4(R.z); N.w = neg_s8x4(R.w);
+      const uint32_t kr = (uint32_t)v * 16u, ki = (uint32_t)kc + (uint32_t)v * 16u;
+      const uint32_t ra = (uint32_t)a, rb = (uint32_t)(nant + a);
+      *reinterpret_cast<uint4*>(st + (kr >> 7) * region + sw128_offset(ra, kr & 127u)) = R;
+      *reinterpret_cast<uint4*>(st + (ki >> 7) * region + sw128_offset(ra, ki & 127u)) = I;
+      *reinterpret_cast<uint4*>(st + (kr >> 7) * region + sw128_offset(rb, kr & 127u)) = I;
+      *reinterpret_cast<uint4*>(st + (ki >> 7) * region + sw128_offset(rb, ki & 127u)) = N;
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < nant * nw; idx += TC_THREADS) {
+      const int a = idx / nw, jj = idx % nw;
+      const int j = q * nw + jj;
+      const int p = j / A.csf, c = j % A.csf;
+      const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(
+          base + ((((size_t)(f * A.ppfv + p) * nant + a) * A.nchan + (size_t)s * A.csf + c) * 4)));
+      const uint32_t R = nib_lo_s8x4(w), I = nib_hi_s8x4(w), N = neg_s8x4(R);
+      const uint32_t kr = (uint32_t)jj * 4u, ki = (uint32_t)kc + (uint32_t)jj * 4u;
+      const uint32_t ra = (uint32_t)a, rb = (uint32_t)(nant + a);
+      *reinterpret_cast<uint32_t*>(st + (kr >> 7) * region + sw128_offset(ra, kr & 127u)) = R;
+      *reinterpret_cast<uint32_t*>(st + (ki >> 7) * region + sw128_offset(ra, ki & 127u)) = I;
+      *reinterpret_cast<uint32_t*>(st + (kr >> 7) * region + sw128_offset(rb, kr & 127u)) = I;
+      *reinterpret_cast<uint32_t*>(st + (ki >> 7) * region + sw128_offset(rb, ki & 127u)) = N;
+    }
+  }
+}
+
+// Read accumulator `buf` (rows b < nant; columns a: Re, nant + a: Im) and
+// emit the upper triangle b <= a at bls(a, b) (conj(E_b) E_a).
+template <int MODE>
+DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, int f, int s,
+                         int* acc_smem) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nant = A.nant;
+  const int b = warp * 32 + lane;
+  const int nbase = nant * (nant + 1) / 2;
+  int gs = 0, cnt = 0;
+  const int* ycell = nullptr;
+  if constexpr (MODE == 1) {
+    gs = g * A.ceff + s;
+    cnt = A.ycnt[gs];
+    ycell = A.ycell + (size_t)gs * nbase;
+    for (int k = threadIdx.x; k < 2 * cnt; k += TC_THREADS) acc_smem[k] = 0;
+    __syncthreads();
+  }
+  if (warp * 32 < nant) {
+    const uint32_t lane_base = tmem_base + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * 256);
+    for (int c0 = 0; c0 < nant; c0 += 16) {
+      if (c0 + 15 < warp * 32) continue;  // whole chunk below this warp's rows
+      uint32_t vr[16], vi[16];
+      tmem_ld16(lane_base + (uint32_t)c0, vr);
+      tmem_ld16(lane_base + (uint32_t)(nant + c0), vi);
+      tmem_ld_wait();
+      if (b < nant) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int a = c0 + j;
+          if (a < b || a >= nant) continue;
+          const int bls = upper_bls(a, b);
+          const int re = (int)vr[j], im = (int)vi[j];
+          if constexpr (MODE == 0) {
+            A.out[(size_t)g * A.o_g + (size_t)f * A.o_f + (size_t)bls * A.o_b + (size_t)s * A.o_s] =
+                make_float2((float)re, (float)im);
+          } else {
+            const int k = ycell[bls];
+            if (k >= 0) {
+              atomicAdd(&acc_smem[2 * k], re);
+              atomicAdd(&acc_smem[2 * k + 1], im);
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  if constexpr (MODE == 1) {
+    __syncthreads();
+    const long long row0 = A.yoff[gs];
+    const long long tp = (A.t_base + f) & A.t_mask;
+    for (int k = threadIdx.x; k < cnt; k += TC_THREADS)
+      A.yout[(row0 + k) * A.y_t_stride + tp] =
+          make_float2((float)acc_smem[2 * k], (float)acc_smem[2 * k + 1]);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* stages = smem;
+  uint64_t* bar_mma = reinterpret_cast<uint64_t*>(stages + (size_t)A.nstage * A.stage_bytes);
+  uint64_t* bar_acc = bar_mma + A.nstage;
+  uint64_t* bar_drain = bar_acc + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_drain + 1);
+  int* acc_smem = reinterpret_cast<int*>(tmem_slot + 4);
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, TC_TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < A.nstage; ++i) mbar_init(&bar_mma[i], 1);
+    mbar_init(&bar_acc[0], 1);
+    mbar_init(&bar_acc[1], 1);
+    mbar_init(bar_drain, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int n_units = A.n_chgroup * A.n_fv * A.ceff;
+  const int my_units =
+      (int)blockIdx.x < n_units ? (n_units - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int n_items = my_units * A.n_chunks;
+  const uint32_t idesc = idesc_i8(128u, (uint32_t)(2 * A.nant));
+  bool ok = true;
+
+  for (int it = 0; it < n_items; ++it) {
+    const int lu = it / A.n_chunks, q = it % A.n_chunks;
+    const int u = (int)blockIdx.x + lu * (int)gridDim.x;
+    int g, f, s;
+    tc_unit_coords(A, u, g, f, s);
+    const int slot = it % A.nstage;
+    bool w_ok = true;
+    if (it >= A.nstage) w_ok = mbar_wait(&bar_mma[slot], (uint32_t)((it / A.nstage - 1) & 1));
+    if (!__syncthreads_and(w_ok)) { ok = false; break; }
+    uint8_t* st = stages + (size_t)slot * A.stage_bytes;
+    tc_fill(A, st, g, f, s, q);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t d = tmem_base + (uint32_t)((lu & 1) * 256);
+      const uint32_t sbase = smem_u32(st);
+      for (int m = 0; m < A.n_mma; ++m) {
+        const uint32_t kb = (uint32_t)m * 32u;
+        const uint64_t desc = sdesc_k_sw128(sbase + (kb >> 7) * (uint32_t)A.rows * 128u + (kb & 127u));
+        umma_i8_ss(d, desc, desc, idesc, (q > 0 || m > 0) ? 1u : 0u);
+      }
+      umma_commit(&bar_mma[slot]);
+      if (q == A.n_chunks - 1) umma_commit(&bar_acc[lu & 1]);
+    }
+    if (q == A.n_chunks - 1 && lu >= 1) {
+      const int pl = lu - 1;
+      const bool a_ok = mbar_wait(&bar_acc[pl & 1], (uint32_t)((pl >> 1) & 1));
+      if (!__syncthreads_and(a_ok)) { ok = false; break; }
+      tc_fence_after();
+      int pg, pf, ps;
+      tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, acc_smem);
+    }
+  }
+  if (ok && my_units > 0) {
+    const int pl = my_units - 1;
+    const bool a_ok = mbar_wait(&bar_acc[pl & 1], (uint32_t)((pl >> 1) & 1));
+    if (__syncthreads_and(a_ok)) {
+      tc_fence_after();
+      int pg, pf, ps;
+      tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, acc_smem);
+    } else {
+      ok = false;
+    }
+  }
+  if (!ok) {
+    if (tid == 0) dsb_flag(A.status, DSB_E_TIMEOUT);
+    // Drain every MMA this CTA issued before releasing tensor memory.
+    if (tid == 0) {
+      umma_commit(bar_drain);
+      mbar_wait(bar_drain, 0u);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TC_TMEM_COLS);
+  }
+}
+
+int g_num_sms = 0;
+int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? DSB_OK : DSB_E_CUDA;
+}
+
+// Fill the derived geometry; returns DSB_OK or an error code.
+int tc_plan(TcArgs& A, int mode) {
+  if (A.nant < 16 || A.nant > 128 || (A.nant % 16) != 0) return DSB_E_UNSUPPORTED;
+  if (A.t_int <= 0 || (A.t_int % 2) != 0 || A.npkt % (A.t_int / 2) != 0) return DSB_E_ARG;
+  if (A.csf <= 0 || A.nchan % A.csf != 0) return DSB_E_ARG;
+  A.ppfv = A.t_int / 2;
+  A.n_fv = A.npkt / A.ppfv;
+  A.ceff = A.nchan / A.csf;
+  const int kprime = 2 * A.t_int * A.csf;  // complex samples per antenna per unit
+  if (kprime % 16 != 0) return DSB_E_UNSUPPORTED;
+  A.kc = std::min(kprime, 128);
+  while (kprime % A.kc != 0) A.kc -= 16;
+  A.n_chunks = kprime / A.kc;
+  A.rows = std::max(128, ((2 * A.nant + 7) / 8) * 8);
+  A.nkblk = (2 * A.kc + 127) / 128;
+  A.stage_bytes = A.nkblk * A.rows * 128;
+  A.n_mma = 2 * A.kc / 32;
+  const int extra = (mode == 1) ? A.ymax * 8 : 0;
+  const int budget = TC_SMEM_BUDGET - extra - 1024 - 256;
+  A.nstage = std::min(4, budget / A.stage_bytes);
+  if (A.nstage < 2) return DSB_E_UNSUPPORTED;
+  return DSB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int dsb_version(void) { return DSB_VERSION; }
+
+const char* dsb_strerror(int code) {
+  switch (code) {
+    case DSB_OK: return "ok";
+    case DSB_E_ARG: return "invalid argument";
+    case DSB_E_CUDA: return "CUDA runtime error";
+    case DSB_E_UNSUPPORTED: return "unsupported geometry";
+    case DSB_E_TIMEOUT: return "device-side bounded wait ran out";
+    case DSB_E_CAPACITY: return "size exceeds a fixed capacity";
+    default: return "unknown error";
+  }
+}
+
+int dsb_unpack_int4(const void* raw, int npkt, int nant, int nchan, int out_dtype, float scale,
+                    void* out_re, void* out_im, cudaStream_t stream) {
+  if (!raw || !out_re || !out_im || npkt <= 0 || nant <= 0 || nchan <= 0) return DSB_E_ARG;
+  const int rows = npkt * nant;
+  dim3 grid((rows + 31) / 32, (nchan + 31) / 32), block(32, 8);
+  const uint32_t* r = static_cast<const uint32_t*>(raw);
+  switch (out_dtype) {
+    case DSB_DT_INT8:
+      unpack_kernel<int8_t><<<grid, block, 0, stream>>>(r, rows, nchan, scale, (int8_t*)out_re,
+                                                        (int8_t*)out_im);
+      break;
+    case DSB_DT_F16:
+      unpack_kernel<__half><<<grid, block, 0, stream>>>(r, rows, nchan, scale, (__half*)out_re,
+                                                        (__half*)out_im);
+      break;
+    case DSB_DT_F32:
+      unpack_kernel<float><<<grid, block, 0, stream>>>(r, rows, nchan, scale, (float*)out_re,
+                                                       (float*)out_im);
+      break;
+    default: return DSB_E_ARG;
+  }
+  return launch_status();
+}
+
+int dsb_corr_split(const void* re, const void* im, int in_dtype, int nchan, int npkt, int nant,
+                   int t_int, int fuse_stokes_i, int csf, void* out, cudaStream_t stream) {
+  if (!re || !im || !out || nchan <= 0 || npkt <= 0 || nant <= 0) return DSB_E_ARG;
+  if (nant > 128 || t_int <= 0 || t_int % 2 || npkt % (t_int / 2)) return DSB_E_ARG;
+  const int nbase = nant * (nant + 1) / 2;
+  if (nbase > GEN_THREADS * GEN_MAXB) return DSB_E_UNSUPPORTED;
+  const int ppfv = t_int / 2, n_fv = npkt / ppfv;
+  int units;
+  if (fuse_stokes_i) {
+    if (csf <= 0 || nchan % csf) return DSB_E_ARG;
+    units = n_fv * (nchan / csf);
+  } else {
+    units = n_fv * nchan * 2;
+  }
+  float2* o = static_cast<float2*>(out);
+  switch (in_dtype) {
+    case DSB_DT_INT8:
+      corr_generic_kernel<int8_t, int><<<units, GEN_THREADS, 0, stream>>>(
+          (const int8_t*)re, (const int8_t*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
+      break;
+    case DSB_DT_F16:
+      corr_generic_kernel<__half, float><<<units, GEN_THREADS, 0, stream>>>(
+          (const __half*)re, (const __half*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
+      break;
+    case DSB_DT_F32:
+      corr_generic_kernel<float, float><<<units, GEN_THREADS, 0, stream>>>(
+          (const float*)re, (const float*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
+      break;
+    default: return DSB_E_ARG;
+  }
+  return launch_status();
+}
+
+int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
+                int nchan, int t_int, int csf, int unit_order, void* out, long long o_g,
+                long long o_f, long long o_b, long long o_s, int max_ctas, int* status,
+                cudaStream_t stream) {
+  if (!raw || !out || n_chgroup <= 0 || npkt <= 0) return DSB_E_ARG;
+  if (((uintptr_t)raw & 15) || (raw_g_stride & 15)) return DSB_E_ARG;
+  TcArgs A{};
+  A.raw = static_cast<const uint8_t*>(raw);
+  A.raw_g_stride = raw_g_stride;
+  A.n_chgroup = n_chgroup; A.npkt = npkt; A.nant = nant; A.nchan = nchan;
+  A.t_int = t_int; A.csf = csf; A.unit_order = unit_order;
+  A.out = static_cast<float2*>(out);
+  A.o_g = o_g; A.o_f = o_f; A.o_b = o_b; A.o_s = o_s;
+  A.status = status;
+  int rc = tc_plan(A, 0);
+  if (rc) return rc;
+  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256, TC_MIN_SMEM);
+  cudaFuncSetAttribute(corr_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int n_units = n_chgroup * A.n_fv * A.ceff;
+  int grid = std::min(n_units, max_ctas > 0 ? max_ctas : num_sms());
+  corr_tc_kernel<0><<<grid, TC_THREADS, smem, stream>>>(A);
+  return launch_status();
+}
+
+int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
+                     int nchan, int t_int, int csf, const int* ycell, const int* yoff,
+                     const int* ycnt, int ymax, void* yout, long long y_t_stride,
+                     long long t_base, long long t_mask, int max_ctas, int* status,
+                     cudaStream_t stream) {
+  if (!raw || !yout || !ycell || !yoff || !ycnt || ymax < 0) return DSB_E_ARG;
+  if (((uintptr_t)raw & 15) || (raw_g_stride & 15)) return DSB_E_ARG;
+  TcArgs A{};
+  A.raw = static_cast<const uint8_t*>(raw);
+  A.raw_g_stride = raw_g_stride;
+  A.n_chgroup = n_chgroup; A.npkt = npkt; A.nant = nant; A.nchan = nchan;
+  A.t_int = t_int; A.csf = csf; A.unit_order = 0;
+  A.ycell = ycell; A.yoff = yoff; A.ycnt = ycnt; A.ymax = ymax;
+  A.yout = static_cast<float2*>(yout);
+  A.y_t_stride = y_t_stride; A.t_base = t_base; A.t_mask = t_mask;
+  A.status = status;
+  int rc = tc_plan(A, 1);
+  if (rc) return rc;
+  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + ymax * 8, TC_MIN_SMEM);
+  cudaFuncSetAttribute(corr_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int n_units = n_chgroup * A.n_fv * A.ceff;
+  int grid = std::min(n_units, max_ctas > 0 ? max_ctas : num_sms());
+  corr_tc_kernel<1><<<grid, TC_THREADS, smem, stream>>>(A);
+  return launch_status();
+}
+
+}  // extern "C"

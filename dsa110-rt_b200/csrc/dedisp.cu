@@ -1,0 +1,296 @@
+// Gridding, stage-1 coarse-DM shift + grid, static-sky subtraction and the
+// stage-2 per-coarse-DM delay (sm_100a).
+//
+// Drop-in forms (reference layouts):
+//   dsb_grid_vis          FastVisGridder.compute       (n_fv, nbase, C) -> (n_fv, n_filled)
+//   dsb_dedisp_vis        Stage1MultiDMCoarseDM window (T, nbase, C)    -> (n_dm, T_d, n_filled)
+//   dsb_static_sky        StaticSkyMean.apply          (n_fv, n_filled) -> same
+//   dsb_stage2_roll       Stage2InterChgroupShiftFifo  ring of cubes    -> aligned cube
+// Pipeline form (time-major rows, ring buffers indexed by absolute time):
+//   dsb_stage1_rows       per-subband gridded rows Y -> per-(chgroup, DM,
+//                         cell) rows written at t + shift2 into the stage-2
+//                         ring, static-sky subtraction fused.
+#include "dsb_common.cuh"
+
+#include <algorithm>
+
+namespace {
+
+__global__ void grid_vis_kernel(const float2* __restrict__ vis, int n_fv, long long nsrc,
+                                const int* __restrict__ off, const int* __restrict__ src,
+                                int n_filled, float2* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_fv * n_filled) return;
+  const int f = (int)(idx / n_filled), cell = (int)(idx % n_filled);
+  const float2* v = vis + (size_t)f * nsrc;
+  float re = 0.f, im = 0.f;
+  for (int j = off[cell]; j < off[cell + 1]; ++j) {
+    const float2 x = v[src[j]];
+    re += x.x;
+    im += x.y;
+  }
+  out[idx] = make_float2(re, im);
+}
+
+// out[d, t, cell] = sum_{src in cell} vis_joined[t + shift[s(src), d], src]
+// where vis_joined = concat(prev[0:n_prev], cur) along time.
+__global__ void dedisp_vis_kernel(const float2* __restrict__ prev, const float2* __restrict__ cur,
+                                  int n_prev, long long nsrc, int ceff,
+                                  const int* __restrict__ off, const int* __restrict__ src,
+                                  const int* __restrict__ shifts, int n_dm, int n_filled,
+                                  int t_dedisp, float2* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per_d = (long long)t_dedisp * n_filled;
+  if (idx >= per_d * n_dm) return;
+  const int d = (int)(idx / per_d);
+  const long long r = idx % per_d;
+  const int t = (int)(r / n_filled), cell = (int)(r % n_filled);
+  float re = 0.f, im = 0.f;
+  for (int j = off[cell]; j < off[cell + 1]; ++j) {
+    const int sj = src[j];
+    const int tt = t + shifts[(sj % ceff) * n_dm + d];
+    const float2 x = tt < n_prev ? prev[(size_t)tt * nsrc + sj] : cur[(size_t)(tt - n_prev) * nsrc + sj];
+    re += x.x;
+    im += x.y;
+  }
+  out[idx] = make_float2(re, im);
+}
+
+// Static-sky mean (per cell): mean of the past `count` block means held in
+// ring[cell*window + w] (float64), subtracted once `subtract` is set; this
+// block's float64 time-mean is written to ring[cell*window + head].
+__global__ void static_sky_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                  int n_t, int n_cells, double2* __restrict__ ring, int window,
+                                  int head, int count, int subtract) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= n_cells) return;
+  double2 m = make_double2(0.0, 0.0);
+  if (subtract && count > 0) {
+    for (int w = 0; w < count; ++w) {
+      const double2 r = ring[(size_t)cell * window + w];
+      m.x += r.x;
+      m.y += r.y;
+    }
+    m.x /= count;
+    m.y /= count;
+  }
+  double sr = 0.0, si = 0.0;
+  for (int t = 0; t < n_t; ++t) {
+    const float2 x = in[(size_t)t * n_cells + cell];
+    sr += x.x;
+    si += x.y;
+    if (subtract && count > 0)
+      out[(size_t)t * n_cells + cell] =
+          make_float2((float)((double)x.x - m.x), (float)((double)x.y - m.y));
+    else
+      out[(size_t)t * n_cells + cell] = x;
+  }
+  ring[(size_t)cell * window + head] = make_double2(sr / n_t, si / n_t);
+}
+
+// Stage-2 aligned cube: out[c, t, :] = stream_c[t - shift[c]] where the
+// stream is the concatenation of past cubes; hist[c][j] points at the cube
+// pushed j ticks ago (j = 0 newest).  warm[c] == 0 -> zeros.
+__global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int depth,
+                                   const int* __restrict__ kblk, const int* __restrict__ rsmp,
+                                   const int* __restrict__ warm, int n_dm, int t_len,
+                                   long long inner, float2* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per_c = (long long)t_len * inner;
+  if (idx >= per_c * n_dm) return;
+  const int c = (int)(idx / per_c);
+  const long long r = idx % per_c;
+  const int t = (int)(r / inner);
+  const long long e = r % inner;
+  float2 v = make_float2(0.f, 0.f);
+  if (warm[c]) {
+    const int k = kblk[c], rr = rsmp[c];
+    int j, ts;
+    if (t < rr) {
+      j = k + 1;
+      ts = t_len - rr + t;
+    } else {
+      j = k;
+      ts = t - rr;
+    }
+    if (j < depth) {
+      const float2* cube = hist[j];
+      v = cube[((size_t)c * t_len + ts) * inner + e];
+    }
+  }
+  out[idx] = v;
+}
+
+// Pipeline stage 1 over per-subband gridded rows.  One block per global cell
+// (all chgroups); loops over coarse DMs; threads along time.
+struct S1Args {
+  const float2* Y;
+  long long y_stride, y_mask;
+  const int* cell_off;    // (n_cells + 1)
+  const int* src_row;     // Y row of each source
+  const int* src_s;       // summed channel of each source
+  const int* cell_g;      // chgroup of each global cell
+  const int* cell_local;  // cell index inside its chgroup
+  const int* shift1;      // (G, ceff, n_dm)
+  const int* shift2;      // (G, n_dm)
+  const int* d_base;      // (G) first D row of the chgroup
+  const int* n_filled;    // (G)
+  float2* D;
+  long long d_stride, d_mask;
+  long long t0;           // absolute time of the first output
+  int n_t, n_dm, ceff;
+  double2* sky_ring;      // (D rows, window) or null
+  int sky_window, sky_head, sky_count, sky_subtract;
+};
+
+constexpr int S1_THREADS = 256;
+constexpr int S1_MAX_SRC = 64;
+
+__global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
+  const int gc = blockIdx.x;
+  const int g = A.cell_g[gc], cl = A.cell_local[gc];
+  const int j0 = A.cell_off[gc], nsrc = min(A.cell_off[gc + 1] - j0, S1_MAX_SRC);
+  __shared__ int s_row[S1_MAX_SRC], s_s[S1_MAX_SRC];
+  __shared__ double red_r[S1_THREADS / 32], red_i[S1_THREADS / 32];
+  for (int j = threadIdx.x; j < nsrc; j += S1_THREADS) {
+    s_row[j] = A.src_row[j0 + j];
+    s_s[j] = A.src_s[j0 + j];
+  }
+  __syncthreads();
+  const int nf = A.n_filled[g];
+  for (int d = 0; d < A.n_dm; ++d) {
+    const long long drow = (long long)A.d_base[g] + (long long)d * nf + cl;
+    double2 m = make_double2(0.0, 0.0);
+    const bool sub = A.sky_ring && A.sky_subtract && A.sky_count > 0;
+    if (sub) {
+      for (int w = 0; w < A.sky_count; ++w) {
+        const double2 r = A.sky_ring[drow * A.sky_window + w];
+        m.x += r.x;
+        m.y += r.y;
+      }
+      m.x /= A.sky_count;
+      m.y /= A.sky_count;
+    }
+    const int sh2 = A.shift2[g * A.n_dm + d];
+    double sr = 0.0, si = 0.0;
+    for (int t = threadIdx.x; t < A.n_t; t += S1_THREADS) {
+      const long long ta = A.t0 + t;
+      float re = 0.f, im = 0.f;
+      for (int j = 0; j < nsrc; ++j) {
+        const int sh = A.shift1[(g * A.ceff + s_s[j]) * A.n_dm + d];
+        const float2 x = A.Y[(long long)s_row[j] * A.y_stride + ((ta + sh) & A.y_mask)];
+        re += x.x;
+        im += x.y;
+      }
+      sr += re;
+      si += im;
+      float2 o = make_float2(re, im);
+      if (sub) o = make_float2((float)((double)re - m.x), (float)((double)im - m.y));
+      A.D[drow * A.d_stride + ((ta + sh2) & A.d_mask)] = o;
+    }
+    if (A.sky_ring) {
+      // block reduction of the block's un-subtracted time sum
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        red_r[threadIdx.x >> 5] = sr;
+        red_i[threadIdx.x >> 5] = si;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double tr = 0.0, ti = 0.0;
+        for (int w = 0; w < S1_THREADS / 32; ++w) {
+          tr += red_r[w];
+          ti += red_i[w];
+        }
+        A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(tr / A.n_t, ti / A.n_t);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+int launch_status() { return cudaGetLastError() == cudaSuccess ? DSB_OK : DSB_E_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+int dsb_grid_vis(const void* vis, int n_fv, long long nsrc, const int* cell_off,
+                 const int* cell_src, int n_filled, void* out, cudaStream_t stream) {
+  if (!vis || !out || !cell_off || !cell_src || n_fv <= 0 || n_filled < 0) return DSB_E_ARG;
+  const long long n = (long long)n_fv * n_filled;
+  if (n == 0) return DSB_OK;
+  grid_vis_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
+      (const float2*)vis, n_fv, nsrc, cell_off, cell_src, n_filled, (float2*)out);
+  return launch_status();
+}
+
+int dsb_dedisp_vis(const void* prev, const void* cur, int n_prev, long long nsrc, int ceff,
+                   const int* cell_off, const int* cell_src, const int* shifts, int n_dm,
+                   int n_filled, int t_dedisp, void* out, cudaStream_t stream) {
+  if (!cur || !out || !cell_off || !cell_src || !shifts || ceff <= 0 || n_dm <= 0) return DSB_E_ARG;
+  if (n_prev > 0 && !prev) return DSB_E_ARG;
+  const long long n = (long long)n_dm * t_dedisp * n_filled;
+  if (n <= 0) return DSB_OK;
+  dedisp_vis_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
+      (const float2*)prev, (const float2*)cur, n_prev, nsrc, ceff, cell_off, cell_src, shifts,
+      n_dm, n_filled, t_dedisp, (float2*)out);
+  return launch_status();
+}
+
+int dsb_static_sky(const void* in, void* out, int n_t, int n_cells, void* ring, int window,
+                   int head, int count, int subtract, cudaStream_t stream) {
+  if (!in || !out || !ring || n_t <= 0 || n_cells < 0 || window <= 0) return DSB_E_ARG;
+  if (head < 0 || head >= window || count < 0 || count > window) return DSB_E_ARG;
+  if (n_cells == 0) return DSB_OK;
+  static_sky_kernel<<<(n_cells + 127) / 128, 128, 0, stream>>>(
+      (const float2*)in, (float2*)out, n_t, n_cells, (double2*)ring, window, head, count,
+      subtract);
+  return launch_status();
+}
+
+int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const int* rsmp,
+                    const int* warm, int n_dm, int t_len, long long inner, void* out,
+                    cudaStream_t stream) {
+  if (!hist || !kblk || !rsmp || !warm || !out || depth <= 0 || n_dm <= 0 || t_len <= 0)
+    return DSB_E_ARG;
+  const long long n = (long long)n_dm * t_len * inner;
+  if (n == 0) return DSB_OK;
+  stage2_roll_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
+      (const float2* const*)hist, depth, kblk, rsmp, warm, n_dm, t_len, inner, (float2*)out);
+  return launch_status();
+}
+
+int dsb_stage1_rows(const void* Y, long long y_stride, long long y_mask, int n_cells,
+                    const int* cell_off, const int* src_row, const int* src_s, const int* cell_g,
+                    const int* cell_local, const int* shift1, const int* shift2,
+                    const int* d_base, const int* n_filled, void* D, long long d_stride,
+                    long long d_mask, long long t0, int n_t, int n_dm, int ceff, void* sky_ring,
+                    int sky_window, int sky_head, int sky_count, int sky_subtract,
+                    int max_src, cudaStream_t stream) {
+  if (!Y || !D || !cell_off || !src_row || !src_s || !cell_g || !cell_local || !shift1 ||
+      !shift2 || !d_base || !n_filled || n_t <= 0 || n_dm <= 0)
+    return DSB_E_ARG;
+  if (max_src > S1_MAX_SRC) return DSB_E_CAPACITY;
+  if (sky_ring && (sky_window <= 0 || sky_head < 0 || sky_head >= sky_window ||
+                   sky_count < 0 || sky_count > sky_window))
+    return DSB_E_ARG;
+  if (n_cells <= 0) return DSB_OK;
+  S1Args A{};
+  A.Y = (const float2*)Y; A.y_stride = y_stride; A.y_mask = y_mask;
+  A.cell_off = cell_off; A.src_row = src_row; A.src_s = src_s;
+  A.cell_g = cell_g; A.cell_local = cell_local;
+  A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
+  A.D = (float2*)D; A.d_stride = d_stride; A.d_mask = d_mask;
+  A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff;
+  A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
+  A.sky_count = sky_count; A.sky_subtract = sky_subtract;
+  stage1_rows_kernel<<<n_cells, S1_THREADS, 0, stream>>>(A);
+  return launch_status();
+}
+
+}  // extern "C"

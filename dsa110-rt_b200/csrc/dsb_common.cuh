@@ -1,0 +1,163 @@
+// Common device helpers for the dsa110-rt B200 fast-search kernels.
+//
+// Status words: every kernel that can give up (a bounded wait that ran out,
+// an index that failed a bounds check in a checked build) records a code in
+// a caller-provided device int; the host reads it after the stream syncs.
+// No kernel traps.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+#include "../../include/dsb200.h"
+
+#define DSB_DEV __device__ __forceinline__
+
+// Iteration limit for every mbarrier spin (each try_wait may itself suspend
+// for a hardware-chosen interval, so this bounds the wait to well under a
+// few seconds on a healthy GPU).
+#ifndef DSB_SPIN_LIMIT
+#define DSB_SPIN_LIMIT (1u << 22)
+#endif
+
+DSB_DEV uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+DSB_DEV void dsb_flag(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier
+// ---------------------------------------------------------------------------
+DSB_DEV void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+DSB_DEV void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+DSB_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Returns false if the barrier phase did not complete within the limit.
+DSB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < DSB_SPIN_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 (5th-generation tensor core, accumulators in tensor memory)
+// ---------------------------------------------------------------------------
+DSB_DEV void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+DSB_DEV void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+DSB_DEV void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Executed by one full warp.
+DSB_DEV void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+}
+DSB_DEV void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+DSB_DEV void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, signed int8 inputs, int32 accumulate.
+DSB_DEV void umma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                        uint32_t accumulate) {
+  uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2),
+      "r"(m3)
+      : "memory");
+}
+
+// Arrive on an mbarrier once every tcgen05.mma issued so far by this thread
+// has completed.
+DSB_DEV void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// Instruction descriptor: kind::i8, signed A and B, S32 accumulator,
+// both operands K-major (bit layout of the sm_100 UMMA instruction
+// descriptor: c_format [4,6), a_format [7,10), b_format [10,13),
+// n_dim = N>>3 at [17,23), m_dim = M>>4 at [24,29)).
+__host__ __device__ constexpr uint32_t idesc_i8(uint32_t M, uint32_t N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor for a K-major operand in the 128-byte
+// swizzle layout: rows of 128 B, 8-row atoms of 1024 B stacked at
+// SBO = 1024 B, LBO unused (1), version 1, layout type SWIZZLE_128B (2).
+DSB_DEV uint64_t sdesc_k_sw128(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+// Byte offset of (row, k byte) inside a K-major SWIZZLE_128B tile whose
+// 8-row atoms are 1024 B apart: the 16-byte chunk index is XOR-ed with the
+// row's position inside its atom.
+DSB_DEV uint32_t sw128_offset(uint32_t row, uint32_t kbyte) {
+  return (row >> 3) * 1024u + (row & 7u) * 128u + ((((kbyte >> 4) ^ (row & 7u)) & 7u) << 4) +
+         (kbyte & 15u);
+}
+
+// Load 16 consecutive 32-bit TMEM columns of this warp's 32 lanes.
+DSB_DEV void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+DSB_DEV void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// int4 helpers: four packed (real | imag << 4) complex samples per 32-bit word
+// ---------------------------------------------------------------------------
+DSB_DEV uint32_t nib_lo_s8x4(uint32_t w) {
+  uint32_t lo = w & 0x0F0F0F0Fu;
+  return __vsub4(lo ^ 0x08080808u, 0x08080808u);
+}
+DSB_DEV uint32_t nib_hi_s8x4(uint32_t w) {
+  uint32_t hi = (w >> 4) & 0x0F0F0F0Fu;
+  return __vsub4(hi ^ 0x08080808u, 0x08080808u);
+}
+DSB_DEV uint32_t neg_s8x4(uint32_t v) { return __vsub4(0u, v); }
+
+DSB_DEV int upper_bls(int a, int b) { return a * (a + 1) / 2 + b; }

@@ -1,0 +1,103 @@
+"""ctypes binding of ``libdsb200.so`` (the C ABI declared in include/dsb200.h).
+
+The library is built in-tree (``__graft_entry__.build()``).  There is no CPU
+fallback anywhere in this package: if the library is missing, or a tensor
+is not on a CUDA device, calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(_HERE, "_native", "libdsb200.so")
+
+DT_INT8, DT_F16, DT_F32 = 0, 1, 2
+
+_c_int, _c_ll, _c_float, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_float, ctypes.c_void_p
+
+# name -> argtypes (all return c_int except where noted)
+_SIGNATURES = {
+    "dsb_version": [],
+    "dsb_unpack_int4": [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp],
+    "dsb_corr_split": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+    "dsb_corr_tc": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp,
+                    _c_ll, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
+    "dsb_corr_tc_grid": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp,
+                         _vp, _c_int, _vp, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+class DsbError(RuntimeError):
+    """A dsb200 C-ABI call returned an error code."""
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO_PATH):
+            raise RuntimeError(
+                f"dsb200 native library missing ({SO_PATH}); build it with "
+                "`python -c 'import __graft_entry__ as g; g.build()'` — there is no CPU fallback")
+        L = ctypes.CDLL(SO_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _c_int
+        L.dsb_strerror.argtypes = [_c_int]
+        L.dsb_strerror.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def declared_symbols():
+    return list(_SIGNATURES) + ["dsb_strerror"]
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib().dsb_strerror(rc).decode()
+        raise DsbError(f"{what}: {msg} (code {rc})")
+
+
+def ptr(t: Optional[torch.Tensor]) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def stream_of(dev: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def require_cuda(t: torch.Tensor, name: str) -> None:
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor, got {type(t).__name__}")
+    if t.device.type != "cuda":
+        raise ValueError(f"{name} must be on a CUDA device (no CPU path), got {t.device}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def cuda_device(device) -> torch.device:
+    dev = torch.device(device)
+    if dev.type != "cuda":
+        raise ValueError(f"dsb200 runs on CUDA devices only (no CPU path); got {dev}")
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    return dev
+
+
+def status_word(dev: torch.device) -> torch.Tensor:
+    return torch.zeros(1, dtype=torch.int32, device=dev)
+
+
+def check_status(status: torch.Tensor, what: str) -> None:
+    code = int(status.item())
+    if code != 0:
+        msg = lib().dsb_strerror(code).decode()
+        raise DsbError(f"{what}: device status {msg} (code {code})")

@@ -1,0 +1,220 @@
+"""Unpack and fast correlator — drop-in for dsa110-rt's
+``unpack_int4_split`` (src/dsart/services/slow_corr_kernel.py:220) and
+``FastCorrKernel`` (src/dsart/services/corr_fast_kernel.py:290-413).
+
+Geometry is parametric (the reference hard-codes 96 antennas x 384
+channels x 2048 packets); defaults equal the reference's.  All compute runs
+in ``libdsb200.so``; tensors must live on a CUDA device.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import (BADA_NPOL, LEGACY_FLUFF_SCALE, NANTS, NCHAN_PER_CHGROUP,
+                        NPACKETS_PER_BLOCK, NPOL, NTIMES_PER_PACKET, nbase_of)
+
+_DT = {torch.int8: _lib.DT_INT8, torch.float16: _lib.DT_F16, torch.float32: _lib.DT_F32}
+
+
+def upper_tri_indices(nants: int = NANTS) -> Tuple[np.ndarray, np.ndarray]:
+    """``(a_idx, b_idx)`` with ``b <= a``, ``bls = a(a+1)/2 + b``
+    (slow_corr_kernel.py:161)."""
+    a = np.repeat(np.arange(nants, dtype=np.int64), np.arange(1, nants + 1))
+    b = np.concatenate([np.arange(k + 1, dtype=np.int64) for k in range(nants)])
+    return a, b
+
+
+def _raw_to_device(raw, dev: torch.device) -> torch.Tensor:
+    if isinstance(raw, torch.Tensor):
+        t = raw.reshape(-1)
+        if t.dtype != torch.uint8:
+            t = t.view(torch.uint8)
+        return t.to(dev, non_blocking=True).contiguous()
+    if isinstance(raw, (bytes, bytearray, memoryview)):
+        arr = np.frombuffer(raw, dtype=np.uint8)
+    elif isinstance(raw, np.ndarray):
+        arr = raw if raw.dtype == np.uint8 else raw.view(np.uint8)
+    else:
+        raise TypeError(f"unsupported raw type {type(raw)!r}")
+    return torch.from_numpy(np.ascontiguousarray(arr).reshape(-1)).to(dev)
+
+
+def unpack_int4_split(
+    raw,
+    *,
+    device="cuda",
+    scale: float = LEGACY_FLUFF_SCALE,
+    out_dtype: torch.dtype = torch.float16,
+    npkt: int = NPACKETS_PER_BLOCK,
+    nant: int = NANTS,
+    nchan: int = NCHAN_PER_CHGROUP,
+) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Fluff one on-wire page into ``(real, imag)`` in GEMM layout
+    ``(nchan, 2t, 2p, npkt, nant)``.  ``out_dtype`` may also be
+    ``torch.int8`` (raw integer codes, ``scale`` ignored)."""
+    dev = _lib.cuda_device(device)
+    if out_dtype not in _DT:
+        raise ValueError(f"out_dtype {out_dtype} not in {list(_DT)}")
+    expected = npkt * nant * nchan * NTIMES_PER_PACKET * NPOL
+    r = _raw_to_device(raw, dev)
+    if r.numel() != expected:
+        raise ValueError(f"fada raw size {r.numel()} != expected {expected} "
+                         f"(= prod{(npkt, nant, nchan, NTIMES_PER_PACKET, NPOL)})")
+    shape = (nchan, NTIMES_PER_PACKET, NPOL, npkt, nant)
+    re = torch.empty(shape, dtype=out_dtype, device=dev)
+    im = torch.empty(shape, dtype=out_dtype, device=dev)
+    _lib.check(_lib.lib().dsb_unpack_int4(_lib.ptr(r), npkt, nant, nchan, _DT[out_dtype],
+                                          float(scale), _lib.ptr(re), _lib.ptr(im),
+                                          _lib.stream_of(dev)), "dsb_unpack_int4")
+    return re, im
+
+
+def validate_fast_voltage_shape(real_v, imag_v, *, t_int_fast_native: int, nants: int = NANTS,
+                                nchan: int = NCHAN_PER_CHGROUP, nvolt_pol: int = NPOL
+                                ) -> Tuple[int, int]:
+    """Same checks and messages as corr_fast_kernel.py:202-284."""
+    if real_v.shape != imag_v.shape:
+        raise ValueError(f"real_v shape {tuple(real_v.shape)} != imag_v shape {tuple(imag_v.shape)}")
+    if real_v.dtype != imag_v.dtype:
+        raise ValueError(f"real_v dtype {real_v.dtype} != imag_v dtype {imag_v.dtype}")
+    if real_v.ndim != 5:
+        raise ValueError(f"voltage tensor must be 5D (nchan, NTIMES_PER_PACKET, nvolt_pol, "
+                         f"n_packets_in, nants), got {real_v.ndim}D shape {tuple(real_v.shape)}")
+    nch, nt, npol, n_packets_in, na = tuple(real_v.shape)
+    if nch != nchan:
+        raise ValueError(f"voltage nchan={nch}, expected {nchan}")
+    if nt != NTIMES_PER_PACKET:
+        raise ValueError(f"voltage NTIMES_PER_PACKET={nt}, expected {NTIMES_PER_PACKET}")
+    if npol != nvolt_pol:
+        raise ValueError(f"voltage nvolt_pol={npol}, expected {nvolt_pol}")
+    if na != nants:
+        raise ValueError(f"voltage nants={na}, expected {nants}")
+    if n_packets_in <= 0:
+        raise ValueError(f"voltage n_packets_in must be > 0, got {n_packets_in}")
+    if t_int_fast_native <= 0:
+        raise ValueError(f"t_int_fast_native must be > 0, got {t_int_fast_native}")
+    if t_int_fast_native % NTIMES_PER_PACKET != 0:
+        raise ValueError(f"t_int_fast_native ({t_int_fast_native}) must be a multiple of "
+                         f"NTIMES_PER_PACKET ({NTIMES_PER_PACKET}); the GEMM layout has no "
+                         f"sub-packet time axis to split on.")
+    ppfv = t_int_fast_native // NTIMES_PER_PACKET
+    if n_packets_in % ppfv != 0:
+        raise ValueError(f"n_packets_in ({n_packets_in}) not a multiple of "
+                         f"packets_per_fast_vis ({ppfv} = t_int_fast_native / NTIMES_PER_PACKET); "
+                         f"cannot tile the voltage block evenly into fast-vis integrations.")
+    return n_packets_in // ppfv, ppfv
+
+
+@dataclass
+class FastCorrKernel:
+    """Fast X-engine (corr_fast_kernel.py:290).  ``compute_split`` takes the
+    reference's GEMM-layout voltages (int8 codes, fp16 or fp32);
+    ``compute_raw`` correlates on-wire bytes directly on the tcgen05 tensor
+    cores (Stokes-I + channel sum, integer exact)."""
+
+    device: torch.device
+    t_int_fast_native: int = 8
+    nants: int = NANTS
+    nchan: int = NCHAN_PER_CHGROUP
+    nvolt_pol: int = NPOL
+    nbada_pol: int = BADA_NPOL
+    accum_dtype: torch.dtype = torch.float32
+    _nbase: int = field(init=False)
+
+    def __post_init__(self) -> None:
+        self.device = _lib.cuda_device(self.device)
+        if self.nbada_pol > self.nvolt_pol:
+            raise ValueError(f"nbada_pol ({self.nbada_pol}) > nvolt_pol ({self.nvolt_pol})")
+        if self.t_int_fast_native % NTIMES_PER_PACKET != 0:
+            raise ValueError(f"t_int_fast_native ({self.t_int_fast_native}) must be a multiple "
+                             f"of NTIMES_PER_PACKET ({NTIMES_PER_PACKET})")
+        if self.t_int_fast_native <= 0:
+            raise ValueError(f"t_int_fast_native must be > 0, got {self.t_int_fast_native}")
+        if self.nvolt_pol != 2 or self.nbada_pol != 2:
+            raise ValueError("dsb200 correlates both parallel hands (nvolt_pol = nbada_pol = 2)")
+        self._nbase = nbase_of(self.nants)
+
+    @property
+    def nbase(self) -> int:
+        return self._nbase
+
+    def compute_split(self, real_v: torch.Tensor, imag_v: torch.Tensor, *,
+                      n_fv_chunk: Optional[int] = None, fuse_stokes_i: bool = False,
+                      chan_sum_factor: int = 1) -> torch.Tensor:
+        n_fv, _ = validate_fast_voltage_shape(real_v, imag_v,
+                                              t_int_fast_native=self.t_int_fast_native,
+                                              nants=self.nants, nchan=self.nchan,
+                                              nvolt_pol=self.nvolt_pol)
+        for t, nm in ((real_v, "real_v"), (imag_v, "imag_v")):
+            if t.device != self.device:
+                raise ValueError(f"{nm} on {t.device}, kernel on {self.device}")
+        if n_fv_chunk is not None and not (1 <= n_fv_chunk <= n_fv):
+            raise ValueError(f"n_fv_chunk={n_fv_chunk} must be in [1, n_fv_total={n_fv}]")
+        if real_v.dtype not in _DT:
+            raise ValueError(f"voltage dtype {real_v.dtype} not supported")
+        re = real_v.contiguous()
+        im = imag_v.contiguous()
+        if fuse_stokes_i:
+            if chan_sum_factor < 1 or self.nchan % chan_sum_factor != 0:
+                raise ValueError(f"chan_sum_factor={chan_sum_factor} must be ≥ 1 "
+                                 f"and divide nchan={self.nchan}")
+            out = torch.empty((n_fv, self._nbase, self.nchan // chan_sum_factor),
+                              dtype=torch.complex64, device=self.device)
+        else:
+            out = torch.empty((n_fv, self._nbase, self.nchan, 2), dtype=torch.complex64,
+                              device=self.device)
+        _lib.check(_lib.lib().dsb_corr_split(
+            _lib.ptr(re), _lib.ptr(im), _DT[re.dtype], self.nchan, re.shape[3], self.nants,
+            self.t_int_fast_native, int(bool(fuse_stokes_i)), int(chan_sum_factor),
+            _lib.ptr(out), _lib.stream_of(self.device)), "dsb_corr_split")
+        return out
+
+    def compute_raw(self, raw: torch.Tensor, *, chan_sum_factor: int, npkt: Optional[int] = None,
+                    out: Optional[torch.Tensor] = None, layout: str = "tbc",
+                    max_ctas: int = 0) -> torch.Tensor:
+        """Correlate on-wire bytes ``(n_chgroup?, npkt, nant, nchan, 2, 2)``
+        (uint8 on the device) on the tensor cores.  ``layout='tbc'`` returns
+        ``(n_fv, nbase, nchan/csf)`` per chgroup (the ``compute_split`` fused
+        layout); ``'bct'`` returns ``(nbase, nchan/csf, n_fv)`` (time innermost,
+        the stage-1 input layout).  A leading chgroup axis is kept when
+        ``raw`` has 6 dims."""
+        _lib.require_cuda(raw, "raw")
+        if raw.dtype != torch.uint8:
+            raise TypeError(f"raw must be uint8, got {raw.dtype}")
+        page = self.nants * self.nchan * NTIMES_PER_PACKET * NPOL
+        n_g = raw.shape[0] if raw.ndim == 6 else 1
+        if npkt is None:
+            npkt = raw.numel() // (n_g * page)
+        if raw.numel() != n_g * npkt * page:
+            raise ValueError(f"raw has {raw.numel()} bytes, expected {n_g}x{npkt}x{page}")
+        ppfv = self.t_int_fast_native // NTIMES_PER_PACKET
+        if npkt % ppfv:
+            raise ValueError(f"npkt={npkt} not a multiple of packets_per_fast_vis={ppfv}")
+        n_fv = npkt // ppfv
+        ceff = self.nchan // chan_sum_factor
+        nb = self._nbase
+        if layout == "tbc":
+            shape = (n_g, n_fv, nb, ceff)
+            strides = (n_fv * nb * ceff, nb * ceff, ceff, 1)
+            order = 1
+        elif layout == "bct":
+            shape = (n_g, nb, ceff, n_fv)
+            strides = (nb * ceff * n_fv, 1, ceff * n_fv, n_fv)
+            order = 0
+        else:
+            raise ValueError(f"layout {layout!r} not in ('tbc', 'bct')")
+        if out is None:
+            out = torch.empty(shape, dtype=torch.complex64, device=self.device)
+        st = _lib.status_word(self.device)
+        _lib.check(_lib.lib().dsb_corr_tc(
+            _lib.ptr(raw), npkt * page, n_g, npkt, self.nants, self.nchan,
+            self.t_int_fast_native, chan_sum_factor, order, _lib.ptr(out), *strides, max_ctas,
+            _lib.ptr(st), _lib.stream_of(self.device)), "dsb_corr_tc")
+        self._last_status = st
+        return out if raw.ndim == 6 else out[0]
