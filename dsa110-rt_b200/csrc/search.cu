@@ -1,0 +1,576 @@
+// Search side: fine-DM combine, image masking, boxcar detector, Layer-1
+// noise estimate, and the FP64 uv-cell geometry kernel (sm_100a).
+#include "dsb_common.cuh"
+
+#include <algorithm>
+
+namespace {
+
+int launch_status() { return cudaGetLastError() == cudaSuccess ? DSB_OK : DSB_E_CUDA; }
+
+// ===========================================================================
+// uv cells (FP64): ix = rint(-(d / (c / (nu*1e9))) / cell) + N/2
+// (grid/sparsity_pattern.py:1090-1170, same operation order as numpy)
+// ===========================================================================
+__global__ void uv_cells_kernel(const double* __restrict__ du, const double* __restrict__ dv,
+                                int n_bl, const double* __restrict__ nu_ghz, int n_ch,
+                                double cell_lambda, int half, int* __restrict__ row,
+                                int* __restrict__ col) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_bl * n_ch) return;
+  const int b = (int)(idx / n_ch), c = (int)(idx % n_ch);
+  const double wl = 299792458.0 / (nu_ghz[c] * 1e9);
+  const double u = -(du[b] / wl);
+  const double v = -(dv[b] / wl);
+  col[idx] = (int)rint(u / cell_lambda) + half;
+  row[idx] = (int)rint(v / cell_lambda) + half;
+}
+
+// ===========================================================================
+// Pipeline combine: Hermitian half-spectrum from stage-2 rings.
+//   G_h[f, t, u, w] = 0.5 * sum_e sign_e(D[row_e(f)][t - sf[f, g_e]]) * (-1)^(u+w)
+// where each entry e of half-cell (u, w) names a chgroup g, a cell inside
+// that chgroup's pattern, and whether it is the conjugate mirror.
+// ===========================================================================
+struct CombArgs {
+  const float2* D;
+  long long d_stride, d_mask;
+  const int* hc_off;     // (n_half_cells + 1) CSR over half cells (u-major)
+  const int* e_g;        // chgroup
+  const int* e_cell;     // cell within the chgroup (negative = mirror, stored as ~cell)
+  const int* d_base;     // (G) first D row of each chgroup
+  const int* n_filled;   // (G)
+  const int* sfine;      // (n_fine_total, G) signed shifts
+  const int* f2c;        // (n_fine_total) coarse index
+  int f0, n_f, G, N;
+  long long t0;          // stream time of output t = 0
+  int n_t;
+  int fftshift;
+  float2* out;           // (n_f, n_t, N, N/2+1)
+};
+
+__global__ void combine_rows_kernel(const CombArgs A) {
+  const int nh = A.N / 2 + 1;
+  const long long n_hc = (long long)A.N * nh;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)A.n_f * A.n_t * n_hc;
+  if (idx >= total) return;
+  const int hc = (int)(idx % n_hc);
+  const long long r = idx / n_hc;
+  const int t = (int)(r % A.n_t);
+  const int fl = (int)(r / A.n_t);
+  const int f = A.f0 + fl;
+  const int c = A.f2c[f];
+  const long long ta = A.t0 + t;
+  double re = 0.0, im = 0.0;
+  for (int j = A.hc_off[hc]; j < A.hc_off[hc + 1]; ++j) {
+    const int g = A.e_g[j];
+    int cell = A.e_cell[j];
+    const bool mirror = cell < 0;
+    if (mirror) cell = ~cell;
+    const long long row = (long long)A.d_base[g] + (long long)c * A.n_filled[g] + cell;
+    const long long ts = ta - A.sfine[(long long)f * A.G + g];
+    const float2 x = A.D[row * A.d_stride + (ts & A.d_mask)];
+    re += x.x;
+    im += mirror ? -(double)x.y : (double)x.y;
+  }
+  float o_re = (float)(0.5 * re), o_im = (float)(0.5 * im);
+  const int u = hc / nh, w = hc % nh;
+  if (A.fftshift && ((u + w) & 1)) {
+    o_re = -o_re;
+    o_im = -o_im;
+  }
+  A.out[idx] = make_float2(o_re, o_im);
+}
+
+// ===========================================================================
+// Reference-layout dense cint8 combine (image/fused_combine_cuda.py:210-300,
+// 560-700): streams [G, T_stream, 2, N, N] int8.
+// ===========================================================================
+template <bool HALF, bool CALIB, bool OUT_F16>
+__global__ void combine_dense_kernel(const int8_t* __restrict__ streams,
+                                     const int* __restrict__ shifts,
+                                     const float* __restrict__ scales,
+                                     const float* __restrict__ off_re,
+                                     const float* __restrict__ off_im, void* __restrict__ out,
+                                     int G, int t_stream, int t_det, int N, int t_lo,
+                                     int fftshift) {
+  const int nw = HALF ? N / 2 + 1 : N;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = blockIdx.y * blockDim.y + threadIdx.y;
+  const int t_out = blockIdx.z * blockDim.z + threadIdx.z;
+  const int t = t_out + t_lo;
+  if (w >= nw || u >= N || t >= t_det) return;
+  const long long nsq = (long long)N * N;
+  const int off_cell = u * N + w;
+  const int off_m = ((N - u) % N) * N + ((N - w) % N);
+  const long long t_stride = 2 * nsq, g_stride = (long long)t_stream * t_stride;
+  float o_re, o_im;
+  if (!CALIB) {
+    int ar = 0, ai = 0, mr = 0, mi = 0;
+    for (int g = 0; g < G; ++g) {
+      const int ts = t - shifts[g];
+      if (ts >= 0 && ts < t_stream) {
+        const long long b = g * g_stride + ts * t_stride;
+        ar += streams[b + off_cell];
+        ai += streams[b + off_cell + nsq];
+        if (HALF) {
+          mr += streams[b + off_m];
+          mi += streams[b + off_m + nsq];
+        }
+      }
+    }
+    if (HALF) {
+      o_re = 0.5f * (float)(ar + mr);
+      o_im = 0.5f * (float)(ai - mi);
+    } else {
+      o_re = (float)ar;
+      o_im = (float)ai;
+    }
+  } else {
+    float ar = 0.f, ai = 0.f, mr = 0.f, mi = 0.f;
+    for (int g = 0; g < G; ++g) {
+      const int ts = t - shifts[g];
+      if (ts >= 0 && ts < t_stream) {
+        const long long b = g * g_stride + ts * t_stride;
+        const float sc = scales[g], orr = off_re[g], oii = off_im[g];
+        ar = fmaf(sc, (float)streams[b + off_cell], ar) + orr;
+        ai = fmaf(sc, (float)streams[b + off_cell + nsq], ai) + oii;
+        if (HALF) {
+          mr = fmaf(sc, (float)streams[b + off_m], mr) + orr;
+          mi = fmaf(sc, (float)streams[b + off_m + nsq], mi) + oii;
+        }
+      }
+    }
+    if (HALF) {
+      o_re = 0.5f * (ar + mr);
+      o_im = 0.5f * (ai - mi);
+    } else {
+      o_re = ar;
+      o_im = ai;
+    }
+  }
+  if (fftshift && ((u + w) & 1)) {
+    o_re = -o_re;
+    o_im = -o_im;
+  }
+  const long long o = (long long)t_out * N * nw + (long long)u * nw + w;
+  if (OUT_F16)
+    reinterpret_cast<__half2*>(out)[o] = __floats2half2_rn(o_re, o_im);
+  else
+    reinterpret_cast<float2*>(out)[o] = make_float2(o_re, o_im);
+}
+
+// ===========================================================================
+// image mask / normalise into the detector cube layout
+//   cube[t, f, h, w] = img[f, t, h, w] * mask_f[f, h, w]
+// ===========================================================================
+template <bool OUT_F16>
+__global__ void mask_to_cube_kernel(const float* __restrict__ img, const float* __restrict__ mask,
+                                    int mask_per_f, int n_f, int n_t, int npix,
+                                    void* __restrict__ cube, int cube_f_total, int cube_f0) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)n_f * n_t * npix;
+  if (idx >= total) return;
+  const int p = (int)(idx % npix);
+  const long long r = idx / npix;
+  const int t = (int)(r % n_t), f = (int)(r / n_t);
+  const float m = mask[(mask_per_f ? (long long)f * npix : 0) + p];
+  const float v = img[idx] * m;
+  const long long o = ((long long)t * cube_f_total + cube_f0 + f) * npix + p;
+  if (OUT_F16)
+    reinterpret_cast<__half*>(cube)[o] = __float2half_rn(v);
+  else
+    reinterpret_cast<float*>(cube)[o] = v;
+}
+
+// ===========================================================================
+// padded cumsum / boxcars (detector/forward.py:250-455,
+// detector/triton_boxcar.py:47-360).  Each prefix is accumulated in float64
+// and rounded once to float32.
+// ===========================================================================
+template <typename T>
+DSB_DEV float ldf(const T* p, long long i);
+template <>
+DSB_DEV float ldf<float>(const float* p, long long i) { return p[i]; }
+template <>
+DSB_DEV float ldf<__half>(const __half* p, long long i) { return __half2float(p[i]); }
+
+template <typename T>
+__global__ void padded_cumsum_kernel(const T* __restrict__ x, int n, long long inner, int max_w,
+                                     float* __restrict__ cs) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= inner) return;
+  const int pl = max_w / 2, pr = max_w - 1 - pl;
+  for (int j = 0; j <= pl; ++j) cs[(long long)j * inner + e] = 0.f;
+  double run = 0.0;
+  float last = 0.f;
+  for (int i = 0; i < n; ++i) {
+    run += (double)ldf<T>(x, (long long)i * inner + e);
+    last = (float)run;
+    cs[(long long)(1 + pl + i) * inner + e] = last;
+  }
+  for (int r = 0; r < pr; ++r) cs[(long long)(1 + pl + n + r) * inner + e] = last;
+}
+
+template <bool OUT_F16>
+__global__ void multi_boxcar_argmax_kernel(const float* __restrict__ cs, long long inner,
+                                           const int* __restrict__ widths,
+                                           const int* __restrict__ offsets,
+                                           const float* __restrict__ sinv, int K, int n_out,
+                                           int t_base, void* __restrict__ out_max,
+                                           int16_t* __restrict__ out_win) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_out * inner) return;
+  const int t = (int)(idx / inner);
+  const long long e = idx % inner;
+  const int ta = t + t_base;
+  float best = (cs[(long long)(ta + offsets[0] + widths[0]) * inner + e] -
+                cs[(long long)(ta + offsets[0]) * inner + e]) * sinv[0];
+  int win = 0;
+  for (int k = 1; k < K; ++k) {
+    const float s = (cs[(long long)(ta + offsets[k] + widths[k]) * inner + e] -
+                     cs[(long long)(ta + offsets[k]) * inner + e]) * sinv[k];
+    if (s > best) {
+      best = s;
+      win = k;
+    }
+  }
+  if (OUT_F16)
+    reinterpret_cast<__half*>(out_max)[idx] = __float2half_rn(best);
+  else
+    reinterpret_cast<float*>(out_max)[idx] = best;
+  out_win[idx] = (int16_t)win;
+}
+
+__global__ void boxcar_from_cs_kernel(const float* __restrict__ cs, long long inner, int width,
+                                      int start, int n_out, float* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_out * inner) return;
+  const int t = (int)(idx / inner);
+  const long long e = idx % inner;
+  out[idx] = cs[(long long)(start + t + width) * inner + e] - cs[(long long)(start + t) * inner + e];
+}
+
+// ===========================================================================
+// Fused streaming detector: per pixel, float64 running prefix rounded to
+// float32 (identical to the padded cumsum above), a register ring of the
+// last MAXW+1 prefixes, boxcar widths 1, 2, 4, ..., MAXW (centred, offsets
+// MAXW/2 - w/2), S/N = (hi - lo) * sinv[k], strict '>' over k, and
+// compaction of every output cell above threshold.
+// ===========================================================================
+struct DetCand {
+  int t;      // output index (t_abs - t_base)
+  int pix;    // (f * H + h) * W + w inside the cube
+  float snr;
+  int k;
+};
+
+template <int LOGW, typename T>
+__global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ cube, int n,
+                                                     long long inner, const float* __restrict__ sinv,
+                                                     int t_base, int n_out, float thr,
+                                                     DetCand* __restrict__ cands, int cap, int pix_off,
+                                                     int* __restrict__ count) {
+  constexpr int MAXW = 1 << LOGW;
+  constexpr int R = MAXW + 1;
+  constexpr int K = LOGW + 1;
+  constexpr int PL = MAXW / 2;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= inner) return;
+  float si[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) si[k] = sinv[k];
+  float ring[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) ring[q] = 0.f;
+  double run = 0.0;
+  float last = 0.f;
+  const int total = n + MAXW;  // cs length
+  for (int J0 = 0; J0 < total; J0 += R) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int J = J0 + q;
+      if (J < total) {
+        float v;
+        if (J <= PL) {
+          v = 0.f;
+        } else if (J <= PL + n) {
+          run += (double)ldf<T>(cube, (long long)(J - 1 - PL) * inner + e);
+          last = (float)run;
+          v = last;
+        } else {
+          v = last;
+        }
+        ring[q] = v;
+        const int ta = J - MAXW;
+        if (ta >= t_base && ta < t_base + n_out) {
+          float best = 0.f;
+          int win = 0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int w = 1 << k;
+            const int off = PL - w / 2;
+            // cs index ta + off  -> ring slot (q - MAXW + off) mod R, etc.
+            const int slo = ((q - MAXW + off) % R + R) % R;
+            const int shi = ((q - MAXW + off + w) % R + R) % R;
+            const float s = (ring[shi] - ring[slo]) * si[k];
+            if (k == 0 || s > best) {
+              best = s;
+              win = k;
+            }
+          }
+          if (best > thr) {
+            const int slot = atomicAdd(count, 1);
+            if (slot < cap) cands[slot] = DetCand{ta - t_base, (int)e + pix_off, best, win};
+          }
+        }
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// Layer-1 sigma-clipped std (noise_norm/layer1.py:53-125): one block per
+// row, rows of at most L1_MAX samples; bitonic sort, then the clipping
+// iterations walk a contiguous range of the sorted row; median is the lower
+// median (torch.nanmedian); sums in float64.
+// ===========================================================================
+constexpr int L1_MAX = 4096;
+constexpr int L1_THREADS = 1024;
+
+__global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const float* __restrict__ x,
+                                                                 int m, float n_sigma, int n_iter,
+                                                                 float* __restrict__ out) {
+  __shared__ float v[L1_MAX];
+  __shared__ double red[L1_THREADS / 32];
+  __shared__ int s_lo, s_hi;
+  const float* row = x + (long long)blockIdx.x * m;
+  int P = 1;
+  while (P < m) P <<= 1;
+  for (int i = threadIdx.x; i < P; i += L1_THREADS) {
+    float a = i < m ? row[i] : __int_as_float(0x7f800000);
+    if (!(a == a) || isinf(a)) a = __int_as_float(0x7f800000);  // non-finite -> +inf (dropped)
+    v[i] = a;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += L1_THREADS) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool up = (i & k) == 0;
+          const float a = v[i], b = v[ixj];
+          if ((a > b) == up) {
+            v[i] = b;
+            v[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // finite count
+  if (threadIdx.x == 0) {
+    int n_fin = 0;
+    int lo = 0, hi = P;
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (isinf(v[mid]) && v[mid] > 0) hi = mid; else lo = mid + 1;
+    }
+    n_fin = lo;
+    s_lo = 0;
+    s_hi = n_fin;
+  }
+  __syncthreads();
+  float sigma = 0.f, med = 0.f;
+  for (int it = 0; it <= n_iter; ++it) {
+    const int lo = s_lo, hi = s_hi;
+    const int cnt = hi - lo;
+    if (cnt <= 0) {
+      sigma = __int_as_float(0x7fc00000);
+      break;
+    }
+    med = v[lo + (cnt - 1) / 2];
+    double acc = 0.0;
+    for (int i = lo + threadIdx.x; i < hi; i += L1_THREADS) {
+      const float d = v[i] - med;
+      acc += (double)(d * d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tot = 0.0;
+      for (int w = 0; w < L1_THREADS / 32; ++w) tot += red[w];
+      red[0] = tot;
+    }
+    __syncthreads();
+    sigma = sqrtf((float)red[0] / (float)cnt);
+    __syncthreads();
+    if (it == n_iter) break;
+    if (threadIdx.x == 0) {
+      const float lo_v = med - n_sigma * sigma, hi_v = med + n_sigma * sigma;
+      int a = lo, b = hi;
+      while (a < hi && v[a] < lo_v) ++a;
+      while (b > a && v[b - 1] > hi_v) --b;
+      s_lo = a;
+      s_hi = b;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = (sigma == sigma) ? sigma : 0.f;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_ghz, int n_ch,
+                 double cell_lambda, int n_grid, int* row, int* col, cudaStream_t stream) {
+  if (!du || !dv || !nu_ghz || !row || !col || n_bl < 0 || n_ch <= 0 || !(cell_lambda > 0))
+    return DSB_E_ARG;
+  const long long n = (long long)n_bl * n_ch;
+  if (n == 0) return DSB_OK;
+  uv_cells_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(du, dv, n_bl, nu_ghz, n_ch,
+                                                                   cell_lambda, n_grid / 2, row,
+                                                                   col);
+  return launch_status();
+}
+
+int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
+                     const int* e_g, const int* e_cell, const int* d_base, const int* n_filled,
+                     const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
+                     long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
+  if (!D || !hc_off || !e_g || !e_cell || !d_base || !n_filled || !sfine || !f2c || !out)
+    return DSB_E_ARG;
+  if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
+  CombArgs A{(const float2*)D, d_stride, d_mask, hc_off, e_g, e_cell, d_base, n_filled, sfine,
+             f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
+  const long long total = (long long)n_f * n_t * N * (N / 2 + 1);
+  combine_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(A);
+  return launch_status();
+}
+
+int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
+                      const float* off_re, const float* off_im, void* out, int out_f16, int half,
+                      int G, int t_stream, int t_det, int N, int t_lo, int fftshift,
+                      cudaStream_t stream) {
+  if (!streams || !shifts || !out || G <= 0 || N <= 0 || t_det <= t_lo || t_lo < 0) return DSB_E_ARG;
+  if (half && (N & 1)) return DSB_E_ARG;
+  const bool calib = scales != nullptr;
+  if (calib && (!off_re || !off_im)) return DSB_E_ARG;
+  const int nw = half ? N / 2 + 1 : N;
+  dim3 block(32, 4, 8);
+  dim3 grid((nw + 31) / 32, (N + 3) / 4, (t_det - t_lo + 7) / 8);
+  const int8_t* s = (const int8_t*)streams;
+#define DSB_CD(H, C, F)                                                                       \
+  combine_dense_kernel<H, C, F><<<grid, block, 0, stream>>>(s, shifts, scales, off_re, off_im, \
+                                                            out, G, t_stream, t_det, N, t_lo, \
+                                                            fftshift)
+  if (half) {
+    if (calib) { if (out_f16) DSB_CD(true, true, true); else DSB_CD(true, true, false); }
+    else { if (out_f16) DSB_CD(true, false, true); else DSB_CD(true, false, false); }
+  } else {
+    if (calib) { if (out_f16) DSB_CD(false, true, true); else DSB_CD(false, true, false); }
+    else { if (out_f16) DSB_CD(false, false, true); else DSB_CD(false, false, false); }
+  }
+#undef DSB_CD
+  return launch_status();
+}
+
+int dsb_mask_to_cube(const float* img, const float* mask, int mask_per_f, int n_f, int n_t,
+                     int npix, void* cube, int cube_f16, int cube_f_total, int cube_f0,
+                     cudaStream_t stream) {
+  if (!img || !mask || !cube || n_f <= 0 || n_t <= 0 || npix <= 0) return DSB_E_ARG;
+  if (cube_f0 < 0 || cube_f0 + n_f > cube_f_total) return DSB_E_ARG;
+  const long long total = (long long)n_f * n_t * npix;
+  if (cube_f16)
+    mask_to_cube_kernel<true><<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(
+        img, mask, mask_per_f, n_f, n_t, npix, cube, cube_f_total, cube_f0);
+  else
+    mask_to_cube_kernel<false><<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(
+        img, mask, mask_per_f, n_f, n_t, npix, cube, cube_f_total, cube_f0);
+  return launch_status();
+}
+
+int dsb_padded_cumsum(const void* x, int x_f16, int n, long long inner, int max_w, float* cs,
+                      cudaStream_t stream) {
+  if (!x || !cs || n <= 0 || inner <= 0 || max_w < 1 || max_w > n) return DSB_E_ARG;
+  const unsigned grid = (unsigned)((inner + 255) / 256);
+  if (x_f16)
+    padded_cumsum_kernel<__half><<<grid, 256, 0, stream>>>((const __half*)x, n, inner, max_w, cs);
+  else
+    padded_cumsum_kernel<float><<<grid, 256, 0, stream>>>((const float*)x, n, inner, max_w, cs);
+  return launch_status();
+}
+
+int dsb_multi_boxcar_argmax(const float* cs, long long inner, const int* widths,
+                            const int* offsets, const float* sigma_inv, int K, int n_out,
+                            int t_base, void* out_max, int out_f16, void* out_win,
+                            cudaStream_t stream) {
+  if (!cs || !widths || !offsets || !sigma_inv || !out_max || !out_win || K < 1 || n_out <= 0)
+    return DSB_E_ARG;
+  const long long total = (long long)n_out * inner;
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  if (out_f16)
+    multi_boxcar_argmax_kernel<true><<<grid, 256, 0, stream>>>(
+        cs, inner, widths, offsets, sigma_inv, K, n_out, t_base, out_max, (int16_t*)out_win);
+  else
+    multi_boxcar_argmax_kernel<false><<<grid, 256, 0, stream>>>(
+        cs, inner, widths, offsets, sigma_inv, K, n_out, t_base, out_max, (int16_t*)out_win);
+  return launch_status();
+}
+
+int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, int n_out,
+                       float* out, cudaStream_t stream) {
+  if (!cs || !out || width < 1 || start < 0 || n_out <= 0) return DSB_E_ARG;
+  const long long total = (long long)n_out * inner;
+  boxcar_from_cs_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(cs, inner, width,
+                                                                             start, n_out, out);
+  return launch_status();
+}
+
+int dsb_detect(const void* cube, int cube_f16, int n, long long inner, int log_maxw,
+               const float* sigma_inv, int t_base, int n_out, float threshold, void* cands,
+               int cap, int pix_off, int* count, cudaStream_t stream) {
+  if (!cube || !sigma_inv || !cands || !count || n <= 0 || inner <= 0 || cap < 0) return DSB_E_ARG;
+  if (log_maxw < 0 || log_maxw > 6 || (1 << log_maxw) > n || t_base < 0 || n_out < 0 ||
+      t_base + n_out > n)
+    return DSB_E_ARG;
+  const unsigned grid = (unsigned)((inner + 255) / 256);
+  DetCand* c = (DetCand*)cands;
+#define DSB_DET(L)                                                                          \
+  do {                                                                                      \
+    if (cube_f16)                                                                           \
+      detect_kernel<L, __half><<<grid, 256, 0, stream>>>((const __half*)cube, n, inner,      \
+                                                         sigma_inv, t_base, n_out, threshold, \
+                                                         c, cap, pix_off, count);                    \
+    else                                                                                    \
+      detect_kernel<L, float><<<grid, 256, 0, stream>>>((const float*)cube, n, inner,        \
+                                                        sigma_inv, t_base, n_out, threshold,  \
+                                                        c, cap, pix_off, count);                     \
+  } while (0)
+  switch (log_maxw) {
+    case 0: DSB_DET(0); break;
+    case 1: DSB_DET(1); break;
+    case 2: DSB_DET(2); break;
+    case 3: DSB_DET(3); break;
+    case 4: DSB_DET(4); break;
+    case 5: DSB_DET(5); break;
+    case 6: DSB_DET(6); break;
+  }
+#undef DSB_DET
+  return launch_status();
+}
+
+int dsb_clipped_std(const float* samples, int rows, int m, float n_sigma, int n_iter, float* out,
+                    cudaStream_t stream) {
+  if (!samples || !out || rows <= 0 || m <= 0 || n_iter < 0) return DSB_E_ARG;
+  if (m > L1_MAX) return DSB_E_CAPACITY;
+  clipped_std_kernel<<<rows, L1_THREADS, 0, stream>>>(samples, m, n_sigma, n_iter, out);
+  return launch_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,396 @@
+"""Streaming fast-search pipeline on one B200: the composition of
+``process_block`` (services/corr_fast_integration.py:2063: corr phase
+:2229 + consume phase :2476) and ``CubePipeline.process``
+(services/cube_pipeline.py:2682) with the inter-node UDP corner turn
+replaced by device-resident rings.
+
+Data flow per time chunk of ``chunk_tiles`` fast-vis tiles (time is the
+absolute fast-vis tile index from the start of the stream):
+
+  raw pages (G, npkt, nant, nchan, 2, 2) uint8
+   -> dsb_corr_tc_grid   : unpack + tcgen05 correlator, Stokes I, channel
+                           sum, gridded per summed channel into rows Y
+                           (ring indexed by tile time)
+   -> dsb_stage1_rows    : coarse-DM shift + sum over summed channels,
+                           static-sky subtraction; written at t + shift2 into
+                           the stage-2 ring D (so the stage-2 FIFO is an index
+                           offset)
+   -> per fine-DM batch:
+      dsb_combine_rows   : fine-DM residual shifts, sum over chgroups,
+                           Hermitian half spectrum, fftshift checkerboard
+      irfft2             : real image
+      dsb_clipped_std    : Layer-1 sigma per fine DM (current cube)
+      dsb_mask_to_cube   : edge mask x 1/sigma into the detector cube
+      dsb_detect         : boxcars 1..2**log_max_width, max over widths,
+                           threshold compaction
+   -> host: top-k (value desc, flat index asc) + merge-radius decode
+
+Detector cubes overlap by 2*t_edge so that their interiors tile time.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
+from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
+from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
+from .search import (CandidateBuffer, Candidate, _nms, compute_edge_mask, irfft2_image,
+                     mask_into_cube, sigma_clipped_std_batched, detect_cube)
+
+
+def _pow2_at_least(n: int) -> int:
+    return 1 << max(0, int(math.ceil(math.log2(max(1, n)))))
+
+
+@dataclass
+class PipelineConfig:
+    nant: int = 96
+    band: Band = DSA110_BAND
+    npkt_block: int = 8192           # packets (2 samples each) per block per chgroup page
+    t_int: int = 8                   # native samples per fast-vis tile
+    csf: int = 16                    # channels summed per subband
+    n_grid: int = 256
+    coarse_dm: np.ndarray = field(default_factory=lambda: np.linspace(0.0, 2000.0, 32))
+    fine_per_coarse: int = 16
+    fine_dm: Optional[np.ndarray] = None
+    fine_to_coarse: Optional[np.ndarray] = None
+    log_max_width: int = 4           # boxcars 1, 2, 4, ..., 2**log_max_width
+    threshold: float = 7.0
+    use_sky: bool = True
+    sky_window: int = 8
+    sky_warmup: int = 8
+    chunk_tiles: int = 512
+    fdm_batch: int = 8
+    n_top: int = 256
+    merge_radius_t: int = 4
+    merge_radius_fdm: int = 5
+    merge_radius_lm: int = 3
+    l1_times: int = 16
+    l1_pixels: int = 256
+    cand_capacity: int = 1 << 22
+
+    def __post_init__(self):
+        self.coarse_dm = np.asarray(self.coarse_dm, np.float64)
+        if self.fine_dm is None:
+            # fine DMs spread evenly around each coarse DM (v2 plan: coarse at the
+            # middle of its bucket, constants.py:240-270)
+            nc = self.coarse_dm.size
+            step = (self.coarse_dm[1] - self.coarse_dm[0]) if nc > 1 else 1.0
+            K = self.fine_per_coarse
+            off = (np.arange(K) - (K - 1) / 2.0) * (step / K)
+            self.fine_dm = (self.coarse_dm[:, None] + off[None, :]).reshape(-1)
+            self.fine_dm = np.maximum(self.fine_dm, 0.0)
+            self.fine_to_coarse = np.repeat(np.arange(nc), K)
+        self.fine_dm = np.asarray(self.fine_dm, np.float64)
+        self.fine_to_coarse = np.asarray(self.fine_to_coarse, np.int64)
+
+    @property
+    def t_int_us(self) -> float:
+        return self.t_int * NATIVE_SAMPLE_US
+
+    @property
+    def n_fv_block(self) -> int:
+        return self.npkt_block * 2 // self.t_int
+
+    @property
+    def ceff(self) -> int:
+        return self.band.nchan // self.csf
+
+    @property
+    def t_edge(self) -> int:
+        return (1 << self.log_max_width) // 2
+
+    @property
+    def block_seconds(self) -> float:
+        return self.npkt_block * 2 * NATIVE_SAMPLE_US * 1e-6
+
+
+@dataclass
+class Tables:
+    """Host-built index tables (one-time, FP64 / integer)."""
+
+    cell_lambda: float
+    patterns: list
+    n_filled: np.ndarray            # (G,)
+    ycell: np.ndarray               # (G*ceff*nbase,) int32
+    yoff: np.ndarray                # (G*ceff,) int32
+    ycnt: np.ndarray
+    ymax: int
+    n_rows_y: int
+    cell_off: np.ndarray            # stage-1 CSR over global cells
+    src_row: np.ndarray
+    src_s: np.ndarray
+    cell_g: np.ndarray
+    cell_local: np.ndarray
+    max_src: int
+    shift1: np.ndarray              # (G, ceff, n_coarse) int32
+    shift2: np.ndarray              # (G, n_coarse) int32
+    d_base: np.ndarray              # (G,)
+    n_rows_d: int
+    sfine: np.ndarray               # (n_fine, G) int32
+    hc_off: np.ndarray              # combine CSR over half cells
+    e_g: np.ndarray
+    e_cell: np.ndarray
+    mask: np.ndarray                # (N, N) float32
+
+
+def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
+    band, G, ceff, N = cfg.band, cfg.band.n_chgroup, cfg.ceff, cfg.n_grid
+    nbase = nbase_of(cfg.nant)
+    cell = compute_top_of_band_cell_lambda(antpos_e, antpos_n, n_grid=N, band=band,
+                                           is_core_baseline_mask=core_mask)
+    pats, cims = [], []
+    for g in range(G):
+        p = build_pattern(antpos_e, antpos_n, chgroup=g, n_grid=N, chan_sum_factor=cfg.csf,
+                          cell_lambda=cell, is_core_baseline_mask=core_mask, band=band,
+                          device=device)
+        pats.append(p)
+        cims.append(cell_index_map_for(p, antpos_e, antpos_n, is_core_baseline_mask=core_mask,
+                                       device=device))
+    n_filled = np.asarray([p.n_filled for p in pats], np.int64)
+    # per-(g, s) Y rows: distinct cells hit by summed channel s, ascending
+    ycell = np.full((G, ceff, nbase), -1, np.int32)
+    yoff = np.zeros(G * ceff, np.int64)
+    ycnt = np.zeros(G * ceff, np.int64)
+    row_cell = []
+    row_g = []
+    row_s = []
+    nrow = 0
+    for g in range(G):
+        for s in range(ceff):
+            col = cims[g][:, s]
+            valid = col < n_filled[g]
+            cells = np.unique(col[valid])
+            ycell[g, s, valid] = np.searchsorted(cells, col[valid]).astype(np.int32)
+            yoff[g * ceff + s] = nrow
+            ycnt[g * ceff + s] = cells.size
+            row_cell.append(cells)
+            row_g.append(np.full(cells.size, g))
+            row_s.append(np.full(cells.size, s))
+            nrow += cells.size
+    row_cell = np.concatenate(row_cell)
+    row_g = np.concatenate(row_g)
+    row_s = np.concatenate(row_s)
+    cell_base = np.concatenate([[0], np.cumsum(n_filled)])
+    gcell = cell_base[row_g] + row_cell
+    order = np.lexsort((row_s, gcell))
+    counts = np.bincount(gcell, minlength=int(cell_base[-1]))
+    cell_off = np.zeros(int(cell_base[-1]) + 1, np.int64)
+    cell_off[1:] = np.cumsum(counts)
+    cell_g = np.repeat(np.arange(G), n_filled)
+    cell_local = np.concatenate([np.arange(n) for n in n_filled])
+    # shift tables
+    plan = DMPlan(dm_pc_cc=cfg.coarse_dm, t_int_fast_us=cfg.t_int_us, chan_sum_factor=cfg.csf,
+                  band=band)
+    shift1 = plan.delay_bins_all().astype(np.int32)
+    shift2 = np.stack([compute_stage2_shifts(chgroup=g, coarse_dm_pc_cm3=cfg.coarse_dm,
+                                             t_int_corr_us=cfg.t_int_us,
+                                             band=band).shifts_samples for g in range(G)])
+    sfine = compute_time_shift_search(coarse_dm_pc_cm3=cfg.coarse_dm, fine_dm_pc_cm3=cfg.fine_dm,
+                                      fine_to_coarse=cfg.fine_to_coarse,
+                                      t_int_search_us=cfg.t_int_us, merge_coarse_rounding=True,
+                                      band=band)
+    n_coarse = cfg.coarse_dm.size
+    d_base = np.concatenate([[0], np.cumsum(n_filled * n_coarse)])[:-1]
+    # combine CSR over half cells (r, c), c in [0, N/2]
+    nh = N // 2 + 1
+    ent = [[] for _ in range(N * nh)]
+    for g, p in enumerate(pats):
+        r = p.ix_row.astype(np.int64)
+        c = p.ix_col.astype(np.int64)
+        for k in range(r.size):
+            if c[k] <= N // 2:
+                ent[r[k] * nh + c[k]].append((g, k))
+            rm, cm = (N - r[k]) % N, (N - c[k]) % N
+            if cm <= N // 2:
+                ent[rm * nh + cm].append((g, ~k))
+    hc_off = np.zeros(N * nh + 1, np.int64)
+    hc_off[1:] = np.cumsum([len(x) for x in ent])
+    e_g = np.asarray([g for x in ent for g, _ in x], np.int32)
+    e_cell = np.asarray([k for x in ent for _, k in x], np.int32)
+    mask = compute_edge_mask(n_grid=N, kernel_support=1)
+    return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled,
+                  ycell=ycell.reshape(-1), yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
+                  ymax=int(ycnt.max()), n_rows_y=int(nrow),
+                  cell_off=cell_off.astype(np.int32), src_row=order.astype(np.int32),
+                  src_s=row_s[order].astype(np.int32), cell_g=cell_g.astype(np.int32),
+                  cell_local=cell_local.astype(np.int32), max_src=int(counts.max()),
+                  shift1=np.ascontiguousarray(shift1), shift2=shift2.astype(np.int32),
+                  d_base=d_base.astype(np.int32), n_rows_d=int(n_filled.sum() * n_coarse),
+                  sfine=sfine.astype(np.int32), hc_off=hc_off.astype(np.int32), e_g=e_g,
+                  e_cell=e_cell, mask=mask.astype(np.float32))
+
+
+@dataclass
+class StreamCandidate:
+    t: int          # absolute fast-vis tile (stage-2 / bottom-of-band time)
+    fdm: int        # fine-DM index
+    l: int          # image row
+    m: int          # image column
+    snr: float
+    width: int      # boxcar width (tiles)
+
+
+class SearchPipeline:
+    """One-GPU streaming fast search with device-resident rings."""
+
+    def __init__(self, cfg: PipelineConfig, antpos_e, antpos_n, device="cuda", core_mask=None):
+        self.cfg = cfg
+        self.dev = _lib.cuda_device(device)
+        self.tab = build_tables(cfg, antpos_e, antpos_n, self.dev, core_mask)
+        T = self.tab
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.dev)  # noqa: E731
+        self.d_ycell, self.d_yoff, self.d_ycnt = d(T.ycell), d(T.yoff), d(T.ycnt)
+        self.d_cell_off, self.d_src_row, self.d_src_s = d(T.cell_off), d(T.src_row), d(T.src_s)
+        self.d_cell_g, self.d_cell_local = d(T.cell_g), d(T.cell_local)
+        self.d_shift1, self.d_shift2 = d(T.shift1), d(T.shift2)
+        self.d_dbase = d(T.d_base)
+        self.d_nfilled = d(T.n_filled.astype(np.int32))
+        self.d_sfine, self.d_f2c = d(T.sfine), d(cfg.fine_to_coarse.astype(np.int32))
+        self.d_hc_off, self.d_eg, self.d_ecell = d(T.hc_off), d(T.e_g), d(T.e_cell)
+        self.d_mask = d(T.mask)
+        C = cfg.chunk_tiles
+        if cfg.n_fv_block % C:
+            raise ValueError("chunk_tiles must divide the block's fast-vis tile count")
+        self.max_sh1 = int(T.shift1.max())
+        self.depth1 = max(0, math.ceil(self.max_sh1 / C))
+        self.L = max(0, -int(T.sfine.min()))
+        self.a = math.ceil(self.L / C)
+        te = cfg.t_edge
+        # warm-up: the first detector cube all of whose times carry data from
+        # every chgroup (the stage-2 delay of the top chgroup has elapsed)
+        self.jc_first = math.ceil((int(T.shift2.max()) + max(0, int(T.sfine.max())) + 2 * te) / C)
+        self.TY = _pow2_at_least((self.depth1 + 1) * C)
+        span_d = (self.a + 1) * C + 2 * te + max(0, int(T.sfine.max())) + int(T.shift2.max()) + C
+        self.TD = _pow2_at_least(span_d)
+        self.Y = torch.zeros((T.n_rows_y, self.TY), dtype=torch.complex64, device=self.dev)
+        self.D = torch.zeros((T.n_rows_d, self.TD), dtype=torch.complex64, device=self.dev)
+        self.sky = (torch.zeros((T.n_rows_d, cfg.sky_window), dtype=torch.complex128,
+                                device=self.dev) if cfg.use_sky else None)
+        self.sky_count = self.sky_head = self.sky_seen = 0
+        self.status = _lib.status_word(self.dev)
+        nt_cube = C + 2 * te
+        nb = cfg.fdm_batch
+        N = cfg.n_grid
+        self.Gh = torch.empty((nb, nt_cube, N, N // 2 + 1), dtype=torch.complex64, device=self.dev)
+        self.cube = torch.empty((nt_cube, nb, N, N), dtype=torch.float32, device=self.dev)
+        widths = [1 << k for k in range(cfg.log_max_width + 1)]
+        self.widths = widths
+        self.sinv = d((np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32))
+        self.cands = CandidateBuffer(self.dev, cfg.cand_capacity)
+        self.chunk = 0              # next absolute chunk index to correlate
+        self.out: List[StreamCandidate] = []
+        self.keep_sigma = False
+        self.l1_sigma: List[torch.Tensor] = []
+        # Layer-1 subsample positions (interior times x active pixels)
+        act = np.nonzero(T.mask.reshape(-1) != 0)[0]
+        self.l1_pix = d(act[np.linspace(0, act.size - 1, cfg.l1_pixels).astype(np.int64)])
+        self.l1_t = d(te + np.linspace(0, C - 1, cfg.l1_times).astype(np.int64))
+
+    # ------------------------------------------------------------------
+    def _corr(self, raw: torch.Tensor, p0: int) -> None:
+        cfg, T = self.cfg, self.tab
+        C = cfg.chunk_tiles
+        ppfv = cfg.t_int // 2
+        row_bytes = cfg.nant * cfg.band.nchan * 4
+        page = cfg.npkt_block * row_bytes
+        base = raw.data_ptr() + p0 * row_bytes
+        _lib.check(_lib.lib().dsb_corr_tc_grid(
+            _lib.ctypes.c_void_p(base), page, cfg.band.n_chgroup, C * ppfv, cfg.nant,
+            cfg.band.nchan, cfg.t_int, cfg.csf, _lib.ptr(self.d_ycell), _lib.ptr(self.d_yoff),
+            _lib.ptr(self.d_ycnt), T.ymax, _lib.ptr(self.Y), self.TY, self.chunk * C, self.TY - 1,
+            0, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_corr_tc_grid")
+
+    def _stage1(self, j: int) -> None:
+        cfg, T = self.cfg, self.tab
+        C = cfg.chunk_tiles
+        sub = int(cfg.use_sky and self.sky_count > 0 and self.sky_seen >= cfg.sky_warmup)
+        _lib.check(_lib.lib().dsb_stage1_rows(
+            _lib.ptr(self.Y), self.TY, self.TY - 1, int(T.cell_off.size - 1),
+            _lib.ptr(self.d_cell_off), _lib.ptr(self.d_src_row), _lib.ptr(self.d_src_s),
+            _lib.ptr(self.d_cell_g), _lib.ptr(self.d_cell_local), _lib.ptr(self.d_shift1),
+            _lib.ptr(self.d_shift2), _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled),
+            _lib.ptr(self.D), self.TD, self.TD - 1, j * C, C, cfg.coarse_dm.size, cfg.ceff,
+            _lib.ptr(self.sky), cfg.sky_window, self.sky_head, self.sky_count, sub, T.max_src,
+            _lib.stream_of(self.dev)), "dsb_stage1_rows")
+        if cfg.use_sky:
+            self.sky_count = min(self.sky_count + 1, cfg.sky_window)
+            self.sky_head = (self.sky_head + 1) % cfg.sky_window
+            self.sky_seen += 1
+
+    def _search(self, jc: int, collect: bool = True) -> None:
+        cfg, T = self.cfg, self.tab
+        C, te, N = cfg.chunk_tiles, cfg.t_edge, cfg.n_grid
+        t0 = jc * C - 2 * te
+        nt = C + 2 * te
+        nfine = cfg.fine_dm.size
+        self.cands.reset()
+        for f0 in range(0, nfine, cfg.fdm_batch):
+            nf = min(cfg.fdm_batch, nfine - f0)
+            gh = self.Gh[:nf]
+            _lib.check(_lib.lib().dsb_combine_rows(
+                _lib.ptr(self.D), self.TD, self.TD - 1, _lib.ptr(self.d_hc_off),
+                _lib.ptr(self.d_eg), _lib.ptr(self.d_ecell), _lib.ptr(self.d_dbase),
+                _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c), f0, nf,
+                cfg.band.n_chgroup, N, t0, nt, 1, _lib.ptr(gh), _lib.stream_of(self.dev)),
+                "dsb_combine_rows")
+            img = irfft2_image(gh, N)                                  # (nf, nt, N, N)
+            samp = img.reshape(nf, nt, N * N)[:, self.l1_t][:, :, self.l1_pix].reshape(nf, -1)
+            sig = sigma_clipped_std_batched(samp)
+            sig = torch.where(sig > 0, sig, torch.ones_like(sig))
+            mask_f = (self.d_mask[None] / sig[:, None, None]).contiguous()
+            cube = self.cube[:, :nf] if nf == cfg.fdm_batch else torch.empty(
+                (nt, nf, N, N), dtype=torch.float32, device=self.dev)
+            mask_into_cube(img.contiguous(), mask_f, cube, 0)
+            detect_cube(cube, log_max_width=cfg.log_max_width, sigma_inv=self.sinv, t_base=te,
+                        n_out=C, threshold=cfg.threshold, cands=self.cands,
+                        pix_offset=f0 * N * N)
+            if collect and self.keep_sigma:
+                self.l1_sigma.append(sig)
+        if collect:
+            got = self.cands.fetch()
+            self._pending = [(float(c["snr"]), int(c["t"]) * (nfine * N * N) + int(c["pix"]),
+                              int(c["k"])) for c in got]
+            res = _nms(self._pending, threshold=cfg.threshold, n_top=cfg.n_top,
+                       shape=(C, nfine, N, N), r_t=cfg.merge_radius_t, r_f=cfg.merge_radius_fdm,
+                       r_lm=cfg.merge_radius_lm)
+            t_first = jc * C - te
+            for t, f, l_, m_, v, k in res:
+                self.out.append(StreamCandidate(t_first + t, f, l_, m_, v, self.widths[k]))
+            self._pending = []
+
+    def process_block(self, raw: torch.Tensor, *, collect: bool = True) -> List[StreamCandidate]:
+        """Push one block of raw pages ``(G, npkt, nant, nchan, 2, 2)`` uint8
+        (device tensor, or host tensor copied here) through the pipeline;
+        returns the candidates whose detector cubes completed."""
+        cfg = self.cfg
+        if raw.device.type != "cuda":
+            raw = raw.to(self.dev, non_blocking=True)
+        if raw.dtype != torch.uint8 or raw.numel() != cfg.band.n_chgroup * cfg.npkt_block * \
+                cfg.nant * cfg.band.nchan * 4:
+            raise ValueError("raw must be uint8 (G, npkt, nant, nchan, 2, 2)")
+        raw = raw.contiguous()
+        self.out = []
+        self._pending = []
+        C = cfg.chunk_tiles
+        ppfv = cfg.t_int // 2
+        for ci in range(cfg.n_fv_block // C):
+            self._corr(raw, ci * C * ppfv)
+            j = self.chunk - self.depth1
+            if j >= 0:
+                self._stage1(j)
+                jc = j - self.a
+                if jc >= self.jc_first:
+                    self._search(jc, collect)
+            self.chunk += 1
+        return self.out
+
+    def check_status(self) -> None:
+        _lib.check_status(self.status, "pipeline")

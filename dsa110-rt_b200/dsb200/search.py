@@ -1,0 +1,347 @@
+"""Search side: fine-DM combine, imaging, boxcar detector, Layer-1 noise —
+drop-in for ``dsart.image.fused_combine_cuda`` (fused_dequant_combine_per_fdm
+:1104, ``_half`` :1359), ``dsart.image.imager`` (compute_edge_mask :112,
+image_mask_npad :57), ``dsart.detector.forward`` (precompute_padded_cumsum
+:250, boxcar_from_padded_cumsum :339), ``dsart.detector.triton_boxcar``
+(multi_boxcar_argmax_triton :305), ``dsart.detector.decoder``
+(decode_topk_argmax_lowmem :388) and ``dsart.noise_norm.layer1``
+(sigma_clipped_std_batched :53).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+
+# ---------------------------------------------------------------------------
+# combine (reference dense cint8 layout)
+# ---------------------------------------------------------------------------
+
+
+def _combine_dense(streams_cint8, shifts, output, *, half, scales, offsets_re, offsets_im,
+                   t_lo, fftshift):
+    for t, nm in ((streams_cint8, "streams_cint8"), (shifts, "shifts"), (output, "output")):
+        _lib.require_cuda(t, nm)
+    if streams_cint8.dtype != torch.int8 or streams_cint8.ndim != 5 or streams_cint8.shape[2] != 2:
+        raise RuntimeError(f"streams_cint8 must be int8 [G, T, 2, N, N]; got "
+                           f"{streams_cint8.dtype} {tuple(streams_cint8.shape)}")
+    G, T, _, N, N2 = streams_cint8.shape
+    if N != N2:
+        raise RuntimeError("streams_cint8 grid must be square")
+    if shifts.dtype != torch.int32 or shifts.shape != (G,):
+        raise RuntimeError(f"shifts must be int32 ({G},)")
+    nw = N // 2 + 1 if half else N
+    if output.ndim != 3 or output.shape[1:] != (N, nw):
+        raise RuntimeError(f"output must be [T_det - t_lo, {N}, {nw}]; got {tuple(output.shape)}")
+    if output.dtype not in (torch.complex32, torch.complex64):
+        raise RuntimeError(f"output dtype {output.dtype} not in (complex32, complex64)")
+    calib = scales is not None
+    if calib:
+        for t, nm in ((scales, "scales"), (offsets_re, "offsets_re"), (offsets_im, "offsets_im")):
+            if t is None or t.dtype != torch.float32 or t.numel() != G:
+                raise RuntimeError(f"{nm} must be float32 ({G},)")
+            _lib.require_cuda(t, nm)
+    t_det = int(t_lo) + int(output.shape[0])
+    _lib.check(_lib.lib().dsb_combine_dense(
+        _lib.ptr(streams_cint8), _lib.ptr(shifts), _lib.ptr(scales if calib else None),
+        _lib.ptr(offsets_re if calib else None), _lib.ptr(offsets_im if calib else None),
+        _lib.ptr(output), int(output.dtype == torch.complex32), int(half), G, T, t_det, N,
+        int(t_lo), int(bool(fftshift)), _lib.stream_of(output.device)), "dsb_combine_dense")
+
+
+def fused_dequant_combine_per_fdm(streams_cint8, shifts, output, *, scales=None, offsets_re=None,
+                                  offsets_im=None, t_lo: int = 0, fftshift: bool = True) -> None:
+    """Full-grid combine into ``output [T_det - t_lo, N, N]`` (fused_combine_cuda.py:1104)."""
+    _combine_dense(streams_cint8, shifts, output, half=False, scales=scales,
+                   offsets_re=offsets_re, offsets_im=offsets_im, t_lo=t_lo, fftshift=fftshift)
+
+
+def fused_dequant_combine_per_fdm_half(streams_cint8, shifts, output, *, scales=None,
+                                       offsets_re=None, offsets_im=None, t_lo: int = 0,
+                                       fftshift: bool = True) -> None:
+    """Hermitian half-spectrum combine into ``[T_det - t_lo, N, N/2+1]``
+    (fused_combine_cuda.py:1359)."""
+    _combine_dense(streams_cint8, shifts, output, half=True, scales=scales,
+                   offsets_re=offsets_re, offsets_im=offsets_im, t_lo=t_lo, fftshift=fftshift)
+
+
+# ---------------------------------------------------------------------------
+# imaging
+# ---------------------------------------------------------------------------
+
+
+def image_mask_npad(*, n_grid: int, kernel_support: int = 5, sigma_l_pix: Optional[float] = None,
+                    envelope_threshold: float = 0.5) -> int:
+    """image/imager.py:57-109."""
+    if n_grid <= 0 or n_grid & (n_grid - 1):
+        raise ValueError(f"n_grid={n_grid}, expected positive power of two")
+    if kernel_support < 1:
+        raise ValueError(f"kernel_support={kernel_support}, expected ≥ 1")
+    if not (0.0 < envelope_threshold <= 1.0):
+        raise ValueError(f"envelope_threshold={envelope_threshold}, expected ∈ (0, 1]")
+    pad_kernel = (kernel_support // 2) + 2
+    pad_env = 0
+    if sigma_l_pix is not None and sigma_l_pix > 0:
+        rad = float(sigma_l_pix) * math.sqrt(2.0 * math.log(1.0 / envelope_threshold))
+        pad_env = max(0, int(math.ceil((n_grid / 2.0) - rad)))
+    return max(pad_kernel, pad_env)
+
+
+def compute_edge_mask(*, n_grid: int, kernel_support: int = 5, sigma_l_pix=None,
+                      envelope_threshold: float = 0.5, drop_dc: bool = True,
+                      dtype=np.float32, apply_ifft2_dc_correction: bool = True) -> np.ndarray:
+    """image/imager.py:112-176 (host table, built once per operating point)."""
+    npad = image_mask_npad(n_grid=n_grid, kernel_support=kernel_support,
+                           sigma_l_pix=sigma_l_pix, envelope_threshold=envelope_threshold)
+    mask = np.zeros((n_grid, n_grid), dtype=dtype)
+    if 2 * npad < n_grid:
+        mask[npad:n_grid - npad, npad:n_grid - npad] = 1.0
+    if drop_dc:
+        mask[n_grid // 2, n_grid // 2] = 0.0
+    if apply_ifft2_dc_correction:
+        ii, jj = np.indices((n_grid, n_grid))
+        mask = mask * (1.0 - 2.0 * ((ii + jj) & 1)).astype(dtype)
+    return mask
+
+
+def irfft2_image(half: torch.Tensor, n_grid: int) -> torch.Tensor:
+    """Real image from the (fftshift-folded) Hermitian half spectrum
+    ``[..., N, N/2+1]`` complex64 -> ``[..., N, N]`` float32."""
+    return torch.fft.irfft2(half, s=(n_grid, n_grid))
+
+
+def mask_into_cube(img: torch.Tensor, mask: torch.Tensor, cube: torch.Tensor, f0: int) -> None:
+    """``cube[t, f0+f, :, :] = img[f, t] * mask[(f,)]`` (imager_gpu.py:604-650)."""
+    _lib.require_cuda(img, "img")
+    _lib.require_cuda(cube, "cube")
+    n_f, n_t, H, W = img.shape
+    per_f = int(mask.ndim == 3)
+    _lib.check(_lib.lib().dsb_mask_to_cube(
+        _lib.ptr(img), _lib.ptr(mask), per_f, n_f, n_t, H * W, _lib.ptr(cube),
+        int(cube.dtype == torch.float16), int(cube.shape[1]), int(f0),
+        _lib.stream_of(img.device)), "dsb_mask_to_cube")
+
+
+# ---------------------------------------------------------------------------
+# detector
+# ---------------------------------------------------------------------------
+
+
+def precompute_padded_cumsum(x: torch.Tensor, *, axis: int, max_width: int,
+                             accum_dtype: Optional[torch.dtype] = None) -> torch.Tensor:
+    """Zero-prefixed, max-width-padded float32 cumsum (detector/forward.py:250)."""
+    if max_width < 1:
+        raise ValueError(f"max_width={max_width}, expected ≥ 1")
+    n = x.shape[axis]
+    if max_width > n:
+        raise ValueError(f"max_width={max_width} exceeds axis-{axis} length {n}")
+    if accum_dtype not in (None, torch.float32):
+        raise ValueError("dsb200 cumsum is float32 (float64 running prefix)")
+    if x.dtype not in (torch.float16, torch.float32):
+        raise ValueError(f"x dtype {x.dtype} not supported")
+    _lib.require_cuda(x, "x")
+    xm = torch.movedim(x, axis, 0).contiguous()
+    inner = xm[0].numel()
+    cs = torch.empty((n + max_width,) + tuple(xm.shape[1:]), dtype=torch.float32, device=x.device)
+    _lib.check(_lib.lib().dsb_padded_cumsum(_lib.ptr(xm), int(xm.dtype == torch.float16), n,
+                                            inner, max_width, _lib.ptr(cs),
+                                            _lib.stream_of(x.device)), "dsb_padded_cumsum")
+    return torch.movedim(cs, 0, axis)
+
+
+def boxcar_from_padded_cumsum(cs: torch.Tensor, *, axis: int, width: int, max_width: int,
+                              n_out: int, t_base: int = 0, out_dtype=None,
+                              w_tile_size=None) -> torch.Tensor:
+    """Centred boxcar from the padded cumsum (detector/forward.py:339)."""
+    if width < 1 or width > max_width:
+        raise ValueError(f"width={width} not in [1, max_width={max_width}]")
+    if t_base < 0:
+        raise ValueError(f"t_base must be >= 0; got {t_base}")
+    start = t_base + max_width // 2 - width // 2
+    if start + width + n_out > int(cs.shape[axis]):
+        raise ValueError("Requested (t_base, n_out, width) window exceeds padded cumsum bounds")
+    c = torch.movedim(cs, axis, 0).contiguous()
+    _lib.require_cuda(c, "cs")
+    out = torch.empty((n_out,) + tuple(c.shape[1:]), dtype=torch.float32, device=c.device)
+    _lib.check(_lib.lib().dsb_boxcar_from_cs(_lib.ptr(c), c[0].numel(), width, start, n_out,
+                                             _lib.ptr(out), _lib.stream_of(c.device)),
+               "dsb_boxcar_from_cs")
+    out = torch.movedim(out, 0, axis)
+    return out if out_dtype is None else out.to(out_dtype)
+
+
+def multi_boxcar_argmax_triton(cs: torch.Tensor, *, widths: torch.Tensor, offsets: torch.Tensor,
+                               sigma_inv: torch.Tensor, n_out: int, t_base: int = 0,
+                               out_max_dtype: Optional[torch.dtype] = None
+                               ) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Fused multi-width boxcar max + winner (triton_boxcar.py:305).  Same
+    name and arguments as the reference (whose Triton kernel this replaces);
+    raises instead of returning ``None`` on unsupported inputs."""
+    if cs.dim() != 4 or cs.dtype != torch.float32:
+        raise ValueError("cs must be float32 [Tpad, F, H, W]")
+    _lib.require_cuda(cs, "cs")
+    K = int(widths.numel())
+    if K < 1 or K > 32 or offsets.numel() != K or sigma_inv.numel() != K:
+        raise ValueError("widths/offsets/sigma_inv must have the same length 1..32")
+    if widths.dtype != torch.int32 or offsets.dtype != torch.int32 or sigma_inv.dtype != torch.float32:
+        raise ValueError("widths/offsets int32, sigma_inv float32")
+    eff = out_max_dtype if out_max_dtype is not None else cs.dtype
+    if eff not in (torch.float16, torch.float32):
+        raise ValueError(f"out_max_dtype {eff} not supported")
+    inner = cs[0].numel()
+    out_max = torch.empty((n_out,) + tuple(cs.shape[1:]), dtype=eff, device=cs.device)
+    out_win = torch.empty((n_out,) + tuple(cs.shape[1:]), dtype=torch.int16, device=cs.device)
+    _lib.check(_lib.lib().dsb_multi_boxcar_argmax(
+        _lib.ptr(cs), inner, _lib.ptr(widths.contiguous()), _lib.ptr(offsets.contiguous()),
+        _lib.ptr(sigma_inv.contiguous()), K, int(n_out), int(t_base), _lib.ptr(out_max),
+        int(eff == torch.float16), _lib.ptr(out_win), _lib.stream_of(cs.device)),
+        "dsb_multi_boxcar_argmax")
+    return out_max, out_win
+
+
+@dataclass
+class Candidate:
+    """Detector output (common/contracts.py:256 subset used by the hot path)."""
+
+    l: float
+    m: float
+    dm_fine: float
+    dm_idx: int
+    event_specnum: int
+    width_samples: int
+    kernel_id: str
+    snr: float
+
+
+def _nms(items, *, threshold, n_top, shape, r_t, r_f, r_lm):
+    """items: (snr, flat_index, k) with snr > threshold; value-descending then
+    flat-index-ascending order, top n_top, greedy merge-radius suppression
+    (decoder.py:455-540)."""
+    T, F, H, W = shape
+    items = sorted(items, key=lambda x: (-x[0], x[1]))[:n_top]
+    acc, out = [], []
+    for v, ix, k in items:
+        if v <= threshold:
+            break
+        t = ix // (F * H * W)
+        rem = ix % (F * H * W)
+        f = rem // (H * W)
+        rem %= H * W
+        l_, m_ = rem // W, rem % W
+        if any(abs(t - a) <= r_t and abs(f - b) <= r_f and abs(l_ - c) <= r_lm and abs(m_ - d) <= r_lm
+               for a, b, c, d in acc):
+            continue
+        acc.append((t, f, l_, m_))
+        out.append((t, f, l_, m_, v, k))
+    return out
+
+
+def decode_topk_argmax_lowmem(score: torch.Tensor, winner_kernel_idx: torch.Tensor, *,
+                              threshold: float, kernel_ids: List[str],
+                              kernel_time_widths: List[int], merge_radius_lm: int,
+                              merge_radius_fdm: int, merge_radius_t: int,
+                              event_specnum: int = 0, fine_to_coarse=None, fine_dm_pc_cm3=None,
+                              n_top: int = 256, **_unused) -> List[Candidate]:
+    """Top-k + merge-radius decode (decoder.py:388).  Cells above threshold
+    are compacted on the device; ties order by flat index ascending."""
+    if score.dim() != 4:
+        raise ValueError(f"score.dim()={score.dim()}, expected 4 [T_det, N_fdm, H, W]")
+    if winner_kernel_idx.shape != score.shape:
+        raise ValueError("winner_kernel_idx.shape != score.shape")
+    if min(merge_radius_lm, merge_radius_fdm, merge_radius_t) < 0:
+        raise ValueError("merge radii must be >= 0")
+    if len(kernel_ids) != len(kernel_time_widths):
+        raise ValueError("kernel_ids and kernel_time_widths length mismatch")
+    if not kernel_ids:
+        return []
+    flat = score.reshape(-1)
+    sel = torch.nonzero(flat > threshold).reshape(-1)
+    if sel.numel() == 0:
+        return []
+    vals = flat[sel].float().cpu().numpy()
+    idx = sel.cpu().numpy()
+    ks = winner_kernel_idx.reshape(-1)[sel].cpu().numpy()
+    got = _nms([(float(v), int(i), int(k)) for v, i, k in zip(vals, idx, ks)], threshold=threshold,
+               n_top=n_top, shape=tuple(score.shape), r_t=merge_radius_t, r_f=merge_radius_fdm,
+               r_lm=merge_radius_lm)
+    f2c = None if fine_to_coarse is None else np.asarray(torch.as_tensor(fine_to_coarse).cpu())
+    fdm = None if fine_dm_pc_cm3 is None else np.asarray(torch.as_tensor(fine_dm_pc_cm3).cpu())
+    out = []
+    for t, f, l_, m_, v, k in got:
+        if k < 0 or k >= len(kernel_ids):
+            continue
+        out.append(Candidate(l=float(l_), m=float(m_),
+                             dm_fine=float(fdm[f]) if fdm is not None else float(f),
+                             dm_idx=int(f2c[f]) if f2c is not None else int(f),
+                             event_specnum=int(event_specnum) + int(t),
+                             width_samples=int(kernel_time_widths[k]), kernel_id=kernel_ids[k],
+                             snr=float(v)))
+    return out
+
+
+DET_CAND_DTYPE = np.dtype([("t", np.int32), ("pix", np.int32), ("snr", np.float32),
+                           ("k", np.int32)])
+
+
+class CandidateBuffer:
+    """Device buffer the fused detector appends above-threshold cells to."""
+
+    def __init__(self, device, capacity: int = 1 << 20):
+        self.device = device
+        self.capacity = int(capacity)
+        self.buf = torch.empty(self.capacity * 4, dtype=torch.int32, device=device)
+        self.count = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def reset(self):
+        self.count.zero_()
+
+    def fetch(self) -> np.ndarray:
+        n = int(self.count.item())
+        if n > self.capacity:
+            raise _lib.DsbError(f"detector candidate buffer overflow ({n} > {self.capacity})")
+        raw = self.buf[: 4 * n].cpu().numpy()
+        return raw.view(DET_CAND_DTYPE)
+
+
+def detect_cube(cube: torch.Tensor, *, log_max_width: int, sigma_inv: torch.Tensor,
+                t_base: int, n_out: int, threshold: float, cands: CandidateBuffer,
+                pix_offset: int = 0) -> None:
+    """Fused padded-cumsum boxcars (widths 1..2**log_max_width), max over
+    widths and threshold compaction on a ``[T, F, H, W]`` cube; candidate
+    ``pix`` is the flat ``(f, h, w)`` index plus ``pix_offset``."""
+    _lib.require_cuda(cube, "cube")
+    n = cube.shape[0]
+    inner = cube[0].numel()
+    _lib.check(_lib.lib().dsb_detect(_lib.ptr(cube), int(cube.dtype == torch.float16), n, inner,
+                                     int(log_max_width), _lib.ptr(sigma_inv), int(t_base),
+                                     int(n_out), float(threshold), _lib.ptr(cands.buf),
+                                     cands.capacity, int(pix_offset), _lib.ptr(cands.count),
+                                     _lib.stream_of(cube.device)), "dsb_detect")
+
+
+# ---------------------------------------------------------------------------
+# Layer-1 noise
+# ---------------------------------------------------------------------------
+
+
+def sigma_clipped_std_batched(samples: torch.Tensor, *, n_sigma: float = 3.0,
+                              n_iterations: int = 3) -> torch.Tensor:
+    """Row-wise sigma-clipped std, lower median (noise_norm/layer1.py:53)."""
+    if samples.dim() != 2:
+        raise ValueError(f"samples.dim()={samples.dim()}, expected 2 [B, M]")
+    B, M = samples.shape
+    _lib.require_cuda(samples, "samples")
+    if B == 0 or M == 0:
+        return torch.zeros((B,), dtype=torch.float32, device=samples.device)
+    s = samples.to(torch.float32).contiguous()
+    out = torch.empty(B, dtype=torch.float32, device=s.device)
+    _lib.check(_lib.lib().dsb_clipped_std(_lib.ptr(s), B, M, float(n_sigma), int(n_iterations),
+                                          _lib.ptr(out), _lib.stream_of(s.device)),
+               "dsb_clipped_std")
+    return out

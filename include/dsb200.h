@@ -81,6 +81,117 @@ int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int
                      long long t_base, long long t_mask, int max_ctas, int* status,
                      cudaStream_t stream);
 
+/* ---- a6: uv cells in FP64 -------------------------------------------------
+ * Replaces the (u, v) -> cell arithmetic of build_pattern / from_pattern
+ * (src/dsart/grid/sparsity_pattern.py:1090-1170, grid/kernel.py:344-374):
+ * col = rint(-(du/wl)/cell)+N/2, row = rint(-(dv/wl)/cell)+N/2,
+ * wl = c/(nu*1e9); outputs (n_bl, n_ch) int32 row-major. */
+int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_ghz, int n_ch,
+                 double cell_lambda, int n_grid, int* row, int* col, cudaStream_t stream);
+
+/* ---- a7: gridder ----------------------------------------------------------
+ * Replaces FastVisGridder.compute (src/dsart/grid/kernel.py:508-611), K=1:
+ * out[f, cell] = sum over CSR sources (flat bls*C + s) of vis[f, src]. */
+int dsb_grid_vis(const void* vis, int n_fv, long long nsrc, const int* cell_off,
+                 const int* cell_src, int n_filled, void* out, cudaStream_t stream);
+
+/* ---- a8: stage-1 shift + grid on visibilities ------------------------------
+ * Replaces Stage1MultiDMCoarseDM._dedisperse_one_window
+ * (src/dsart/services/corr_fast_integration.py:727-915) and the fused
+ * Triton dedisp kernel (src/dsart/services/triton_dedisp.py:104):
+ * out[d, t, cell] = sum_src vis_joined[t + shift[s, d], src], vis_joined =
+ * prev[0:n_prev] ++ cur along time (the F34 sliding window). */
+int dsb_dedisp_vis(const void* prev, const void* cur, int n_prev, long long nsrc, int ceff,
+                   const int* cell_off, const int* cell_src, const int* shifts, int n_dm,
+                   int n_filled, int t_dedisp, void* out, cudaStream_t stream);
+
+/* ---- a9: static-sky mean ----------------------------------------------------
+ * Replaces StaticSkyMean.apply (src/dsart/services/corr_fast_integration.py:1049-1240).
+ * ring: (n_cells, window) float64 complex block means. */
+int dsb_static_sky(const void* in, void* out, int n_t, int n_cells, void* ring, int window,
+                   int head, int count, int subtract, cudaStream_t stream);
+
+/* ---- a10: stage-2 aligned cube ----------------------------------------------
+ * Replaces the slice assembly of Stage2InterChgroupShiftFifo.push
+ * (src/dsart/coarse_dm/stage2_chgroup_alignment.py:264-338). hist[j] = device
+ * pointer of the cube pushed j ticks ago. */
+int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const int* rsmp,
+                    const int* warm, int n_dm, int t_len, long long inner, void* out,
+                    cudaStream_t stream);
+
+/* ---- a8-a10 pipeline form ---------------------------------------------------
+ * Stage 1 over per-subband gridded rows (dsb_corr_tc_grid output), static-sky
+ * subtraction fused, each output written at (t + shift2[g, d]) of the
+ * stage-2 ring D, i.e. stage 1 + StaticSkyMean + the stage-2 FIFO
+ * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264). */
+int dsb_stage1_rows(const void* Y, long long y_stride, long long y_mask, int n_cells,
+                    const int* cell_off, const int* src_row, const int* src_s, const int* cell_g,
+                    const int* cell_local, const int* shift1, const int* shift2,
+                    const int* d_base, const int* n_filled, void* D, long long d_stride,
+                    long long d_mask, long long t0, int n_t, int n_dm, int ceff, void* sky_ring,
+                    int sky_window, int sky_head, int sky_count, int sky_subtract,
+                    int max_src, cudaStream_t stream);
+
+/* ---- a12: fine-DM combine ---------------------------------------------------
+ * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
+ * the Hermitian half-spectrum fold and fftshift checkerboard of
+ * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
+ * reads the stage-2 rings directly, writes (n_f, n_t, N, N/2+1) complex64. */
+int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
+                     const int* e_g, const int* e_cell, const int* d_base, const int* n_filled,
+                     const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
+                     long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
+
+/* Reference-layout combine on dense cint8 streams [G, T, 2, N, N]: replaces
+ * fused_dequant_combine_per_fdm[_half] and the calibrated variants
+ * (src/dsart/image/fused_combine_cuda.py:1104, :1359; kernels :210-700).
+ * scales/off_* null -> integer path; out complex32 (out_f16) or complex64. */
+int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
+                      const float* off_re, const float* off_im, void* out, int out_f16, int half,
+                      int G, int t_stream, int t_det, int N, int t_lo, int fftshift,
+                      cudaStream_t stream);
+
+/* ---- a13/a14: edge mask x Layer-1 normalisation into the detector cube -----
+ * Replaces the mask multiply + cube write of GpuImager.process_cube
+ * (src/dsart/image/imager_gpu.py:604-650): cube[t, f0+f, p] = img[f, t, p] *
+ * mask[(f,) p]. */
+int dsb_mask_to_cube(const float* img, const float* mask, int mask_per_f, int n_f, int n_t,
+                     int npix, void* cube, int cube_f16, int cube_f_total, int cube_f0,
+                     cudaStream_t stream);
+
+/* ---- a15: boxcar detector ----------------------------------------------------
+ * precompute_padded_cumsum (src/dsart/detector/forward.py:250): float64
+ * running prefix rounded to float32, max_w//2 zero rows on the left,
+ * max_w-1-max_w//2 copies of the last prefix on the right. */
+int dsb_padded_cumsum(const void* x, int x_f16, int n, long long inner, int max_w, float* cs,
+                      cudaStream_t stream);
+
+/* multi_boxcar_argmax_triton (src/dsart/detector/triton_boxcar.py:305, kernel
+ * :193): snr_k = (cs[t+off_k+w_k] - cs[t+off_k]) * sigma_inv_k, strict '>'. */
+int dsb_multi_boxcar_argmax(const float* cs, long long inner, const int* widths,
+                            const int* offsets, const float* sigma_inv, int K, int n_out,
+                            int t_base, void* out_max, int out_f16, void* out_win,
+                            cudaStream_t stream);
+
+/* boxcar_from_padded_cumsum (src/dsart/detector/forward.py:339). */
+int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, int n_out,
+                       float* out, cudaStream_t stream);
+
+/* Fused streaming form of the three above plus the threshold test of
+ * decode_topk_argmax_lowmem (src/dsart/detector/decoder.py:388): widths
+ * 1..2^log_maxw, every output cell with max S/N > threshold appended to
+ * cands (struct {int t, pix; float snr; int k;}), *count incremented
+ * (entries past cap are counted, not written). */
+int dsb_detect(const void* cube, int cube_f16, int n, long long inner, int log_maxw,
+               const float* sigma_inv, int t_base, int n_out, float threshold, void* cands,
+               int cap, int pix_off, int* count, cudaStream_t stream);
+
+/* ---- a18: Layer-1 sigma-clipped std ---------------------------------------------
+ * sigma_clipped_std_batched (src/dsart/noise_norm/layer1.py:53): rows of at
+ * most 4096 samples; lower median; non-finite samples dropped. */
+int dsb_clipped_std(const float* samples, int rows, int m, float n_sigma, int n_iter, float* out,
+                    cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -754,3 +754,124 @@ def sigma_clipped_std_batched(samples: np.ndarray, n_sigma: float = 3.0,
             sig = np.float32(np.sqrt(np.float32(np.sum(d * d, dtype=np.float64)) / np.float32(cnt)))
         out[r] = 0.0 if np.isnan(sig) else sig
     return out
+
+
+# ---------------------------------------------------------------------------
+# End-to-end streaming pipeline (services/corr_fast_integration.py:2063 corr +
+# consume phases; services/cube_pipeline.py:2682 search cube), in the
+# stream-time form the CUDA pipeline implements: time = absolute fast-vis tile.
+# ---------------------------------------------------------------------------
+
+
+def pipeline_tables(band: Band, antpos_e, antpos_n, *, nant, csf, n_grid, coarse_dm, fine_dm,
+                    fine_to_coarse, t_int):
+    G = band.n_chgroup
+    cell = top_of_band_cell_lambda(antpos_e, antpos_n, band, n_grid)
+    pats, cims = [], []
+    for g in range(G):
+        r, c = build_pattern(antpos_e, antpos_n, band, g, n_grid=n_grid, csf=csf, cell_lambda=cell)
+        pats.append((r, c))
+        cims.append(cell_index_map(antpos_e, antpos_n, band, g, n_grid=n_grid, csf=csf,
+                                   cell_lambda=cell, ix_row_pat=r, ix_col_pat=c))
+    t_int_us = t_int * NATIVE_SAMPLE_US
+    sh1 = stage1_bin_shifts(band, coarse_dm, csf, t_int_us)                 # (G, C, K)
+    sh2 = np.stack([stage2_shifts(band, g, coarse_dm, t_int_us) for g in range(G)])
+    sf = time_shift_search(band, coarse_dm, fine_dm, fine_to_coarse, t_int_us, True)
+    return dict(cell=cell, pats=pats, cims=cims, sh1=sh1, sh2=sh2, sf=sf)
+
+
+def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block, t_int, csf,
+                 n_grid, coarse_dm, fine_dm, fine_to_coarse, log_max_width, threshold, chunk,
+                 use_sky=True, sky_window=8, sky_warmup=8, n_top=256, r_t=4, r_f=5, r_lm=3,
+                 l1_times=16, l1_pixels=256, keep=None):
+    """Oracle of the CUDA streaming pipeline; returns candidate tuples
+    ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates."""
+    keep = {} if keep is None else keep
+    G = band.n_chgroup
+    tb = pipeline_tables(band, antpos_e, antpos_n, nant=nant, csf=csf, n_grid=n_grid,
+                         coarse_dm=coarse_dm, fine_dm=fine_dm, fine_to_coarse=fine_to_coarse,
+                         t_int=t_int)
+    n_coarse = len(coarse_dm)
+    n_fine = len(fine_dm)
+    N = n_grid
+    # correlate every block -> integer vis stream per chgroup (T, nbase, C)
+    vis = [[] for _ in range(G)]
+    for blk in raw_blocks:
+        for g in range(G):
+            vr, vi = corr_fast_from_raw(blk[g].reshape(-1), npkt=npkt_block, nant=nant,
+                                        nchan=band.nchan, t_int=t_int, csf=csf)
+            vis[g].append(vr + 1j * vi)
+    vis = [np.concatenate(v, axis=0) for v in vis]
+    T_total = vis[0].shape[0]
+    max_sh1 = int(tb["sh1"].max())
+    depth1 = -(-max_sh1 // chunk)
+    n_chunks = T_total // chunk
+    n_s1 = n_chunks - depth1                       # stage-1 chunks emitted
+    sky = StaticSkyMean(sky_window, sky_warmup, n_dm=G * n_coarse) if use_sky else None
+    # stage-1 output streams D1[g][d] (T1, n_filled)
+    D1 = [[np.zeros((max(0, n_s1) * chunk, tb["pats"][g][0].size), np.complex128)
+           for _ in range(n_coarse)] for g in range(G)]
+    for j in range(max(0, n_s1)):
+        for g in range(G):
+            r, _ = tb["pats"][g]
+            win = vis[g][j * chunk: (j + 1) * chunk + max_sh1]
+            pad = (j + 1) * chunk + max_sh1 - j * chunk - win.shape[0]
+            if pad > 0:
+                win = np.concatenate([win, np.zeros((pad,) + win.shape[1:], win.dtype)])
+            o_re = stage1_dedisp(np.rint(win.real).astype(np.int64), tb["sh1"][g],
+                                 tb["cims"][g], r.size, chunk)
+            o_im = stage1_dedisp(np.rint(win.imag).astype(np.int64), tb["sh1"][g],
+                                 tb["cims"][g], r.size, chunk)
+            for d in range(n_coarse):
+                x = (o_re[d] + 1j * o_im[d]).astype(np.complex64)
+                if sky is not None:
+                    x = sky.apply(x, dm_slot=g * n_coarse + d)
+                D1[g][d][j * chunk:(j + 1) * chunk] = x
+    keep["D1"] = D1
+    # search cubes
+    L = max(0, -int(tb["sf"].min()))
+    a = -(-L // chunk)
+    te = (1 << log_max_width) // 2
+    widths = [1 << k for k in range(log_max_width + 1)]
+    sinv = (np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32)
+    offs = boxcar_offsets(widths, 1 << log_max_width)
+    mask = edge_mask(N, kernel_support=1)
+    act = np.nonzero(mask.reshape(-1) != 0)[0]
+    l1_pix = act[np.linspace(0, act.size - 1, l1_pixels).astype(np.int64)]
+    l1_t = te + np.linspace(0, chunk - 1, l1_times).astype(np.int64)
+    T1 = max(0, n_s1) * chunk
+    cands = []
+    images = []
+    # first cube whose every time has data from every chgroup (warm-up)
+    jc_first = -(-(int(tb["sh2"].max()) + max(0, int(tb["sf"].max())) + 2 * te) // chunk)
+    for jc in range(jc_first, max(0, n_s1 - a)):
+        t0 = jc * chunk - 2 * te
+        nt = chunk + 2 * te
+        cube = np.zeros((nt, n_fine, N, N), np.float32)
+        for f in range(n_fine):
+            c = int(fine_to_coarse[f])
+            streams = np.zeros((G, nt, N, N), np.complex128)
+            for g in range(G):
+                r, cc = tb["pats"][g]
+                for t in range(nt):
+                    ts = t0 + t - int(tb["sf"][f, g]) - int(tb["sh2"][g, c])
+                    if 0 <= ts < T1:
+                        streams[g, t, r.astype(np.int64), cc.astype(np.int64)] = D1[g][c][ts]
+            half = combine_half(streams, np.zeros(G, np.int64), nt, 0, fftshift=True)
+            img = image_from_half(half, N)                            # float64 (nt, N, N)
+            img32 = img.astype(np.float32)
+            samp = img32.reshape(nt, N * N)[l1_t][:, l1_pix].reshape(1, -1)
+            sig = sigma_clipped_std_batched(samp)[0]
+            sig = np.float32(sig if sig > 0 else 1.0)
+            mf = (mask / sig).astype(np.float32)
+            cube[:, f] = (img32 * mf[None]).astype(np.float32)
+            images.append(img)
+        cs = padded_cumsum(cube, 1 << log_max_width)
+        score, win = multi_boxcar_argmax(cs, widths, offs, sinv, chunk, te)
+        for cd in decode_topk(score, win, threshold=threshold, n_top=n_top, r_t=r_t, r_f=r_f,
+                              r_lm=r_lm):
+            cands.append((jc * chunk - te + cd.t, cd.f, cd.l, cd.m, cd.snr, widths[cd.k]))
+        keep.setdefault("cubes", []).append(cube)
+    keep["images"] = images
+    keep["tables"] = tb
+    return cands

@@ -1,0 +1,242 @@
+"""GPU parity of the drop-in API kernels against the reference's golden
+fixtures (tests/golden) and the CPU oracle.  Integer/index work is
+compared bit-exactly; float32 arithmetic with the tolerance stated per test."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+import dsb_oracle as O
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import make_golden as MG  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _z(golden_dir, name):
+    return np.load(os.path.join(golden_dir, name), allow_pickle=False)
+
+
+def test_pattern_cellmap_gridder_vs_reference(dev, golden_dir):
+    from dsb200.grid import FastVisGridder, build_pattern, compute_top_of_band_cell_lambda
+    z = _z(golden_dir, "grid_plan.npz")
+    e, n = z["antpos_e"], z["antpos_n"]
+    cell = compute_top_of_band_cell_lambda(e, n, n_grid=int(z["n_grid"]))
+    assert cell == float(z["cell_lambda"])
+    for g in (0, 15):
+        pat = build_pattern(e, n, chgroup=g, n_grid=int(z["n_grid"]),
+                            chan_sum_factor=int(z["csf"]), cell_lambda=cell, device=dev)
+        np.testing.assert_array_equal(pat.ix_row, z[f"ix_row_{g}"])
+        np.testing.assert_array_equal(pat.ix_col, z[f"ix_col_{g}"])
+        grd = FastVisGridder.from_pattern(pat, e, n, device=dev)
+        np.testing.assert_array_equal(grd.cell_index_map.numpy().reshape(4656, -1),
+                                      z[f"cim_{g}"].astype(np.int64))
+        np.testing.assert_array_equal(grd.cell_weights.cpu().numpy(), z[f"cellw_{g}"])
+        if g == 15:
+            vis = MG.stage1_vis(2, 4656, 48, seed=int(z["grid_in_seed"]))
+            out = grd.compute(torch.from_numpy(vis).to(dev)).cpu().numpy()
+            np.testing.assert_array_equal(out, z["grid_out"])
+
+
+def test_stage1_sliding_window_vs_reference(dev, golden_dir):
+    from dsb200.dedisp import DMPlan, Stage1MultiDMCoarseDM
+    from dsb200.grid import FastVisGridder, build_pattern, compute_top_of_band_cell_lambda
+    z = _z(golden_dir, "stage1.npz")
+    e, n = MG.t_layout_antpos(96, seed=11)
+    g, csf = int(z["chgroup"]), int(z["csf"])
+    cell = compute_top_of_band_cell_lambda(e, n, n_grid=int(z["n_grid"]))
+    pat = build_pattern(e, n, chgroup=g, n_grid=int(z["n_grid"]), chan_sum_factor=csf,
+                        cell_lambda=cell, device=dev)
+    grd = FastVisGridder.from_pattern(pat, e, n, device=dev)
+    plan = DMPlan(dm_pc_cc=np.linspace(0.0, float(z["dm_max"]), int(z["n_coarse"])),
+                  t_int_fast_us=8 * 32.768, chan_sum_factor=csf)
+    np.testing.assert_array_equal(plan.delay_bins_per_chgroup(g), z["bins"])
+    st = Stage1MultiDMCoarseDM(plan=plan, gridder=grd, chgroup=g, sliding_window=True)
+    for blk in range(3):
+        vis = MG.stage1_vis(int(z["n_fv"]), 4656, 48, seed=int(z["seed"]) + blk)
+        o = st.dedisperse_from_vis(torch.from_numpy(vis).to(dev), block_n=blk).cpu().numpy()
+        assert o.shape == tuple(z[f"b{blk}_shape"])
+        re, im = o.real.astype(np.int64), o.imag.astype(np.int64)
+        np.testing.assert_array_equal(re.sum(axis=1), z[f"b{blk}_sum_t_re"])
+        np.testing.assert_array_equal(im.sum(axis=1), z[f"b{blk}_sum_t_im"])
+        np.testing.assert_array_equal(re.sum(axis=2), z[f"b{blk}_sum_c_re"])
+        np.testing.assert_array_equal(im.sum(axis=2), z[f"b{blk}_sum_c_im"])
+        idx = z[f"b{blk}_idx"]
+        np.testing.assert_array_equal(o.real.reshape(-1)[idx], z[f"b{blk}_re_s"])
+        np.testing.assert_array_equal(o.imag.reshape(-1)[idx], z[f"b{blk}_im_s"])
+    st2 = Stage1MultiDMCoarseDM(plan=plan, gridder=grd, chgroup=g, sliding_window=False)
+    vis = MG.stage1_vis(int(z["n_fv"]), 4656, 48, seed=int(z["seed"]) + 9)
+    o = st2.dedisperse_from_vis(torch.from_numpy(vis).to(dev), block_n=0).cpu().numpy()
+    assert o.shape == tuple(z["ns_shape"])
+    np.testing.assert_array_equal(o.real.astype(np.int64).sum(axis=1), z["ns_sum_t_re"])
+    np.testing.assert_array_equal(o.imag.astype(np.int64).sum(axis=2), z["ns_sum_c_im"])
+
+
+def test_static_sky_vs_oracle_and_reference(dev, golden_dir):
+    from dsb200.dedisp import StaticSkyMean
+    z = _z(golden_dir, "fifo_sky.npz")
+    sky = StaticSkyMean(window_blocks=3, warmup_cubes=2, n_dm=2)
+    osky = O.StaticSkyMean(window_blocks=3, warmup_cubes=2, n_dm=2)
+    for i, (x, ref) in enumerate(zip(z["sky_in"], z["sky_out"])):
+        got = sky.apply(torch.from_numpy(x).to(dev), dm_slot=i % 2).cpu().numpy()
+        np.testing.assert_array_equal(got, osky.apply(x, dm_slot=i % 2))   # same definition
+        np.testing.assert_allclose(got, ref, rtol=0, atol=2e-6 * max(1.0, np.abs(ref).max()))
+
+
+def test_stage2_fifos_vs_reference(dev, golden_dir):
+    from dsb200.dedisp import (PerCoarseDmStage2FIFO, Stage2FIFO, Stage2InterChgroupShiftFifo,
+                               compute_stage2_shifts)
+    z = _z(golden_dir, "fifo_sky.npz")
+    cd = np.asarray([0.0, 300.0, 900.0, 1600.0, 2500.0])
+    tab = compute_stage2_shifts(chgroup=2, coarse_dm_pc_cm3=cd, t_int_corr_us=262.144 * 32)
+    np.testing.assert_array_equal(tab.shifts_samples, z["ics_shifts"])
+    f = Stage2InterChgroupShiftFifo(chgroup=2, coarse_dm_pc_cm3=cd, t_dedisp=16, shift_table=tab)
+    for i, (x, ref, n) in enumerate(zip(z["ics_in"], z["ics_out"], z["ics_emitted"])):
+        r = f.push(torch.from_numpy(x).to(dev), block_n=i)
+        assert len(r) == int(n)
+        if r:
+            np.testing.assert_array_equal(r[0].cpu().numpy(), ref)
+    pf = PerCoarseDmStage2FIFO([0, 1, 3])
+    seq = []
+    for i in range(6):
+        for c in range(3):
+            r = pf.push(c, torch.full((2,), float(10 * i + c), device=dev))
+            seq.append(-1 if r is None else int(r[0].item()))
+    np.testing.assert_array_equal(np.asarray(seq), z["pdf_seq"])
+    q = Stage2FIFO(depth=2)
+    a, b, c = (torch.zeros(3, device=dev) + k for k in range(3))
+    assert q.push(a) is None and q.push(b) is None and q.push(c) is a
+    with pytest.raises(ValueError):
+        q.push(torch.zeros(4, device=dev))
+
+
+@pytest.mark.parametrize("half", [False, True])
+@pytest.mark.parametrize("calib", [False, True])
+def test_dense_combine_vs_oracle(dev, half, calib):
+    from dsb200.search import fused_dequant_combine_per_fdm, fused_dequant_combine_per_fdm_half
+    rng = np.random.default_rng(4)
+    G, T, N, t_det, t_lo = 5, 12, 16, 10, 3
+    streams = rng.integers(-100, 100, (G, T, 2, N, N)).astype(np.int8)
+    shifts = rng.integers(-3, 4, G).astype(np.int32)
+    nw = N // 2 + 1 if half else N
+    out = torch.zeros((t_det - t_lo, N, nw), dtype=torch.complex64, device=dev)
+    kw = {}
+    if calib:
+        kw = dict(scales=torch.ones(G, device=dev), offsets_re=torch.zeros(G, device=dev),
+                  offsets_im=torch.zeros(G, device=dev))
+    fn = fused_dequant_combine_per_fdm_half if half else fused_dequant_combine_per_fdm
+    fn(torch.from_numpy(streams).to(dev), torch.from_numpy(shifts).to(dev), out, t_lo=t_lo,
+       fftshift=True, **kw)
+    cplx = streams[:, :, 0].astype(np.float64) + 1j * streams[:, :, 1].astype(np.float64)
+    want = (O.combine_half if half else O.combine_full)(cplx, shifts, t_det, t_lo, fftshift=True)
+    np.testing.assert_array_equal(out.cpu().numpy(), want.astype(np.complex64))
+
+
+def test_edge_mask_and_image_vs_reference(dev, golden_dir):
+    from dsb200.search import compute_edge_mask, irfft2_image
+    z = _z(golden_dir, "image_detector.npz")
+    np.testing.assert_array_equal(compute_edge_mask(n_grid=32), z["img_mask"])
+    # half-spectrum identity on the device, vs the reference's dirty image
+    uv = z["img_uv"].astype(np.complex128)
+    N = uv.shape[-1]
+    u = np.arange(N)
+    shifted = uv * (1 - 2 * ((u[:, None] + u[None, :]) & 1))   # fftshift folded into the grid
+    um = (N - u) % N
+    half = 0.5 * (shifted + np.conj(shifted[:, um][:, :, um]))
+    half = half[:, :, : N // 2 + 1]
+    img = irfft2_image(torch.from_numpy(half.astype(np.complex64)).to(dev), N).cpu().numpy()
+    ref = z["img_out"]
+    assert np.abs(img - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_cumsum_boxcars_argmax_vs_reference(dev, golden_dir):
+    from dsb200.search import (boxcar_from_padded_cumsum, multi_boxcar_argmax_triton,
+                               precompute_padded_cumsum)
+    z = _z(golden_dir, "image_detector.npz")
+    cube = torch.from_numpy(z["bc_cube"]).to(dev)
+    cs = precompute_padded_cumsum(cube, axis=0, max_width=16)
+    np.testing.assert_array_equal(cs.cpu().numpy(), z["bc_cs"])
+    widths = [1, 2, 4, 8, 16]
+    for k, w in enumerate(widths):
+        bx = boxcar_from_padded_cumsum(cs, axis=0, width=w, max_width=16, n_out=24, t_base=8)
+        np.testing.assert_array_equal(bx.cpu().numpy(), z["bc_box"][k])
+    sinv = np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))
+    offs = O.boxcar_offsets(widths, 16)
+    mx, win = multi_boxcar_argmax_triton(
+        cs, widths=torch.tensor(widths, dtype=torch.int32, device=dev),
+        offsets=torch.tensor(offs, dtype=torch.int32, device=dev),
+        sigma_inv=torch.from_numpy(sinv).to(dev), n_out=24, t_base=8)
+    omx, owin = O.multi_boxcar_argmax(z["bc_cs"], widths, offs, sinv, 24, 8)
+    np.testing.assert_array_equal(mx.cpu().numpy(), omx)
+    np.testing.assert_array_equal(win.cpu().numpy(), owin)
+
+
+@pytest.mark.parametrize("log_w", [2, 4])
+@pytest.mark.parametrize("f16", [False, True])
+def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16):
+    from dsb200.search import CandidateBuffer, detect_cube
+    rng = np.random.default_rng(10 + log_w)
+    T, F, H, W = 70, 3, 12, 10
+    x = rng.normal(size=(T, F, H, W)).astype(np.float16 if f16 else np.float32)
+    x[30:34, 1, 5, 5] += 6.0
+    widths = [1 << k for k in range(log_w + 1)]
+    maxw = widths[-1]
+    t_base, n_out = maxw // 2, T - 2 * (maxw // 2)
+    sinv = (np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32)
+    buf = CandidateBuffer(dev, 1 << 16)
+    detect_cube(torch.from_numpy(x).to(dev), log_max_width=log_w,
+                sigma_inv=torch.from_numpy(sinv).to(dev), t_base=t_base, n_out=n_out,
+                threshold=2.5, cands=buf)
+    got = buf.fetch()
+    cs = O.padded_cumsum(x.astype(np.float32), maxw)
+    mx, win = O.multi_boxcar_argmax(cs, widths, O.boxcar_offsets(widths, maxw), sinv, n_out, t_base)
+    sel = np.nonzero(mx.reshape(-1) > 2.5)[0]
+    inner = F * H * W
+    want = sorted((int(i // inner), int(i % inner), float(mx.reshape(-1)[i]), int(win.reshape(-1)[i]))
+                  for i in sel)
+    have = sorted((int(c["t"]), int(c["pix"]), float(c["snr"]), int(c["k"])) for c in got)
+    assert have == want
+
+
+def test_decode_vs_reference(dev, golden_dir):
+    from dsb200.search import decode_topk_argmax_lowmem
+    z = _z(golden_dir, "image_detector.npz")
+    widths = [1, 2, 4, 8, 16]
+    c = decode_topk_argmax_lowmem(torch.from_numpy(z["dec_score"]).to(dev),
+                                  torch.from_numpy(z["dec_winner"]).to(dev), threshold=3.5,
+                                  kernel_ids=[f"unit_d1_b{w}" for w in widths],
+                                  kernel_time_widths=widths, merge_radius_lm=3,
+                                  merge_radius_fdm=5, merge_radius_t=4, n_top=64)
+    got = np.asarray([[x.event_specnum, x.dm_idx, x.l, x.m, x.width_samples, x.snr] for x in c])
+    np.testing.assert_array_equal(got, z["dec_out"])
+
+
+def test_layer1_vs_reference(dev, golden_dir):
+    from dsb200.search import sigma_clipped_std_batched
+    z = _z(golden_dir, "image_detector.npz")
+    got = sigma_clipped_std_batched(torch.from_numpy(z["l1_in"]).to(dev)).cpu().numpy()
+    np.testing.assert_allclose(got, z["l1_out"], rtol=2e-6)
+    np.testing.assert_allclose(got, O.sigma_clipped_std_batched(z["l1_in"]), rtol=2e-6)
+
+
+def test_uv_cells_fp64_gpu_equals_numpy(dev):
+    from dsb200.grid import per_baseline_uv_meters, uv_cells_gpu
+    e, n = MG.t_layout_antpos(96, seed=3)
+    du, dv, _ = per_baseline_uv_meters(e, n)
+    nu = np.linspace(1.31, 1.5, 48)
+    cell = 7.3
+    r, c = uv_cells_gpu(du, dv, nu, cell, 256, dev)
+    wl = 299792458.0 / (nu * 1e9)
+    np.testing.assert_array_equal(c, np.rint(-(du[:, None] / wl[None, :]) / cell).astype(np.int64) + 128)
+    np.testing.assert_array_equal(r, np.rint(-(dv[:, None] / wl[None, :]) / cell).astype(np.int64) + 128)
