@@ -1,0 +1,362 @@
+"""Benchmark: real-time factor of the one-GPU fast search path.
+
+A step is one voltage block (16 chgroup pages of 8192 packets x 96
+antennas x 384 channels, 0.537 data-seconds) pushed through the streaming
+pipeline: unpack + tensor-core correlator + per-subband gridding, stage-1
+coarse dedispersion + static sky + stage-2 ring, and for every detector cube
+the fine-DM combine, 2-D FFT imaging, Layer-1 noise, edge mask and the
+boxcar detector.  ``value`` = data-seconds processed per wall-second (all
+ranks), inputs resident in HBM; ``e2e`` is the same through the public API
+from pinned host buffers (H2D inside the timed region).
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(the oracle) on the host cores on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "dsa110-rt_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "real-time factor at 96-ant/6144-ch (data-seconds per second)"
+
+
+def workload_config(name: str):
+    from dsb200.constants import DSA110_BAND
+    from dsb200.pipeline import PipelineConfig
+    if name == "dsa110-full":
+        return PipelineConfig(nant=96, band=DSA110_BAND, npkt_block=8192, t_int=8, csf=16,
+                              n_grid=256, coarse_dm=np.linspace(0.0, 2000.0, 32),
+                              fine_per_coarse=16, log_max_width=4, threshold=7.0,
+                              chunk_tiles=512, fdm_batch=8)
+    if name == "small":
+        from dsb200.constants import Band
+        return PipelineConfig(nant=96, band=Band(n_chgroup=4), npkt_block=1024, t_int=8, csf=16,
+                              n_grid=256, coarse_dm=np.linspace(0.0, 500.0, 8),
+                              fine_per_coarse=4, log_max_width=4, threshold=7.0,
+                              chunk_tiles=256, fdm_batch=8)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_desc(name, cfg):
+    return {"workload": f"{name}: {cfg.nant} ant, {cfg.band.n_chgroup}x{cfg.band.nchan} ch "
+                        f"(csf {cfg.csf} -> {cfg.band.n_chgroup * cfg.ceff} subbands), "
+                        f"{cfg.npkt_block * 2}-sample blocks, t_int {cfg.t_int}, "
+                        f"{cfg.n_grid}^2 grid, {cfg.fine_dm.size} DMs "
+                        f"({cfg.coarse_dm.size} coarse x {cfg.fine_per_coarse} fine) "
+                        f"0-{cfg.coarse_dm.max():.0f}, boxcars 1..{1 << cfg.log_max_width}",
+            "block_seconds": cfg.block_seconds, "l2": "inputs larger than L2 (19 GB/block)",
+            "chunk_tiles": cfg.chunk_tiles, "fdm_batch": cfg.fdm_batch}
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}",
+                                          f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1].split()[0]))
+                smax = float(p[2].split()[0])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        busy = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": float(np.median(busy)) if busy else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work per launch (for the roofline of the dominant kernel)
+# ---------------------------------------------------------------------------
+
+
+def stage_work(pipe):
+    cfg, T = pipe.cfg, pipe.tab
+    C, N = cfg.chunk_tiles, cfg.n_grid
+    nt = C + 2 * cfg.t_edge
+    nb = cfg.fdm_batch
+    nbase = cfg.nant * (cfg.nant + 1) // 2
+    nchan = cfg.band.n_chgroup * cfg.band.nchan
+    half = N * (N // 2 + 1)
+    coarse_per_batch = max(1, nb // cfg.fine_per_coarse) if cfg.fine_per_coarse else nb
+    return {
+        # tensor-core flops: 16 flops per (baseline, channel, native sample) (XX+YY complex MAC)
+        "corr": ("tensor", 16.0 * nbase * nchan * C * cfg.t_int,
+                 cfg.band.n_chgroup * C * cfg.t_int // 2 * cfg.nant * cfg.band.nchan * 4
+                 + T.n_rows_y * C * 8),
+        "stage1": ("hbm", None, T.n_rows_y * C * 8 + T.n_rows_d * C * 8),
+        # fused combine + FFT: stage-2 ring slices of the batch's coarse DM(s)
+        # read once, float32 images written once
+        "image": ("hbm", None, int(T.n_filled.sum()) * coarse_per_batch * nt * 8
+                  + nb * nt * N * N * 4),
+        "detect": ("hbm", None, nb * nt * N * N * 4),
+        "layer1": ("hbm", None, nb * cfg.l1_times * cfg.l1_pixels * 4),
+    }
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (restatement of the reference algorithm) on a
+# bounded sample, extrapolated per data-second stage by stage
+# ---------------------------------------------------------------------------
+
+
+def cpu_baseline(cfg, threads: int, budget_s: float = 20.0):
+    import dsb_oracle as O
+    try:
+        import threadpoolctl
+        limiter = threadpoolctl.threadpool_limits(threads)
+    except Exception:  # noqa: BLE001
+        limiter = None
+    rng = np.random.default_rng(0)
+    G, C = cfg.band.n_chgroup, cfg.band.nchan
+    tiles_per_s = 1e6 / cfg.t_int_us
+    out = {}
+    # correlator: one chgroup page, 8 tiles
+    npkt = 8 * cfg.t_int // 2
+    raw = rng.integers(0, 256, npkt * cfg.nant * C * 4, dtype=np.uint8)
+    t0 = time.perf_counter()
+    vr, vi = O.corr_fast_from_raw(raw, npkt=npkt, nant=cfg.nant, nchan=C, t_int=cfg.t_int,
+                                  csf=cfg.csf)
+    out["corr"] = (time.perf_counter() - t0) * G * tiles_per_s / 8
+    # stage 1: one chgroup, one coarse DM, 64 tiles
+    nbase = cfg.nant * (cfg.nant + 1) // 2
+    ceff = C // cfg.csf
+    n_filled = 2000
+    cim = rng.integers(0, n_filled + 1, (nbase, ceff))
+    vis = rng.integers(-50, 51, (64 + 32, nbase, ceff))
+    sh = rng.integers(0, 32, (ceff, 1))
+    t0 = time.perf_counter()
+    O.stage1_dedisp(vis, sh, cim, n_filled, 64)
+    out["stage1"] = (time.perf_counter() - t0) * 2 * G * cfg.coarse_dm.size * tiles_per_s / 64
+    # search: one fine DM x 32 images: combine + FFT + boxcar detector
+    N = cfg.n_grid
+    streams = (rng.normal(size=(G, 32, N, N)) + 1j * rng.normal(size=(G, 32, N, N)))
+    t0 = time.perf_counter()
+    half = O.combine_half(streams, np.zeros(G, np.int64), 32, 0)
+    img = O.image_from_half(half, N).astype(np.float32)
+    mw = 1 << cfg.log_max_width
+    cs = O.padded_cumsum(img[:, None], mw)
+    widths = [1 << k for k in range(cfg.log_max_width + 1)]
+    O.multi_boxcar_argmax(cs, widths, O.boxcar_offsets(widths, mw),
+                          np.ones(len(widths), np.float32), 32 - mw, mw // 2)
+    out["search"] = (time.perf_counter() - t0) * cfg.fine_dm.size * tiles_per_s / 32
+    if limiter is not None:
+        limiter.unregister() if hasattr(limiter, "unregister") else None
+    sec_per_data_s = sum(out.values())
+    return {"value": 1.0 / sec_per_data_s, "unit": "data-seconds/s", "cores": threads,
+            "kind": "port",
+            "sample": ("oracle (numpy restatement of the reference algorithm): correlator on one "
+                       "chgroup page x 8 tiles, stage 1 on one chgroup x one coarse DM x 64 tiles, "
+                       "combine+FFT+boxcars for one fine DM x 32 images; each stage's CPU seconds "
+                       "scaled to one data-second of the full workload and summed"),
+            "cpu_seconds_per_data_second": {k: round(v, 3) for k, v in out.items()}}
+
+
+# ---------------------------------------------------------------------------
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dsa110-full")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--stage-times", action="store_true", help="print per-stage device times")
+    a = ap.parse_args()
+    a.warmup = max(3, a.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = workload_config(a.workload)
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        res = [cpu_baseline(cfg, threads) for _ in range(max(1, a.steps))]
+        v = float(np.median([r["value"] for r in res]))
+        cb = dict(res[0])
+        cb["value"] = v
+        line = {"metric": METRIC, "value": v, "unit": "data-seconds/s", "n_gpus": a.gpus,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": cfg.block_seconds / v * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": workload_desc(a.workload, cfg), "impl": "reference",
+                "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": "data-seconds/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import torch.distributed as dist
+    from dsb200 import synth
+    from dsb200.pipeline import SearchPipeline
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    e, n = synth.t_layout(cfg.nant, seed=11)
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    pipe.skip_warmup()
+    blocks = [synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=cfg.npkt_block,
+                                        device=dev, seed=1000 * rank + i) for i in range(2)]
+    block_bytes = blocks[0].numel()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def run(k, host=None, staging=None, timing=False):
+        pipe.timing = timing
+        for i in range(k):
+            if host is not None:
+                staging.copy_(host[i % len(host)], non_blocking=True)
+                pipe.process_block(staging)
+            else:
+                pipe.process_block(blocks[i % 2])
+        pipe.timing = False
+
+    # warm-up
+    run(a.warmup)
+    torch.cuda.synchronize()
+    pipe.events = {}
+    launches0 = pipe.launches
+    clocks = Clocks(torch.cuda.current_device())
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    run(a.steps, timing=True)
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = (pipe.launches - launches0) // max(1, a.steps)
+    stages = pipe.stage_times_ms()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / a.steps
+    value = world * cfg.block_seconds * a.steps / (ms / 1e3)
+
+    # e2e: pinned host buffers through the public API (H2D inside the timed region)
+    e2e = None
+    if not a.no_e2e:
+        host = [torch.empty(blocks[0].shape, dtype=torch.uint8, pin_memory=True)]
+        host[0].copy_(blocks[0])
+        staging = torch.empty_like(blocks[0])
+        run(1, host, staging)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ev0.record()
+        run(a.steps, host, staging)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms_e = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms_e], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e = float(t.item())
+        e2e = {"value": world * cfg.block_seconds * a.steps / (ms_e / 1e3),
+               "unit": "data-seconds/s", "h2d_bytes_per_step": int(block_bytes),
+               "d2h_bytes_per_step": int(pipe.last_d2h_bytes), "wall_s": time.perf_counter() - t0}
+        del host, staging
+
+    # roofline of the dominant kernel
+    hbm, bf16, peak_src = load_peaks()
+    work = stage_work(pipe)
+    dom = max(stages, key=lambda k: stages[k]["total_ms"])
+    kind, flops, nbytes = work[dom]
+    mean_s = stages[dom]["mean_ms"] / 1e3
+    if kind == "tensor":
+        achieved = flops / mean_s / 1e12
+        peak = 2.0 * bf16
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None, "kernel": dom,
+                "peak_note": f"int8 dense = 2 x {peak_src} bf16"}
+    else:
+        achieved = nbytes / mean_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "kernel": dom,
+                "peak_note": f"{peak_src} copy bandwidth"}
+    roof["algorithmic_bytes_per_launch"] = nbytes
+    roof["mean_launch_ms"] = stages[dom]["mean_ms"]
+
+    if rank == 0:
+        cb = None
+        if not a.no_cpu:
+            cb = cpu_baseline(cfg, threads=os.cpu_count() or 1)
+        line = {"metric": METRIC, "value": value, "unit": "data-seconds/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int8 (correlator) / f32", "data": "synthetic (seeded 4-bit Gaussian "
+                "voltages, sigma 3, T-layout antennas)", "config": workload_desc(a.workload, cfg),
+                "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+                "cpu_baseline": cb,
+                "stages_ms_per_step": {k: round(v["total_ms"] / a.steps, 3)
+                                       for k, v in stages.items()}}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(GEN_THREADS) corr_generic_kernel(
 // ===========================================================================
 // tensor-core correlator (tcgen05, kind::i8)
 // ===========================================================================
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;
 constexpr int TC_TMEM_COLS = 512;   // two accumulators of <= 256 columns
 constexpr int TC_SMEM_BUDGET = 200 * 1024;
 // Every CTA requests more than half an SM's shared memory so that exactly
@@ -192,10 +192,10 @@ struct TcArgs {
   float2* out;
   long long o_g, o_f, o_b, o_s;
   // mode 1
-  const int* ycell;   // (n_chgroup*ceff, nbase) local row or -1
   const int* yoff;    // (n_chgroup*ceff) first global row of the group
   const int* ycnt;    // (n_chgroup*ceff) rows in the group
-  int ymax;           // max rows over groups (shared accumulator size)
+  const int* row_off; // (n_rows + 1) CSR over rows: baselines gridded into each row
+  const int* row_bls; // baseline index of each CSR entry
   float2* yout;
   long long y_t_stride;
   long long t_base;
@@ -263,26 +263,20 @@ DSB_DEV void tc_fill(const TcArgs& A, uint8_t* st, int g, int f, int s, int q) {
 
 // Read accumulator `buf` (rows b < nant; columns a: Re, nant + a: Im) and
 // emit the upper triangle b <= a at bls(a, b) (conj(E_b) E_a).
+// Warp w reads TMEM lane quarter (w & 3) (rows 32*(w&3) ...) and every
+// other 16-column chunk (w >> 2 picks the parity).
 template <int MODE>
 DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, int f, int s,
-                         int* acc_smem) {
+                         int2* vbuf) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quarter = warp & 3, half = warp >> 2;
   const int nant = A.nant;
-  const int b = warp * 32 + lane;
-  const int nbase = nant * (nant + 1) / 2;
-  int gs = 0, cnt = 0;
-  const int* ycell = nullptr;
-  if constexpr (MODE == 1) {
-    gs = g * A.ceff + s;
-    cnt = A.ycnt[gs];
-    ycell = A.ycell + (size_t)gs * nbase;
-    for (int k = threadIdx.x; k < 2 * cnt; k += TC_THREADS) acc_smem[k] = 0;
-    __syncthreads();
-  }
-  if (warp * 32 < nant) {
-    const uint32_t lane_base = tmem_base + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * 256);
-    for (int c0 = 0; c0 < nant; c0 += 16) {
-      if (c0 + 15 < warp * 32) continue;  // whole chunk below this warp's rows
+  const int b = quarter * 32 + lane;
+  if (quarter * 32 < nant) {
+    const uint32_t lane_base =
+        tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * 256);
+    for (int c0 = half * 16; c0 < nant; c0 += 32) {
+      if (c0 + 15 < quarter * 32) continue;  // whole chunk below this warp's rows
       uint32_t vr[16], vi[16];
       tmem_ld16(lane_base + (uint32_t)c0, vr);
       tmem_ld16(lane_base + (uint32_t)(nant + c0), vi);
@@ -298,11 +292,7 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
             A.out[(size_t)g * A.o_g + (size_t)f * A.o_f + (size_t)bls * A.o_b + (size_t)s * A.o_s] =
                 make_float2((float)re, (float)im);
           } else {
-            const int k = ycell[bls];
-            if (k >= 0) {
-              atomicAdd(&acc_smem[2 * k], re);
-              atomicAdd(&acc_smem[2 * k + 1], im);
-            }
+            vbuf[bls] = make_int2(re, im);
           }
         }
       }
@@ -310,12 +300,22 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
   }
   tc_fence_before();
   if constexpr (MODE == 1) {
+    // per-cell sum over the baselines gridded into it (exact int32)
     __syncthreads();
+    const int gs = g * A.ceff + s;
     const long long row0 = A.yoff[gs];
+    const int cnt = A.ycnt[gs];
     const long long tp = (A.t_base + f) & A.t_mask;
-    for (int k = threadIdx.x; k < cnt; k += TC_THREADS)
-      A.yout[(row0 + k) * A.y_t_stride + tp] =
-          make_float2((float)acc_smem[2 * k], (float)acc_smem[2 * k + 1]);
+    for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
+      const long long r = row0 + k;
+      int sr = 0, si = 0;
+      for (int j = A.row_off[r]; j < A.row_off[r + 1]; ++j) {
+        const int2 v = vbuf[A.row_bls[j]];
+        sr += v.x;
+        si += v.y;
+      }
+      A.yout[tp * A.y_t_stride + r] = make_float2((float)sr, (float)si);
+    }
   }
 }
 
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   uint64_t* bar_acc = bar_mma + A.nstage;
   uint64_t* bar_drain = bar_acc + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_drain + 1);
-  int* acc_smem = reinterpret_cast<int*>(tmem_slot + 4);
+  int2* vbuf = reinterpret_cast<int2*>(tmem_slot + 4);
 
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
       tc_fence_after();
       int pg, pf, ps;
       tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
-      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, acc_smem);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf);
     }
   }
   if (ok && my_units > 0) {
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
       tc_fence_after();
       int pg, pf, ps;
       tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
-      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, acc_smem);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf);
     } else {
       ok = false;
     }
@@ -450,7 +450,7 @@ int tc_plan(TcArgs& A, int mode) {
   A.nkblk = (2 * A.kc + 127) / 128;
   A.stage_bytes = A.nkblk * A.rows * 128;
   A.n_mma = 2 * A.kc / 32;
-  const int extra = (mode == 1) ? A.ymax * 8 : 0;
+  const int extra = (mode == 1) ? A.nant * (A.nant + 1) / 2 * 8 : 0;
   const int budget = TC_SMEM_BUDGET - extra - 1024 - 256;
   A.nstage = std::min(4, budget / A.stage_bytes);
   if (A.nstage < 2) return DSB_E_UNSUPPORTED;
@@ -560,24 +560,25 @@ int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt
 }
 
 int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
-                     int nchan, int t_int, int csf, const int* ycell, const int* yoff,
-                     const int* ycnt, int ymax, void* yout, long long y_t_stride,
+                     int nchan, int t_int, int csf, const int* yoff, const int* ycnt,
+                     const int* row_off, const int* row_bls, void* yout, long long y_t_stride,
                      long long t_base, long long t_mask, int max_ctas, int* status,
                      cudaStream_t stream) {
-  if (!raw || !yout || !ycell || !yoff || !ycnt || ymax < 0) return DSB_E_ARG;
+  if (!raw || !yout || !yoff || !ycnt || !row_off || !row_bls) return DSB_E_ARG;
   if (((uintptr_t)raw & 15) || (raw_g_stride & 15)) return DSB_E_ARG;
   TcArgs A{};
   A.raw = static_cast<const uint8_t*>(raw);
   A.raw_g_stride = raw_g_stride;
   A.n_chgroup = n_chgroup; A.npkt = npkt; A.nant = nant; A.nchan = nchan;
   A.t_int = t_int; A.csf = csf; A.unit_order = 0;
-  A.ycell = ycell; A.yoff = yoff; A.ycnt = ycnt; A.ymax = ymax;
+  A.yoff = yoff; A.ycnt = ycnt; A.row_off = row_off; A.row_bls = row_bls;
   A.yout = static_cast<float2*>(yout);
   A.y_t_stride = y_t_stride; A.t_base = t_base; A.t_mask = t_mask;
   A.status = status;
   int rc = tc_plan(A, 1);
   if (rc) return rc;
-  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + ymax * 8, TC_MIN_SMEM);
+  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + A.nant * (A.nant + 1) / 2 * 8,
+                           TC_MIN_SMEM);
   cudaFuncSetAttribute(corr_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int n_units = n_chgroup * A.n_fv * A.ceff;
   int grid = std::min(n_units, max_ctas > 0 ? max_ctas : num_sms());

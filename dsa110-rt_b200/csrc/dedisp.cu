@@ -121,96 +121,81 @@ __global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int d
   out[idx] = v;
 }
 
-// Pipeline stage 1 over per-subband gridded rows.  One block per global cell
-// (all chgroups); loops over coarse DMs; threads along time.
+// Pipeline stage 1 over per-subband gridded rows, time-major rings:
+//   Y[(t & y_mask) * y_rows + row],  D[(t & d_mask) * d_rows + drow].
+// One thread per cell of one chgroup (blocks never straddle chgroups), one
+// grid row per coarse DM; every thread walks time, so threads that read the
+// same summed channel read the same time sample of adjacent rows.
 struct S1Args {
   const float2* Y;
-  long long y_stride, y_mask;
-  const int* cell_off;    // (n_cells + 1)
-  const int* src_row;     // Y row of each source
-  const int* src_s;       // summed channel of each source
-  const int* cell_g;      // chgroup of each global cell
-  const int* cell_local;  // cell index inside its chgroup
+  long long y_rows, y_mask;
+  const int* rowtab;      // [cell_base[g]*ceff + s*nf[g] + cell] = Y row or -1
+  const int* blk_g;       // chgroup of each block
+  const int* blk_c0;      // first cell of each block
+  const int* cell_base;   // (G) first global cell of the chgroup
   const int* shift1;      // (G, ceff, n_dm)
   const int* shift2;      // (G, n_dm)
   const int* d_base;      // (G) first D row of the chgroup
   const int* n_filled;    // (G)
   float2* D;
-  long long d_stride, d_mask;
+  long long d_rows, d_mask;
   long long t0;           // absolute time of the first output
   int n_t, n_dm, ceff;
   double2* sky_ring;      // (D rows, window) or null
   int sky_window, sky_head, sky_count, sky_subtract;
 };
 
-constexpr int S1_THREADS = 256;
-constexpr int S1_MAX_SRC = 64;
+constexpr int S1_THREADS = 128;
+constexpr int S1_MAX_C = 64;
 
 __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
-  const int gc = blockIdx.x;
-  const int g = A.cell_g[gc], cl = A.cell_local[gc];
-  const int j0 = A.cell_off[gc], nsrc = min(A.cell_off[gc + 1] - j0, S1_MAX_SRC);
-  __shared__ int s_row[S1_MAX_SRC], s_s[S1_MAX_SRC];
-  __shared__ double red_r[S1_THREADS / 32], red_i[S1_THREADS / 32];
-  for (int j = threadIdx.x; j < nsrc; j += S1_THREADS) {
-    s_row[j] = A.src_row[j0 + j];
-    s_s[j] = A.src_s[j0 + j];
-  }
-  __syncthreads();
+  __shared__ int s_row[S1_MAX_C][S1_THREADS];
+  __shared__ int s_sh[S1_MAX_C];
+  const int g = A.blk_g[blockIdx.x];
+  const int d = blockIdx.y;
   const int nf = A.n_filled[g];
-  for (int d = 0; d < A.n_dm; ++d) {
-    const long long drow = (long long)A.d_base[g] + (long long)d * nf + cl;
-    double2 m = make_double2(0.0, 0.0);
-    const bool sub = A.sky_ring && A.sky_subtract && A.sky_count > 0;
-    if (sub) {
-      for (int w = 0; w < A.sky_count; ++w) {
-        const double2 r = A.sky_ring[drow * A.sky_window + w];
-        m.x += r.x;
-        m.y += r.y;
-      }
-      m.x /= A.sky_count;
-      m.y /= A.sky_count;
+  const int cl = A.blk_c0[blockIdx.x] + threadIdx.x;
+  const int ceff = A.ceff;
+  for (int s = threadIdx.x; s < ceff; s += S1_THREADS)
+    s_sh[s] = A.shift1[(g * ceff + s) * A.n_dm + d];
+  const bool live = cl < nf;
+  const int* rt = A.rowtab + (long long)A.cell_base[g] * ceff;
+  for (int s = 0; s < ceff; ++s) s_row[s][threadIdx.x] = live ? rt[(long long)s * nf + cl] : -1;
+  __syncthreads();
+  if (!live) return;
+  const long long drow = (long long)A.d_base[g] + (long long)d * nf + cl;
+  double mr = 0.0, mi = 0.0;
+  const bool sub = A.sky_ring && A.sky_subtract && A.sky_count > 0;
+  if (sub) {
+    for (int w = 0; w < A.sky_count; ++w) {
+      const double2 r = A.sky_ring[drow * A.sky_window + w];
+      mr += r.x;
+      mi += r.y;
     }
-    const int sh2 = A.shift2[g * A.n_dm + d];
-    double sr = 0.0, si = 0.0;
-    for (int t = threadIdx.x; t < A.n_t; t += S1_THREADS) {
-      const long long ta = A.t0 + t;
-      float re = 0.f, im = 0.f;
-      for (int j = 0; j < nsrc; ++j) {
-        const int sh = A.shift1[(g * A.ceff + s_s[j]) * A.n_dm + d];
-        const float2 x = A.Y[(long long)s_row[j] * A.y_stride + ((ta + sh) & A.y_mask)];
+    mr /= A.sky_count;
+    mi /= A.sky_count;
+  }
+  const int sh2 = A.shift2[g * A.n_dm + d];
+  double sr = 0.0, si = 0.0;
+  for (int t = 0; t < A.n_t; ++t) {
+    const long long ta = A.t0 + t;
+    float re = 0.f, im = 0.f;
+    for (int s = 0; s < ceff; ++s) {
+      const int row = s_row[s][threadIdx.x];
+      if (row >= 0) {
+        const float2 x = A.Y[((ta + s_sh[s]) & A.y_mask) * A.y_rows + row];
         re += x.x;
         im += x.y;
       }
-      sr += re;
-      si += im;
-      float2 o = make_float2(re, im);
-      if (sub) o = make_float2((float)((double)re - m.x), (float)((double)im - m.y));
-      A.D[drow * A.d_stride + ((ta + sh2) & A.d_mask)] = o;
     }
-    if (A.sky_ring) {
-      // block reduction of the block's un-subtracted time sum
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-        si += __shfl_xor_sync(0xffffffffu, si, o);
-      }
-      if ((threadIdx.x & 31) == 0) {
-        red_r[threadIdx.x >> 5] = sr;
-        red_i[threadIdx.x >> 5] = si;
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double tr = 0.0, ti = 0.0;
-        for (int w = 0; w < S1_THREADS / 32; ++w) {
-          tr += red_r[w];
-          ti += red_i[w];
-        }
-        A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(tr / A.n_t, ti / A.n_t);
-      }
-      __syncthreads();
-    }
+    sr += re;
+    si += im;
+    float2 o = make_float2(re, im);
+    if (sub) o = make_float2((float)((double)re - mr), (float)((double)im - mi));
+    A.D[((ta + sh2) & A.d_mask) * A.d_rows + drow] = o;
   }
+  if (A.sky_ring)
+    A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(sr / A.n_t, si / A.n_t);
 }
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? DSB_OK : DSB_E_CUDA; }
@@ -265,32 +250,33 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
   return launch_status();
 }
 
-int dsb_stage1_rows(const void* Y, long long y_stride, long long y_mask, int n_cells,
-                    const int* cell_off, const int* src_row, const int* src_s, const int* cell_g,
-                    const int* cell_local, const int* shift1, const int* shift2,
-                    const int* d_base, const int* n_filled, void* D, long long d_stride,
-                    long long d_mask, long long t0, int n_t, int n_dm, int ceff, void* sky_ring,
-                    int sky_window, int sky_head, int sky_count, int sky_subtract,
-                    int max_src, cudaStream_t stream) {
-  if (!Y || !D || !cell_off || !src_row || !src_s || !cell_g || !cell_local || !shift1 ||
-      !shift2 || !d_base || !n_filled || n_t <= 0 || n_dm <= 0)
+int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
+                    const int* blk_g, const int* blk_c0, const int* rowtab, const int* cell_base,
+                    const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
+                    void* D, long long d_rows, long long d_mask, long long t0, int n_t, int n_dm,
+                    int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
+                    int sky_subtract, cudaStream_t stream) {
+  if (!Y || !D || !blk_g || !blk_c0 || !rowtab || !cell_base || !shift1 || !shift2 ||
+      !d_base || !n_filled || n_t <= 0 || n_dm <= 0 || ceff <= 0)
     return DSB_E_ARG;
-  if (max_src > S1_MAX_SRC) return DSB_E_CAPACITY;
+  if (ceff > S1_MAX_C) return DSB_E_CAPACITY;
   if (sky_ring && (sky_window <= 0 || sky_head < 0 || sky_head >= sky_window ||
                    sky_count < 0 || sky_count > sky_window))
     return DSB_E_ARG;
-  if (n_cells <= 0) return DSB_OK;
+  if (n_blocks <= 0) return DSB_OK;
   S1Args A{};
-  A.Y = (const float2*)Y; A.y_stride = y_stride; A.y_mask = y_mask;
-  A.cell_off = cell_off; A.src_row = src_row; A.src_s = src_s;
-  A.cell_g = cell_g; A.cell_local = cell_local;
+  A.Y = (const float2*)Y; A.y_rows = y_rows; A.y_mask = y_mask;
+  A.rowtab = rowtab; A.blk_g = blk_g; A.blk_c0 = blk_c0; A.cell_base = cell_base;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
-  A.D = (float2*)D; A.d_stride = d_stride; A.d_mask = d_mask;
+  A.D = (float2*)D; A.d_rows = d_rows; A.d_mask = d_mask;
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
   A.sky_count = sky_count; A.sky_subtract = sky_subtract;
-  stage1_rows_kernel<<<n_cells, S1_THREADS, 0, stream>>>(A);
+  dim3 grid(n_blocks, n_dm);
+  stage1_rows_kernel<<<grid, S1_THREADS, 0, stream>>>(A);
   return launch_status();
 }
+
+int dsb_stage1_block_size(void) { return S1_THREADS; }
 
 }  // extern "C"

@@ -49,38 +49,54 @@ struct CombArgs {
   float2* out;           // (n_f, n_t, N, N/2+1)
 };
 
-__global__ void combine_rows_kernel(const CombArgs A) {
+// One thread per (half cell, fine DM); time is walked in tiles of CB_T
+// samples so every ring row is read sequentially (L1 sector reuse) and each
+// output time is written coalesced across the half cells of a warp.
+constexpr int CB_T = 8;
+
+__global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
   const int nh = A.N / 2 + 1;
-  const long long n_hc = (long long)A.N * nh;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)A.n_f * A.n_t * n_hc;
-  if (idx >= total) return;
-  const int hc = (int)(idx % n_hc);
-  const long long r = idx / n_hc;
-  const int t = (int)(r % A.n_t);
-  const int fl = (int)(r / A.n_t);
+  const int n_hc = A.N * nh;
+  const int hc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hc >= n_hc) return;
+  const int fl = blockIdx.y;
   const int f = A.f0 + fl;
   const int c = A.f2c[f];
-  const long long ta = A.t0 + t;
-  double re = 0.0, im = 0.0;
-  for (int j = A.hc_off[hc]; j < A.hc_off[hc + 1]; ++j) {
-    const int g = A.e_g[j];
-    int cell = A.e_cell[j];
-    const bool mirror = cell < 0;
-    if (mirror) cell = ~cell;
-    const long long row = (long long)A.d_base[g] + (long long)c * A.n_filled[g] + cell;
-    const long long ts = ta - A.sfine[(long long)f * A.G + g];
-    const float2 x = A.D[row * A.d_stride + (ts & A.d_mask)];
-    re += x.x;
-    im += mirror ? -(double)x.y : (double)x.y;
-  }
-  float o_re = (float)(0.5 * re), o_im = (float)(0.5 * im);
   const int u = hc / nh, w = hc % nh;
-  if (A.fftshift && ((u + w) & 1)) {
-    o_re = -o_re;
-    o_im = -o_im;
+  const bool flip = A.fftshift && ((u + w) & 1);
+  float2* out = A.out + (size_t)fl * A.n_t * n_hc + hc;
+  const int j0 = A.hc_off[hc], j1 = A.hc_off[hc + 1];
+  for (int tt = 0; tt < A.n_t; tt += CB_T) {
+    double re[CB_T], im[CB_T];
+#pragma unroll
+    for (int i = 0; i < CB_T; ++i) re[i] = im[i] = 0.0;
+    for (int j = j0; j < j1; ++j) {
+      const int g = A.e_g[j];
+      int cell = A.e_cell[j];
+      const bool mirror = cell < 0;
+      if (mirror) cell = ~cell;
+      const long long row = (long long)A.d_base[g] + (long long)c * A.n_filled[g] + cell;
+      const long long ts0 = A.t0 + tt - A.sfine[(long long)f * A.G + g];
+      const float2* src = A.D + row;
+#pragma unroll
+      for (int i = 0; i < CB_T; ++i) {
+        const float2 x = src[((ts0 + i) & A.d_mask) * A.d_stride];
+        re[i] += x.x;
+        im[i] += mirror ? -(double)x.y : (double)x.y;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < CB_T; ++i) {
+      if (tt + i < A.n_t) {
+        float o_re = (float)(0.5 * re[i]), o_im = (float)(0.5 * im[i]);
+        if (flip) {
+          o_re = -o_re;
+          o_im = -o_im;
+        }
+        out[(size_t)(tt + i) * n_hc] = make_float2(o_re, o_im);
+      }
+    }
   }
-  A.out[idx] = make_float2(o_re, o_im);
 }
 
 // ===========================================================================
@@ -266,9 +282,15 @@ struct DetCand {
   int k;
 };
 
+// Element e = f * npix + p of time t is read at x[f*f_stride + t*t_stride + p]
+// and multiplied by mask[f*npix + p] when a mask is given (the per-fine-DM
+// edge mask x 1/sigma), so the detector consumes the FFT output directly.
 template <int LOGW, typename T>
-__global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ cube, int n,
-                                                     long long inner, const float* __restrict__ sinv,
+__global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, int n, int npix,
+                                                     long long inner, long long f_stride,
+                                                     long long t_stride,
+                                                     const float* __restrict__ mask,
+                                                     const float* __restrict__ sinv,
                                                      int t_base, int n_out, float thr,
                                                      DetCand* __restrict__ cands, int cap, int pix_off,
                                                      int* __restrict__ count) {
@@ -278,6 +300,9 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ cube,
   constexpr int PL = MAXW / 2;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= inner) return;
+  const long long fidx = e / npix, p = e % npix;
+  const T* cube = x + fidx * f_stride + p;
+  const float mval = mask ? mask[e] : 1.0f;
   float si[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) si[k] = sinv[k];
@@ -288,6 +313,13 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ cube,
   float last = 0.f;
   const int total = n + MAXW;  // cs length
   for (int J0 = 0; J0 < total; J0 += R) {
+    // issue this block's R loads before any of them is consumed
+    float xin[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = J0 + q - 1 - PL;
+      xin[q] = (i >= 0 && i < n) ? ldf<T>(cube, (long long)i * t_stride) : 0.f;
+    }
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const int J = J0 + q;
@@ -296,7 +328,8 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ cube,
         if (J <= PL) {
           v = 0.f;
         } else if (J <= PL + n) {
-          run += (double)ldf<T>(cube, (long long)(J - 1 - PL) * inner + e);
+          const float xv = mask ? xin[q] * mval : xin[q];
+          run += (double)xv;
           last = (float)run;
           v = last;
         } else {
@@ -448,8 +481,9 @@ int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const 
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
   CombArgs A{(const float2*)D, d_stride, d_mask, hc_off, e_g, e_cell, d_base, n_filled, sfine,
              f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
-  const long long total = (long long)n_f * n_t * N * (N / 2 + 1);
-  combine_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(A);
+  const int n_hc = N * (N / 2 + 1);
+  dim3 grid((n_hc + 127) / 128, n_f);
+  combine_rows_kernel<<<grid, 128, 0, stream>>>(A);
   return launch_status();
 }
 
@@ -532,25 +566,28 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
   return launch_status();
 }
 
-int dsb_detect(const void* cube, int cube_f16, int n, long long inner, int log_maxw,
-               const float* sigma_inv, int t_base, int n_out, float threshold, void* cands,
-               int cap, int pix_off, int* count, cudaStream_t stream) {
-  if (!cube || !sigma_inv || !cands || !count || n <= 0 || inner <= 0 || cap < 0) return DSB_E_ARG;
+int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
+               long long t_stride, const float* mask, int log_maxw, const float* sigma_inv,
+               int t_base, int n_out, float threshold, void* cands, int cap, int pix_off,
+               int* count, cudaStream_t stream) {
+  if (!cube || !sigma_inv || !cands || !count || n <= 0 || n_f <= 0 || npix <= 0 || cap < 0)
+    return DSB_E_ARG;
   if (log_maxw < 0 || log_maxw > 6 || (1 << log_maxw) > n || t_base < 0 || n_out < 0 ||
       t_base + n_out > n)
     return DSB_E_ARG;
+  const long long inner = (long long)n_f * npix;
   const unsigned grid = (unsigned)((inner + 255) / 256);
   DetCand* c = (DetCand*)cands;
-#define DSB_DET(L)                                                                          \
-  do {                                                                                      \
-    if (cube_f16)                                                                           \
-      detect_kernel<L, __half><<<grid, 256, 0, stream>>>((const __half*)cube, n, inner,      \
-                                                         sigma_inv, t_base, n_out, threshold, \
-                                                         c, cap, pix_off, count);                    \
-    else                                                                                    \
-      detect_kernel<L, float><<<grid, 256, 0, stream>>>((const float*)cube, n, inner,        \
-                                                        sigma_inv, t_base, n_out, threshold,  \
-                                                        c, cap, pix_off, count);                     \
+#define DSB_DET(L)                                                                        \
+  do {                                                                                    \
+    if (cube_f16)                                                                         \
+      detect_kernel<L, __half><<<grid, 256, 0, stream>>>(                                 \
+          (const __half*)cube, n, npix, inner, f_stride, t_stride, mask, sigma_inv, t_base, \
+          n_out, threshold, c, cap, pix_off, count);                                      \
+    else                                                                                  \
+      detect_kernel<L, float><<<grid, 256, 0, stream>>>(                                  \
+          (const float*)cube, n, npix, inner, f_stride, t_stride, mask, sigma_inv, t_base,  \
+          n_out, threshold, c, cap, pix_off, count);                                      \
   } while (0)
   switch (log_maxw) {
     case 0: DSB_DET(0); break;

@@ -28,16 +28,20 @@ _SIGNATURES = {
     "dsb_corr_tc": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp,
                     _c_ll, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
     "dsb_corr_tc_grid": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp,
-                         _vp, _c_int, _vp, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
+                         _vp, _vp, _vp, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
     "dsb_uv_cells": [_vp, _vp, _c_int, _vp, _c_int, ctypes.c_double, _c_int, _vp, _vp, _vp],
     "dsb_grid_vis": [_vp, _c_int, _c_ll, _vp, _vp, _c_int, _vp, _vp],
     "dsb_dedisp_vis": [_vp, _vp, _c_int, _c_ll, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_int,
                        _vp, _vp],
     "dsb_static_sky": [_vp, _vp, _c_int, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_stage2_roll": [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_ll, _vp, _vp],
-    "dsb_stage1_rows": [_vp, _c_ll, _c_ll, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+    "dsb_stage1_rows": [_vp, _c_ll, _c_ll, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                         _vp, _c_ll, _c_ll, _c_ll, _c_int, _c_int, _c_int, _vp, _c_int, _c_int,
-                        _c_int, _c_int, _c_int, _vp],
+                        _c_int, _c_int, _vp],
+    "dsb_stage1_block_size": [],
+    "dsb_image_cluster_size": [_c_int],
+    "dsb_image_fft": [_vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
+                      _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],
     "dsb_combine_rows": [_vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
                          _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp],
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
@@ -48,8 +52,8 @@ _SIGNATURES = {
     "dsb_multi_boxcar_argmax": [_vp, _c_ll, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _c_int,
                                 _vp, _vp],
     "dsb_boxcar_from_cs": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp],
-    "dsb_detect": [_vp, _c_int, _c_int, _c_ll, _c_int, _vp, _c_int, _c_int, _c_float, _vp, _c_int,
-                   _c_int, _vp, _vp],
+    "dsb_detect": [_vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_ll, _vp, _c_int, _vp, _c_int,
+                   _c_int, _c_float, _vp, _c_int, _c_int, _vp, _vp],
     "dsb_clipped_std": [_vp, _c_int, _c_int, _c_float, _c_int, _vp, _vp],
 }
 

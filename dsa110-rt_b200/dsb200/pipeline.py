@@ -16,13 +16,13 @@ absolute fast-vis tile index from the start of the stream):
                            the stage-2 ring D (so the stage-2 FIFO is an index
                            offset)
    -> per fine-DM batch:
-      dsb_combine_rows   : fine-DM residual shifts, sum over chgroups,
-                           Hermitian half spectrum, fftshift checkerboard
-      irfft2             : real image
+      dsb_image_fft      : fine-DM residual shifts, sum over chgroups into the
+                           Hermitian half spectrum (fftshift checkerboard) in
+                           shared memory, 2-D inverse real FFT -> image
       dsb_clipped_std    : Layer-1 sigma per fine DM (current cube)
-      dsb_mask_to_cube   : edge mask x 1/sigma into the detector cube
-      dsb_detect         : boxcars 1..2**log_max_width, max over widths,
-                           threshold compaction
+      dsb_detect         : edge mask x 1/sigma applied on read, boxcars
+                           1..2**log_max_width, max over widths, threshold
+                           compaction
    -> host: top-k (value desc, flat index asc) + merge-radius decode
 
 Detector cubes overlap by 2*t_edge so that their interiors tile time.
@@ -41,8 +41,8 @@ from . import _lib
 from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
 from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
 from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
-from .search import (CandidateBuffer, Candidate, _nms, compute_edge_mask, irfft2_image,
-                     mask_into_cube, sigma_clipped_std_batched, detect_cube)
+from .search import (CandidateBuffer, _nms, compute_edge_mask, detect_images, irfft2_image,
+                     sigma_clipped_std_batched)
 
 
 def _pow2_at_least(n: int) -> int:
@@ -119,17 +119,15 @@ class Tables:
     cell_lambda: float
     patterns: list
     n_filled: np.ndarray            # (G,)
-    ycell: np.ndarray               # (G*ceff*nbase,) int32
-    yoff: np.ndarray                # (G*ceff,) int32
+    yoff: np.ndarray                # (G*ceff,) int32 first Y row of each (chgroup, subband)
     ycnt: np.ndarray
-    ymax: int
+    row_off: np.ndarray             # (n_rows_y + 1) CSR: baselines gridded into each Y row
+    row_bls: np.ndarray
     n_rows_y: int
-    cell_off: np.ndarray            # stage-1 CSR over global cells
-    src_row: np.ndarray
-    src_s: np.ndarray
-    cell_g: np.ndarray
-    cell_local: np.ndarray
-    max_src: int
+    rowtab: np.ndarray              # stage 1: Y row of (g, s, cell) or -1
+    blk_g: np.ndarray               # stage-1 thread blocks: chgroup, first cell
+    blk_c0: np.ndarray
+    cell_base: np.ndarray           # (G,) first global cell of each chgroup
     shift1: np.ndarray              # (G, ceff, n_coarse) int32
     shift2: np.ndarray              # (G, n_coarse) int32
     d_base: np.ndarray              # (G,)
@@ -138,6 +136,9 @@ class Tables:
     hc_off: np.ndarray              # combine CSR over half cells
     e_g: np.ndarray
     e_cell: np.ndarray
+    sc_off: np.ndarray              # (CL + 1) image-kernel scatter entries per cluster rank
+    sc_meta: np.ndarray             # (n, 2) int32 {cell | g<<16 | mirror<<31, smem target}
+    twiddles: np.ndarray            # (N,) complex64 exp(+2 pi i e / N)
     mask: np.ndarray                # (N, N) float32
 
 
@@ -156,36 +157,41 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
                                        device=device))
     n_filled = np.asarray([p.n_filled for p in pats], np.int64)
     # per-(g, s) Y rows: distinct cells hit by summed channel s, ascending
-    ycell = np.full((G, ceff, nbase), -1, np.int32)
     yoff = np.zeros(G * ceff, np.int64)
     ycnt = np.zeros(G * ceff, np.int64)
     row_cell = []
     row_g = []
     row_s = []
+    row_cnt = []
+    row_bls = []
     nrow = 0
     for g in range(G):
         for s in range(ceff):
             col = cims[g][:, s]
-            valid = col < n_filled[g]
-            cells = np.unique(col[valid])
-            ycell[g, s, valid] = np.searchsorted(cells, col[valid]).astype(np.int32)
+            valid = np.nonzero(col < n_filled[g])[0]
+            cells, k = np.unique(col[valid], return_inverse=True)
+            order = np.argsort(k, kind="stable")
+            row_bls.append(valid[order])
+            row_cnt.append(np.bincount(k, minlength=cells.size))
             yoff[g * ceff + s] = nrow
             ycnt[g * ceff + s] = cells.size
             row_cell.append(cells)
             row_g.append(np.full(cells.size, g))
             row_s.append(np.full(cells.size, s))
             nrow += cells.size
+    row_off = np.concatenate([[0], np.cumsum(np.concatenate(row_cnt))])
+    row_bls = np.concatenate(row_bls)
     row_cell = np.concatenate(row_cell)
     row_g = np.concatenate(row_g)
     row_s = np.concatenate(row_s)
     cell_base = np.concatenate([[0], np.cumsum(n_filled)])
-    gcell = cell_base[row_g] + row_cell
-    order = np.lexsort((row_s, gcell))
-    counts = np.bincount(gcell, minlength=int(cell_base[-1]))
-    cell_off = np.zeros(int(cell_base[-1]) + 1, np.int64)
-    cell_off[1:] = np.cumsum(counts)
-    cell_g = np.repeat(np.arange(G), n_filled)
-    cell_local = np.concatenate([np.arange(n) for n in n_filled])
+    # stage-1 table: Y row of (chgroup, summed channel, cell) or -1, and the
+    # thread blocks (never straddling a chgroup)
+    rowtab = np.full(int(cell_base[-1]) * ceff, -1, np.int64)
+    rowtab[cell_base[row_g] * ceff + row_s * n_filled[row_g] + row_cell] = np.arange(nrow)
+    bs = int(_lib.lib().dsb_stage1_block_size())
+    blk_g = np.concatenate([np.full(-(-int(n) // bs), g) for g, n in enumerate(n_filled)])
+    blk_c0 = np.concatenate([np.arange(0, int(n), bs) for n in n_filled])
     # shift tables
     plan = DMPlan(dm_pc_cc=cfg.coarse_dm, t_int_fast_us=cfg.t_int_us, chan_sum_factor=cfg.csf,
                   band=band)
@@ -215,17 +221,43 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     hc_off[1:] = np.cumsum([len(x) for x in ent])
     e_g = np.asarray([g for x in ent for g, _ in x], np.int32)
     e_cell = np.asarray([k for x in ent for _, k in x], np.int32)
+    # image-kernel scatter lists: rank r owns half-cell columns [r*CW, ...);
+    # entry = {cell | g << 16 | mirror << 31, shared-memory target wl*(N+1) + u}
+    CL = int(_lib.lib().dsb_image_cluster_size(N)) or 1
+    CW = -(-nh // CL)
+    sc_off = np.zeros(CL + 1, np.int64)
+    sc_meta = []
+    for r in range(CL):
+        lo, hi = r * CW, min(nh, (r + 1) * CW)
+        for g, p in enumerate(pats):
+            u = p.ix_row.astype(np.int64)
+            w = p.ix_col.astype(np.int64)
+            k = np.arange(u.size, dtype=np.int64)
+            for mirror in (0, 1):
+                uu, ww = ((N - u) % N, (N - w) % N) if mirror else (u, w)
+                sel = (ww >= lo) & (ww < hi)
+                m = np.empty((int(sel.sum()), 2), np.int64)
+                m[:, 0] = k[sel] | (g << 16) | (mirror << 31)
+                m[:, 1] = (ww[sel] - lo) * (N + 1) + uu[sel]
+                sc_meta.append(m)
+        sc_off[r + 1] = sum(x.shape[0] for x in sc_meta)
+    if int(n_filled.max()) >= 1 << 16 or G > 1 << 15:
+        raise ValueError("image scatter entries need cells < 65536 and G < 32768")
+    sc_meta = np.concatenate(sc_meta).astype(np.uint32).view(np.int32)
     mask = compute_edge_mask(n_grid=N, kernel_support=1)
+    e = np.arange(N)
+    tw = np.exp(2j * np.pi * e / N).astype(np.complex64)
     return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled,
-                  ycell=ycell.reshape(-1), yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
-                  ymax=int(ycnt.max()), n_rows_y=int(nrow),
-                  cell_off=cell_off.astype(np.int32), src_row=order.astype(np.int32),
-                  src_s=row_s[order].astype(np.int32), cell_g=cell_g.astype(np.int32),
-                  cell_local=cell_local.astype(np.int32), max_src=int(counts.max()),
+                  yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
+                  row_off=row_off.astype(np.int32), row_bls=row_bls.astype(np.int32),
+                  n_rows_y=int(nrow), rowtab=rowtab.astype(np.int32),
+                  blk_g=blk_g.astype(np.int32), blk_c0=blk_c0.astype(np.int32),
+                  cell_base=cell_base[:-1].astype(np.int32),
                   shift1=np.ascontiguousarray(shift1), shift2=shift2.astype(np.int32),
                   d_base=d_base.astype(np.int32), n_rows_d=int(n_filled.sum() * n_coarse),
                   sfine=sfine.astype(np.int32), hc_off=hc_off.astype(np.int32), e_g=e_g,
-                  e_cell=e_cell, mask=mask.astype(np.float32))
+                  e_cell=e_cell, sc_off=sc_off.astype(np.int32), sc_meta=sc_meta,
+                  twiddles=tw, mask=mask.astype(np.float32))
 
 
 @dataclass
@@ -247,9 +279,12 @@ class SearchPipeline:
         self.tab = build_tables(cfg, antpos_e, antpos_n, self.dev, core_mask)
         T = self.tab
         d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.dev)  # noqa: E731
-        self.d_ycell, self.d_yoff, self.d_ycnt = d(T.ycell), d(T.yoff), d(T.ycnt)
-        self.d_cell_off, self.d_src_row, self.d_src_s = d(T.cell_off), d(T.src_row), d(T.src_s)
-        self.d_cell_g, self.d_cell_local = d(T.cell_g), d(T.cell_local)
+        self.d_yoff, self.d_ycnt = d(T.yoff), d(T.ycnt)
+        self.d_row_off, self.d_row_bls = d(T.row_off), d(T.row_bls)
+        self.d_rowtab, self.d_blk_g, self.d_blk_c0 = d(T.rowtab), d(T.blk_g), d(T.blk_c0)
+        self.d_cell_base = d(T.cell_base)
+        self.d_sc_off, self.d_sc_meta = d(T.sc_off), d(T.sc_meta)
+        self.d_tw = d(T.twiddles)
         self.d_shift1, self.d_shift2 = d(T.shift1), d(T.shift2)
         self.d_dbase = d(T.d_base)
         self.d_nfilled = d(T.n_filled.astype(np.int32))
@@ -270,8 +305,9 @@ class SearchPipeline:
         self.TY = _pow2_at_least((self.depth1 + 1) * C)
         span_d = (self.a + 1) * C + 2 * te + max(0, int(T.sfine.max())) + int(T.shift2.max()) + C
         self.TD = _pow2_at_least(span_d)
-        self.Y = torch.zeros((T.n_rows_y, self.TY), dtype=torch.complex64, device=self.dev)
-        self.D = torch.zeros((T.n_rows_d, self.TD), dtype=torch.complex64, device=self.dev)
+        # time-major rings: [time & (T-1)][row]
+        self.Y = torch.zeros((self.TY, T.n_rows_y), dtype=torch.complex64, device=self.dev)
+        self.D = torch.zeros((self.TD, T.n_rows_d), dtype=torch.complex64, device=self.dev)
         self.sky = (torch.zeros((T.n_rows_d, cfg.sky_window), dtype=torch.complex128,
                                 device=self.dev) if cfg.use_sky else None)
         self.sky_count = self.sky_head = self.sky_seen = 0
@@ -279,14 +315,17 @@ class SearchPipeline:
         nt_cube = C + 2 * te
         nb = cfg.fdm_batch
         N = cfg.n_grid
-        self.Gh = torch.empty((nb, nt_cube, N, N // 2 + 1), dtype=torch.complex64, device=self.dev)
-        self.cube = torch.empty((nt_cube, nb, N, N), dtype=torch.float32, device=self.dev)
+        self.img = torch.empty((nb, nt_cube, N, N), dtype=torch.float32, device=self.dev)
         widths = [1 << k for k in range(cfg.log_max_width + 1)]
         self.widths = widths
         self.sinv = d((np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32))
         self.cands = CandidateBuffer(self.dev, cfg.cand_capacity)
         self.chunk = 0              # next absolute chunk index to correlate
         self.out: List[StreamCandidate] = []
+        self.timing = False          # record CUDA events around each stage when set
+        self.events: dict = {}
+        self.launches = 0            # dsb200 kernel launches issued
+        self.last_d2h_bytes = 0
         self.keep_sigma = False
         self.l1_sigma: List[torch.Tensor] = []
         # Layer-1 subsample positions (interior times x active pixels)
@@ -295,6 +334,41 @@ class SearchPipeline:
         self.l1_t = d(te + np.linspace(0, C - 1, cfg.l1_times).astype(np.int64))
 
     # ------------------------------------------------------------------
+    class _Mark:
+        def __init__(self, pipe, name):
+            self.pipe, self.name = pipe, name
+
+        def __enter__(self):
+            if self.pipe.timing:
+                self.e0 = torch.cuda.Event(enable_timing=True)
+                self.e0.record(torch.cuda.current_stream(self.pipe.dev))
+
+        def __exit__(self, *exc):
+            if self.pipe.timing:
+                e1 = torch.cuda.Event(enable_timing=True)
+                e1.record(torch.cuda.current_stream(self.pipe.dev))
+                self.pipe.events.setdefault(self.name, []).append((self.e0, e1))
+            return False
+
+    def _mark(self, name: str) -> "_Mark":
+        return SearchPipeline._Mark(self, name)
+
+    def skip_warmup(self) -> None:
+        """Start the stream in steady state: the next block already runs
+        stage 1 and the detector on every chunk (rings start at zero), so that
+        every block a benchmark times carries the full per-block work."""
+        self.chunk = self.jc_first + self.depth1 + self.a
+        self.sky_seen = self.cfg.sky_warmup
+
+    def stage_times_ms(self) -> dict:
+        """Mean and total device milliseconds per recorded stage."""
+        torch.cuda.synchronize(self.dev)
+        out = {}
+        for k, v in self.events.items():
+            ts = [a.elapsed_time(b) for a, b in v]
+            out[k] = {"n": len(ts), "total_ms": float(sum(ts)), "mean_ms": float(np.mean(ts))}
+        return out
+
     def _corr(self, raw: torch.Tensor, p0: int) -> None:
         cfg, T = self.cfg, self.tab
         C = cfg.chunk_tiles
@@ -302,24 +376,29 @@ class SearchPipeline:
         row_bytes = cfg.nant * cfg.band.nchan * 4
         page = cfg.npkt_block * row_bytes
         base = raw.data_ptr() + p0 * row_bytes
-        _lib.check(_lib.lib().dsb_corr_tc_grid(
-            _lib.ctypes.c_void_p(base), page, cfg.band.n_chgroup, C * ppfv, cfg.nant,
-            cfg.band.nchan, cfg.t_int, cfg.csf, _lib.ptr(self.d_ycell), _lib.ptr(self.d_yoff),
-            _lib.ptr(self.d_ycnt), T.ymax, _lib.ptr(self.Y), self.TY, self.chunk * C, self.TY - 1,
-            0, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_corr_tc_grid")
+        with self._mark("corr"):
+            _lib.check(_lib.lib().dsb_corr_tc_grid(
+                _lib.ctypes.c_void_p(base), page, cfg.band.n_chgroup, C * ppfv, cfg.nant,
+                cfg.band.nchan, cfg.t_int, cfg.csf, _lib.ptr(self.d_yoff), _lib.ptr(self.d_ycnt),
+                _lib.ptr(self.d_row_off), _lib.ptr(self.d_row_bls), _lib.ptr(self.Y),
+                self.tab.n_rows_y, self.chunk * C, self.TY - 1, 0, _lib.ptr(self.status),
+                _lib.stream_of(self.dev)), "dsb_corr_tc_grid")
+        self.launches += 1
 
     def _stage1(self, j: int) -> None:
         cfg, T = self.cfg, self.tab
         C = cfg.chunk_tiles
         sub = int(cfg.use_sky and self.sky_count > 0 and self.sky_seen >= cfg.sky_warmup)
-        _lib.check(_lib.lib().dsb_stage1_rows(
-            _lib.ptr(self.Y), self.TY, self.TY - 1, int(T.cell_off.size - 1),
-            _lib.ptr(self.d_cell_off), _lib.ptr(self.d_src_row), _lib.ptr(self.d_src_s),
-            _lib.ptr(self.d_cell_g), _lib.ptr(self.d_cell_local), _lib.ptr(self.d_shift1),
-            _lib.ptr(self.d_shift2), _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled),
-            _lib.ptr(self.D), self.TD, self.TD - 1, j * C, C, cfg.coarse_dm.size, cfg.ceff,
-            _lib.ptr(self.sky), cfg.sky_window, self.sky_head, self.sky_count, sub, T.max_src,
-            _lib.stream_of(self.dev)), "dsb_stage1_rows")
+        with self._mark("stage1"):
+            _lib.check(_lib.lib().dsb_stage1_rows(
+                _lib.ptr(self.Y), T.n_rows_y, self.TY - 1, int(T.blk_g.size),
+                _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_rowtab),
+                _lib.ptr(self.d_cell_base), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
+                _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D), T.n_rows_d,
+                self.TD - 1, j * C, C, cfg.coarse_dm.size, cfg.ceff, _lib.ptr(self.sky),
+                cfg.sky_window, self.sky_head, self.sky_count, sub, _lib.stream_of(self.dev)),
+                "dsb_stage1_rows")
+        self.launches += 1
         if cfg.use_sky:
             self.sky_count = min(self.sky_count + 1, cfg.sky_window)
             self.sky_head = (self.sky_head + 1) % cfg.sky_window
@@ -334,28 +413,29 @@ class SearchPipeline:
         self.cands.reset()
         for f0 in range(0, nfine, cfg.fdm_batch):
             nf = min(cfg.fdm_batch, nfine - f0)
-            gh = self.Gh[:nf]
-            _lib.check(_lib.lib().dsb_combine_rows(
-                _lib.ptr(self.D), self.TD, self.TD - 1, _lib.ptr(self.d_hc_off),
-                _lib.ptr(self.d_eg), _lib.ptr(self.d_ecell), _lib.ptr(self.d_dbase),
-                _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c), f0, nf,
-                cfg.band.n_chgroup, N, t0, nt, 1, _lib.ptr(gh), _lib.stream_of(self.dev)),
-                "dsb_combine_rows")
-            img = irfft2_image(gh, N)                                  # (nf, nt, N, N)
-            samp = img.reshape(nf, nt, N * N)[:, self.l1_t][:, :, self.l1_pix].reshape(nf, -1)
-            sig = sigma_clipped_std_batched(samp)
-            sig = torch.where(sig > 0, sig, torch.ones_like(sig))
-            mask_f = (self.d_mask[None] / sig[:, None, None]).contiguous()
-            cube = self.cube[:, :nf] if nf == cfg.fdm_batch else torch.empty(
-                (nt, nf, N, N), dtype=torch.float32, device=self.dev)
-            mask_into_cube(img.contiguous(), mask_f, cube, 0)
-            detect_cube(cube, log_max_width=cfg.log_max_width, sigma_inv=self.sinv, t_base=te,
-                        n_out=C, threshold=cfg.threshold, cands=self.cands,
-                        pix_offset=f0 * N * N)
+            img = self.img[:nf]
+            with self._mark("image"):
+                _lib.check(_lib.lib().dsb_image_fft(
+                    _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_sc_off),
+                    _lib.ptr(self.d_sc_meta), _lib.ptr(self.d_dbase),
+                    _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
+                    _lib.ptr(self.d_tw), f0, nf, cfg.band.n_chgroup, N, t0, nt, 1, _lib.ptr(img),
+                    0, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_image_fft")
+            with self._mark("layer1"):
+                samp = img.reshape(nf, nt, N * N)[:, self.l1_t][:, :, self.l1_pix].reshape(nf, -1)
+                sig = sigma_clipped_std_batched(samp)
+                sig = torch.where(sig > 0, sig, torch.ones_like(sig))
+                mask_f = (self.d_mask[None] / sig[:, None, None]).contiguous()
+            with self._mark("detect"):
+                detect_images(img, mask_f, log_max_width=cfg.log_max_width, sigma_inv=self.sinv,
+                              t_base=te, n_out=C, threshold=cfg.threshold, cands=self.cands,
+                              pix_offset=f0 * N * N)
+            self.launches += 3
             if collect and self.keep_sigma:
                 self.l1_sigma.append(sig)
         if collect:
             got = self.cands.fetch()
+            self.last_d2h_bytes += 4 + got.nbytes
             self._pending = [(float(c["snr"]), int(c["t"]) * (nfine * N * N) + int(c["pix"]),
                               int(c["k"])) for c in got]
             res = _nms(self._pending, threshold=cfg.threshold, n_top=cfg.n_top,
@@ -379,6 +459,7 @@ class SearchPipeline:
         raw = raw.contiguous()
         self.out = []
         self._pending = []
+        self.last_d2h_bytes = 0
         C = cfg.chunk_tiles
         ppfv = cfg.t_int // 2
         for ci in range(cfg.n_fv_block // C):

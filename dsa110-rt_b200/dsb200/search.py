@@ -318,11 +318,29 @@ def detect_cube(cube: torch.Tensor, *, log_max_width: int, sigma_inv: torch.Tens
     _lib.require_cuda(cube, "cube")
     n = cube.shape[0]
     inner = cube[0].numel()
-    _lib.check(_lib.lib().dsb_detect(_lib.ptr(cube), int(cube.dtype == torch.float16), n, inner,
-                                     int(log_max_width), _lib.ptr(sigma_inv), int(t_base),
-                                     int(n_out), float(threshold), _lib.ptr(cands.buf),
-                                     cands.capacity, int(pix_offset), _lib.ptr(cands.count),
+    _lib.check(_lib.lib().dsb_detect(_lib.ptr(cube), int(cube.dtype == torch.float16), n, 1,
+                                     inner, 0, inner, None, int(log_max_width),
+                                     _lib.ptr(sigma_inv), int(t_base), int(n_out),
+                                     float(threshold), _lib.ptr(cands.buf), cands.capacity,
+                                     int(pix_offset), _lib.ptr(cands.count),
                                      _lib.stream_of(cube.device)), "dsb_detect")
+
+
+def detect_images(img: torch.Tensor, mask_f: torch.Tensor, *, log_max_width: int,
+                  sigma_inv: torch.Tensor, t_base: int, n_out: int, threshold: float,
+                  cands: CandidateBuffer, pix_offset: int = 0) -> None:
+    """Detector on FFT output ``img [F, T, H, W]`` with the per-F mask
+    ``mask_f [F, H, W]`` applied while reading (no masked copy)."""
+    _lib.require_cuda(img, "img")
+    _lib.require_cuda(mask_f, "mask_f")
+    F, T, H, W = img.shape
+    npix = H * W
+    _lib.check(_lib.lib().dsb_detect(_lib.ptr(img), int(img.dtype == torch.float16), T, F, npix,
+                                     T * npix, npix, _lib.ptr(mask_f), int(log_max_width),
+                                     _lib.ptr(sigma_inv), int(t_base), int(n_out),
+                                     float(threshold), _lib.ptr(cands.buf), cands.capacity,
+                                     int(pix_offset), _lib.ptr(cands.count),
+                                     _lib.stream_of(img.device)), "dsb_detect")
 
 
 # ---------------------------------------------------------------------------

@@ -72,12 +72,13 @@ int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt
 
 /* Same correlator with the gridder folded into its epilogue: replaces
  * FastVisGridder.compute (src/dsart/grid/kernel.py:508) applied per summed
- * channel.  ycell[(g*ceff + s)*nbase + bls] = row within group (g, s) or -1;
- * group rows start at yoff[g*ceff+s] and number ycnt[...] (<= ymax).
- * Output row r, tile f -> yout[r*y_t_stride + ((t_base + f) & t_mask)]. */
+ * channel.  Group (g, s) owns rows [yoff[g*ceff+s], + ycnt[...]); row r sums
+ * the baselines row_bls[row_off[r] .. row_off[r+1]) (exact int32).
+ * Output row r, tile f -> yout[((t_base + f) & t_mask)*y_t_stride + r]
+ * (time-major ring; y_t_stride >= number of rows). */
 int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
-                     int nchan, int t_int, int csf, const int* ycell, const int* yoff,
-                     const int* ycnt, int ymax, void* yout, long long y_t_stride,
+                     int nchan, int t_int, int csf, const int* yoff, const int* ycnt,
+                     const int* row_off, const int* row_bls, void* yout, long long y_t_stride,
                      long long t_base, long long t_mask, int max_ctas, int* status,
                      cudaStream_t stream);
 
@@ -123,20 +124,25 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * Stage 1 over per-subband gridded rows (dsb_corr_tc_grid output), static-sky
  * subtraction fused, each output written at (t + shift2[g, d]) of the
  * stage-2 ring D, i.e. stage 1 + StaticSkyMean + the stage-2 FIFO
- * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264). */
-int dsb_stage1_rows(const void* Y, long long y_stride, long long y_mask, int n_cells,
-                    const int* cell_off, const int* src_row, const int* src_s, const int* cell_g,
-                    const int* cell_local, const int* shift1, const int* shift2,
-                    const int* d_base, const int* n_filled, void* D, long long d_stride,
-                    long long d_mask, long long t0, int n_t, int n_dm, int ceff, void* sky_ring,
-                    int sky_window, int sky_head, int sky_count, int sky_subtract,
-                    int max_src, cudaStream_t stream);
+ * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264).
+ * Rings are time-major: Y[(t & y_mask)*y_rows + row], D[(t & d_mask)*d_rows + r].
+ * Block b covers cells [blk_c0[b], + dsb_stage1_block_size()) of chgroup
+ * blk_g[b]; rowtab[cell_base[g]*ceff + s*nf[g] + cell] = Y row of (cell, s)
+ * or -1; D row of (g, d, cell) = d_base[g] + d*nf[g] + cell. */
+int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
+                    const int* blk_g, const int* blk_c0, const int* rowtab, const int* cell_base,
+                    const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
+                    void* D, long long d_rows, long long d_mask, long long t0, int n_t, int n_dm,
+                    int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
+                    int sky_subtract, cudaStream_t stream);
+int dsb_stage1_block_size(void);
 
 /* ---- a12: fine-DM combine ---------------------------------------------------
  * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
  * the Hermitian half-spectrum fold and fftshift checkerboard of
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
- * reads the stage-2 rings directly, writes (n_f, n_t, N, N/2+1) complex64. */
+ * reads the time-major stage-2 ring D[(t & d_mask)*d_stride + row] directly,
+ * writes (n_f, n_t, N, N/2+1) complex64. */
 int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
                      const int* e_g, const int* e_cell, const int* d_base, const int* n_filled,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
@@ -150,6 +156,26 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
                       const float* off_re, const float* off_im, void* out, int out_f16, int half,
                       int G, int t_stream, int t_det, int N, int t_lo, int fftshift,
                       cudaStream_t stream);
+
+/* ---- a12/a13: fused combine + 2-D inverse real FFT ------------------------------
+ * Replaces fused_dequant_combine_per_fdm_half + torch.fft.irfft2 inside
+ * GpuImager.process_cube (src/dsart/image/fused_combine_cuda.py:1359,
+ * src/dsart/image/imager_gpu.py:575-605): for each (fine DM f0+fl, time t0+t)
+ * the Hermitian half spectrum is combined from the time-major stage-2 ring
+ * into shared memory and transformed there; out (n_f, n_t, N, N) float32 =
+ * irfft2(G_h) with 1/N^2 normalisation.  Half cells are split over the
+ * dsb_image_cluster_size(N) CTAs of a cluster by column: rank r owns columns
+ * [r*CW, ...), CW = ceil((N/2+1)/CL); rank r scatters the entries
+ * sc_meta[sc_off[r] .. sc_off[r+1]) = {cell | g << 16 | mirror << 31,
+ * target wl*(N+1) + u}: the value of chgroup g's coarse-DM slice at `cell`
+ * (its conjugate for mirror entries) is added to half cell (u, r*CW + wl).
+ * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256. */
+int dsb_image_cluster_size(int n_grid);
+int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const int* sc_off,
+                  const void* sc_meta, const int* d_base, const int* n_filled,
+                  const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
+                  int N, long long t0, int n_t, int fftshift, void* out, int max_clusters,
+                  int* status, cudaStream_t stream);
 
 /* ---- a13/a14: edge mask x Layer-1 normalisation into the detector cube -----
  * Replaces the mask multiply + cube write of GpuImager.process_cube
@@ -179,12 +205,16 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
 
 /* Fused streaming form of the three above plus the threshold test of
  * decode_topk_argmax_lowmem (src/dsart/detector/decoder.py:388): widths
- * 1..2^log_maxw, every output cell with max S/N > threshold appended to
- * cands (struct {int t, pix; float snr; int k;}), *count incremented
- * (entries past cap are counted, not written). */
-int dsb_detect(const void* cube, int cube_f16, int n, long long inner, int log_maxw,
-               const float* sigma_inv, int t_base, int n_out, float threshold, void* cands,
-               int cap, int pix_off, int* count, cudaStream_t stream);
+ * 1..2^log_maxw over n samples of n_f*npix cells; cell e = f*npix + p at time
+ * t is read at cube[f*f_stride + t*t_stride + p] and multiplied by mask[e]
+ * (the edge mask x 1/sigma) when mask is non-null.  Every output cell with
+ * max S/N > threshold is appended to cands (struct {int t, pix; float snr;
+ * int k;}, pix = e + pix_off); *count counts them (entries past cap are
+ * counted, not written). */
+int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
+               long long t_stride, const float* mask, int log_maxw, const float* sigma_inv,
+               int t_base, int n_out, float threshold, void* cands, int cap, int pix_off,
+               int* count, cudaStream_t stream);
 
 /* ---- a18: Layer-1 sigma-clipped std ---------------------------------------------
  * sigma_clipped_std_batched (src/dsart/noise_norm/layer1.py:53): rows of at

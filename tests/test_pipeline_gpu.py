@@ -32,7 +32,7 @@ def _setup(n_blocks=8, amp=1.0):
     from dsb200.constants import band_from_edges
     band = band_from_edges(2, 32, 1.49875, 1.31125)
     ob = O.Band(band.n_chgroup, band.nchan, band.f0_ghz, band.dnu_ghz, band.ch0)
-    nant, npkt, N = 16, 256, 32
+    nant, npkt, N = 16, 256, 64
     e, n = synth.t_layout(nant, seed=5)
     cell = O.top_of_band_cell_lambda(e, n, ob, N)
     coarse = np.linspace(0, 30, 4)
@@ -76,7 +76,7 @@ def test_pipeline_matches_oracle(dev):
         for d in range(len(kw["coarse_dm"])):
             rows = T.d_base[g] + d * T.n_filled[g] + np.arange(T.n_filled[g])
             pos = (t1 + T.shift2[g, d]) & (pipe.TD - 1)
-            np.testing.assert_array_equal(D[rows][:, pos].T, keep["D1"][g][d][t1].astype(np.complex64))
+            np.testing.assert_array_equal(D[pos][:, rows], keep["D1"][g][d][t1].astype(np.complex64))
 
     key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
     g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
@@ -88,15 +88,53 @@ def test_pipeline_matches_oracle(dev):
             v = g_map.get(k, w_map.get(k))
             assert abs(v - 6.0) < EPS_BAND * 6.0, f"unmatched candidate {k} snr={v}"
     # the injected burst is recovered at its pixel
-    assert any(c.l == 19 and c.m == 11 for c in got)
+    assert any(c.l == 32 + 3 and c.m == 32 - 5 for c in got)
 
 
 def test_pipeline_rejects_wrong_raw_size(dev):
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
-    cfg = PipelineConfig(band=band, nant=16, npkt_block=256, t_int=8, csf=4, n_grid=32,
+    cfg = PipelineConfig(band=band, nant=16, npkt_block=256, t_int=8, csf=4, n_grid=64,
                          coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
                          fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, chunk_tiles=32)
     pipe = SearchPipeline(cfg, e, n, device=dev)
     with pytest.raises(ValueError):
         pipe.process_block(torch.zeros(100, dtype=torch.uint8, device=dev))
+
+
+@pytest.mark.parametrize("N", [64, 256])
+def test_image_fft_matches_combine_and_irfft2(dev, N):
+    """Fused combine + 2-D c2r FFT == dsb_combine_rows + torch.fft.irfft2 on
+    the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale."""
+    from dsb200 import _lib
+    from dsb200.pipeline import PipelineConfig, SearchPipeline
+    band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
+    cfg = PipelineConfig(band=band, nant=16, npkt_block=256, t_int=8, csf=4, n_grid=N,
+                         coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
+                         fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, chunk_tiles=32)
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    T = pipe.tab
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    pipe.D.copy_(torch.randn(pipe.D.shape, dtype=torch.complex64, device=dev, generator=g))
+    nf, nt, t0 = 5, 20, 37
+    out = torch.empty((nf, nt, N, N), dtype=torch.float32, device=dev)
+    L = _lib.lib()
+    _lib.check(L.dsb_image_fft(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1, _lib.ptr(pipe.d_sc_off),
+                               _lib.ptr(pipe.d_sc_meta),
+                               _lib.ptr(pipe.d_dbase), _lib.ptr(pipe.d_nfilled),
+                               _lib.ptr(pipe.d_sfine), _lib.ptr(pipe.d_f2c), _lib.ptr(pipe.d_tw),
+                               1, nf, band.n_chgroup, N, t0, nt, 1, _lib.ptr(out), 3,
+                               _lib.ptr(pipe.status), _lib.stream_of(dev)), "image")
+    gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
+    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1,
+                                  _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
+                                  _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_dbase),
+                                  _lib.ptr(pipe.d_nfilled), _lib.ptr(pipe.d_sfine),
+                                  _lib.ptr(pipe.d_f2c), 1, nf, band.n_chgroup, N, t0, nt, 1,
+                                  _lib.ptr(gh), _lib.stream_of(dev)), "combine")
+    want = torch.fft.irfft2(gh.to(torch.complex128), s=(N, N))
+    torch.cuda.synchronize()
+    pipe.check_status()
+    err = (out.double() - want).abs().max().item()
+    assert err <= 2e-6 * want.abs().max().item(), err
