@@ -611,3 +611,71 @@ int dsb_clipped_std(const float* samples, int rows, int m, float n_sigma, int n_
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Boxcar S/N argmax without allocation.
+//
+// dsb_padded_cumsum + dsb_multi_boxcar_argmax need a caller-owned prefix-sum
+// buffer of (n + max_w) x inner floats.  Some callers cannot allocate one: a
+// host program that hands all of the GPU's memory to its own fixed arena at
+// start-up, or a real-time loop where an allocation or free would stall
+// every stream on the device (cudaFree synchronises the device).  For them,
+// dsb_boxcar_argmax_noalloc keeps the prefix sums in the file-scope array
+// below, DSB_NOALLOC_SCRATCH_BYTES (16 MiB) long, which every GPU that
+// loads this file's device code holds until the process exits.
+// ===========================================================================
+#include <atomic>
+#include <mutex>
+
+static __device__ __align__(256) float g_boxcar_cs_scratch[DSB_NOALLOC_SCRATCH_BYTES / 4];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::atomic<float*> g_boxcar_cs_ptr[kNoallocMaxDevices];
+std::mutex g_boxcar_cs_mu;
+
+// Device address of the scratch array on the current device, looked up once
+// per device (on that device's first call) and cached.  Null on failure.
+float* boxcar_cs_scratch(int dev) {
+  float* p = g_boxcar_cs_ptr[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lock(g_boxcar_cs_mu);
+  p = g_boxcar_cs_ptr[dev].load(std::memory_order_relaxed);
+  if (p) return p;
+  void* addr = nullptr;
+  if (cudaGetSymbolAddress(&addr, g_boxcar_cs_scratch) != cudaSuccess || !addr) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  p = static_cast<float*>(addr);
+  g_boxcar_cs_ptr[dev].store(p, std::memory_order_release);
+  return p;
+}
+
+}  // namespace
+
+extern "C" int dsb_boxcar_argmax_noalloc(const void* x, int x_f16, int n, long long inner,
+                                         int max_w, const int* widths, const int* offsets,
+                                         const float* sigma_inv, int K, int n_out, int t_base,
+                                         void* out_max, int out_f16, void* out_win,
+                                         cudaStream_t stream) {
+  if (!x || !widths || !offsets || !sigma_inv || !out_max || !out_win) return DSB_E_ARG;
+  if (n <= 0 || inner <= 0 || max_w < 1 || max_w > n || K < 1 || n_out <= 0 || t_base < 0 ||
+      (long long)t_base + n_out > n)
+    return DSB_E_ARG;
+  if ((long long)(n + max_w) * inner > (long long)(DSB_NOALLOC_SCRATCH_BYTES / 4))
+    return DSB_E_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DSB_E_CUDA;
+  if (dev < 0 || dev >= kNoallocMaxDevices) return DSB_E_UNSUPPORTED;
+  float* cs = boxcar_cs_scratch(dev);
+  if (!cs) return DSB_E_CUDA;
+  // padded_cumsum_kernel writes every one of the (n + max_w) x inner prefix
+  // values, its zero padding rows included, so nothing left in the array by
+  // an earlier call is read.
+  const int rc = dsb_padded_cumsum(x, x_f16, n, inner, max_w, cs, stream);
+  if (rc != DSB_OK) return rc;
+  return dsb_multi_boxcar_argmax(cs, inner, widths, offsets, sigma_inv, K, n_out, t_base,
+                                 out_max, out_f16, out_win, stream);
+}

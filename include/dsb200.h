@@ -199,6 +199,24 @@ int dsb_multi_boxcar_argmax(const float* cs, long long inner, const int* widths,
                             int t_base, void* out_max, int out_f16, void* out_win,
                             cudaStream_t stream);
 
+/* The two calls above in one, for callers that cannot allocate device memory
+ * (a host that gives all of the GPU's memory to its own fixed arena, or a
+ * real-time loop where an allocation or free would stall every stream on the
+ * device).  No counterpart in dsa110-rt: it has no such callers.  The prefix
+ * sums live in a fixed array inside the library, DSB_NOALLOC_SCRATCH_BYTES
+ * long, held on every GPU that loads the library until the process exits;
+ * (n + max_w) * inner * 4 bytes beyond it return DSB_E_CAPACITY.  The first
+ * call on each device looks up that array's address, so make it before any
+ * stream capture.  Every call shares the one array: calls that overlap on
+ * the GPU (two streams, or two host threads) race and must be serialised by
+ * the caller.  Needs t_base + n_out <= n and the centred offsets
+ * max_w/2 - widths[k]/2 with widths[k] <= max_w.  Allocates nothing. */
+#define DSB_NOALLOC_SCRATCH_BYTES (16u << 20)
+int dsb_boxcar_argmax_noalloc(const void* x, int x_f16, int n, long long inner, int max_w,
+                              const int* widths, const int* offsets, const float* sigma_inv,
+                              int K, int n_out, int t_base, void* out_max, int out_f16,
+                              void* out_win, cudaStream_t stream);
+
 /* boxcar_from_padded_cumsum (src/dsart/detector/forward.py:339). */
 int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, int n_out,
                        float* out, cudaStream_t stream);
