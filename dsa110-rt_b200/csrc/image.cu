@@ -6,24 +6,34 @@
 // which replaces fused_dequant_combine_per_fdm_half + torch.fft.irfft2
 // (src/dsart/image/fused_combine_cuda.py:560-620, image/imager_gpu.py:590).
 //
-// Layout of the work: a cluster of CL CTAs owns one image at a time.  CTA r
-// holds the half-spectrum columns [r*CW, ...) in shared memory (column-major,
-// column stride N+1 to keep row reads conflict-free), combines them straight
-// from the time-major stage-2 ring, runs the column transforms, and after a
-// cluster barrier transforms its rows, reading the other CTAs' columns
-// through distributed shared memory.  Two real output rows are packed into
-// one complex transform (x_a + i x_b).
+// One CTA owns one image at a time (persistent loop over images), in three
+// steps that never leave the SM except for one small L2-resident scratch:
 //
-// Every N-point transform (N = R*R) runs on a group of R threads: an R-point
-// DFT in registers, the twiddles w_N^(j*x1), one padded shared-memory
+//  1. Combine.  The non-zero half-spectrum cells S (the union of every
+//     chgroup's uv pattern, a few thousand cells) are summed in shared memory
+//     from the time-major stage-2 ring: one coalesced read of each chgroup's
+//     coarse-DM slice, shared-memory float atomics into S.  S is copied to
+//     this CTA's row of the workspace (it stays in L2).
+//  2. Column transforms by decimation in frequency.  Columns w = 0 and N/2
+//     of G_h are Hermitian in u, so their transforms are real: they ride
+//     together as one complex column (w = 0 + i * w = N/2), leaving N/2
+//     complex columns.  With N = FOLD * LC, output rows x = FOLD*m + p are
+//         A[FOLD m + p, w] = sum_n' W_LC^(n' m) W_N^(n' p)
+//                              sum_q i^(q p) G_h[n' + LC q, w]      (FOLD = 4)
+//     so pass p (p = 0..3) folds S into LC-point columns and transforms them
+//     in place: a shared buffer of LC x N/2 complex values (66 KB for
+//     N = 256), small enough for three CTAs per SM.
+//  3. Row transforms of the pass's LC rows, two real rows per complex
+//     transform (x_a + i x_b), staged in shared memory and written as float4.
+//
+// Every transform of length L = R*R runs on a group of R threads: an R-point
+// DFT in registers, the twiddles W_L^(j*x1), one XOR-swizzled shared-memory
 // transpose, and a second R-point DFT (the classic two-step factorisation).
+// The shared-memory atomics of step 1 add in no fixed order, so an image can
+// differ from run to run in the last bits of a float32 sum.
 #include "dsb_common.cuh"
 
-#include <cooperative_groups.h>
-
 #include <algorithm>
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -35,6 +45,15 @@ DSB_DEV float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 DSB_DEV float2 cmul_i(float2 a) { return make_float2(-a.y, a.x); }  // i * a
+// a * i^k
+DSB_DEV float2 crot(float2 a, int k) {
+  switch (k & 3) {
+    case 1: return make_float2(-a.y, a.x);
+    case 2: return make_float2(-a.x, -a.y);
+    case 3: return make_float2(a.y, -a.x);
+    default: return a;
+  }
+}
 
 // cos/sin of multiples of pi/8 (exact mathematical constants, float-rounded)
 constexpr float C8 = 0.92387953251128674f;   // cos(pi/8)
@@ -101,230 +120,258 @@ DSB_DEV void idft16(float2 (&a)[16]) {
 template <int R>
 DSB_DEV void idftR(float2 (&a)[R]) {
   if constexpr (R == 16) idft16(a);
-  else idft8(a);
-}
-
-// One N-point inverse complex transform (N = R*R) by the R threads of a group
-// (thread j).  load(i) returns input element i; store(i, v) writes output i.
-template <int R, typename Load, typename Store>
-DSB_DEV void fft_group(int j, unsigned mask, float2* scr, const float2* tw, Load load,
-                       Store store) {
-  constexpr int N = R * R;
-  float2 a[R];
-#pragma unroll
-  for (int k = 0; k < R; ++k) a[k] = load(j + R * k);
-  idftR<R>(a);
-#pragma unroll
-  for (int x1 = 1; x1 < R; ++x1) a[x1] = cmul(a[x1], tw[(j * x1) & (N - 1)]);
-#pragma unroll
-  for (int x1 = 0; x1 < R; ++x1) scr[x1 * (R + 1) + j] = a[x1];
-  __syncwarp(mask);
-#pragma unroll
-  for (int jj = 0; jj < R; ++jj) a[jj] = scr[j * (R + 1) + jj];
-  __syncwarp(mask);
-  idftR<R>(a);
-#pragma unroll
-  for (int x2 = 0; x2 < R; ++x2) store(j + R * x2, a[x2]);
+  else if constexpr (R == 8) idft8(a);
+  else idft4(a[0], a[1], a[2], a[3]);
 }
 
 struct ImgArgs {
   const float2* D;
   long long d_rows, d_mask;
-  const int* sc_off;    // (CL + 1): rank r's scatter entries are [sc_off[r], sc_off[r+1])
-  const int2* sc_meta;  // {cell | g << 16 | mirror << 31, target wl*(N+1) + u}
-  const int* d_base;    // (G)
-  const int* n_filled;  // (G)
-  const int* sfine;     // (n_fine, G)
-  const int* f2c;       // (n_fine)
-  const float2* tw;     // (N) w_N^e = exp(+2 pi i e / N)
+  const unsigned* c_meta;   // (sum n_filled) per pattern cell: tgt | conj << 16 | g << 17
+  const int* cell_base;     // (G + 1)
+  const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
+  int n_c2;
+  const int* so;            // (N/2 * LC + 1) S entries of (packed column, folded row)
+  const uint8_t* sq;        // (n_s) q | packed << 2 | parity(u + w) << 3
+  int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
+  const int* d_base;        // (G)
+  const int* n_filled;      // (G)
+  const int* sfine;         // (n_fine, G)
+  const int* f2c;           // (n_fine)
+  const float2* tw;         // (N) W_N^e = exp(+2 pi i e / N)
   int f0, n_f, G;
   long long t0;
   int n_t;
   int fftshift;
-  float* out;           // (n_f, n_t, N, N)
+  float* out;               // (n_f, n_t, N, N)
+  float2* ws;               // (gridDim.x, ws_stride)
   int* status;
 };
 
-template <int N, int CL>
+constexpr int IMG_MAX_G = 64;
+
+template <int N>
 struct ImgGeom {
-  static constexpr int R = (N == 256) ? 16 : 8;
-  static constexpr int NH = N / 2 + 1;
-  static constexpr int CW = (NH + CL - 1) / CL;  // columns per CTA (last may have fewer)
-  static constexpr int CS = N + 1;               // column stride (float2)
-  static constexpr int HREG = (CW * CS + 1) / 2 * 2;  // H region, float2, 16-byte multiple
-  static constexpr int RW = N / CL;              // output rows per CTA
+  static constexpr int FOLD = 4;
+  static constexpr int LC = N / FOLD;             // folded column length
+  static constexpr int C1 = (LC == 64) ? 8 : 4;    // LC = C1 * C1
+  static constexpr int NC = N / 2;                // packed columns
+  static constexpr int P = NC + 2;                // buffer row pitch (float2), = 2 mod 16
+  static constexpr int RR = (N == 256) ? 16 : 8;  // N = RR * RR
   static constexpr int THREADS = 256;
-  static constexpr int GROUPS = THREADS / R;
-  static_assert((R * (R + 1) * 8) % 16 == 0, "group scratch must keep 16-byte alignment");
-  static_assert(2 * N * 4 <= R * (R + 1) * 8, "two output rows must fit a group's scratch");
-  static constexpr size_t SMEM = (size_t)HREG * 8 + (size_t)GROUPS * R * (R + 1) * 8 +
-                                 (size_t)N * 8 + 48 * 8 + 48 * 4 + 256;
+  static constexpr int CG = THREADS / C1;         // column groups
+  static constexpr int RG = THREADS / RR;         // row groups
+  static constexpr int BUF = LC * P;              // float2 slots
+  static_assert(C1 * C1 == LC && RR * RR == N, "unsupported size");
+  static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
+  static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
+  static constexpr size_t SMEM = (size_t)BUF * 8 + (size_t)N * 8 + IMG_MAX_G * 8 +
+                                 (IMG_MAX_G + 1) * 4;
 };
 
-template <int N, int CL>
-__global__ void __launch_bounds__(256, 1) image_kernel(const ImgArgs A) {
-  using Gm = ImgGeom<N, CL>;
-  constexpr int R = Gm::R, CW = Gm::CW, CS = Gm::CS, RW = Gm::RW, NH = Gm::NH;
+template <int N>
+__global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
+  using Gm = ImgGeom<N>;
+  constexpr int FOLD = Gm::FOLD, LC = Gm::LC, C1 = Gm::C1, NC = Gm::NC, P = Gm::P,
+                RR = Gm::RR, THREADS = Gm::THREADS;
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  float2* H = reinterpret_cast<float2*>(smem_raw);
-  float2* scr_all = H + Gm::HREG;  // 16-byte aligned (float4 staging)
-  float2* tw = scr_all + Gm::GROUPS * R * (R + 1);
-  const float2** s_slice = reinterpret_cast<const float2**>(tw + N);  // (G) slice starts
-  int* s_misc = reinterpret_cast<int*>(s_slice + 48);                 // (G) n_filled
+  float2* buf = reinterpret_cast<float2*>(smem_raw);  // S in step 1, columns in 2-3
+  float2* tw = buf + Gm::BUF;
+  const float2** s_slice = reinterpret_cast<const float2**>(tw + N);
+  int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
 
-  int rank = 0;
-  if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
-  const int cluster_id = (int)blockIdx.x / CL;
-  const int n_clusters = (int)gridDim.x / CL;
-  const int tid = threadIdx.x, grp = tid / R, j = tid % R;
-  float2* scr = scr_all + grp * R * (R + 1);
-  // lanes of this thread's group inside its warp (groups never straddle warps)
-  const unsigned gmask = (R == 32 ? 0xffffffffu : ((1u << R) - 1u)) << ((tid & 31) / R * R);
-  const int w0 = rank * CW;
-  const int ncol = min(CW, NH - w0);
-  const int* sc_off = A.sc_off + rank;
-  // base pointers of every rank's column block (own block is local)
-  const float2* colbase[CL];
-#pragma unroll
-  for (int r = 0; r < CL; ++r) {
-    colbase[r] = H;
-    if constexpr (CL > 1) {
-      if (r != rank) colbase[r] = cg::this_cluster().map_shared_rank(H, r);
-    }
-  }
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  for (int i = tid; i < N; i += THREADS) tw[i] = A.tw[i];
+  for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
 
-  for (int i = tid; i < N; i += Gm::THREADS) tw[i] = A.tw[i];
-  for (int g = tid; g < A.G; g += Gm::THREADS) s_misc[g] = A.n_filled[g];
-  __syncthreads();
-
-  const float scale = 1.0f / (float)(N * N);
+  float2* ws = A.ws + (size_t)blockIdx.x * A.ws_stride;
+  const int n_tot = A.cell_base[A.G];
+  const float scale = 0.5f / (float)(N * N);
   const int n_img = A.n_f * A.n_t;
-  for (int img = cluster_id; img < n_img; img += n_clusters) {
-    const int fl = img / A.n_t, t = img % A.n_t;
+  // column groups: C1 lanes; row groups: RR lanes (groups never straddle warps)
+  const int cgi = tid / C1, cj = tid % C1;
+  const unsigned cmask = ((1u << C1) - 1u) << (lane / C1 * C1);
+  const int rgi = tid / RR, rj = tid % RR;
+  const unsigned rmask = ((1u << RR) - 1u) << (lane / RR * RR);
+  const int shift_rot = A.fftshift ? 2 : 0;
+
+  for (int img = blockIdx.x; img < n_img; img += gridDim.x) {
+    // fine DM fastest: CTAs that run together share coarse-DM slices in L2
+    const int fl = img % A.n_f, t = img / A.n_f;
     const int f = A.f0 + fl;
     const int c = A.f2c[f];
     const long long ta = A.t0 + t;
-    // per-image start of each chgroup's coarse-DM slice in the stage-2 ring
-    for (int g = tid; g < A.G; g += Gm::THREADS)
+    __syncthreads();  // the previous image is done with buf and s_slice
+    for (int g = tid; g < A.G; g += THREADS)
       s_slice[g] = A.D + ((ta - A.sfine[(long long)f * A.G + g]) & A.d_mask) * A.d_rows +
-                   A.d_base[g] + (long long)c * s_misc[g];
-    for (int i = tid; i < CW * CS; i += Gm::THREADS) H[i] = make_float2(0.f, 0.f);
-    __syncthreads();
-    // ---- phase A: scatter every chgroup's stage-2 slice into my half-spectrum
-    //      columns (shared-memory float atomics; entry = {cell | g<<16 |
-    //      mirror<<31, target}) ----
+                   A.d_base[g] + (long long)c * A.n_filled[g];
     {
-      const int e0 = sc_off[0], e1 = sc_off[1];
+      float4* b4 = reinterpret_cast<float4*>(buf);
+      for (int i = tid; i < A.ws_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    // ---- 1. combine into S (shared-memory float atomics) ----
+    {
+      auto add = [&](unsigned m, float2 v) {
+        float2* d = buf + (m & 0xffffu);
+        atomicAdd(&d->x, v.x);
+        atomicAdd(&d->y, ((m >> 16) & 1u) ? -v.y : v.y);
+      };
       constexpr int U = 4;
-      int e = e0 + tid;
-      for (; e + (U - 1) * Gm::THREADS < e1; e += U * Gm::THREADS) {
-        int2 md[U];
-        float2 x[U];
+      int e = tid;
+      for (; e + (U - 1) * THREADS < n_tot; e += U * THREADS) {
+        unsigned m[U];
+        float2 v[U];
 #pragma unroll
-        for (int q = 0; q < U; ++q) md[q] = A.sc_meta[e + q * Gm::THREADS];
-#pragma unroll
-        for (int q = 0; q < U; ++q) x[q] = s_slice[(md[q].x >> 16) & 0x7fff][md[q].x & 0xffff];
+        for (int q = 0; q < U; ++q) m[q] = __ldg(A.c_meta + e + q * THREADS);
 #pragma unroll
         for (int q = 0; q < U; ++q) {
-          atomicAdd(&H[md[q].y].x, x[q].x);
-          atomicAdd(&H[md[q].y].y, md[q].x < 0 ? -x[q].y : x[q].y);
+          const int g = (int)(m[q] >> 17) & (IMG_MAX_G - 1);
+          v[q] = s_slice[g][e + q * THREADS - s_cbase[g]];
         }
+#pragma unroll
+        for (int q = 0; q < U; ++q) add(m[q], v[q]);
       }
-      for (; e < e1; e += Gm::THREADS) {
-        const int2 md = A.sc_meta[e];
-        const float2 x = s_slice[(md.x >> 16) & 0x7fff][md.x & 0xffff];
-        atomicAdd(&H[md.y].x, x.x);
-        atomicAdd(&H[md.y].y, md.x < 0 ? -x.y : x.y);
+      for (; e < n_tot; e += THREADS) {
+        const unsigned m = __ldg(A.c_meta + e);
+        const int g = (int)(m >> 17) & (IMG_MAX_G - 1);
+        add(m, s_slice[g][e - s_cbase[g]]);
+      }
+      for (int i = tid; i < A.n_c2; i += THREADS) {
+        const int2 cm = __ldg(A.c2 + i);
+        add((unsigned)cm.y, s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)][cm.x & 0xffff]);
       }
     }
     __syncthreads();
-    // ---- phase B: column transforms (along u) in place; the combine's 0.5
-    //      and the fftshift checkerboard (-1)^(u+w) are applied on load ----
-    for (int col = grp; col < ncol; col += Gm::GROUPS) {
-      float2* colp = H + col * CS;
-      const int w = w0 + col;
-      fft_group<R>(j, gmask, scr, tw,
-                   [&](int i) {
-                     const float2 v = colp[i];
-                     const float s = (A.fftshift && ((i + w) & 1)) ? -0.5f : 0.5f;
-                     return make_float2(v.x * s, v.y * s);
-                   },
-                   [&](int i, float2 v) { colp[i] = v; });
+    {
+      const float4* b4 = reinterpret_cast<const float4*>(buf);
+      float4* w4 = reinterpret_cast<float4*>(ws);
+      for (int i = tid; i < A.ws_stride / 2; i += THREADS) w4[i] = b4[i];
     }
-    if constexpr (CL > 1) cg::this_cluster().sync();
-    else __syncthreads();
-    // ---- phase C: row transforms, two real rows per complex transform ----
-    // Z[w] = Y_a[w] + i Y_b[w] (w <= N/2), conj-extended above N/2, with the
-    // imaginary parts of Y[0] and Y[N/2] dropped (c2r convention).
-    for (int pr = grp; pr < RW / 2; pr += Gm::GROUPS) {
-      const int xa = rank * RW + 2 * pr, xb = xa + 1;
-      auto colptr = [&](int w) -> const float2* {
-        const int owner = w / CW;
-        return colbase[owner] + (w - owner * CW) * CS;
-      };
-      auto load = [&](int i) -> float2 {
-        if (i == 0 || i == N / 2) {
-          const float2* cp = colptr(i);
-          return make_float2(cp[xa].x, cp[xb].x);
-        }
-        if (i < N / 2) {
-          const float2* cp = colptr(i);
-          const float2 ya = cp[xa], yb = cp[xb];
-          return make_float2(ya.x - yb.y, ya.y + yb.x);           // ya + i yb
-        }
-        const float2* cp = colptr(N - i);
-        const float2 ya = cp[xa], yb = cp[xb];
-        return make_float2(ya.x + yb.y, -ya.y + yb.x);            // conj(ya) + i conj(yb)
-      };
-      // rows x_a = Re, x_b = Im of the transform; staged through the group's
-      // scratch and written as float4
-      float* stage = reinterpret_cast<float*>(scr);
-      fft_group<R>(j, gmask, scr, tw, load, [&](int i, float2 v) {
-        stage[i] = v.x * scale;
-        stage[N + i] = v.y * scale;
-      });
-      __syncwarp(gmask);
-      float4* o4 = reinterpret_cast<float4*>(A.out + (((size_t)fl * A.n_t + t) * N + xa) * N);
-      const float4* s4 = reinterpret_cast<const float4*>(stage);
+    __syncthreads();
+
+    for (int p = 0; p < FOLD; ++p) {
+      // ---- 2. folded column transforms of pass p (in place in buf) ----
+      for (int col = cgi; col < NC; col += Gm::CG) {
+        float2 y[C1];
+        const int* so = A.so + col * LC;
 #pragma unroll
-      for (int q = j; q < N / 2; q += R) o4[q] = s4[q];
-      __syncwarp(gmask);
+        for (int k = 0; k < C1; ++k) {
+          const int n1 = cj + C1 * k;
+          const int r0 = __ldg(so + n1), r1 = __ldg(so + n1 + 1);
+          float2 acc = make_float2(0.f, 0.f);
+          for (int e = r0; e < r1; ++e) {
+            const int qq = __ldg(A.sq + e);
+            const int rot = (qq & 3) * p + ((qq >> 2) & 1) + (((qq >> 3) & 1) ? shift_rot : 0);
+            acc = cadd(acc, crot(ws[e], rot));
+          }
+          y[k] = cmul(acc, tw[(n1 * p) & (N - 1)]);
+        }
+        idftR<C1>(y);
+#pragma unroll
+        for (int m1 = 1; m1 < C1; ++m1) y[m1] = cmul(y[m1], tw[(cj * m1 * (N / LC)) & (N - 1)]);
+        float2* colp = buf + col;
+#pragma unroll
+        for (int m1 = 0; m1 < C1; ++m1) colp[((cj ^ m1) + C1 * m1) * P] = y[m1];
+        __syncwarp(cmask);
+#pragma unroll
+        for (int jj = 0; jj < C1; ++jj) y[jj] = colp[((jj ^ cj) + C1 * cj) * P];
+        __syncwarp(cmask);
+        idftR<C1>(y);
+#pragma unroll
+        for (int m2 = 0; m2 < C1; ++m2) colp[(cj + C1 * m2) * P] = y[m2];
+      }
+      __syncthreads();
+      // ---- 3. row transforms: folded rows (2pr, 2pr + 1) are image rows
+      //      FOLD*2pr + p and FOLD*(2pr+1) + p ----
+      for (int pr = rgi; pr < LC / 2; pr += Gm::RG) {
+        float2* reg = buf + 2 * pr * P;
+        const float2* ra = reg;
+        const float2* rb = reg + P;
+        float2 a[RR];
+#pragma unroll
+        for (int k = 0; k < RR; ++k) {
+          const int i = rj + RR * k;
+          float2 z;
+          if (i == 0) {
+            z = make_float2(ra[0].x, rb[0].x);
+          } else if (i == N / 2) {
+            z = make_float2(ra[0].y, rb[0].y);
+          } else if (i < N / 2) {
+            const float2 ya = ra[i], yb = rb[i];
+            z = make_float2(ya.x - yb.y, ya.y + yb.x);   // ya + i yb
+          } else {
+            const float2 ya = ra[N - i], yb = rb[N - i];
+            z = make_float2(ya.x + yb.y, -ya.y + yb.x);  // conj(ya) + i conj(yb)
+          }
+          a[k] = z;
+        }
+        idftR<RR>(a);
+#pragma unroll
+        for (int x1 = 1; x1 < RR; ++x1) a[x1] = cmul(a[x1], tw[(rj * x1) & (N - 1)]);
+        __syncwarp(rmask);  // every lane has read the pair's rows
+#pragma unroll
+        for (int x1 = 0; x1 < RR; ++x1) reg[rj * RR + (x1 ^ rj)] = a[x1];
+        __syncwarp(rmask);
+#pragma unroll
+        for (int jj = 0; jj < RR; ++jj) a[jj] = reg[jj * RR + (rj ^ jj)];
+        __syncwarp(rmask);
+        idftR<RR>(a);
+        float* stage = reinterpret_cast<float*>(reg);
+#pragma unroll
+        for (int x2 = 0; x2 < RR; ++x2) {
+          stage[rj + RR * x2] = a[x2].x * scale;
+          stage[N + rj + RR * x2] = a[x2].y * scale;
+        }
+        __syncwarp(rmask);
+        const size_t ibase = ((size_t)fl * A.n_t + t) * N;
+        float4* oa = reinterpret_cast<float4*>(A.out + (ibase + FOLD * (2 * pr) + p) * N);
+        float4* ob = reinterpret_cast<float4*>(A.out + (ibase + FOLD * (2 * pr + 1) + p) * N);
+        const float4* s4 = reinterpret_cast<const float4*>(stage);
+#pragma unroll
+        for (int q = rj; q < N / 4; q += RR) {
+          oa[q] = s4[q];
+          ob[q] = s4[N / 4 + q];
+        }
+      }
+      __syncthreads();
     }
-    // the other CTAs may still read my columns
-    if constexpr (CL > 1) cg::this_cluster().sync();
-    else __syncthreads();
   }
 }
 
-template <int N, int CL>
-int launch_image(const ImgArgs& A, int max_clusters, cudaStream_t stream) {
-  using Gm = ImgGeom<N, CL>;
-  static bool configured = false;
-  if (!configured) {
-    if (cudaFuncSetAttribute(image_kernel<N, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// Resident CTAs for image_kernel<N> on this device (the persistent grid).
+template <int N>
+int image_grid(int* blocks) {
+  using Gm = ImgGeom<N>;
+  static int cached = 0;
+  if (!cached) {
+    if (cudaFuncSetAttribute(image_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Gm::SMEM) != cudaSuccess)
       return DSB_E_CUDA;
-    configured = true;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, image_kernel<N>, Gm::THREADS,
+                                                      Gm::SMEM) != cudaSuccess)
+      return DSB_E_CUDA;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cached = std::max(1, occ) * sms;
   }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int n_clusters = sms / CL;
-  if (max_clusters > 0) n_clusters = std::min(n_clusters, max_clusters);
-  n_clusters = std::max(1, std::min(n_clusters, A.n_f * A.n_t));
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(n_clusters * CL);
-  cfg.blockDim = dim3(Gm::THREADS);
-  cfg.dynamicSmemBytes = Gm::SMEM;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = CL;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (cudaLaunchKernelEx(&cfg, image_kernel<N, CL>, A) != cudaSuccess) return DSB_E_CUDA;
+  *blocks = cached;
+  return DSB_OK;
+}
+
+template <int N>
+int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
+  using Gm = ImgGeom<N>;
+  if (A.ws_stride > Gm::BUF) return DSB_E_CAPACITY;
+  int blocks = 0;
+  const int rc = image_grid<N>(&blocks);
+  if (rc != DSB_OK) return rc;
+  blocks = std::min(blocks, max_blocks);
+  blocks = std::max(1, std::min(blocks, A.n_f * A.n_t));
+  image_kernel<N><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
   return launch_status();
 }
 
@@ -332,27 +379,51 @@ int launch_image(const ImgArgs& A, int max_clusters, cudaStream_t stream) {
 
 extern "C" {
 
-int dsb_image_cluster_size(int n_grid) {
+int dsb_image_fold(int n_grid) {
   switch (n_grid) {
-    case 64: return 1;
-    case 256: return 2;
+    case 64:
+    case 256: return ImgGeom<256>::FOLD;
     default: return 0;
   }
 }
 
-int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const int* sc_off,
-                  const void* sc_meta, const int* d_base, const int* n_filled,
+long long dsb_image_workspace_bytes(int n_grid, int n_s) {
+  if (n_s <= 0) return -1;
+  int blocks = 0;
+  int rc = DSB_E_UNSUPPORTED;
+  switch (n_grid) {
+    case 64: rc = image_grid<64>(&blocks); break;
+    case 256: rc = image_grid<256>(&blocks); break;
+    default: break;
+  }
+  if (rc != DSB_OK) return -1;
+  return (long long)blocks * ((n_s + 1) & ~1) * 8;
+}
+
+int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
+                  const int* cell_base, const void* c2, int n_c2, const int* so,
+                  const unsigned char* sq, int n_s, const int* d_base, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
-                  int N, long long t0, int n_t, int fftshift, void* out, int max_clusters,
-                  int* status, cudaStream_t stream) {
-  if (!D || !sc_off || !sc_meta || !d_base || !n_filled || !sfine || !f2c ||
-      !twiddles || !out || n_f <= 0 || n_t <= 0 || G <= 0 || G > 48)
+                  int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
+                  long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream) {
+  if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !so || !sq || n_s <= 0 ||
+      n_s > 65536 || !d_base || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace ||
+      n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
-  ImgArgs A{(const float2*)D, d_rows, d_mask, sc_off, (const int2*)sc_meta, d_base, n_filled, sfine,
-            f2c, (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out, status};
+  if ((reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
+    return DSB_E_ARG;
+  const int stride = (n_s + 1) & ~1;
+  const long long rows = workspace_bytes / ((long long)stride * 8);
+  if (rows <= 0) return DSB_E_CAPACITY;
+  int cap = (int)std::min<long long>(rows, 1 << 30);
+  if (max_blocks > 0) cap = std::min(cap, max_blocks);
+  ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, so,
+            (const uint8_t*)sq, n_s, stride, d_base, n_filled, sfine, f2c,
+            (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
+            (float2*)workspace, status};
   switch (N) {
-    case 64: return launch_image<64, 1>(A, max_clusters, stream);
-    case 256: return launch_image<256, 2>(A, max_clusters, stream);
+    case 64: return launch_image<64>(A, cap, stream);
+    case 256: return launch_image<256>(A, cap, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

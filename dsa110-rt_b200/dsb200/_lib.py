@@ -20,7 +20,7 @@ DT_INT8, DT_F16, DT_F32 = 0, 1, 2
 
 _c_int, _c_ll, _c_float, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_float, ctypes.c_void_p
 
-# name -> argtypes (all return c_int except where noted)
+# name -> argtypes (all return c_int except those in _RESTYPES)
 _SIGNATURES = {
     "dsb_version": [],
     "dsb_unpack_int4": [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp],
@@ -39,9 +39,11 @@ _SIGNATURES = {
                         _vp, _c_ll, _c_ll, _c_ll, _c_int, _c_int, _c_int, _vp, _c_int, _c_int,
                         _c_int, _c_int, _vp],
     "dsb_stage1_block_size": [],
-    "dsb_image_cluster_size": [_c_int],
-    "dsb_image_fft": [_vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
-                      _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],
+    "dsb_image_fold": [_c_int],
+    "dsb_image_workspace_bytes": [_c_int, _c_int],
+    "dsb_image_fft": [_vp, _c_ll, _c_ll, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _vp,
+                      _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp,
+                      _c_ll, _c_int, _vp, _vp],
     "dsb_combine_rows": [_vp, _c_ll, _c_ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
                          _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp],
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
@@ -58,6 +60,8 @@ _SIGNATURES = {
                    _c_int, _c_float, _vp, _c_int, _c_int, _vp, _vp],
     "dsb_clipped_std": [_vp, _c_int, _c_int, _c_float, _c_int, _vp, _vp],
 }
+
+_RESTYPES = {"dsb_image_workspace_bytes": _c_ll}
 
 _lib: Optional[ctypes.CDLL] = None
 
@@ -77,7 +81,7 @@ def lib() -> ctypes.CDLL:
         for name, args in _SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = _c_int
+            fn.restype = _RESTYPES.get(name, _c_int)
         L.dsb_strerror.argtypes = [_c_int]
         L.dsb_strerror.restype = ctypes.c_char_p
         _lib = L

@@ -136,10 +136,77 @@ class Tables:
     hc_off: np.ndarray              # combine CSR over half cells
     e_g: np.ndarray
     e_cell: np.ndarray
-    sc_off: np.ndarray              # (CL + 1) image-kernel scatter entries per cluster rank
-    sc_meta: np.ndarray             # (n, 2) int32 {cell | g<<16 | mirror<<31, smem target}
+    img: "ImageTables"              # tables of the fused combine + FFT kernel
     twiddles: np.ndarray            # (N,) complex64 exp(+2 pi i e / N)
     mask: np.ndarray                # (N, N) float32
+
+
+@dataclass
+class ImageTables:
+    """Tables of dsb_image_fft: the distinct non-zero half cells S and how
+    every pattern cell of every chgroup lands on them."""
+    n_s: int
+    c_meta: np.ndarray      # (sum n_filled) uint32: s | conj << 16 | g << 17
+    cell_base: np.ndarray   # (G + 1) int32
+    c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
+    so: np.ndarray          # (N/2 * LC + 1) int32
+    sq: np.ndarray          # (n_s) uint8: q | packed << 2 | parity(u + w) << 3
+
+
+def build_image_tables(pats, N: int) -> ImageTables:
+    """Half-spectrum cell tables for dsb_image_fft.  Pattern cell (u, w) of
+    chgroup g adds to half cell (u, w) when w <= N/2 and, conjugated, to its
+    mirror ((N-u) % N, (N-w) % N) when that column is <= N/2 (both for
+    w = 0 and w = N/2): the Hermitian fold of fused_combine_cuda.py:560-620."""
+    fold = int(_lib.lib().dsb_image_fold(N))
+    if fold <= 0:
+        raise ValueError(f"dsb_image_fft does not support N={N}")
+    LC, NC = N // fold, N // 2
+    G = len(pats)
+    if G > 63:
+        raise ValueError("dsb_image_fft supports at most 63 chgroups")
+    us, ws, gs, ks = [], [], [], []
+    for g, p in enumerate(pats):
+        us.append(p.ix_row.astype(np.int64))
+        ws.append(p.ix_col.astype(np.int64))
+        gs.append(np.full(p.ix_row.size, g, np.int64))
+        ks.append(np.arange(p.ix_row.size, dtype=np.int64))
+    u, w, g, k = (np.concatenate(x) for x in (us, ws, gs, ks))
+    if k.size and int(k.max()) >= 1 << 16:
+        raise ValueError("dsb_image_fft needs fewer than 65536 cells per chgroup")
+    direct = w <= N // 2
+    um, wm = (N - u) % N, (N - w) % N
+    mirror = wm <= N // 2
+    # first target: direct if valid, else the mirror (conjugated)
+    t1u = np.where(direct, u, um)
+    t1w = np.where(direct, w, wm)
+    t1c = (~direct).astype(np.int64)
+    both = direct & mirror
+    t2u, t2w = um[both], wm[both]
+    allu = np.concatenate([t1u, t2u])
+    allw = np.concatenate([t1w, t2w])
+    packed = (allw == N // 2).astype(np.int64)
+    wp = np.where(packed == 1, 0, allw)
+    key = ((wp * LC + allu % LC) * fold + allu // LC) * 2 + packed
+    ukey, inv = np.unique(key, return_inverse=True)
+    n_s = int(ukey.size)
+    if n_s >= 1 << 16:
+        raise ValueError("dsb_image_fft needs fewer than 65536 distinct half cells")
+    s_pk = ukey & 1
+    s_q = (ukey >> 1) % fold
+    s_slot = (ukey >> 1) // fold          # wp * LC + n'
+    s_wp, s_n = s_slot // LC, s_slot % LC
+    s_u = s_n + LC * s_q
+    s_w = np.where(s_pk == 1, N // 2, s_wp)
+    sq = (s_q | (s_pk << 2) | (((s_u + s_w) & 1) << 3)).astype(np.uint8)
+    so = np.zeros(NC * LC + 1, np.int64)
+    so[1:] = np.cumsum(np.bincount(s_slot, minlength=NC * LC))
+    n1 = u.size
+    c_meta = (inv[:n1] | (t1c << 16) | (g << 17)).astype(np.uint32)
+    c2 = np.stack([k[both] | (g[both] << 16), inv[n1:] | (1 << 16)], axis=1).astype(np.int32)
+    cell_base = np.concatenate([[0], np.cumsum([p.ix_row.size for p in pats])]).astype(np.int32)
+    return ImageTables(n_s=n_s, c_meta=c_meta, cell_base=cell_base,
+                       c2=np.ascontiguousarray(c2.reshape(-1, 2)), so=so.astype(np.int32), sq=sq)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -221,29 +288,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     hc_off[1:] = np.cumsum([len(x) for x in ent])
     e_g = np.asarray([g for x in ent for g, _ in x], np.int32)
     e_cell = np.asarray([k for x in ent for _, k in x], np.int32)
-    # image-kernel scatter lists: rank r owns half-cell columns [r*CW, ...);
-    # entry = {cell | g << 16 | mirror << 31, shared-memory target wl*(N+1) + u}
-    CL = int(_lib.lib().dsb_image_cluster_size(N)) or 1
-    CW = -(-nh // CL)
-    sc_off = np.zeros(CL + 1, np.int64)
-    sc_meta = []
-    for r in range(CL):
-        lo, hi = r * CW, min(nh, (r + 1) * CW)
-        for g, p in enumerate(pats):
-            u = p.ix_row.astype(np.int64)
-            w = p.ix_col.astype(np.int64)
-            k = np.arange(u.size, dtype=np.int64)
-            for mirror in (0, 1):
-                uu, ww = ((N - u) % N, (N - w) % N) if mirror else (u, w)
-                sel = (ww >= lo) & (ww < hi)
-                m = np.empty((int(sel.sum()), 2), np.int64)
-                m[:, 0] = k[sel] | (g << 16) | (mirror << 31)
-                m[:, 1] = (ww[sel] - lo) * (N + 1) + uu[sel]
-                sc_meta.append(m)
-        sc_off[r + 1] = sum(x.shape[0] for x in sc_meta)
-    if int(n_filled.max()) >= 1 << 16 or G > 1 << 15:
-        raise ValueError("image scatter entries need cells < 65536 and G < 32768")
-    sc_meta = np.concatenate(sc_meta).astype(np.uint32).view(np.int32)
+    img = build_image_tables(pats, N)
     mask = compute_edge_mask(n_grid=N, kernel_support=1)
     e = np.arange(N)
     tw = np.exp(2j * np.pi * e / N).astype(np.complex64)
@@ -256,7 +301,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
                   shift1=np.ascontiguousarray(shift1), shift2=shift2.astype(np.int32),
                   d_base=d_base.astype(np.int32), n_rows_d=int(n_filled.sum() * n_coarse),
                   sfine=sfine.astype(np.int32), hc_off=hc_off.astype(np.int32), e_g=e_g,
-                  e_cell=e_cell, sc_off=sc_off.astype(np.int32), sc_meta=sc_meta,
+                  e_cell=e_cell, img=img,
                   twiddles=tw, mask=mask.astype(np.float32))
 
 
@@ -283,7 +328,14 @@ class SearchPipeline:
         self.d_row_off, self.d_row_bls = d(T.row_off), d(T.row_bls)
         self.d_rowtab, self.d_blk_g, self.d_blk_c0 = d(T.rowtab), d(T.blk_g), d(T.blk_c0)
         self.d_cell_base = d(T.cell_base)
-        self.d_sc_off, self.d_sc_meta = d(T.sc_off), d(T.sc_meta)
+        it = T.img
+        self.d_img_cmeta = d(it.c_meta.view(np.int32))
+        self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
+        self.d_img_so, self.d_img_sq = d(it.so), d(it.sq)
+        ws_bytes = int(_lib.lib().dsb_image_workspace_bytes(cfg.n_grid, it.n_s))
+        if ws_bytes <= 0:
+            raise ValueError(f"dsb_image_fft does not support N={cfg.n_grid}")
+        self.img_ws = torch.empty(ws_bytes // 4, dtype=torch.float32, device=self.dev)
         self.d_tw = d(T.twiddles)
         self.d_shift1, self.d_shift2 = d(T.shift1), d(T.shift2)
         self.d_dbase = d(T.d_base)
@@ -404,6 +456,24 @@ class SearchPipeline:
             self.sky_head = (self.sky_head + 1) % cfg.sky_window
             self.sky_seen += 1
 
+    def image(self, f0: int, n_f: int, t0: int, n_t: int, out: torch.Tensor,
+              max_blocks: int = 0) -> None:
+        """Fused combine + irfft2 (fftshifted) of fine DMs [f0, f0 + n_f) at
+        absolute times [t0, t0 + n_t) from the stage-2 ring into ``out``
+        (n_f, n_t, N, N) float32."""
+        cfg, T, it = self.cfg, self.tab, self.tab.img
+        N = cfg.n_grid
+        if out.shape != (n_f, n_t, N, N) or out.dtype != torch.float32 or not out.is_contiguous():
+            raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
+        _lib.check(_lib.lib().dsb_image_fft(
+            _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_img_cmeta),
+            _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
+            _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq), it.n_s, _lib.ptr(self.d_dbase),
+            _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
+            _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
+            _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),
+            _lib.stream_of(self.dev)), "dsb_image_fft")
+
     def _search(self, jc: int, collect: bool = True) -> None:
         cfg, T = self.cfg, self.tab
         C, te, N = cfg.chunk_tiles, cfg.t_edge, cfg.n_grid
@@ -415,12 +485,7 @@ class SearchPipeline:
             nf = min(cfg.fdm_batch, nfine - f0)
             img = self.img[:nf]
             with self._mark("image"):
-                _lib.check(_lib.lib().dsb_image_fft(
-                    _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_sc_off),
-                    _lib.ptr(self.d_sc_meta), _lib.ptr(self.d_dbase),
-                    _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
-                    _lib.ptr(self.d_tw), f0, nf, cfg.band.n_chgroup, N, t0, nt, 1, _lib.ptr(img),
-                    0, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_image_fft")
+                self.image(f0, nf, t0, nt, img)
             with self._mark("layer1"):
                 samp = img.reshape(nf, nt, N * N)[:, self.l1_t][:, :, self.l1_pix].reshape(nf, -1)
                 sig = sigma_clipped_std_batched(samp)

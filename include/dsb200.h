@@ -162,20 +162,30 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * GpuImager.process_cube (src/dsart/image/fused_combine_cuda.py:1359,
  * src/dsart/image/imager_gpu.py:575-605): for each (fine DM f0+fl, time t0+t)
  * the Hermitian half spectrum is combined from the time-major stage-2 ring
- * into shared memory and transformed there; out (n_f, n_t, N, N) float32 =
- * irfft2(G_h) with 1/N^2 normalisation.  Half cells are split over the
- * dsb_image_cluster_size(N) CTAs of a cluster by column: rank r owns columns
- * [r*CW, ...), CW = ceil((N/2+1)/CL); rank r scatters the entries
- * sc_meta[sc_off[r] .. sc_off[r+1]) = {cell | g << 16 | mirror << 31,
- * target wl*(N+1) + u}: the value of chgroup g's coarse-DM slice at `cell`
- * (its conjugate for mirror entries) is added to half cell (u, r*CW + wl).
- * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256. */
-int dsb_image_cluster_size(int n_grid);
-int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const int* sc_off,
-                  const void* sc_meta, const int* d_base, const int* n_filled,
+ * and transformed on chip; out (n_f, n_t, N, N) float32 = irfft2(G_h) with
+ * 1/N^2 normalisation (fftshifted when fftshift != 0).
+ * Tables (built once per pattern set):
+ *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
+ *      (packed column w' = (w == N/2 ? 0 : w), u mod LC, u div LC), LC =
+ *      N / dsb_image_fold(N);
+ *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k of
+ *      chgroup g adds its value (conjugated if conj) to S entry s;
+ *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
+ *      w = N/2 that also land on their mirror);
+ *   so[(w' * LC + n') .. + 1]: S range of packed column w', folded row n';
+ *   sq[s] = (u div LC) | (w == N/2) << 2 | ((u + w) & 1) << 3.
+ * workspace: >= dsb_image_workspace_bytes(N, n_s) bytes, 16-byte aligned (one
+ * L2-resident row of S per resident CTA).  twiddles: (N) complex64
+ * exp(+2 pi i e/N).  Supported N: 64, 256; n_s must fit the kernel's
+ * shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY is returned. */
+int dsb_image_fold(int n_grid);
+long long dsb_image_workspace_bytes(int n_grid, int n_s);
+int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
+                  const int* cell_base, const void* c2, int n_c2, const int* so,
+                  const unsigned char* sq, int n_s, const int* d_base, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
-                  int N, long long t0, int n_t, int fftshift, void* out, int max_clusters,
-                  int* status, cudaStream_t stream);
+                  int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
+                  long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream);
 
 /* ---- a13/a14: edge mask x Layer-1 normalisation into the detector cube -----
  * Replaces the mask multiply + cube write of GpuImager.process_cube

@@ -13,7 +13,8 @@ HEADER = os.path.join(ROOT, "include", "dsb200.h")
 
 def _declared():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(dsb_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(dsb_\w+)\s*\(", src,
+                                 re.M)))
 
 
 def test_header_declares_entry_points():

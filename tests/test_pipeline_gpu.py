@@ -120,12 +120,7 @@ def test_image_fft_matches_combine_and_irfft2(dev, N):
     nf, nt, t0 = 5, 20, 37
     out = torch.empty((nf, nt, N, N), dtype=torch.float32, device=dev)
     L = _lib.lib()
-    _lib.check(L.dsb_image_fft(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1, _lib.ptr(pipe.d_sc_off),
-                               _lib.ptr(pipe.d_sc_meta),
-                               _lib.ptr(pipe.d_dbase), _lib.ptr(pipe.d_nfilled),
-                               _lib.ptr(pipe.d_sfine), _lib.ptr(pipe.d_f2c), _lib.ptr(pipe.d_tw),
-                               1, nf, band.n_chgroup, N, t0, nt, 1, _lib.ptr(out), 3,
-                               _lib.ptr(pipe.status), _lib.stream_of(dev)), "image")
+    pipe.image(1, nf, t0, nt, out, max_blocks=3)
     gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
     _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1,
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
