@@ -131,8 +131,10 @@ struct ImgArgs {
   const int* cell_base;     // (G + 1)
   const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
   int n_c2;
-  const int* so;            // (N/2 * LC + 1) S entries of (packed column, folded row)
-  const uint8_t* sq;        // (n_s) q | packed << 2 | parity(u + w) << 3
+  const int* corder;        // (N/2) packed columns in work order (balanced over groups)
+  const int* so;            // (N/2 * C1 + 1) S entries of (packed column, lane j)
+  const uint16_t* sq;       // (n_s) q | packed << 2 | parity(u + w) << 3 | (u mod LC) << 4
+                            //       | last entry of its folded slot << 10
   int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
   const int* d_base;        // (G)
   const int* n_filled;      // (G)
@@ -165,7 +167,8 @@ struct ImgGeom {
   static_assert(C1 * C1 == LC && RR * RR == N, "unsupported size");
   static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
-  static constexpr size_t SMEM = (size_t)BUF * 8 + (size_t)N * 8 + IMG_MAX_G * 8 +
+  // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases
+  static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
                                  (IMG_MAX_G + 1) * 4;
 };
 
@@ -177,12 +180,20 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   float2* buf = reinterpret_cast<float2*>(smem_raw);  // S in step 1, columns in 2-3
   float2* tw = buf + Gm::BUF;
-  const float2** s_slice = reinterpret_cast<const float2**>(tw + N);
+  // twiddles laid out so that the lanes of a group read consecutive slots:
+  // rtw[x1*RR + j] = W_N^(j x1), ctw[m1*C1 + j] = W_LC^(j m1)
+  float2* rtw = tw + N;
+  float2* ctw = rtw + RR * RR;
+  const float2** s_slice = reinterpret_cast<const float2**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   for (int i = tid; i < N; i += THREADS) tw[i] = A.tw[i];
+  for (int i = tid; i < RR * RR; i += THREADS)
+    rtw[i] = A.tw[((i % RR) * (i / RR)) & (N - 1)];
+  for (int i = tid; i < C1 * C1; i += THREADS)
+    ctw[i] = A.tw[((i % C1) * (i / C1) * (N / LC)) & (N - 1)];
   for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
 
   float2* ws = A.ws + (size_t)blockIdx.x * A.ws_stride;
@@ -253,25 +264,38 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
 
     for (int p = 0; p < FOLD; ++p) {
       // ---- 2. folded column transforms of pass p (in place in buf) ----
-      for (int col = cgi; col < NC; col += Gm::CG) {
-        float2 y[C1];
-        const int* so = A.so + col * LC;
+      for (int ci = cgi; ci < NC; ci += Gm::CG) {
+        // fold column col's S entries into its LC slots of buf, lane j owning
+        // the slots n' = j (mod C1): its entries are one contiguous run
+        // sorted by slot, each slot written once (after its last entry)
+        const int col = __ldg(A.corder + ci);
+        float2* colp = buf + col;
 #pragma unroll
-        for (int k = 0; k < C1; ++k) {
-          const int n1 = cj + C1 * k;
-          const int r0 = __ldg(so + n1), r1 = __ldg(so + n1 + 1);
+        for (int k = 0; k < C1; ++k) colp[(cj + C1 * k) * P] = make_float2(0.f, 0.f);
+        {
+          const int e1 = __ldg(A.so + col * C1 + cj + 1);
           float2 acc = make_float2(0.f, 0.f);
-          for (int e = r0; e < r1; ++e) {
+#pragma unroll 4
+          for (int e = __ldg(A.so + col * C1 + cj); e < e1; ++e) {
             const int qq = __ldg(A.sq + e);
             const int rot = (qq & 3) * p + ((qq >> 2) & 1) + (((qq >> 3) & 1) ? shift_rot : 0);
             acc = cadd(acc, crot(ws[e], rot));
+            if (qq & 1024) {
+              colp[((qq >> 4) & (LC - 1)) * P] = acc;
+              acc = make_float2(0.f, 0.f);
+            }
           }
-          y[k] = cmul(acc, tw[(n1 * p) & (N - 1)]);
+        }
+        float2 y[C1];
+#pragma unroll
+        for (int k = 0; k < C1; ++k) {
+          const int n1 = cj + C1 * k;
+          y[k] = cmul(colp[n1 * P], tw[(n1 * p) & (N - 1)]);
         }
         idftR<C1>(y);
 #pragma unroll
-        for (int m1 = 1; m1 < C1; ++m1) y[m1] = cmul(y[m1], tw[(cj * m1 * (N / LC)) & (N - 1)]);
-        float2* colp = buf + col;
+        for (int m1 = 1; m1 < C1; ++m1) y[m1] = cmul(y[m1], ctw[m1 * C1 + cj]);
+        __syncwarp(cmask);  // every lane has read its slots of the column
 #pragma unroll
         for (int m1 = 0; m1 < C1; ++m1) colp[((cj ^ m1) + C1 * m1) * P] = y[m1];
         __syncwarp(cmask);
@@ -309,7 +333,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         }
         idftR<RR>(a);
 #pragma unroll
-        for (int x1 = 1; x1 < RR; ++x1) a[x1] = cmul(a[x1], tw[(rj * x1) & (N - 1)]);
+        for (int x1 = 1; x1 < RR; ++x1) a[x1] = cmul(a[x1], rtw[x1 * RR + rj]);
         __syncwarp(rmask);  // every lane has read the pair's rows
 #pragma unroll
         for (int x1 = 0; x1 < RR; ++x1) reg[rj * RR + (x1 ^ rj)] = a[x1];
@@ -401,12 +425,13 @@ long long dsb_image_workspace_bytes(int n_grid, int n_s) {
 }
 
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
-                  const int* cell_base, const void* c2, int n_c2, const int* so,
-                  const unsigned char* sq, int n_s, const int* d_base, const int* n_filled,
+                  const int* cell_base, const void* c2, int n_c2, const int* corder,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream) {
-  if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !so || !sq || n_s <= 0 ||
+  if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq ||
+      n_s <= 0 ||
       n_s > 65536 || !d_base || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace ||
       n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
@@ -417,8 +442,8 @@ int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsig
   if (rows <= 0) return DSB_E_CAPACITY;
   int cap = (int)std::min<long long>(rows, 1 << 30);
   if (max_blocks > 0) cap = std::min(cap, max_blocks);
-  ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, so,
-            (const uint8_t*)sq, n_s, stride, d_base, n_filled, sfine, f2c,
+  ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, corder,
+            so, (const uint16_t*)sq, n_s, stride, d_base, n_filled, sfine, f2c,
             (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
             (float2*)workspace, status};
   switch (N) {

@@ -149,8 +149,9 @@ class ImageTables:
     c_meta: np.ndarray      # (sum n_filled) uint32: s | conj << 16 | g << 17
     cell_base: np.ndarray   # (G + 1) int32
     c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
-    so: np.ndarray          # (N/2 * LC + 1) int32
-    sq: np.ndarray          # (n_s) uint8: q | packed << 2 | parity(u + w) << 3
+    corder: np.ndarray      # (N/2) int32: packed columns in work order
+    so: np.ndarray          # (N/2 * C1 + 1) int32: S range of (packed column, n' mod C1)
+    sq: np.ndarray          # (n_s) uint16: q | packed << 2 | parity << 3 | n' << 4 | last << 10
 
 
 def build_image_tables(pats, N: int) -> ImageTables:
@@ -187,26 +188,46 @@ def build_image_tables(pats, N: int) -> ImageTables:
     allw = np.concatenate([t1w, t2w])
     packed = (allw == N // 2).astype(np.int64)
     wp = np.where(packed == 1, 0, allw)
-    key = ((wp * LC + allu % LC) * fold + allu // LC) * 2 + packed
+    C1 = int(round(np.sqrt(LC)))
+    n1 = allu % LC
+    # slot order inside a column: lane j = n' mod C1 first, then n' div C1
+    lane_slot = (n1 % C1) * C1 + n1 // C1
+    key = ((wp * LC + lane_slot) * fold + allu // LC) * 2 + packed
     ukey, inv = np.unique(key, return_inverse=True)
     n_s = int(ukey.size)
     if n_s >= 1 << 16:
         raise ValueError("dsb_image_fft needs fewer than 65536 distinct half cells")
     s_pk = ukey & 1
     s_q = (ukey >> 1) % fold
-    s_slot = (ukey >> 1) // fold          # wp * LC + n'
-    s_wp, s_n = s_slot // LC, s_slot % LC
+    s_slot = (ukey >> 1) // fold          # wp * LC + lane_slot
+    s_wp, s_ls = s_slot // LC, s_slot % LC
+    s_n = (s_ls % C1) * C1 + s_ls // C1   # back to n'
     s_u = s_n + LC * s_q
     s_w = np.where(s_pk == 1, N // 2, s_wp)
-    sq = (s_q | (s_pk << 2) | (((s_u + s_w) & 1) << 3)).astype(np.uint8)
-    so = np.zeros(NC * LC + 1, np.int64)
-    so[1:] = np.cumsum(np.bincount(s_slot, minlength=NC * LC))
+    last = np.ones(n_s, np.int64)
+    last[:-1] = (s_slot[1:] != s_slot[:-1]).astype(np.int64)
+    sq = (s_q | (s_pk << 2) | (((s_u + s_w) & 1) << 3) | (s_n << 4) | (last << 10)
+          ).astype(np.uint16)
+    so = np.zeros(NC * C1 + 1, np.int64)
+    so[1:] = np.cumsum(np.bincount(s_wp * C1 + s_ls // C1, minlength=NC * C1))
+    # work order: columns by entry count, dealt round-robin back and forth
+    # over the thread groups (group i takes corder[i], corder[i + n_groups], ...)
+    cnt = np.bincount(s_wp, minlength=NC)
+    n_groups = 256 // C1
+    by = np.argsort(-cnt, kind="stable")
+    corder = np.empty(NC, np.int64)
+    for r in range(0, NC, n_groups):
+        chunk = by[r:r + n_groups]
+        if (r // n_groups) % 2:
+            chunk = chunk[::-1]
+        corder[r:r + chunk.size] = chunk
     n1 = u.size
     c_meta = (inv[:n1] | (t1c << 16) | (g << 17)).astype(np.uint32)
     c2 = np.stack([k[both] | (g[both] << 16), inv[n1:] | (1 << 16)], axis=1).astype(np.int32)
     cell_base = np.concatenate([[0], np.cumsum([p.ix_row.size for p in pats])]).astype(np.int32)
     return ImageTables(n_s=n_s, c_meta=c_meta, cell_base=cell_base,
-                       c2=np.ascontiguousarray(c2.reshape(-1, 2)), so=so.astype(np.int32), sq=sq)
+                       c2=np.ascontiguousarray(c2.reshape(-1, 2)), corder=corder.astype(np.int32),
+                       so=so.astype(np.int32), sq=sq)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -331,7 +352,8 @@ class SearchPipeline:
         it = T.img
         self.d_img_cmeta = d(it.c_meta.view(np.int32))
         self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
-        self.d_img_so, self.d_img_sq = d(it.so), d(it.sq)
+        self.d_img_corder, self.d_img_so = d(it.corder), d(it.so)
+        self.d_img_sq = d(it.sq.view(np.int16))
         ws_bytes = int(_lib.lib().dsb_image_workspace_bytes(cfg.n_grid, it.n_s))
         if ws_bytes <= 0:
             raise ValueError(f"dsb_image_fft does not support N={cfg.n_grid}")
@@ -468,7 +490,7 @@ class SearchPipeline:
         _lib.check(_lib.lib().dsb_image_fft(
             _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
-            _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq), it.n_s, _lib.ptr(self.d_dbase),
+            _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq), it.n_s, _lib.ptr(self.d_dbase),
             _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
             _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),

@@ -166,14 +166,17 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * 1/N^2 normalisation (fftshifted when fftshift != 0).
  * Tables (built once per pattern set):
  *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
- *      (packed column w' = (w == N/2 ? 0 : w), u mod LC, u div LC), LC =
- *      N / dsb_image_fold(N);
+ *      (packed column w' = (w == N/2 ? 0 : w), n' mod C1, n' div C1, u div LC,
+ *      w == N/2) with n' = u mod LC, LC = N / dsb_image_fold(N), C1*C1 = LC;
  *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k of
  *      chgroup g adds its value (conjugated if conj) to S entry s;
  *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
  *      w = N/2 that also land on their mirror);
- *   so[(w' * LC + n') .. + 1]: S range of packed column w', folded row n';
- *   sq[s] = (u div LC) | (w == N/2) << 2 | ((u + w) & 1) << 3.
+ *   corder: (N/2) packed columns in the order the kernel's thread groups
+ *      take them (any permutation; balance dense and sparse columns);
+ *   so[w'*C1 + j .. + 1]: S range of packed column w', n' mod C1 = j;
+ *   sq[s] = (u div LC) | (w == N/2) << 2 | ((u + w) & 1) << 3 | n' << 4 |
+ *      (s is the last entry of its (w', n')) << 10.
  * workspace: >= dsb_image_workspace_bytes(N, n_s) bytes, 16-byte aligned (one
  * L2-resident row of S per resident CTA).  twiddles: (N) complex64
  * exp(+2 pi i e/N).  Supported N: 64, 256; n_s must fit the kernel's
@@ -181,8 +184,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
 int dsb_image_fold(int n_grid);
 long long dsb_image_workspace_bytes(int n_grid, int n_s);
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
-                  const int* cell_base, const void* c2, int n_c2, const int* so,
-                  const unsigned char* sq, int n_s, const int* d_base, const int* n_filled,
+                  const int* cell_base, const void* c2, int n_c2, const int* corder,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream);

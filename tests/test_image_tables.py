@@ -50,7 +50,9 @@ def _emulate(T, slices, N, fftshift):
     q = (T.sq & 3).astype(np.int64)
     pk = ((T.sq >> 2) & 1).astype(np.int64)
     par = ((T.sq >> 3) & 1).astype(np.int64)
-    slot = np.repeat(np.arange(NC * LC), np.diff(T.so))
+    C1 = int(round(np.sqrt(LC)))
+    col = np.repeat(np.arange(NC * C1), np.diff(T.so)) // C1
+    slot = col * LC + ((T.sq >> 4) & (LC - 1)).astype(np.int64)
     for p in range(fold):
         rot = q * p + pk + (2 * par if fftshift else 0)
         y = np.zeros(NC * LC, np.complex128)
@@ -100,7 +102,18 @@ def test_image_tables_layout():
     T = build_image_tables(pats, N)
     LC = N // 4
     assert T.so[0] == 0 and T.so[-1] == T.n_s and np.all(np.diff(T.so) >= 0)
-    assert T.so.size == N // 2 * LC + 1
+    C1 = 8
+    assert T.so.size == N // 2 * C1 + 1
+    assert sorted(T.corder.tolist()) == list(range(N // 2))
+    # lane j = n' mod C1 of column w' owns exactly the entries of its run
+    lane = np.repeat(np.arange(N // 2 * C1), np.diff(T.so)) % C1
+    n1 = (T.sq >> 4) & (LC - 1)
+    assert np.array_equal(n1 % C1, lane)
+    # "last" marks the final entry of each (column, n') run of equal slots
+    col = np.repeat(np.arange(N // 2 * C1), np.diff(T.so)) // C1
+    slot = col * LC + n1
+    last = np.append(slot[1:] != slot[:-1], True)
+    assert np.array_equal(((T.sq >> 10) & 1).astype(bool), last)
     assert T.cell_base[-1] == T.c_meta.size
     assert T.n_s <= LC * (N // 2 + 2)          # fits the kernel's shared buffer
     # every S entry is hit by at least one pattern cell
