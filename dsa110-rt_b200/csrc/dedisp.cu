@@ -122,20 +122,24 @@ __global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int d
 }
 
 // Pipeline stage 1 over per-subband gridded rows, time-major rings:
-//   Y[(t & y_mask) * y_rows + row],  D[(t & d_mask) * d_rows + drow].
-// One thread per cell of one chgroup (blocks never straddle chgroups), one
-// grid row per coarse DM; every thread walks time, so threads that read the
-// same summed channel read the same time sample of adjacent rows.
+//   Y[(t & y_mask) * y_rows + y_base[g] + s * pitch[g] + cell],
+//   D[(t & d_mask) * d_rows + d_base[g] + d * pitch[g] + cell].
+// Rows are dense per (chgroup, subband) and (chgroup, coarse DM) with an
+// even pitch, so one thread owns two adjacent cells (16-byte loads and
+// stores) and the 32 lanes of a warp read 512 contiguous bytes.  Blocks
+// never straddle chgroups; one grid row per coarse DM.  Time is walked in
+// tiles of S1_TT samples: for each subband the tile's S1_TT loads are
+// independent.
 struct S1Args {
   const float2* Y;
   long long y_rows, y_mask;
-  const int* rowtab;      // [cell_base[g]*ceff + s*nf[g] + cell] = Y row or -1
   const int* blk_g;       // chgroup of each block
-  const int* blk_c0;      // first cell of each block
-  const int* cell_base;   // (G) first global cell of the chgroup
+  const int* blk_c0;      // first cell of each block (even)
+  const int* y_base;      // (G) first Y row of the chgroup (even)
+  const int* pitch;       // (G) even row pitch between subbands / coarse DMs
   const int* shift1;      // (G, ceff, n_dm)
   const int* shift2;      // (G, n_dm)
-  const int* d_base;      // (G) first D row of the chgroup
+  const int* d_base;      // (G) first D row of the chgroup (even)
   const int* n_filled;    // (G)
   float2* D;
   long long d_rows, d_mask;
@@ -147,55 +151,78 @@ struct S1Args {
 
 constexpr int S1_THREADS = 128;
 constexpr int S1_MAX_C = 64;
+constexpr int S1_TT = 8;
 
 __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
-  __shared__ int s_row[S1_MAX_C][S1_THREADS];
   __shared__ int s_sh[S1_MAX_C];
   const int g = A.blk_g[blockIdx.x];
   const int d = blockIdx.y;
   const int nf = A.n_filled[g];
-  const int cl = A.blk_c0[blockIdx.x] + threadIdx.x;
+  const int pitch = A.pitch[g];
+  const int cl = A.blk_c0[blockIdx.x] + 2 * threadIdx.x;
   const int ceff = A.ceff;
   for (int s = threadIdx.x; s < ceff; s += S1_THREADS)
     s_sh[s] = A.shift1[(g * ceff + s) * A.n_dm + d];
-  const bool live = cl < nf;
-  const int* rt = A.rowtab + (long long)A.cell_base[g] * ceff;
-  for (int s = 0; s < ceff; ++s) s_row[s][threadIdx.x] = live ? rt[(long long)s * nf + cl] : -1;
   __syncthreads();
-  if (!live) return;
-  const long long drow = (long long)A.d_base[g] + (long long)d * nf + cl;
-  double mr = 0.0, mi = 0.0;
+  if (cl >= nf) return;  // cl + 1 <= pitch - 1: a pad cell at most
+  const float4* Y4 = reinterpret_cast<const float4*>(A.Y);
+  float4* D4 = reinterpret_cast<float4*>(A.D);
+  const long long y_rows2 = A.y_rows / 2, d_rows2 = A.d_rows / 2;
+  const long long ycol2 = (A.y_base[g] + cl) / 2;
+  const long long drow = (long long)A.d_base[g] + (long long)d * pitch + cl;
+  double mr[2] = {0.0, 0.0}, mi[2] = {0.0, 0.0};
   const bool sub = A.sky_ring && A.sky_subtract && A.sky_count > 0;
   if (sub) {
-    for (int w = 0; w < A.sky_count; ++w) {
-      const double2 r = A.sky_ring[drow * A.sky_window + w];
-      mr += r.x;
-      mi += r.y;
+    for (int c = 0; c < 2; ++c) {
+      for (int w = 0; w < A.sky_count; ++w) {
+        const double2 r = A.sky_ring[(drow + c) * A.sky_window + w];
+        mr[c] += r.x;
+        mi[c] += r.y;
+      }
+      mr[c] /= A.sky_count;
+      mi[c] /= A.sky_count;
     }
-    mr /= A.sky_count;
-    mi /= A.sky_count;
   }
   const int sh2 = A.shift2[g * A.n_dm + d];
-  double sr = 0.0, si = 0.0;
-  for (int t = 0; t < A.n_t; ++t) {
+  double sr[2] = {0.0, 0.0}, si[2] = {0.0, 0.0};
+  for (int t = 0; t < A.n_t; t += S1_TT) {
     const long long ta = A.t0 + t;
-    float re = 0.f, im = 0.f;
+    float4 acc[S1_TT];
+#pragma unroll
+    for (int i = 0; i < S1_TT; ++i) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int s = 0; s < ceff; ++s) {
-      const int row = s_row[s][threadIdx.x];
-      if (row >= 0) {
-        const float2 x = A.Y[((ta + s_sh[s]) & A.y_mask) * A.y_rows + row];
-        re += x.x;
-        im += x.y;
+      const long long col = ycol2 + (long long)s * (pitch / 2);
+      const long long p0 = ta + s_sh[s];
+#pragma unroll
+      for (int i = 0; i < S1_TT; ++i) {
+        const float4 v = Y4[((p0 + i) & A.y_mask) * y_rows2 + col];
+        acc[i].x += v.x;
+        acc[i].y += v.y;
+        acc[i].z += v.z;
+        acc[i].w += v.w;
       }
     }
-    sr += re;
-    si += im;
-    float2 o = make_float2(re, im);
-    if (sub) o = make_float2((float)((double)re - mr), (float)((double)im - mi));
-    A.D[((ta + sh2) & A.d_mask) * A.d_rows + drow] = o;
+#pragma unroll
+    for (int i = 0; i < S1_TT; ++i) {
+      if (t + i < A.n_t) {
+        const float4 a = acc[i];
+        sr[0] += a.x;
+        si[0] += a.y;
+        sr[1] += a.z;
+        si[1] += a.w;
+        float4 o = a;
+        if (sub)
+          o = make_float4((float)((double)a.x - mr[0]), (float)((double)a.y - mi[0]),
+                          (float)((double)a.z - mr[1]), (float)((double)a.w - mi[1]));
+        D4[((ta + i + sh2) & A.d_mask) * d_rows2 + drow / 2] = o;
+      }
+    }
   }
-  if (A.sky_ring)
-    A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(sr / A.n_t, si / A.n_t);
+  if (A.sky_ring) {
+    A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(sr[0] / A.n_t, si[0] / A.n_t);
+    A.sky_ring[(drow + 1) * A.sky_window + A.sky_head] =
+        make_double2(sr[1] / A.n_t, si[1] / A.n_t);
+  }
 }
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? DSB_OK : DSB_E_CUDA; }
@@ -251,13 +278,17 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
 }
 
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
-                    const int* blk_g, const int* blk_c0, const int* rowtab, const int* cell_base,
+                    const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, long long d_rows, long long d_mask, long long t0, int n_t, int n_dm,
                     int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
                     int sky_subtract, cudaStream_t stream) {
-  if (!Y || !D || !blk_g || !blk_c0 || !rowtab || !cell_base || !shift1 || !shift2 ||
+  if (!Y || !D || !blk_g || !blk_c0 || !y_base || !pitch || !shift1 || !shift2 ||
       !d_base || !n_filled || n_t <= 0 || n_dm <= 0 || ceff <= 0)
+    return DSB_E_ARG;
+  // two cells per 16-byte access: rings 16-byte aligned, row counts even
+  if ((reinterpret_cast<uintptr_t>(Y) & 15) || (reinterpret_cast<uintptr_t>(D) & 15) ||
+      (y_rows & 1) || (d_rows & 1))
     return DSB_E_ARG;
   if (ceff > S1_MAX_C) return DSB_E_CAPACITY;
   if (sky_ring && (sky_window <= 0 || sky_head < 0 || sky_head >= sky_window ||
@@ -266,7 +297,7 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   if (n_blocks <= 0) return DSB_OK;
   S1Args A{};
   A.Y = (const float2*)Y; A.y_rows = y_rows; A.y_mask = y_mask;
-  A.rowtab = rowtab; A.blk_g = blk_g; A.blk_c0 = blk_c0; A.cell_base = cell_base;
+  A.blk_g = blk_g; A.blk_c0 = blk_c0; A.y_base = y_base; A.pitch = pitch;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
   A.D = (float2*)D; A.d_rows = d_rows; A.d_mask = d_mask;
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff;
@@ -277,6 +308,6 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   return launch_status();
 }
 
-int dsb_stage1_block_size(void) { return S1_THREADS; }
+int dsb_stage1_block_size(void) { return 2 * S1_THREADS; }
 
 }  // extern "C"

@@ -137,7 +137,7 @@ struct ImgArgs {
                             //       | last entry of its folded slot << 10
   int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
   const int* d_base;        // (G)
-  const int* n_filled;      // (G)
+  const int* d_pitch;       // (G) D rows between coarse DMs of a chgroup
   const int* sfine;         // (n_fine, G)
   const int* f2c;           // (n_fine)
   const float2* tw;         // (N) W_N^e = exp(+2 pi i e / N)
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     __syncthreads();  // the previous image is done with buf and s_slice
     for (int g = tid; g < A.G; g += THREADS)
       s_slice[g] = A.D + ((ta - A.sfine[(long long)f * A.G + g]) & A.d_mask) * A.d_rows +
-                   A.d_base[g] + (long long)c * A.n_filled[g];
+                   A.d_base[g] + (long long)c * A.d_pitch[g];
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
       for (int i = tid; i < A.ws_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -426,13 +426,13 @@ long long dsb_image_workspace_bytes(int n_grid, int n_s) {
 
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
                   const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* n_filled,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* d_pitch,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream) {
   if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq ||
       n_s <= 0 ||
-      n_s > 65536 || !d_base || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace ||
+      n_s > 65536 || !d_base || !d_pitch || !sfine || !f2c || !twiddles || !out || !workspace ||
       n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
   if ((reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
@@ -443,7 +443,7 @@ int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsig
   int cap = (int)std::min<long long>(rows, 1 << 30);
   if (max_blocks > 0) cap = std::min(cap, max_blocks);
   ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, corder,
-            so, (const uint16_t*)sq, n_s, stride, d_base, n_filled, sfine, f2c,
+            so, (const uint16_t*)sq, n_s, stride, d_base, d_pitch, sfine, f2c,
             (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
             (float2*)workspace, status};
   switch (N) {

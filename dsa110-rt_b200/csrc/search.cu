@@ -39,7 +39,7 @@ struct CombArgs {
   const int* e_g;        // chgroup
   const int* e_cell;     // cell within the chgroup (negative = mirror, stored as ~cell)
   const int* d_base;     // (G) first D row of each chgroup
-  const int* n_filled;   // (G)
+  const int* d_pitch;    // (G) D rows between coarse DMs of a chgroup
   const int* sfine;      // (n_fine_total, G) signed shifts
   const int* f2c;        // (n_fine_total) coarse index
   int f0, n_f, G, N;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
       int cell = A.e_cell[j];
       const bool mirror = cell < 0;
       if (mirror) cell = ~cell;
-      const long long row = (long long)A.d_base[g] + (long long)c * A.n_filled[g] + cell;
+      const long long row = (long long)A.d_base[g] + (long long)c * A.d_pitch[g] + cell;
       const long long ts0 = A.t0 + tt - A.sfine[(long long)f * A.G + g];
       const float2* src = A.D + row;
 #pragma unroll
@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   if (e >= inner) return;
   const long long fidx = e / npix, p = e % npix;
   const T* cube = x + fidx * f_stride + p;
+  // x * 1.0f == x exactly, so an absent mask costs one exact multiply
   const float mval = mask ? mask[e] : 1.0f;
   float si[K];
 #pragma unroll
@@ -312,9 +313,57 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   double run = 0.0;
   float last = 0.f;
   const int total = n + MAXW;  // cs length
+  // exact strict-'>' winner of the boxcars ending at ring slot q (the rare
+  // path: called only when the max over widths passed the threshold)
+  auto emit = [&](int q, int ta) {
+    float best = 0.f;
+    int win = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int w = 1 << k;
+      const int off = PL - w / 2;
+      const int slo = ((q - MAXW + off) % R + R) % R;
+      const int shi = ((q - MAXW + off + w) % R + R) % R;
+      const float s = (ring[shi] - ring[slo]) * si[k];
+      if (k == 0 || s > best) {
+        best = s;
+        win = k;
+      }
+    }
+    if (best > thr) {
+      const int slot = atomicAdd(count, 1);
+      if (slot < cap) cands[slot] = DetCand{ta - t_base, (int)e + pix_off, best, win};
+    }
+  };
   for (int J0 = 0; J0 < total; J0 += R) {
     // issue this block's R loads before any of them is consumed
+    const bool interior = J0 >= PL + 1 && J0 + R - 1 <= PL + n && J0 - MAXW >= t_base &&
+                          J0 + R - 1 - MAXW < t_base + n_out;
     float xin[R];
+    if (interior) {
+      // steady state: every sample loaded, every time an output; the screen
+      // is the max over widths (fmaxf skips NaN, so it never hides a value
+      // the strict-'>' chain of emit() would report)
+#pragma unroll
+      for (int q = 0; q < R; ++q) xin[q] = ldf<T>(cube, (long long)(J0 + q - 1 - PL) * t_stride);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        run += (double)(xin[q] * mval);
+        ring[q] = (float)run;
+        float best = -INFINITY;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int w = 1 << k;
+          const int off = PL - w / 2;
+          const int slo = ((q - MAXW + off) % R + R) % R;
+          const int shi = ((q - MAXW + off + w) % R + R) % R;
+          best = fmaxf(best, (ring[shi] - ring[slo]) * si[k]);
+        }
+        if (best > thr) emit(q, J0 + q - MAXW);
+      }
+      last = ring[R - 1];
+      continue;
+    }
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const int i = J0 + q - 1 - PL;
@@ -328,8 +377,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
         if (J <= PL) {
           v = 0.f;
         } else if (J <= PL + n) {
-          const float xv = mask ? xin[q] * mval : xin[q];
-          run += (double)xv;
+          run += (double)(xin[q] * mval);
           last = (float)run;
           v = last;
         } else {
@@ -337,27 +385,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
         }
         ring[q] = v;
         const int ta = J - MAXW;
-        if (ta >= t_base && ta < t_base + n_out) {
-          float best = 0.f;
-          int win = 0;
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int w = 1 << k;
-            const int off = PL - w / 2;
-            // cs index ta + off  -> ring slot (q - MAXW + off) mod R, etc.
-            const int slo = ((q - MAXW + off) % R + R) % R;
-            const int shi = ((q - MAXW + off + w) % R + R) % R;
-            const float s = (ring[shi] - ring[slo]) * si[k];
-            if (k == 0 || s > best) {
-              best = s;
-              win = k;
-            }
-          }
-          if (best > thr) {
-            const int slot = atomicAdd(count, 1);
-            if (slot < cap) cands[slot] = DetCand{ta - t_base, (int)e + pix_off, best, win};
-          }
-        }
+        if (ta >= t_base && ta < t_base + n_out) emit(q, ta);
       }
     }
   }
@@ -473,13 +501,13 @@ int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_
 }
 
 int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
-                     const int* e_g, const int* e_cell, const int* d_base, const int* n_filled,
+                     const int* e_g, const int* e_cell, const int* d_base, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
-  if (!D || !hc_off || !e_g || !e_cell || !d_base || !n_filled || !sfine || !f2c || !out)
+  if (!D || !hc_off || !e_g || !e_cell || !d_base || !d_pitch || !sfine || !f2c || !out)
     return DSB_E_ARG;
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
-  CombArgs A{(const float2*)D, d_stride, d_mask, hc_off, e_g, e_cell, d_base, n_filled, sfine,
+  CombArgs A{(const float2*)D, d_stride, d_mask, hc_off, e_g, e_cell, d_base, d_pitch, sfine,
              f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
   const int n_hc = N * (N / 2 + 1);
   dim3 grid((n_hc + 127) / 128, n_f);

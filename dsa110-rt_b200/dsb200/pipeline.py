@@ -124,13 +124,14 @@ class Tables:
     row_off: np.ndarray             # (n_rows_y + 1) CSR: baselines gridded into each Y row
     row_bls: np.ndarray
     n_rows_y: int
-    rowtab: np.ndarray              # stage 1: Y row of (g, s, cell) or -1
+    y_base: np.ndarray              # (G,) first Y row of each chgroup (even)
+    pitch: np.ndarray               # (G,) even row pitch between subbands / coarse DMs
     blk_g: np.ndarray               # stage-1 thread blocks: chgroup, first cell
     blk_c0: np.ndarray
     cell_base: np.ndarray           # (G,) first global cell of each chgroup
     shift1: np.ndarray              # (G, ceff, n_coarse) int32
     shift2: np.ndarray              # (G, n_coarse) int32
-    d_base: np.ndarray              # (G,)
+    d_base: np.ndarray              # (G,) first D row of each chgroup (even)
     n_rows_d: int
     sfine: np.ndarray               # (n_fine, G) int32
     hc_off: np.ndarray              # combine CSR over half cells
@@ -244,39 +245,31 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
         cims.append(cell_index_map_for(p, antpos_e, antpos_n, is_core_baseline_mask=core_mask,
                                        device=device))
     n_filled = np.asarray([p.n_filled for p in pats], np.int64)
-    # per-(g, s) Y rows: distinct cells hit by summed channel s, ascending
+    # dense rows with an even pitch per chgroup (two cells per 16-byte access):
+    # Y row of (g, s, cell) = y_base[g] + s*pitch[g] + cell, D row of
+    # (g, coarse DM d, cell) = d_base[g] + d*pitch[g] + cell; the correlator's
+    # group (g, s) writes every cell of its chgroup (0 where no baseline lands)
+    pitch = (n_filled + 1) // 2 * 2
+    y_base = np.concatenate([[0], np.cumsum(pitch * ceff)])
+    n_rows_y = int(y_base[-1])
     yoff = np.zeros(G * ceff, np.int64)
     ycnt = np.zeros(G * ceff, np.int64)
-    row_cell = []
-    row_g = []
-    row_s = []
-    row_cnt = []
+    row_cnt = np.zeros(n_rows_y, np.int64)
     row_bls = []
-    nrow = 0
     for g in range(G):
         for s in range(ceff):
             col = cims[g][:, s]
             valid = np.nonzero(col < n_filled[g])[0]
-            cells, k = np.unique(col[valid], return_inverse=True)
-            order = np.argsort(k, kind="stable")
-            row_bls.append(valid[order])
-            row_cnt.append(np.bincount(k, minlength=cells.size))
-            yoff[g * ceff + s] = nrow
-            ycnt[g * ceff + s] = cells.size
-            row_cell.append(cells)
-            row_g.append(np.full(cells.size, g))
-            row_s.append(np.full(cells.size, s))
-            nrow += cells.size
-    row_off = np.concatenate([[0], np.cumsum(np.concatenate(row_cnt))])
+            order = valid[np.argsort(col[valid], kind="stable")]
+            r0 = y_base[g] + s * pitch[g]
+            yoff[g * ceff + s] = r0
+            ycnt[g * ceff + s] = n_filled[g]
+            row_cnt[r0:r0 + n_filled[g]] = np.bincount(col[valid], minlength=int(n_filled[g]))
+            row_bls.append(order)
+    row_off = np.concatenate([[0], np.cumsum(row_cnt)])
     row_bls = np.concatenate(row_bls)
-    row_cell = np.concatenate(row_cell)
-    row_g = np.concatenate(row_g)
-    row_s = np.concatenate(row_s)
     cell_base = np.concatenate([[0], np.cumsum(n_filled)])
-    # stage-1 table: Y row of (chgroup, summed channel, cell) or -1, and the
-    # thread blocks (never straddling a chgroup)
-    rowtab = np.full(int(cell_base[-1]) * ceff, -1, np.int64)
-    rowtab[cell_base[row_g] * ceff + row_s * n_filled[row_g] + row_cell] = np.arange(nrow)
+    # stage-1 thread blocks (never straddling a chgroup)
     bs = int(_lib.lib().dsb_stage1_block_size())
     blk_g = np.concatenate([np.full(-(-int(n) // bs), g) for g, n in enumerate(n_filled)])
     blk_c0 = np.concatenate([np.arange(0, int(n), bs) for n in n_filled])
@@ -292,7 +285,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
                                       t_int_search_us=cfg.t_int_us, merge_coarse_rounding=True,
                                       band=band)
     n_coarse = cfg.coarse_dm.size
-    d_base = np.concatenate([[0], np.cumsum(n_filled * n_coarse)])[:-1]
+    d_base = np.concatenate([[0], np.cumsum(pitch * n_coarse)])
     # combine CSR over half cells (r, c), c in [0, N/2]
     nh = N // 2 + 1
     ent = [[] for _ in range(N * nh)]
@@ -316,11 +309,12 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled,
                   yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
                   row_off=row_off.astype(np.int32), row_bls=row_bls.astype(np.int32),
-                  n_rows_y=int(nrow), rowtab=rowtab.astype(np.int32),
+                  n_rows_y=n_rows_y, y_base=y_base[:-1].astype(np.int32),
+                  pitch=pitch.astype(np.int32),
                   blk_g=blk_g.astype(np.int32), blk_c0=blk_c0.astype(np.int32),
                   cell_base=cell_base[:-1].astype(np.int32),
                   shift1=np.ascontiguousarray(shift1), shift2=shift2.astype(np.int32),
-                  d_base=d_base.astype(np.int32), n_rows_d=int(n_filled.sum() * n_coarse),
+                  d_base=d_base[:-1].astype(np.int32), n_rows_d=int(d_base[-1]),
                   sfine=sfine.astype(np.int32), hc_off=hc_off.astype(np.int32), e_g=e_g,
                   e_cell=e_cell, img=img,
                   twiddles=tw, mask=mask.astype(np.float32))
@@ -347,8 +341,8 @@ class SearchPipeline:
         d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.dev)  # noqa: E731
         self.d_yoff, self.d_ycnt = d(T.yoff), d(T.ycnt)
         self.d_row_off, self.d_row_bls = d(T.row_off), d(T.row_bls)
-        self.d_rowtab, self.d_blk_g, self.d_blk_c0 = d(T.rowtab), d(T.blk_g), d(T.blk_c0)
-        self.d_cell_base = d(T.cell_base)
+        self.d_blk_g, self.d_blk_c0 = d(T.blk_g), d(T.blk_c0)
+        self.d_ybase, self.d_pitch = d(T.y_base), d(T.pitch)
         it = T.img
         self.d_img_cmeta = d(it.c_meta.view(np.int32))
         self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
@@ -466,8 +460,8 @@ class SearchPipeline:
         with self._mark("stage1"):
             _lib.check(_lib.lib().dsb_stage1_rows(
                 _lib.ptr(self.Y), T.n_rows_y, self.TY - 1, int(T.blk_g.size),
-                _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_rowtab),
-                _lib.ptr(self.d_cell_base), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
+                _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_ybase),
+                _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D), T.n_rows_d,
                 self.TD - 1, j * C, C, cfg.coarse_dm.size, cfg.ceff, _lib.ptr(self.sky),
                 cfg.sky_window, self.sky_head, self.sky_count, sub, _lib.stream_of(self.dev)),
@@ -491,7 +485,7 @@ class SearchPipeline:
             _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq), it.n_s, _lib.ptr(self.d_dbase),
-            _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
+            _lib.ptr(self.d_pitch), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
             _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),
             _lib.stream_of(self.dev)), "dsb_image_fft")

@@ -125,26 +125,28 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * subtraction fused, each output written at (t + shift2[g, d]) of the
  * stage-2 ring D, i.e. stage 1 + StaticSkyMean + the stage-2 FIFO
  * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264).
- * Rings are time-major: Y[(t & y_mask)*y_rows + row], D[(t & d_mask)*d_rows + r].
- * Block b covers cells [blk_c0[b], + dsb_stage1_block_size()) of chgroup
- * blk_g[b]; rowtab[cell_base[g]*ceff + s*nf[g] + cell] = Y row of (cell, s)
- * or -1; D row of (g, d, cell) = d_base[g] + d*nf[g] + cell. */
+ * Rings are time-major with dense rows of even pitch p[g] per chgroup:
+ *   Y[(t & y_mask)*y_rows + y_base[g] + s*p[g] + cell]   (subband s),
+ *   D[(t & d_mask)*d_rows + d_base[g] + d*p[g] + cell]   (coarse DM d);
+ * y_base, d_base, p, y_rows, d_rows even and Y, D 16-byte aligned (two
+ * cells per access; a pad cell at nf[g] when nf[g] is odd).  Block b covers
+ * cells [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b]. */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
-                    const int* blk_g, const int* blk_c0, const int* rowtab, const int* cell_base,
+                    const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, long long d_rows, long long d_mask, long long t0, int n_t, int n_dm,
                     int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
                     int sky_subtract, cudaStream_t stream);
 int dsb_stage1_block_size(void);
-
 /* ---- a12: fine-DM combine ---------------------------------------------------
  * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
  * the Hermitian half-spectrum fold and fftshift checkerboard of
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
- * reads the time-major stage-2 ring D[(t & d_mask)*d_stride + row] directly,
- * writes (n_f, n_t, N, N/2+1) complex64. */
+ * reads the time-major stage-2 ring D[(t & d_mask)*d_stride + row] directly
+ * (row of (g, coarse DM c, cell) = d_base[g] + c*d_pitch[g] + cell), writes
+ * (n_f, n_t, N, N/2+1) complex64. */
 int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
-                     const int* e_g, const int* e_cell, const int* d_base, const int* n_filled,
+                     const int* e_g, const int* e_cell, const int* d_base, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
 
@@ -162,7 +164,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * GpuImager.process_cube (src/dsart/image/fused_combine_cuda.py:1359,
  * src/dsart/image/imager_gpu.py:575-605): for each (fine DM f0+fl, time t0+t)
  * the Hermitian half spectrum is combined from the time-major stage-2 ring
- * and transformed on chip; out (n_f, n_t, N, N) float32 = irfft2(G_h) with
+ * (row of (g, coarse DM c, cell) = d_base[g] + c*d_pitch[g] + cell) and
+ * transformed on chip; out (n_f, n_t, N, N) float32 = irfft2(G_h) with
  * 1/N^2 normalisation (fftshifted when fftshift != 0).
  * Tables (built once per pattern set):
  *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
@@ -185,7 +188,7 @@ int dsb_image_fold(int n_grid);
 long long dsb_image_workspace_bytes(int n_grid, int n_s);
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
                   const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* n_filled,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* d_pitch,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream);

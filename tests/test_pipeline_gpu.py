@@ -74,7 +74,7 @@ def test_pipeline_matches_oracle(dev):
     t1 = np.arange(T1 - 32, T1)
     for g in range(band.n_chgroup):
         for d in range(len(kw["coarse_dm"])):
-            rows = T.d_base[g] + d * T.n_filled[g] + np.arange(T.n_filled[g])
+            rows = T.d_base[g] + d * T.pitch[g] + np.arange(T.n_filled[g])
             pos = (t1 + T.shift2[g, d]) & (pipe.TD - 1)
             np.testing.assert_array_equal(D[pos][:, rows], keep["D1"][g][d][t1].astype(np.complex64))
 
@@ -125,7 +125,7 @@ def test_image_fft_matches_combine_and_irfft2(dev, N):
     _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1,
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
                                   _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_dbase),
-                                  _lib.ptr(pipe.d_nfilled), _lib.ptr(pipe.d_sfine),
+                                  _lib.ptr(pipe.d_pitch), _lib.ptr(pipe.d_sfine),
                                   _lib.ptr(pipe.d_f2c), 1, nf, band.n_chgroup, N, t0, nt, 1,
                                   _lib.ptr(gh), _lib.stream_of(dev)), "combine")
     want = torch.fft.irfft2(gh.to(torch.complex128), s=(N, N))
