@@ -290,6 +290,8 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
                                                      long long inner, long long f_stride,
                                                      long long t_stride,
                                                      const float* __restrict__ mask,
+                                                     long long mask_f_stride,
+                                                     const float* __restrict__ sig_f,
                                                      const float* __restrict__ sinv,
                                                      int t_base, int n_out, float thr,
                                                      DetCand* __restrict__ cands, int cap, int pix_off,
@@ -303,7 +305,8 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   const long long fidx = e / npix, p = e % npix;
   const T* cube = x + fidx * f_stride + p;
   // x * 1.0f == x exactly, so an absent mask costs one exact multiply
-  const float mval = mask ? mask[e] : 1.0f;
+  float mval = mask ? mask[fidx * mask_f_stride + p] : 1.0f;
+  if (sig_f) mval = mval / sig_f[fidx];
   float si[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) si[k] = sinv[k];
@@ -400,17 +403,36 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
 constexpr int L1_MAX = 4096;
 constexpr int L1_THREADS = 1024;
 
-__global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const float* __restrict__ x,
-                                                                 int m, float n_sigma, int n_iter,
+// Where a row's samples come from: a [rows, m] matrix, or (GATHER) the
+// images themselves, sample i of row f = img[f*f_stride + times[i / n_pix] *
+// t_stride + pix[i % n_pix]] (the Layer-1 subsample of the pipeline).
+struct L1Src {
+  const float* x;
+  long long f_stride, t_stride;
+  const int* times;
+  const int* pix;
+  int n_pix;
+  int nonpos_to_one;  // report sigma <= 0 (or NaN) as 1 (the mask divisor)
+};
+
+template <bool GATHER>
+__global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const L1Src src, int m,
+                                                                 float n_sigma, int n_iter,
                                                                  float* __restrict__ out) {
   __shared__ float v[L1_MAX];
   __shared__ double red[L1_THREADS / 32];
   __shared__ int s_lo, s_hi;
-  const float* row = x + (long long)blockIdx.x * m;
+  const float* row = src.x + (long long)blockIdx.x * (GATHER ? src.f_stride : m);
   int P = 1;
   while (P < m) P <<= 1;
   for (int i = threadIdx.x; i < P; i += L1_THREADS) {
-    float a = i < m ? row[i] : __int_as_float(0x7f800000);
+    float a = __int_as_float(0x7f800000);
+    if (i < m) {
+      if constexpr (GATHER)
+        a = row[src.times[i / src.n_pix] * src.t_stride + src.pix[i % src.n_pix]];
+      else
+        a = row[i];
+    }
     if (!(a == a) || isinf(a)) a = __int_as_float(0x7f800000);  // non-finite -> +inf (dropped)
     v[i] = a;
   }
@@ -481,7 +503,11 @@ __global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const float* __
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[blockIdx.x] = (sigma == sigma) ? sigma : 0.f;
+  if (threadIdx.x == 0) {
+    float o = (sigma == sigma) ? sigma : 0.f;
+    if (src.nonpos_to_one && !(o > 0.f)) o = 1.f;
+    out[blockIdx.x] = o;
+  }
 }
 
 }  // namespace
@@ -595,7 +621,8 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
 }
 
 int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
-               long long t_stride, const float* mask, int log_maxw, const float* sigma_inv,
+               long long t_stride, const float* mask, long long mask_f_stride,
+               const float* sig_f, int log_maxw, const float* sigma_inv,
                int t_base, int n_out, float threshold, void* cands, int cap, int pix_off,
                int* count, cudaStream_t stream) {
   if (!cube || !sigma_inv || !cands || !count || n <= 0 || n_f <= 0 || npix <= 0 || cap < 0)
@@ -610,11 +637,13 @@ int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long lo
   do {                                                                                    \
     if (cube_f16)                                                                         \
       detect_kernel<L, __half><<<grid, 256, 0, stream>>>(                                 \
-          (const __half*)cube, n, npix, inner, f_stride, t_stride, mask, sigma_inv, t_base, \
+          (const __half*)cube, n, npix, inner, f_stride, t_stride, mask, mask_f_stride,   \
+          sig_f, sigma_inv, t_base,                                                       \
           n_out, threshold, c, cap, pix_off, count);                                      \
     else                                                                                  \
       detect_kernel<L, float><<<grid, 256, 0, stream>>>(                                  \
-          (const float*)cube, n, npix, inner, f_stride, t_stride, mask, sigma_inv, t_base,  \
+          (const float*)cube, n, npix, inner, f_stride, t_stride, mask, mask_f_stride,    \
+          sig_f, sigma_inv, t_base,                                                       \
           n_out, threshold, c, cap, pix_off, count);                                      \
   } while (0)
   switch (log_maxw) {
@@ -634,7 +663,20 @@ int dsb_clipped_std(const float* samples, int rows, int m, float n_sigma, int n_
                     cudaStream_t stream) {
   if (!samples || !out || rows <= 0 || m <= 0 || n_iter < 0) return DSB_E_ARG;
   if (m > L1_MAX) return DSB_E_CAPACITY;
-  clipped_std_kernel<<<rows, L1_THREADS, 0, stream>>>(samples, m, n_sigma, n_iter, out);
+  L1Src src{samples, 0, 0, nullptr, nullptr, 1, 0};
+  clipped_std_kernel<false><<<rows, L1_THREADS, 0, stream>>>(src, m, n_sigma, n_iter, out);
+  return launch_status();
+}
+
+int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, int n_f,
+                     const int* times, int n_times, const int* pix, int n_pix, float n_sigma,
+                     int n_iter, float* sigma, cudaStream_t stream) {
+  if (!img || !times || !pix || !sigma || n_f <= 0 || n_times <= 0 || n_pix <= 0 || n_iter < 0)
+    return DSB_E_ARG;
+  if ((long long)n_times * n_pix > L1_MAX) return DSB_E_CAPACITY;
+  L1Src src{img, f_stride, t_stride, times, pix, n_pix, 1};
+  clipped_std_kernel<true><<<n_f, L1_THREADS, 0, stream>>>(src, n_times * n_pix, n_sigma, n_iter,
+                                                            sigma);
   return launch_status();
 }
 

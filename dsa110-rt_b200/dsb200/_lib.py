@@ -57,9 +57,11 @@ _SIGNATURES = {
     "dsb_boxcar_from_cs": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp],
     "dsb_boxcar_argmax_noalloc": [_vp, _c_int, _c_int, _c_ll, _c_int, _vp, _vp, _vp, _c_int,
                                   _c_int, _c_int, _vp, _c_int, _vp, _vp],
-    "dsb_detect": [_vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_ll, _vp, _c_int, _vp, _c_int,
-                   _c_int, _c_float, _vp, _c_int, _c_int, _vp, _vp],
+    "dsb_detect": [_vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_ll, _vp, _c_ll, _vp, _c_int,
+                   _vp, _c_int, _c_int, _c_float, _vp, _c_int, _c_int, _vp, _vp],
     "dsb_clipped_std": [_vp, _c_int, _c_int, _c_float, _c_int, _vp, _vp],
+    "dsb_layer1_sigma": [_vp, _c_ll, _c_ll, _c_int, _vp, _c_int, _vp, _c_int, _c_float, _c_int,
+                         _vp, _vp],
 }
 
 _RESTYPES = {"dsb_image_workspace_bytes": _c_ll}

@@ -42,7 +42,7 @@ from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
 from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
 from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
 from .search import (CandidateBuffer, _nms, compute_edge_mask, detect_images, irfft2_image,
-                     sigma_clipped_std_batched)
+                     layer1_sigma)
 
 
 def _pow2_at_least(n: int) -> int:
@@ -398,8 +398,10 @@ class SearchPipeline:
         self.l1_sigma: List[torch.Tensor] = []
         # Layer-1 subsample positions (interior times x active pixels)
         act = np.nonzero(T.mask.reshape(-1) != 0)[0]
-        self.l1_pix = d(act[np.linspace(0, act.size - 1, cfg.l1_pixels).astype(np.int64)])
-        self.l1_t = d(te + np.linspace(0, C - 1, cfg.l1_times).astype(np.int64))
+        self.l1_pix = d(act[np.linspace(0, act.size - 1, cfg.l1_pixels).astype(np.int64)]
+                        .astype(np.int32))
+        self.l1_t = d((te + np.linspace(0, C - 1, cfg.l1_times).astype(np.int64)).astype(np.int32))
+        self.l1_sig = torch.empty(cfg.fdm_batch, dtype=torch.float32, device=self.dev)
 
     # ------------------------------------------------------------------
     class _Mark:
@@ -503,17 +505,14 @@ class SearchPipeline:
             with self._mark("image"):
                 self.image(f0, nf, t0, nt, img)
             with self._mark("layer1"):
-                samp = img.reshape(nf, nt, N * N)[:, self.l1_t][:, :, self.l1_pix].reshape(nf, -1)
-                sig = sigma_clipped_std_batched(samp)
-                sig = torch.where(sig > 0, sig, torch.ones_like(sig))
-                mask_f = (self.d_mask[None] / sig[:, None, None]).contiguous()
+                sig = layer1_sigma(img, self.l1_t, self.l1_pix, out=self.l1_sig[:nf])
             with self._mark("detect"):
-                detect_images(img, mask_f, log_max_width=cfg.log_max_width, sigma_inv=self.sinv,
-                              t_base=te, n_out=C, threshold=cfg.threshold, cands=self.cands,
-                              pix_offset=f0 * N * N)
+                detect_images(img, self.d_mask, log_max_width=cfg.log_max_width,
+                              sigma_inv=self.sinv, t_base=te, n_out=C, threshold=cfg.threshold,
+                              cands=self.cands, pix_offset=f0 * N * N, sigma_f=sig)
             self.launches += 3
             if collect and self.keep_sigma:
-                self.l1_sigma.append(sig)
+                self.l1_sigma.append(sig.clone())
         if collect:
             got = self.cands.fetch()
             self.last_d2h_bytes += 4 + got.nbytes

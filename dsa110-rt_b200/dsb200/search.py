@@ -319,24 +319,34 @@ def detect_cube(cube: torch.Tensor, *, log_max_width: int, sigma_inv: torch.Tens
     n = cube.shape[0]
     inner = cube[0].numel()
     _lib.check(_lib.lib().dsb_detect(_lib.ptr(cube), int(cube.dtype == torch.float16), n, 1,
-                                     inner, 0, inner, None, int(log_max_width),
+                                     inner, 0, inner, None, 0, None, int(log_max_width),
                                      _lib.ptr(sigma_inv), int(t_base), int(n_out),
                                      float(threshold), _lib.ptr(cands.buf), cands.capacity,
                                      int(pix_offset), _lib.ptr(cands.count),
                                      _lib.stream_of(cube.device)), "dsb_detect")
 
 
-def detect_images(img: torch.Tensor, mask_f: torch.Tensor, *, log_max_width: int,
+def detect_images(img: torch.Tensor, mask: torch.Tensor, *, log_max_width: int,
                   sigma_inv: torch.Tensor, t_base: int, n_out: int, threshold: float,
-                  cands: CandidateBuffer, pix_offset: int = 0) -> None:
-    """Detector on FFT output ``img [F, T, H, W]`` with the per-F mask
-    ``mask_f [F, H, W]`` applied while reading (no masked copy)."""
+                  cands: CandidateBuffer, pix_offset: int = 0,
+                  sigma_f: Optional[torch.Tensor] = None) -> None:
+    """Detector on FFT output ``img [F, T, H, W]``, each pixel multiplied while
+    reading by ``mask`` (``[F, H, W]`` per fine DM, or one ``[H, W]`` for
+    all) and divided by ``sigma_f[F]`` (the Layer-1 sigma) when given."""
     _lib.require_cuda(img, "img")
-    _lib.require_cuda(mask_f, "mask_f")
+    _lib.require_cuda(mask, "mask")
     F, T, H, W = img.shape
     npix = H * W
+    if mask.numel() not in (npix, F * npix):
+        raise ValueError(f"mask has {mask.numel()} cells; expected {npix} or {F * npix}")
+    if sigma_f is not None:
+        _lib.require_cuda(sigma_f, "sigma_f")
+        if sigma_f.numel() != F or sigma_f.dtype != torch.float32:
+            raise ValueError("sigma_f must be float32 [F]")
     _lib.check(_lib.lib().dsb_detect(_lib.ptr(img), int(img.dtype == torch.float16), T, F, npix,
-                                     T * npix, npix, _lib.ptr(mask_f), int(log_max_width),
+                                     T * npix, npix, _lib.ptr(mask),
+                                     npix if mask.numel() == F * npix else 0, _lib.ptr(sigma_f),
+                                     int(log_max_width),
                                      _lib.ptr(sigma_inv), int(t_base), int(n_out),
                                      float(threshold), _lib.ptr(cands.buf), cands.capacity,
                                      int(pix_offset), _lib.ptr(cands.count),
@@ -346,6 +356,29 @@ def detect_images(img: torch.Tensor, mask_f: torch.Tensor, *, log_max_width: int
 # ---------------------------------------------------------------------------
 # Layer-1 noise
 # ---------------------------------------------------------------------------
+
+
+def layer1_sigma(img: torch.Tensor, times: torch.Tensor, pix: torch.Tensor, *,
+                 n_sigma: float = 3.0, n_iterations: int = 3,
+                 out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Layer-1 sigma of each fine DM of ``img [F, T, H, W]`` over the samples
+    at ``times x pix`` (int32): sigma_clipped_std_batched of that subsample,
+    with values that are not > 0 reported as 1 (the mask divisor)."""
+    _lib.require_cuda(img, "img")
+    F, T, H, W = img.shape
+    if img.dtype != torch.float32:
+        raise ValueError("img must be float32")
+    for name, t in (("times", times), ("pix", pix)):
+        _lib.require_cuda(t, name)
+        if t.dtype != torch.int32:
+            raise ValueError(f"{name} must be int32")
+    if out is None:
+        out = torch.empty(F, dtype=torch.float32, device=img.device)
+    _lib.check(_lib.lib().dsb_layer1_sigma(_lib.ptr(img), T * H * W, H * W, F, _lib.ptr(times),
+                                           times.numel(), _lib.ptr(pix), pix.numel(),
+                                           float(n_sigma), int(n_iterations), _lib.ptr(out),
+                                           _lib.stream_of(img.device)), "dsb_layer1_sigma")
+    return out
 
 
 def sigma_clipped_std_batched(samples: torch.Tensor, *, n_sigma: float = 3.0,

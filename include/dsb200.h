@@ -240,21 +240,32 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
 /* Fused streaming form of the three above plus the threshold test of
  * decode_topk_argmax_lowmem (src/dsart/detector/decoder.py:388): widths
  * 1..2^log_maxw over n samples of n_f*npix cells; cell e = f*npix + p at time
- * t is read at cube[f*f_stride + t*t_stride + p] and multiplied by mask[e]
- * (the edge mask x 1/sigma) when mask is non-null.  Every output cell with
- * max S/N > threshold is appended to cands (struct {int t, pix; float snr;
- * int k;}, pix = e + pix_off); *count counts them (entries past cap are
- * counted, not written). */
+ * t is read at cube[f*f_stride + t*t_stride + p] and multiplied by
+ * mask[f*mask_f_stride + p] (the edge mask; mask_f_stride 0 shares one mask
+ * over the fine DMs), divided by sig_f[f] (the Layer-1 sigma) when sig_f is
+ * non-null.  Every output cell with max S/N > threshold is appended to
+ * cands (struct {int t, pix; float snr; int k;}, pix = e + pix_off); *count
+ * counts them (entries past cap are counted, not written). */
 int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
-               long long t_stride, const float* mask, int log_maxw, const float* sigma_inv,
-               int t_base, int n_out, float threshold, void* cands, int cap, int pix_off,
-               int* count, cudaStream_t stream);
+               long long t_stride, const float* mask, long long mask_f_stride,
+               const float* sig_f, int log_maxw, const float* sigma_inv, int t_base, int n_out,
+               float threshold, void* cands, int cap, int pix_off, int* count,
+               cudaStream_t stream);
 
 /* ---- a18: Layer-1 sigma-clipped std ---------------------------------------------
  * sigma_clipped_std_batched (src/dsart/noise_norm/layer1.py:53): rows of at
  * most 4096 samples; lower median; non-finite samples dropped. */
 int dsb_clipped_std(const float* samples, int rows, int m, float n_sigma, int n_iter, float* out,
                     cudaStream_t stream);
+
+/* Layer-1 sigma of each fine DM straight from the images, as
+ * CubePipeline._layer1_normalise (src/dsart/services/cube_pipeline.py:2226)
+ * with sigma_clipped_std_batched: row f's samples are img[f*f_stride +
+ * times[i]*t_stride + pix[j]] for every (i, j) (n_times*n_pix <= 4096);
+ * sigma[f] = the clipped std, or 1 where that is not > 0 (the mask divisor). */
+int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, int n_f,
+                     const int* times, int n_times, const int* pix, int n_pix, float n_sigma,
+                     int n_iter, float* sigma, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

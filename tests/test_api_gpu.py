@@ -240,3 +240,38 @@ def test_uv_cells_fp64_gpu_equals_numpy(dev):
     wl = 299792458.0 / (nu * 1e9)
     np.testing.assert_array_equal(c, np.rint(-(du[:, None] / wl[None, :]) / cell).astype(np.int64) + 128)
     np.testing.assert_array_equal(r, np.rint(-(dv[:, None] / wl[None, :]) / cell).astype(np.int64) + 128)
+
+
+def test_layer1_sigma_and_detector_divisor_match_indexed_path(dev):
+    """dsb_layer1_sigma (subsample gathered in the kernel) and the detector's
+    per-fine-DM sigma divisor give the same bits as indexing the subsample in
+    torch, sigma_clipped_std_batched, and a precomputed mask / sigma."""
+    from dsb200.search import (CandidateBuffer, detect_images, layer1_sigma,
+                               sigma_clipped_std_batched)
+    g = torch.Generator(device="cpu").manual_seed(21)
+    F, T, H, W = 3, 40, 16, 16
+    img = torch.randn((F, T, H, W), generator=g).to(dev)
+    img[1] *= 0.0                          # a fine DM whose sigma is 0 -> divisor 1
+    img[2, 20:23, 5, 7] += 9.0
+    times = torch.tensor([2, 9, 17, 30, 37], dtype=torch.int32, device=dev)
+    pix = torch.arange(3, H * W, 7, dtype=torch.int32, device=dev)
+    mask = torch.rand((H, W), generator=g).to(dev) + 0.5
+    sig = layer1_sigma(img, times, pix)
+    samp = img.reshape(F, T, H * W)[:, times.long()][:, :, pix.long()].reshape(F, -1)
+    ref = sigma_clipped_std_batched(samp)
+    ref = torch.where(ref > 0, ref, torch.ones_like(ref))
+    assert torch.equal(sig, ref)
+    sinv = (1.0 / torch.sqrt(torch.tensor([1.0, 2.0, 4.0, 8.0]))).to(dev)
+    runs = []
+    for use_div in (True, False):
+        buf = CandidateBuffer(dev, 1 << 16)
+        if use_div:
+            detect_images(img, mask, log_max_width=3, sigma_inv=sinv, t_base=4, n_out=T - 8,
+                          threshold=2.0, cands=buf, sigma_f=sig)
+        else:
+            mask_f = (mask[None] / ref[:, None, None]).contiguous()
+            detect_images(img, mask_f, log_max_width=3, sigma_inv=sinv, t_base=4, n_out=T - 8,
+                          threshold=2.0, cands=buf)
+        runs.append(sorted((int(c["t"]), int(c["pix"]), float(c["snr"]), int(c["k"]))
+                           for c in buf.fetch()))
+    assert runs[0] == runs[1] and len(runs[0]) > 0
