@@ -116,6 +116,13 @@ class Clocks:
 # algorithmic work per launch (for the roofline of the dominant kernel)
 # ---------------------------------------------------------------------------
 
+# DRAM traffic of image_kernel<256> measured by ncu (--set full, one launch)
+# on the medium workload: 302.19 MB written for 1152 images, 105.06 MB read
+# for 2 coarse DMs x 144 times
+IMAGE_DRAM_WRITE_PER_IMAGE = 302.187264e6 / 1152
+IMAGE_DRAM_READ_PER_SLICE_TIME = 105.063168e6 / (2 * 144)
+# ---------------------------------------------------------------------------
+
 
 def stage_work(pipe):
     cfg, T = pipe.cfg, pipe.tab
@@ -346,6 +353,18 @@ def main():
                 "peak_note": f"{peak_src} copy bandwidth"}
     roof["algorithmic_bytes_per_launch"] = nbytes
     roof["mean_launch_ms"] = stages[dom]["mean_ms"]
+    if dom == "image":
+        # DRAM bytes of one image_kernel launch from an ncu capture of the same
+        # kernel on the medium workload (same per-image shape), scaled to this
+        # launch: writes by images, reads by coarse-DM slice-times
+        cfg_ = pipe.cfg
+        nt = cfg_.chunk_tiles + 2 * cfg_.t_edge
+        nb = cfg_.fdm_batch
+        cpb = max(1, nb // cfg_.fine_per_coarse)
+        roof["traffic"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt
+                           + IMAGE_DRAM_READ_PER_SLICE_TIME * cpb * nt)
+        roof["traffic_note"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel on "
+                                "the medium workload (1152 images), scaled to this launch")
 
     if rank == 0:
         cb = None
