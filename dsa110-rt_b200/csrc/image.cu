@@ -127,8 +127,9 @@ DSB_DEV void idftR(float2 (&a)[R]) {
 struct ImgArgs {
   const float2* D;
   long long d_rows, d_mask;
-  const unsigned* c_meta;   // (sum n_filled) per pattern cell: tgt | conj << 16 | g << 17
-  const int* cell_base;     // (G + 1)
+  const unsigned* c_meta;   // (cell_base[G]) per pattern cell: tgt | conj << 16 | g << 17;
+                            // 0xffffffff pads each chgroup's run to a multiple of 32
+  const int* cell_base;     // (G + 1) multiples of 32
   const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
   int n_c2;
   const int* corder;        // (N/2) packed columns in work order (balanced over groups)
@@ -138,6 +139,7 @@ struct ImgArgs {
   int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
   const int* d_base;        // (G)
   const int* d_pitch;       // (G) D rows between coarse DMs of a chgroup
+  const int* n_filled;      // (G) pattern cells of each chgroup
   const int* sfine;         // (n_fine, G)
   const int* f2c;           // (n_fine)
   const float2* tw;         // (N) W_N^e = exp(+2 pi i e / N)
@@ -151,6 +153,7 @@ struct ImgArgs {
 };
 
 constexpr int IMG_MAX_G = 64;
+constexpr int IMG_MAX_CHUNKS = 2048;  // 32-entry chunks of c_meta (chunk -> chgroup table)
 
 template <int N>
 struct ImgGeom {
@@ -169,7 +172,7 @@ struct ImgGeom {
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
   // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases
   static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
-                                 (IMG_MAX_G + 1) * 4;
+                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + IMG_MAX_CHUNKS;
 };
 
 template <int N>
@@ -186,6 +189,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   float2* ctw = rtw + RR * RR;
   const float2** s_slice = reinterpret_cast<const float2**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
+  int* s_nf = s_cbase + IMG_MAX_G + 1;
+  uint8_t* s_chunkg = reinterpret_cast<uint8_t*>(s_nf + IMG_MAX_G);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -195,6 +200,17 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   for (int i = tid; i < C1 * C1; i += THREADS)
     ctw[i] = A.tw[((i % C1) * (i / C1) * (N / LC)) & (N - 1)];
   for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
+  for (int g = tid; g < A.G; g += THREADS) s_nf[g] = A.n_filled[g];
+  if (A.cell_base[A.G] > 32 * IMG_MAX_CHUNKS) {  // uniform: every thread leaves
+    if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
+    return;
+  }
+  // chunk -> chgroup (each chgroup's run of c_meta is a whole number of chunks)
+  for (int c = tid; c < A.cell_base[A.G] / 32; c += THREADS) {
+    int g = 0;
+    while (g + 1 < A.G && A.cell_base[g + 1] <= 32 * c) ++g;
+    s_chunkg[c] = (uint8_t)g;
+  }
 
   float2* ws = A.ws + (size_t)blockIdx.x * A.ws_stride;
   const int n_tot = A.cell_base[A.G];
@@ -229,25 +245,29 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         atomicAdd(&d->x, v.x);
         atomicAdd(&d->y, ((m >> 16) & 1u) ? -v.y : v.y);
       };
-      constexpr int U = 4;
-      int e = tid;
-      for (; e + (U - 1) * THREADS < n_tot; e += U * THREADS) {
+      // metadata and value loads of a step are independent (the chgroup of an
+      // entry comes from its chunk), 8 of each in flight per thread
+      constexpr int U = 8;
+      for (int e0 = 0; e0 < n_tot; e0 += U * THREADS) {
         unsigned m[U];
         float2 v[U];
 #pragma unroll
-        for (int q = 0; q < U; ++q) m[q] = __ldg(A.c_meta + e + q * THREADS);
-#pragma unroll
         for (int q = 0; q < U; ++q) {
-          const int g = (int)(m[q] >> 17) & (IMG_MAX_G - 1);
-          v[q] = s_slice[g][e + q * THREADS - s_cbase[g]];
+          const int e = e0 + q * THREADS + tid;
+          m[q] = 0xffffffffu;
+          v[q] = make_float2(0.f, 0.f);
+          if (e < n_tot) {
+            const int g = s_chunkg[e >> 5];
+            const int k = e - s_cbase[g];
+            if (k < s_nf[g]) {
+              m[q] = __ldg(A.c_meta + e);
+              v[q] = s_slice[g][k];
+            }
+          }
         }
 #pragma unroll
-        for (int q = 0; q < U; ++q) add(m[q], v[q]);
-      }
-      for (; e < n_tot; e += THREADS) {
-        const unsigned m = __ldg(A.c_meta + e);
-        const int g = (int)(m >> 17) & (IMG_MAX_G - 1);
-        add(m, s_slice[g][e - s_cbase[g]]);
+        for (int q = 0; q < U; ++q)
+          if (m[q] != 0xffffffffu) add(m[q], v[q]);
       }
       for (int i = tid; i < A.n_c2; i += THREADS) {
         const int2 cm = __ldg(A.c2 + i);
@@ -426,13 +446,15 @@ long long dsb_image_workspace_bytes(int n_grid, int n_s) {
 
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
                   const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* d_pitch,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base,
+                  const int* d_pitch, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream) {
   if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq ||
       n_s <= 0 ||
-      n_s > 65536 || !d_base || !d_pitch || !sfine || !f2c || !twiddles || !out || !workspace ||
+      n_s > 65536 || !d_base || !d_pitch || !n_filled || !sfine || !f2c || !twiddles || !out ||
+      !workspace ||
       n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
   if ((reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
@@ -443,7 +465,7 @@ int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsig
   int cap = (int)std::min<long long>(rows, 1 << 30);
   if (max_blocks > 0) cap = std::min(cap, max_blocks);
   ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, corder,
-            so, (const uint16_t*)sq, n_s, stride, d_base, d_pitch, sfine, f2c,
+            so, (const uint16_t*)sq, n_s, stride, d_base, d_pitch, n_filled, sfine, f2c,
             (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
             (float2*)workspace, status};
   switch (N) {

@@ -32,7 +32,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
-from typing import List, Optional, Tuple
+from typing import Iterable, Iterator, List, Optional, Tuple
 
 import numpy as np
 import torch
@@ -147,7 +147,7 @@ class ImageTables:
     """Tables of dsb_image_fft: the distinct non-zero half cells S and how
     every pattern cell of every chgroup lands on them."""
     n_s: int
-    c_meta: np.ndarray      # (sum n_filled) uint32: s | conj << 16 | g << 17
+    c_meta: np.ndarray      # uint32 s | conj << 16 | g << 17; chgroup runs padded to 32
     cell_base: np.ndarray   # (G + 1) int32
     c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
     corder: np.ndarray      # (N/2) int32: packed columns in work order
@@ -223,9 +223,14 @@ def build_image_tables(pats, N: int) -> ImageTables:
             chunk = chunk[::-1]
         corder[r:r + chunk.size] = chunk
     n1 = u.size
-    c_meta = (inv[:n1] | (t1c << 16) | (g << 17)).astype(np.uint32)
+    # each chgroup's run padded with 0xffffffff to a whole number of 32-entry
+    # chunks (the kernel finds an entry's chgroup from its chunk)
+    nfs = np.asarray([p.ix_row.size for p in pats], np.int64)
+    cell_base = np.concatenate([[0], np.cumsum((nfs + 31) // 32 * 32)])
+    c_meta = np.full(int(cell_base[-1]), 0xFFFFFFFF, np.uint32)
+    c_meta[cell_base[g] + k] = (inv[:n1] | (t1c << 16) | (g << 17)).astype(np.uint32)
     c2 = np.stack([k[both] | (g[both] << 16), inv[n1:] | (1 << 16)], axis=1).astype(np.int32)
-    cell_base = np.concatenate([[0], np.cumsum([p.ix_row.size for p in pats])]).astype(np.int32)
+    cell_base = cell_base.astype(np.int32)
     return ImageTables(n_s=n_s, c_meta=c_meta, cell_base=cell_base,
                        c2=np.ascontiguousarray(c2.reshape(-1, 2)), corder=corder.astype(np.int32),
                        so=so.astype(np.int32), sq=sq)
@@ -486,8 +491,9 @@ class SearchPipeline:
         _lib.check(_lib.lib().dsb_image_fft(
             _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
-            _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq), it.n_s, _lib.ptr(self.d_dbase),
-            _lib.ptr(self.d_pitch), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
+            _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq),
+            it.n_s, _lib.ptr(self.d_dbase), _lib.ptr(self.d_pitch), _lib.ptr(self.d_nfilled),
+            _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
             _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),
             _lib.stream_of(self.dev)), "dsb_image_fft")
@@ -552,6 +558,54 @@ class SearchPipeline:
                     self._search(jc, collect)
             self.chunk += 1
         return self.out
+
+    def process_blocks(self, blocks: Iterable[torch.Tensor], *,
+                       collect: bool = True) -> Iterator[List[StreamCandidate]]:
+        """Stream blocks held in (pinned) host memory: while block k runs,
+        block k+1 is copied to the device on a separate stream into the other
+        of two device buffers, so the host-to-device transfer overlaps the
+        compute (the block pipelining of corr_fast_integration.py:2593).
+        Yields each block's candidates in order."""
+        cfg = self.cfg
+        shape = (cfg.band.n_chgroup, cfg.npkt_block, cfg.nant, cfg.band.nchan, 2, 2)
+        if getattr(self, "_stage", None) is None:
+            self._stage = [torch.empty(shape, dtype=torch.uint8, device=self.dev)
+                           for _ in range(2)]
+            self._copy_stream = torch.cuda.Stream(self.dev)
+        compute = torch.cuda.current_stream(self.dev)
+        copied = [torch.cuda.Event(), torch.cuda.Event()]
+        free = [None, None]
+
+        def submit(i: int, host: torch.Tensor) -> None:
+            if host.dtype != torch.uint8 or host.numel() != self._stage[0].numel():
+                raise ValueError("raw must be uint8 (G, npkt, nant, nchan, 2, 2)")
+            q = i % 2
+            with torch.cuda.stream(self._copy_stream):
+                if free[q] is not None:
+                    self._copy_stream.wait_event(free[q])   # block i-2 is done with it
+                self._stage[q].view(-1).copy_(host.reshape(-1), non_blocking=True)
+                copied[q].record(self._copy_stream)
+
+        it = iter(blocks)
+        try:
+            nxt = next(it)
+        except StopIteration:
+            return
+        submit(0, nxt)
+        i = 0
+        while nxt is not None:
+            try:
+                nxt = next(it)
+                submit(i + 1, nxt)
+            except StopIteration:
+                nxt = None
+            q = i % 2
+            compute.wait_event(copied[q])
+            out = self.process_block(self._stage[q], collect=collect)
+            free[q] = torch.cuda.Event()
+            free[q].record(compute)
+            yield out
+            i += 1
 
     def check_status(self) -> None:
         _lib.check_status(self.status, "pipeline")

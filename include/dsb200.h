@@ -171,8 +171,10 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
  *      (packed column w' = (w == N/2 ? 0 : w), n' mod C1, n' div C1, u div LC,
  *      w == N/2) with n' = u mod LC, LC = N / dsb_image_fold(N), C1*C1 = LC;
- *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k of
- *      chgroup g adds its value (conjugated if conj) to S entry s;
+ *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k <
+ *      n_filled[g] of chgroup g adds its value (conjugated if conj) to S
+ *      entry s; each chgroup's run is padded with 0xffffffff to a multiple
+ *      of 32 entries (cell_base[g] multiples of 32, cell_base[G] <= 65536);
  *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
  *      w = N/2 that also land on their mirror);
  *   corder: (N/2) packed columns in the order the kernel's thread groups
@@ -188,7 +190,8 @@ int dsb_image_fold(int n_grid);
 long long dsb_image_workspace_bytes(int n_grid, int n_s);
 int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
                   const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base, const int* d_pitch,
+                  const int* so, const unsigned short* sq, int n_s, const int* d_base,
+                  const int* d_pitch, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
                   long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream);

@@ -39,7 +39,7 @@ def _emulate(T, slices, N, fftshift):
     LC, NC = N // fold, N // 2
     S = np.zeros(T.n_s, np.complex128)
     for g, v in enumerate(slices):
-        m = T.c_meta[T.cell_base[g]:T.cell_base[g + 1]].astype(np.int64)
+        m = T.c_meta[T.cell_base[g]:T.cell_base[g] + v.size].astype(np.int64)
         vv = np.where((m >> 16) & 1, np.conj(v), v)
         np.add.at(S, m & 0xFFFF, vv)
     for kg, sc in T.c2.astype(np.int64):
@@ -114,10 +114,13 @@ def test_image_tables_layout():
     slot = col * LC + n1
     last = np.append(slot[1:] != slot[:-1], True)
     assert np.array_equal(((T.sq >> 10) & 1).astype(bool), last)
-    assert T.cell_base[-1] == T.c_meta.size
+    assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 32 == 0)
+    for g, p in enumerate(pats):                # padding after each chgroup's run
+        assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
     assert T.n_s <= LC * (N // 2 + 2)          # fits the kernel's shared buffer
     # every S entry is hit by at least one pattern cell
     hit = np.zeros(T.n_s, bool)
-    hit[T.c_meta & 0xFFFF] = True
+    live = T.c_meta != 0xFFFFFFFF
+    hit[T.c_meta[live] & 0xFFFF] = True
     hit[T.c2[:, 1] & 0xFFFF] = True
     assert hit.all()

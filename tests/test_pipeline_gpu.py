@@ -91,6 +91,28 @@ def test_pipeline_matches_oracle(dev):
     assert any(c.l == 32 + 3 and c.m == 32 - 5 for c in got)
 
 
+def test_streaming_host_blocks_match_device_blocks(dev):
+    """process_blocks (pinned host blocks, H2D overlapped with compute) gives
+    the same candidates as process_block on device blocks."""
+    from dsb200.pipeline import PipelineConfig, SearchPipeline
+    band, ob, e, n, blocks, kw = _setup(n_blocks=8)
+    cfg = PipelineConfig(band=band, nant=kw["nant"], npkt_block=kw["npkt_block"],
+                         t_int=kw["t_int"], csf=kw["csf"], n_grid=kw["n_grid"],
+                         coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
+                         fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, threshold=6.0,
+                         sky_window=2, sky_warmup=1, chunk_tiles=32, fdm_batch=3)
+    ref = SearchPipeline(cfg, e, n, device=dev)
+    want = [ref.process_block(torch.from_numpy(b).to(dev)) for b in blocks]
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    host = [torch.from_numpy(b).pin_memory() for b in blocks]
+    got = list(pipe.process_blocks(host))
+    torch.cuda.synchronize()
+    assert len(got) == len(want)
+    assert [[tuple(vars(c).values()) for c in blk] for blk in got] == \
+        [[tuple(vars(c).values()) for c in blk] for blk in want]
+    assert sum(len(blk) for blk in got) >= 1
+
+
 def test_pipeline_rejects_wrong_raw_size(dev):
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
