@@ -240,10 +240,14 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     __syncthreads();
     // ---- 1. combine into S (shared-memory float atomics) ----
     {
+      // separate real and imaginary arrays: a warp's 32 atomics spread over
+      // all 32 banks instead of the even (or odd) half
+      float* s_re = reinterpret_cast<float*>(buf);
+      float* s_im = s_re + A.ws_stride;
       auto add = [&](unsigned m, float2 v) {
-        float2* d = buf + (m & 0xffffu);
-        atomicAdd(&d->x, v.x);
-        atomicAdd(&d->y, ((m >> 16) & 1u) ? -v.y : v.y);
+        const unsigned t = m & 0xffffu;
+        atomicAdd(s_re + t, v.x);
+        atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
       };
       // metadata and value loads of a step are independent (the chgroup of an
       // entry comes from its chunk), 8 of each in flight per thread
@@ -276,9 +280,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     }
     __syncthreads();
     {
-      const float4* b4 = reinterpret_cast<const float4*>(buf);
+      const float2* re2 = reinterpret_cast<const float2*>(buf);
+      const float2* im2 = re2 + A.ws_stride / 2;
       float4* w4 = reinterpret_cast<float4*>(ws);
-      for (int i = tid; i < A.ws_stride / 2; i += THREADS) w4[i] = b4[i];
+      for (int i = tid; i < A.ws_stride / 2; i += THREADS) {
+        const float2 r = re2[i], m = im2[i];
+        w4[i] = make_float4(r.x, m.x, r.y, m.y);
+      }
     }
     __syncthreads();
 
