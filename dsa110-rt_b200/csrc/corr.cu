@@ -177,7 +177,9 @@ __global__ void __launch_bounds__(GEN_THREADS) corr_generic_kernel(
 // ===========================================================================
 constexpr int TC_THREADS = 256;
 constexpr int TC_TMEM_COLS = 512;   // two accumulators of <= 256 columns
-constexpr int TC_SMEM_BUDGET = 200 * 1024;
+constexpr int TC_SMEM_BUDGET = 224 * 1024;
+constexpr int TC_PRE = 4;          // 16-byte raw loads per thread per item (nant <= 128)
+constexpr int TC_CAP_ROWS = 4096;  // gridding rows of one (chgroup, subband) kept in smem
 // Every CTA requests more than half an SM's shared memory so that exactly
 // one CTA (and one 512-column tensor-memory allocation) lives on each SM.
 constexpr int TC_MIN_SMEM = 120 * 1024;
@@ -213,6 +215,51 @@ DSB_DEV void tc_unit_coords(const TcArgs& A, int u, int& g, int& f, int& s) {
   } else {
     s = r % A.ceff;
     f = r / A.ceff;
+  }
+}
+
+// The 16-byte raw words of one K chunk of one unit (vectorised path: csf and
+// nchan multiples of 4): thread t loads words t, t + 256, ... of the chunk.
+DSB_DEV void tc_load(const TcArgs& A, int g, int f, int s, int q, uint4 (&w)[TC_PRE]) {
+  const int nv = A.kc / 16;
+  const uint8_t* base = A.raw + (size_t)g * A.raw_g_stride;
+#pragma unroll
+  for (int r = 0; r < TC_PRE; ++r) {
+    const int idx = threadIdx.x + r * TC_THREADS;
+    if (idx < A.nant * nv) {
+      const int a = idx / nv, v = idx % nv;
+      const int j = q * (A.kc / 4) + v * 4;
+      const int p = j / A.csf, c = j % A.csf;
+      w[r] = __ldg(reinterpret_cast<const uint4*>(
+          base + ((((size_t)(f * A.ppfv + p) * A.nant + a) * A.nchan + (size_t)s * A.csf + c) * 4)));
+    }
+  }
+}
+
+// Unpack the words of tc_load into the operand stage (same layout as tc_fill).
+DSB_DEV void tc_store(const TcArgs& A, uint8_t* st, const uint4 (&w)[TC_PRE]) {
+  const int nv = A.kc / 16;
+  const int kc = A.kc;
+  const uint32_t region = (uint32_t)A.rows * 128u;
+  const int nant = A.nant;
+#pragma unroll
+  for (int r = 0; r < TC_PRE; ++r) {
+    const int idx = threadIdx.x + r * TC_THREADS;
+    if (idx < nant * nv) {
+      const int a = idx / nv, v = idx % nv;
+      uint4 R, I, N;
+      R.x = nib_lo_s8x4(w[r].x); R.y = nib_lo_s8x4(w[r].y);
+      R.z = nib_lo_s8x4(w[r].z); R.w = nib_lo_s8x4(w[r].w);
+      I.x = nib_hi_s8x4(w[r].x); I.y = nib_hi_s8x4(w[r].y);
+      I.z = nib_hi_s8x4(w[r].z); I.w = nib_hi_s8x4(w[r].w);
+      N.x = neg_s8x4(R.x); N.y = neg_s8x4(R.y); N.z = neg_s8x4(R.z); N.w = neg_s8x4(R.w);
+      const uint32_t kr = (uint32_t)v * 16u, ki = (uint32_t)kc + (uint32_t)v * 16u;
+      const uint32_t ra = (uint32_t)a, rb = (uint32_t)(nant + a);
+      *reinterpret_cast<uint4*>(st + (kr >> 7) * region + sw128_offset(ra, kr & 127u)) = R;
+      *reinterpret_cast<uint4*>(st + (ki >> 7) * region + sw128_offset(ra, ki & 127u)) = I;
+      *reinterpret_cast<uint4*>(st + (kr >> 7) * region + sw128_offset(rb, kr & 127u)) = I;
+      *reinterpret_cast<uint4*>(st + (ki >> 7) * region + sw128_offset(rb, ki & 127u)) = N;
+    }
   }
 }
 
@@ -265,9 +312,16 @@ DSB_DEV void tc_fill(const TcArgs& A, uint8_t* st, int g, int f, int s, int q) {
 // emit the upper triangle b <= a at bls(a, b) (conj(E_b) E_a).
 // Warp w reads TMEM lane quarter (w & 3) (rows 32*(w&3) ...) and every
 // other 16-column chunk (w >> 2 picks the parity).
+// Shared copies of the gridding CSR of the (chgroup, subband) last used.
+struct TcTab {
+  int* roff;        // (TC_CAP_ROWS + 1) row offsets relative to the group's first entry
+  uint16_t* bls;    // (nbase) baseline of each entry
+  int* cached;      // group index whose tables are loaded (-1 none)
+};
+
 template <int MODE>
 DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, int f, int s,
-                         int2* vbuf) {
+                         int2* vbuf, const TcTab& tab) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int quarter = warp & 3, half = warp >> 2;
   const int nant = A.nant;
@@ -300,21 +354,46 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
   }
   tc_fence_before();
   if constexpr (MODE == 1) {
-    // per-cell sum over the baselines gridded into it (exact int32)
-    __syncthreads();
+    // per-cell sum over the baselines gridded into it (exact int32); the
+    // group's CSR is copied to shared memory when the group changes (a CTA
+    // walks consecutive tiles of one group)
     const int gs = g * A.ceff + s;
     const long long row0 = A.yoff[gs];
     const int cnt = A.ycnt[gs];
+    const int e0 = A.row_off[row0];
+    const int ne = A.row_off[row0 + cnt] - e0;
+    const bool use_tab = cnt <= TC_CAP_ROWS && ne <= A.nant * (A.nant + 1) / 2;
+    const bool reload = use_tab && *tab.cached != gs;
+    if (reload) {
+      for (int k = threadIdx.x; k <= cnt; k += TC_THREADS) tab.roff[k] = A.row_off[row0 + k] - e0;
+      for (int j = threadIdx.x; j < ne; j += TC_THREADS) tab.bls[j] = (uint16_t)A.row_bls[e0 + j];
+    }
+    __syncthreads();
+    if (reload && threadIdx.x == 0) *tab.cached = gs;
     const long long tp = (A.t_base + f) & A.t_mask;
-    for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
-      const long long r = row0 + k;
-      int sr = 0, si = 0;
-      for (int j = A.row_off[r]; j < A.row_off[r + 1]; ++j) {
-        const int2 v = vbuf[A.row_bls[j]];
-        sr += v.x;
-        si += v.y;
+    float2* yrow = A.yout + tp * A.y_t_stride + row0;
+    if (use_tab) {
+      for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
+        int sr = 0, si = 0;
+        const int j1 = tab.roff[k + 1];
+        for (int j = tab.roff[k]; j < j1; ++j) {
+          const int2 v = vbuf[tab.bls[j]];
+          sr += v.x;
+          si += v.y;
+        }
+        yrow[k] = make_float2((float)sr, (float)si);
       }
-      A.yout[tp * A.y_t_stride + r] = make_float2((float)sr, (float)si);
+    } else {
+      for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
+        const long long r = row0 + k;
+        int sr = 0, si = 0;
+        for (int j = A.row_off[r]; j < A.row_off[r + 1]; ++j) {
+          const int2 v = vbuf[A.row_bls[j]];
+          sr += v.x;
+          si += v.y;
+        }
+        yrow[k] = make_float2((float)sr, (float)si);
+      }
     }
   }
 }
@@ -329,6 +408,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   uint64_t* bar_drain = bar_acc + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_drain + 1);
   int2* vbuf = reinterpret_cast<int2*>(tmem_slot + 4);
+  TcTab tab{};
+  if constexpr (MODE == 1) {
+    tab.cached = reinterpret_cast<int*>(vbuf + A.nant * (A.nant + 1) / 2);
+    tab.roff = tab.cached + 4;
+    tab.bls = reinterpret_cast<uint16_t*>(tab.roff + TC_CAP_ROWS + 1);
+  }
 
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
@@ -336,6 +421,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     tmem_relinquish();
   }
   if (tid == 0) {
+    if constexpr (MODE == 1) *tab.cached = -1;
     for (int i = 0; i < A.nstage; ++i) mbar_init(&bar_mma[i], 1);
     mbar_init(&bar_acc[0], 1);
     mbar_init(&bar_acc[1], 1);
@@ -347,16 +433,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  // each CTA walks a contiguous range of units (consecutive fast-vis tiles
+  // of one (chgroup, subband) share the gridding tables)
   const int n_units = A.n_chgroup * A.n_fv * A.ceff;
-  const int my_units =
-      (int)blockIdx.x < n_units ? (n_units - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int per_cta = (n_units + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int u_begin = (int)blockIdx.x * per_cta;
+  const int my_units = max(0, min(per_cta, n_units - u_begin));
   const int n_items = my_units * A.n_chunks;
   const uint32_t idesc = idesc_i8(128u, (uint32_t)(2 * A.nant));
+  const bool vec = (A.csf & 3) == 0 && (A.nchan & 3) == 0;
   bool ok = true;
+  // the raw words of the next item are loaded while this one is unpacked
+  uint4 pre[TC_PRE];
+  if (vec && n_items > 0) {
+    int g0, f0, s0;
+    tc_unit_coords(A, u_begin, g0, f0, s0);
+    tc_load(A, g0, f0, s0, 0, pre);
+  }
 
   for (int it = 0; it < n_items; ++it) {
     const int lu = it / A.n_chunks, q = it % A.n_chunks;
-    const int u = (int)blockIdx.x + lu * (int)gridDim.x;
+    const int u = u_begin + lu;
     int g, f, s;
     tc_unit_coords(A, u, g, f, s);
     const int slot = it % A.nstage;
@@ -364,7 +461,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     if (it >= A.nstage) w_ok = mbar_wait(&bar_mma[slot], (uint32_t)((it / A.nstage - 1) & 1));
     if (!__syncthreads_and(w_ok)) { ok = false; break; }
     uint8_t* st = stages + (size_t)slot * A.stage_bytes;
-    tc_fill(A, st, g, f, s, q);
+    if (vec) {
+      uint4 cur[TC_PRE];
+#pragma unroll
+      for (int r = 0; r < TC_PRE; ++r) cur[r] = pre[r];
+      if (it + 1 < n_items) {
+        const int nlu = (it + 1) / A.n_chunks, nq = (it + 1) % A.n_chunks;
+        int ng, nf, ns;
+        tc_unit_coords(A, u_begin + nlu, ng, nf, ns);
+        tc_load(A, ng, nf, ns, nq, pre);
+      }
+      tc_store(A, st, cur);
+    } else {
+      tc_fill(A, st, g, f, s, q);
+    }
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -385,8 +495,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
       if (!__syncthreads_and(a_ok)) { ok = false; break; }
       tc_fence_after();
       int pg, pf, ps;
-      tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
-      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf);
+      tc_unit_coords(A, u_begin + pl, pg, pf, ps);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf, tab);
     }
   }
   if (ok && my_units > 0) {
@@ -395,8 +505,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     if (__syncthreads_and(a_ok)) {
       tc_fence_after();
       int pg, pf, ps;
-      tc_unit_coords(A, (int)blockIdx.x + pl * (int)gridDim.x, pg, pf, ps);
-      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf);
+      tc_unit_coords(A, u_begin + pl, pg, pf, ps);
+      tc_epilogue<MODE>(A, tmem_base, pl & 1, pg, pf, ps, vbuf, tab);
     } else {
       ok = false;
     }
@@ -433,6 +543,14 @@ int launch_status() {
   return e == cudaSuccess ? DSB_OK : DSB_E_CUDA;
 }
 
+// Shared memory beyond the operand stages: mode 1 keeps the upper-triangle
+// visibilities of one unit (int2) and the gridding tables of one group.
+int tc_extra_bytes(const TcArgs& A, int mode) {
+  if (mode != 1) return 0;
+  const int nbase = A.nant * (A.nant + 1) / 2;
+  return nbase * 8 + 16 + (TC_CAP_ROWS + 1) * 4 + nbase * 2 + 16;
+}
+
 // Fill the derived geometry; returns DSB_OK or an error code.
 int tc_plan(TcArgs& A, int mode) {
   if (A.nant < 16 || A.nant > 128 || (A.nant % 16) != 0) return DSB_E_UNSUPPORTED;
@@ -450,7 +568,7 @@ int tc_plan(TcArgs& A, int mode) {
   A.nkblk = (2 * A.kc + 127) / 128;
   A.stage_bytes = A.nkblk * A.rows * 128;
   A.n_mma = 2 * A.kc / 32;
-  const int extra = (mode == 1) ? A.nant * (A.nant + 1) / 2 * 8 : 0;
+  const int extra = tc_extra_bytes(A, mode);
   const int budget = TC_SMEM_BUDGET - extra - 1024 - 256;
   A.nstage = std::min(4, budget / A.stage_bytes);
   if (A.nstage < 2) return DSB_E_UNSUPPORTED;
@@ -577,7 +695,7 @@ int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int
   A.status = status;
   int rc = tc_plan(A, 1);
   if (rc) return rc;
-  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + A.nant * (A.nant + 1) / 2 * 8,
+  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + tc_extra_bytes(A, 1),
                            TC_MIN_SMEM);
   cudaFuncSetAttribute(corr_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int n_units = n_chgroup * A.n_fv * A.ceff;
