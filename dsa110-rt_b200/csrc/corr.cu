@@ -236,6 +236,72 @@ DSB_DEV void tc_load(const TcArgs& A, int g, int f, int s, int q, uint4 (&w)[TC_
   }
 }
 
+// Per-thread offsets of the vectorised fill, computed once per kernel (no
+// divisions per item): byte offset of word r of chunk 0 inside a unit's raw
+// data, and the four shared-memory destinations of its unpacked words.  Valid
+// when a chunk covers whole packets (kc/4 a multiple of csf): chunk q is then
+// chunk 0 moved by q * (kc/4/csf) packets.
+struct TcFillPlan {
+  int ld[TC_PRE];
+  uint32_t st[TC_PRE][4];
+  long long q_step;   // bytes between chunks
+  long long f_step;   // bytes between fast-vis tiles
+  int s_step;         // bytes between summed channels
+};
+
+DSB_DEV void tc_fill_plan(const TcArgs& A, TcFillPlan& P) {
+  const int nv = A.kc / 16;
+  const uint32_t region = (uint32_t)A.rows * 128u;
+  const long long pkt = (long long)A.nant * A.nchan * 4;
+#pragma unroll
+  for (int r = 0; r < TC_PRE; ++r) {
+    const int idx = threadIdx.x + r * TC_THREADS;
+    const int a = idx / nv, v = idx % nv;
+    const int p = (v * 4) / A.csf, c = (v * 4) % A.csf;
+    P.ld[r] = (int)(((long long)p * A.nant + a) * A.nchan * 4 + (long long)c * 4);
+    const uint32_t kr = (uint32_t)v * 16u, ki = (uint32_t)A.kc + (uint32_t)v * 16u;
+    const uint32_t ra = (uint32_t)a, rb = (uint32_t)(A.nant + a);
+    P.st[r][0] = (kr >> 7) * region + sw128_offset(ra, kr & 127u);
+    P.st[r][1] = (ki >> 7) * region + sw128_offset(ra, ki & 127u);
+    P.st[r][2] = (kr >> 7) * region + sw128_offset(rb, kr & 127u);
+    P.st[r][3] = (ki >> 7) * region + sw128_offset(rb, ki & 127u);
+  }
+  P.q_step = (long long)(A.kc / 4 / A.csf) * pkt;
+  P.f_step = (long long)A.ppfv * pkt;
+  P.s_step = A.csf * 4;
+}
+
+DSB_DEV void tc_load_planned(const TcArgs& A, const TcFillPlan& P, int g, int f, int s, int q,
+                             uint4 (&w)[TC_PRE]) {
+  const uint8_t* base = A.raw + (size_t)g * A.raw_g_stride + (long long)f * P.f_step +
+                        (long long)s * P.s_step + (long long)q * P.q_step;
+  const int n = A.nant * (A.kc / 16);
+#pragma unroll
+  for (int r = 0; r < TC_PRE; ++r)
+    if (threadIdx.x + r * TC_THREADS < n)
+      w[r] = __ldg(reinterpret_cast<const uint4*>(base + P.ld[r]));
+}
+
+DSB_DEV void tc_store_planned(const TcArgs& A, const TcFillPlan& P, uint8_t* st,
+                              const uint4 (&w)[TC_PRE]) {
+  const int n = A.nant * (A.kc / 16);
+#pragma unroll
+  for (int r = 0; r < TC_PRE; ++r) {
+    if (threadIdx.x + r * TC_THREADS < n) {
+      uint4 R, I, N;
+      R.x = nib_lo_s8x4(w[r].x); R.y = nib_lo_s8x4(w[r].y);
+      R.z = nib_lo_s8x4(w[r].z); R.w = nib_lo_s8x4(w[r].w);
+      I.x = nib_hi_s8x4(w[r].x); I.y = nib_hi_s8x4(w[r].y);
+      I.z = nib_hi_s8x4(w[r].z); I.w = nib_hi_s8x4(w[r].w);
+      N.x = neg_s8x4(R.x); N.y = neg_s8x4(R.y); N.z = neg_s8x4(R.z); N.w = neg_s8x4(R.w);
+      *reinterpret_cast<uint4*>(st + P.st[r][0]) = R;
+      *reinterpret_cast<uint4*>(st + P.st[r][1]) = I;
+      *reinterpret_cast<uint4*>(st + P.st[r][2]) = I;
+      *reinterpret_cast<uint4*>(st + P.st[r][3]) = N;
+    }
+  }
+}
+
 // Unpack the words of tc_load into the operand stage (same layout as tc_fill).
 DSB_DEV void tc_store(const TcArgs& A, uint8_t* st, const uint4 (&w)[TC_PRE]) {
   const int nv = A.kc / 16;
@@ -442,13 +508,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   const int n_items = my_units * A.n_chunks;
   const uint32_t idesc = idesc_i8(128u, (uint32_t)(2 * A.nant));
   const bool vec = (A.csf & 3) == 0 && (A.nchan & 3) == 0;
+  const bool planned = vec && ((A.kc / 4) % A.csf) == 0;
+  TcFillPlan plan{};
+  if (planned) tc_fill_plan(A, plan);
   bool ok = true;
   // the raw words of the next item are loaded while this one is unpacked
   uint4 pre[TC_PRE];
   if (vec && n_items > 0) {
     int g0, f0, s0;
     tc_unit_coords(A, u_begin, g0, f0, s0);
-    tc_load(A, g0, f0, s0, 0, pre);
+    if (planned) tc_load_planned(A, plan, g0, f0, s0, 0, pre);
+    else tc_load(A, g0, f0, s0, 0, pre);
   }
 
   for (int it = 0; it < n_items; ++it) {
@@ -469,9 +539,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
         const int nlu = (it + 1) / A.n_chunks, nq = (it + 1) % A.n_chunks;
         int ng, nf, ns;
         tc_unit_coords(A, u_begin + nlu, ng, nf, ns);
-        tc_load(A, ng, nf, ns, nq, pre);
+        if (planned) tc_load_planned(A, plan, ng, nf, ns, nq, pre);
+        else tc_load(A, ng, nf, ns, nq, pre);
       }
-      tc_store(A, st, cur);
+      if (planned) tc_store_planned(A, plan, st, cur);
+      else tc_store(A, st, cur);
     } else {
       tc_fill(A, st, g, f, s, q);
     }
