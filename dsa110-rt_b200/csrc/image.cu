@@ -126,7 +126,9 @@ DSB_DEV void idftR(float2 (&a)[R]) {
 
 struct ImgArgs {
   const float2* D;
-  long long d_rows, d_mask;
+  const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
+  const int* seg_mask;        // (G * n_coarse) segment depth - 1
+  int n_coarse;
   const unsigned* c_meta;   // (cell_base[G]) per pattern cell: tgt | conj << 16 | g << 17;
                             // 0xffffffff pads each chgroup's run to a multiple of 32
   const int* cell_base;     // (G + 1) multiples of 32
@@ -137,8 +139,7 @@ struct ImgArgs {
   const uint16_t* sq;       // (n_s) q | packed << 2 | parity(u + w) << 3 | (u mod LC) << 4
                             //       | last entry of its folded slot << 10
   int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
-  const int* d_base;        // (G)
-  const int* d_pitch;       // (G) D rows between coarse DMs of a chgroup
+  const int* d_pitch;       // (G) cells (row pitch) of each chgroup's segments
   const int* n_filled;      // (G) pattern cells of each chgroup
   const int* sfine;         // (n_fine, G)
   const int* f2c;           // (n_fine)
@@ -231,8 +232,11 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     const long long ta = A.t0 + t;
     __syncthreads();  // the previous image is done with buf and s_slice
     for (int g = tid; g < A.G; g += THREADS)
-      s_slice[g] = A.D + ((ta - A.sfine[(long long)f * A.G + g]) & A.d_mask) * A.d_rows +
-                   A.d_base[g] + (long long)c * A.d_pitch[g];
+    {
+      const int gc = g * A.n_coarse + c;
+      s_slice[g] = A.D + A.seg_base[gc] +
+                   ((ta - A.sfine[(long long)f * A.G + g]) & A.seg_mask[gc]) * A.d_pitch[g];
+    }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
       for (int i = tid; i < A.ws_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -452,18 +456,17 @@ long long dsb_image_workspace_bytes(int n_grid, int n_s) {
   return (long long)blocks * ((n_s + 1) & ~1) * 8;
 }
 
-int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
-                  const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base,
-                  const int* d_pitch, const int* n_filled,
-                  const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
-                  int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
-                  long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream) {
-  if (!D || !c_meta || !cell_base || (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq ||
-      n_s <= 0 ||
-      n_s > 65536 || !d_base || !d_pitch || !n_filled || !sfine || !f2c || !twiddles || !out ||
-      !workspace ||
-      n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
+int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+                  const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
+                  const int* corder, const int* so, const unsigned short* sq, int n_s,
+                  const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,
+                  const void* twiddles, int f0, int n_f, int G, int N, long long t0, int n_t,
+                  int fftshift, void* out, void* workspace, long long workspace_bytes,
+                  int max_blocks, int* status, cudaStream_t stream) {
+  if (!D || !seg_base || !seg_mask || n_coarse <= 0 || !c_meta || !cell_base ||
+      (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq || n_s <= 0 || n_s > 65536 ||
+      !d_pitch || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace || n_f <= 0 ||
+      n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
   if ((reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
     return DSB_E_ARG;
@@ -472,8 +475,8 @@ int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsig
   if (rows <= 0) return DSB_E_CAPACITY;
   int cap = (int)std::min<long long>(rows, 1 << 30);
   if (max_blocks > 0) cap = std::min(cap, max_blocks);
-  ImgArgs A{(const float2*)D, d_rows, d_mask, c_meta, cell_base, (const int2*)c2, n_c2, corder,
-            so, (const uint16_t*)sq, n_s, stride, d_base, d_pitch, n_filled, sfine, f2c,
+  ImgArgs A{(const float2*)D, seg_base, seg_mask, n_coarse, c_meta, cell_base, (const int2*)c2,
+            n_c2, corder, so, (const uint16_t*)sq, n_s, stride, d_pitch, n_filled, sfine, f2c,
             (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
             (float2*)workspace, status};
   switch (N) {

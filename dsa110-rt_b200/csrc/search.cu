@@ -34,12 +34,13 @@ __global__ void uv_cells_kernel(const double* __restrict__ du, const double* __r
 // ===========================================================================
 struct CombArgs {
   const float2* D;
-  long long d_stride, d_mask;
+  const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
+  const int* seg_mask;        // (G * n_coarse) segment depth - 1
+  int n_coarse;
   const int* hc_off;     // (n_half_cells + 1) CSR over half cells (u-major)
   const int* e_g;        // chgroup
   const int* e_cell;     // cell within the chgroup (negative = mirror, stored as ~cell)
-  const int* d_base;     // (G) first D row of each chgroup
-  const int* d_pitch;    // (G) D rows between coarse DMs of a chgroup
+  const int* d_pitch;    // (G) cells (row pitch) of each chgroup's segments
   const int* sfine;      // (n_fine_total, G) signed shifts
   const int* f2c;        // (n_fine_total) coarse index
   int f0, n_f, G, N;
@@ -75,12 +76,14 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
       int cell = A.e_cell[j];
       const bool mirror = cell < 0;
       if (mirror) cell = ~cell;
-      const long long row = (long long)A.d_base[g] + (long long)c * A.d_pitch[g] + cell;
+      const int gc = g * A.n_coarse + c;
       const long long ts0 = A.t0 + tt - A.sfine[(long long)f * A.G + g];
-      const float2* src = A.D + row;
+      const float2* src = A.D + A.seg_base[gc] + cell;
+      const int msk = A.seg_mask[gc];
+      const long long pitch = A.d_pitch[g];
 #pragma unroll
       for (int i = 0; i < CB_T; ++i) {
-        const float2 x = src[((ts0 + i) & A.d_mask) * A.d_stride];
+        const float2 x = src[((ts0 + i) & msk) * pitch];
         re[i] += x.x;
         im[i] += mirror ? -(double)x.y : (double)x.y;
       }
@@ -526,15 +529,16 @@ int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_
   return launch_status();
 }
 
-int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
-                     const int* e_g, const int* e_cell, const int* d_base, const int* d_pitch,
+int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+                     const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
-  if (!D || !hc_off || !e_g || !e_cell || !d_base || !d_pitch || !sfine || !f2c || !out)
+  if (!D || !seg_base || !seg_mask || n_coarse <= 0 || !hc_off || !e_g || !e_cell ||
+      !d_pitch || !sfine || !f2c || !out)
     return DSB_E_ARG;
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
-  CombArgs A{(const float2*)D, d_stride, d_mask, hc_off, e_g, e_cell, d_base, d_pitch, sfine,
-             f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
+  CombArgs A{(const float2*)D, seg_base, seg_mask, n_coarse, hc_off, e_g, e_cell, d_pitch,
+             sfine, f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
   const int n_hc = N * (N / 2 + 1);
   dim3 grid((n_hc + 127) / 128, n_f);
   combine_rows_kernel<<<grid, 128, 0, stream>>>(A);

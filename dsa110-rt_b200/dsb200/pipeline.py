@@ -376,11 +376,21 @@ class SearchPipeline:
         # every chgroup (the stage-2 delay of the top chgroup has elapsed)
         self.jc_first = math.ceil((int(T.shift2.max()) + max(0, int(T.sfine.max())) + 2 * te) / C)
         self.TY = _pow2_at_least((self.depth1 + 1) * C)
-        span_d = (self.a + 1) * C + 2 * te + max(0, int(T.sfine.max())) + int(T.shift2.max()) + C
-        self.TD = _pow2_at_least(span_d)
-        # time-major rings: [time & (T-1)][row]
+        # stage-2 ring: one time-major segment per (chgroup, coarse DM), as deep
+        # as its own stage-2 delay needs (a value written at t + shift2 is read
+        # by the image kernel up to (a + 1) chunks + 2 t_edge + the largest
+        # fine shift later)
+        margin = (self.a + 1) * C + 2 * te + max(0, int(T.sfine.max())) + C
+        G, n_coarse = T.shift2.shape
+        depth = np.asarray([[_pow2_at_least(int(T.shift2[g, d]) + margin) for d in range(n_coarse)]
+                            for g in range(G)], np.int64)
+        seg_elems = depth * T.pitch.astype(np.int64)[:, None]
+        self.seg_base = np.concatenate([[0], np.cumsum(seg_elems.reshape(-1))]).astype(np.int64)
+        self.seg_mask = (depth - 1).reshape(-1).astype(np.int32)
+        self.d_segbase, self.d_segmask = d(self.seg_base[:-1]), d(self.seg_mask)
+        # time-major rings: Y [time & (TY-1)][row]; D segmented as above
         self.Y = torch.zeros((self.TY, T.n_rows_y), dtype=torch.complex64, device=self.dev)
-        self.D = torch.zeros((self.TD, T.n_rows_d), dtype=torch.complex64, device=self.dev)
+        self.D = torch.zeros(int(self.seg_base[-1]), dtype=torch.complex64, device=self.dev)
         self.sky = (torch.zeros((T.n_rows_d, cfg.sky_window), dtype=torch.complex128,
                                 device=self.dev) if cfg.use_sky else None)
         self.sky_count = self.sky_head = self.sky_seen = 0
@@ -469,8 +479,9 @@ class SearchPipeline:
                 _lib.ptr(self.Y), T.n_rows_y, self.TY - 1, int(T.blk_g.size),
                 _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_ybase),
                 _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
-                _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D), T.n_rows_d,
-                self.TD - 1, j * C, C, cfg.coarse_dm.size, cfg.ceff, _lib.ptr(self.sky),
+                _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
+                _lib.ptr(self.d_segbase), _lib.ptr(self.d_segmask), j * C, C, cfg.coarse_dm.size,
+                cfg.ceff, _lib.ptr(self.sky),
                 cfg.sky_window, self.sky_head, self.sky_count, sub, _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
         self.launches += 1
@@ -489,10 +500,11 @@ class SearchPipeline:
         if out.shape != (n_f, n_t, N, N) or out.dtype != torch.float32 or not out.is_contiguous():
             raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
         _lib.check(_lib.lib().dsb_image_fft(
-            _lib.ptr(self.D), T.n_rows_d, self.TD - 1, _lib.ptr(self.d_img_cmeta),
+            _lib.ptr(self.D), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segmask),
+            cfg.coarse_dm.size, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq),
-            it.n_s, _lib.ptr(self.d_dbase), _lib.ptr(self.d_pitch), _lib.ptr(self.d_nfilled),
+            it.n_s, _lib.ptr(self.d_pitch), _lib.ptr(self.d_nfilled),
             _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
             _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),
@@ -606,6 +618,17 @@ class SearchPipeline:
             free[q].record(compute)
             yield out
             i += 1
+
+    def ring_values(self, g: int, d: int, times) -> np.ndarray:
+        """Stage-2 ring values of chgroup g, coarse DM d at absolute times
+        (as stage 1 wrote them, already delayed by shift2): [len(times), nf]."""
+        nf = int(self.tab.n_filled[g])
+        pitch = int(self.tab.pitch[g])
+        gd = g * self.tab.shift2.shape[1] + d
+        base, msk = int(self.seg_base[gd]), int(self.seg_mask[gd])
+        seg = self.D[base:base + (msk + 1) * pitch].view(msk + 1, pitch)
+        rows = torch.as_tensor(np.asarray(times, np.int64) & msk, device=self.dev)
+        return seg[rows, :nf].cpu().numpy()
 
     def check_status(self) -> None:
         _lib.check_status(self.status, "pipeline")

@@ -127,14 +127,18 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264).
  * Rings are time-major with dense rows of even pitch p[g] per chgroup:
  *   Y[(t & y_mask)*y_rows + y_base[g] + s*p[g] + cell]   (subband s),
- *   D[(t & d_mask)*d_rows + d_base[g] + d*p[g] + cell]   (coarse DM d);
- * y_base, d_base, p, y_rows, d_rows even and Y, D 16-byte aligned (two
- * cells per access; a pad cell at nf[g] when nf[g] is odd).  Block b covers
- * cells [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b]. */
+ *   D[seg_base[gd] + (t & seg_mask[gd])*p[g] + cell]     (gd = g*n_dm + d),
+ * each (chgroup, coarse DM) its own ring segment of power-of-two depth
+ * seg_mask + 1 (deep enough for its own stage-2 delay); the float64 sky ring
+ * of (g, d, cell) is row d_base[g] + d*p[g] + cell.  y_base, seg_base, p,
+ * y_rows even and Y, D 16-byte aligned (two cells per access; a pad cell at
+ * nf[g] when nf[g] is odd).  Block b covers cells [blk_c0[b], +
+ * dsb_stage1_block_size()) of chgroup blk_g[b]. */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
-                    void* D, long long d_rows, long long d_mask, long long t0, int n_t, int n_dm,
+                    void* D, const long long* seg_base, const int* seg_mask, long long t0,
+                    int n_t, int n_dm,
                     int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
                     int sky_subtract, cudaStream_t stream);
 int dsb_stage1_block_size(void);
@@ -142,11 +146,12 @@ int dsb_stage1_block_size(void);
  * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
  * the Hermitian half-spectrum fold and fftshift checkerboard of
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
- * reads the time-major stage-2 ring D[(t & d_mask)*d_stride + row] directly
- * (row of (g, coarse DM c, cell) = d_base[g] + c*d_pitch[g] + cell), writes
- * (n_f, n_t, N, N/2+1) complex64. */
-int dsb_combine_rows(const void* D, long long d_stride, long long d_mask, const int* hc_off,
-                     const int* e_g, const int* e_cell, const int* d_base, const int* d_pitch,
+ * reads the segmented stage-2 ring directly (value of (g, coarse DM c,
+ * cell) at time t: D[seg_base[g*n_coarse + c] + (t & seg_mask[...])*d_pitch[g]
+ * + cell], as dsb_stage1_rows writes it), writes (n_f, n_t, N, N/2+1)
+ * complex64. */
+int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+                     const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
 
@@ -163,8 +168,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * Replaces fused_dequant_combine_per_fdm_half + torch.fft.irfft2 inside
  * GpuImager.process_cube (src/dsart/image/fused_combine_cuda.py:1359,
  * src/dsart/image/imager_gpu.py:575-605): for each (fine DM f0+fl, time t0+t)
- * the Hermitian half spectrum is combined from the time-major stage-2 ring
- * (row of (g, coarse DM c, cell) = d_base[g] + c*d_pitch[g] + cell) and
+ * the Hermitian half spectrum is combined from the segmented stage-2 ring
+ * (as dsb_combine_rows reads it) and
  * transformed on chip; out (n_f, n_t, N, N) float32 = irfft2(G_h) with
  * 1/N^2 normalisation (fftshifted when fftshift != 0).
  * Tables (built once per pattern set):
@@ -188,13 +193,13 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY is returned. */
 int dsb_image_fold(int n_grid);
 long long dsb_image_workspace_bytes(int n_grid, int n_s);
-int dsb_image_fft(const void* D, long long d_rows, long long d_mask, const unsigned* c_meta,
-                  const int* cell_base, const void* c2, int n_c2, const int* corder,
-                  const int* so, const unsigned short* sq, int n_s, const int* d_base,
-                  const int* d_pitch, const int* n_filled,
-                  const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
-                  int N, long long t0, int n_t, int fftshift, void* out, void* workspace,
-                  long long workspace_bytes, int max_blocks, int* status, cudaStream_t stream);
+int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+                  const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
+                  const int* corder, const int* so, const unsigned short* sq, int n_s,
+                  const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,
+                  const void* twiddles, int f0, int n_f, int G, int N, long long t0, int n_t,
+                  int fftshift, void* out, void* workspace, long long workspace_bytes,
+                  int max_blocks, int* status, cudaStream_t stream);
 
 /* ---- a13/a14: edge mask x Layer-1 normalisation into the detector cube -----
  * Replaces the mask multiply + cube write of GpuImager.process_cube

@@ -69,14 +69,12 @@ def test_pipeline_matches_oracle(dev):
 
     # stage-2 ring vs oracle stage-1 streams (last emitted chunk), bit-exact
     T = pipe.tab
-    D = pipe.D.cpu().numpy()
     T1 = keep["D1"][0][0].shape[0]
     t1 = np.arange(T1 - 32, T1)
     for g in range(band.n_chgroup):
         for d in range(len(kw["coarse_dm"])):
-            rows = T.d_base[g] + d * T.pitch[g] + np.arange(T.n_filled[g])
-            pos = (t1 + T.shift2[g, d]) & (pipe.TD - 1)
-            np.testing.assert_array_equal(D[pos][:, rows], keep["D1"][g][d][t1].astype(np.complex64))
+            got_d = pipe.ring_values(g, d, t1 + T.shift2[g, d])
+            np.testing.assert_array_equal(got_d, keep["D1"][g][d][t1].astype(np.complex64))
 
     key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
     g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
@@ -144,12 +142,13 @@ def test_image_fft_matches_combine_and_irfft2(dev, N):
     L = _lib.lib()
     pipe.image(1, nf, t0, nt, out, max_blocks=3)
     gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
-    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), T.n_rows_d, pipe.TD - 1,
+    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), _lib.ptr(pipe.d_segbase),
+                                  _lib.ptr(pipe.d_segmask), len(kw["coarse_dm"]),
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
-                                  _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_dbase),
-                                  _lib.ptr(pipe.d_pitch), _lib.ptr(pipe.d_sfine),
-                                  _lib.ptr(pipe.d_f2c), 1, nf, band.n_chgroup, N, t0, nt, 1,
-                                  _lib.ptr(gh), _lib.stream_of(dev)), "combine")
+                                  _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_pitch),
+                                  _lib.ptr(pipe.d_sfine), _lib.ptr(pipe.d_f2c), 1, nf,
+                                  band.n_chgroup, N, t0, nt, 1, _lib.ptr(gh),
+                                  _lib.stream_of(dev)), "combine")
     want = torch.fft.irfft2(gh.to(torch.complex128), s=(N, N))
     torch.cuda.synchronize()
     pipe.check_status()
