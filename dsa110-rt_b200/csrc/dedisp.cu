@@ -123,7 +123,7 @@ __global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int d
 
 // Pipeline stage 1 over per-subband gridded rows, time-major rings:
 //   Y[(t & y_mask) * y_rows + y_base[g] + s * pitch[g] + cell],
-//   D[seg_base[g*n_dm + d] + (t & seg_mask[g*n_dm + d]) * pitch[g] + cell]
+//   D[seg_base[g*n_dm + d] + (t mod seg_depth[g*n_dm + d]) * pitch[g] + cell]
 // (each (chgroup, coarse DM) a ring segment as deep as its own stage-2 delay
 // needs); the sky ring is indexed by d_base[g] + d * pitch[g] + cell.
 // Rows are dense per (chgroup, subband) and (chgroup, coarse DM) with an
@@ -145,7 +145,7 @@ struct S1Args {
   const int* n_filled;    // (G)
   float2* D;
   const long long* seg_base;  // (G * n_dm) first element of each ring segment (even)
-  const int* seg_mask;        // (G * n_dm) segment depth - 1 (depth a power of two)
+  const int* seg_depth;       // (G * n_dm) time slots of each segment
   long long t0;           // absolute time of the first output
   int n_t, n_dm, ceff;
   double2* sky_ring;      // (D rows, window) or null
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
   float4* D4 = reinterpret_cast<float4*>(A.D);
   const long long y_rows2 = A.y_rows / 2;
   const long long seg = (long long)A.seg_base[g * A.n_dm + d] + cl;
-  const int seg_mask = A.seg_mask[g * A.n_dm + d];
+  const long long dep = A.seg_depth[g * A.n_dm + d];
   const long long ycol2 = (A.y_base[g] + cl) / 2;
   const long long drow = (long long)A.d_base[g] + (long long)d * pitch + cl;
   double mr[2] = {0.0, 0.0}, mi[2] = {0.0, 0.0};
@@ -192,6 +192,8 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
   double sr[2] = {0.0, 0.0}, si[2] = {0.0, 0.0};
   for (int t = 0; t < A.n_t; t += S1_TT) {
     const long long ta = A.t0 + t;
+    long long wpos = (ta + sh2) % dep;  // write slot of time ta (wraps below)
+    if (wpos < 0) wpos += dep;
     float4 acc[S1_TT];
 #pragma unroll
     for (int i = 0; i < S1_TT; ++i) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -219,7 +221,9 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
         if (sub)
           o = make_float4((float)((double)a.x - mr[0]), (float)((double)a.y - mi[0]),
                           (float)((double)a.z - mr[1]), (float)((double)a.w - mi[1]));
-        D4[(seg + ((ta + i + sh2) & seg_mask) * pitch) / 2] = o;
+        long long slot = wpos + i;
+        if (slot >= dep) slot -= dep;
+        D4[(seg + slot * pitch) / 2] = o;
       }
     }
   }
@@ -285,12 +289,12 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
-                    void* D, const long long* seg_base, const int* seg_mask, long long t0,
+                    void* D, const long long* seg_base, const int* seg_depth, long long t0,
                     int n_t, int n_dm,
                     int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
                     int sky_subtract, cudaStream_t stream) {
   if (!Y || !D || !blk_g || !blk_c0 || !y_base || !pitch || !shift1 || !shift2 ||
-      !d_base || !n_filled || !seg_base || !seg_mask || n_t <= 0 || n_dm <= 0 || ceff <= 0)
+      !d_base || !n_filled || !seg_base || !seg_depth || n_t <= 0 || n_dm <= 0 || ceff <= 0)
     return DSB_E_ARG;
   // two cells per 16-byte access: rings 16-byte aligned, row counts even
   if ((reinterpret_cast<uintptr_t>(Y) & 15) || (reinterpret_cast<uintptr_t>(D) & 15) ||
@@ -305,7 +309,7 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   A.Y = (const float2*)Y; A.y_rows = y_rows; A.y_mask = y_mask;
   A.blk_g = blk_g; A.blk_c0 = blk_c0; A.y_base = y_base; A.pitch = pitch;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
-  A.D = (float2*)D; A.seg_base = seg_base; A.seg_mask = seg_mask;
+  A.D = (float2*)D; A.seg_base = seg_base; A.seg_depth = seg_depth;
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
   A.sky_count = sky_count; A.sky_subtract = sky_subtract;

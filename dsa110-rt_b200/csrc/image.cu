@@ -127,7 +127,7 @@ DSB_DEV void idftR(float2 (&a)[R]) {
 struct ImgArgs {
   const float2* D;
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
-  const int* seg_mask;        // (G * n_coarse) segment depth - 1
+  const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
   const unsigned* c_meta;   // (cell_base[G]) per pattern cell: tgt | conj << 16 | g << 17;
                             // 0xffffffff pads each chgroup's run to a multiple of 32
@@ -234,8 +234,10 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     for (int g = tid; g < A.G; g += THREADS)
     {
       const int gc = g * A.n_coarse + c;
-      s_slice[g] = A.D + A.seg_base[gc] +
-                   ((ta - A.sfine[(long long)f * A.G + g]) & A.seg_mask[gc]) * A.d_pitch[g];
+      const long long dep = A.seg_depth[gc];
+      long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
+      if (slot < 0) slot += dep;
+      s_slice[g] = A.D + A.seg_base[gc] + slot * A.d_pitch[g];
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
@@ -456,14 +458,14 @@ long long dsb_image_workspace_bytes(int n_grid, int n_s) {
   return (long long)blocks * ((n_s + 1) & ~1) * 8;
 }
 
-int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* corder, const int* so, const unsigned short* sq, int n_s,
                   const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,
                   const void* twiddles, int f0, int n_f, int G, int N, long long t0, int n_t,
                   int fftshift, void* out, void* workspace, long long workspace_bytes,
                   int max_blocks, int* status, cudaStream_t stream) {
-  if (!D || !seg_base || !seg_mask || n_coarse <= 0 || !c_meta || !cell_base ||
+  if (!D || !seg_base || !seg_depth || n_coarse <= 0 || !c_meta || !cell_base ||
       (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq || n_s <= 0 || n_s > 65536 ||
       !d_pitch || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace || n_f <= 0 ||
       n_t <= 0 || G <= 0 || G > IMG_MAX_G)
@@ -475,7 +477,7 @@ int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_mask,
   if (rows <= 0) return DSB_E_CAPACITY;
   int cap = (int)std::min<long long>(rows, 1 << 30);
   if (max_blocks > 0) cap = std::min(cap, max_blocks);
-  ImgArgs A{(const float2*)D, seg_base, seg_mask, n_coarse, c_meta, cell_base, (const int2*)c2,
+  ImgArgs A{(const float2*)D, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
             n_c2, corder, so, (const uint16_t*)sq, n_s, stride, d_pitch, n_filled, sfine, f2c,
             (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
             (float2*)workspace, status};

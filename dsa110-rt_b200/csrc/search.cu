@@ -35,7 +35,7 @@ __global__ void uv_cells_kernel(const double* __restrict__ du, const double* __r
 struct CombArgs {
   const float2* D;
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
-  const int* seg_mask;        // (G * n_coarse) segment depth - 1
+  const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
   const int* hc_off;     // (n_half_cells + 1) CSR over half cells (u-major)
   const int* e_g;        // chgroup
@@ -79,11 +79,15 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
       const int gc = g * A.n_coarse + c;
       const long long ts0 = A.t0 + tt - A.sfine[(long long)f * A.G + g];
       const float2* src = A.D + A.seg_base[gc] + cell;
-      const int msk = A.seg_mask[gc];
+      const long long dep = A.seg_depth[gc];
       const long long pitch = A.d_pitch[g];
+      long long slot0 = ts0 % dep;
+      if (slot0 < 0) slot0 += dep;
 #pragma unroll
       for (int i = 0; i < CB_T; ++i) {
-        const float2 x = src[((ts0 + i) & msk) * pitch];
+        long long slot = slot0 + i;
+        if (slot >= dep) slot -= dep;
+        const float2 x = src[slot * pitch];
         re[i] += x.x;
         im[i] += mirror ? -(double)x.y : (double)x.y;
       }
@@ -529,15 +533,15 @@ int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_
   return launch_status();
 }
 
-int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
-  if (!D || !seg_base || !seg_mask || n_coarse <= 0 || !hc_off || !e_g || !e_cell ||
+  if (!D || !seg_base || !seg_depth || n_coarse <= 0 || !hc_off || !e_g || !e_cell ||
       !d_pitch || !sfine || !f2c || !out)
     return DSB_E_ARG;
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
-  CombArgs A{(const float2*)D, seg_base, seg_mask, n_coarse, hc_off, e_g, e_cell, d_pitch,
+  CombArgs A{(const float2*)D, seg_base, seg_depth, n_coarse, hc_off, e_g, e_cell, d_pitch,
              sfine, f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
   const int n_hc = N * (N / 2 + 1);
   dim3 grid((n_hc + 127) / 128, n_f);

@@ -31,6 +31,7 @@ Detector cubes overlap by 2*t_edge so that their interiors tile time.
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 from typing import Iterable, Iterator, List, Optional, Tuple
 
@@ -382,12 +383,11 @@ class SearchPipeline:
         # fine shift later)
         margin = (self.a + 1) * C + 2 * te + max(0, int(T.sfine.max())) + C
         G, n_coarse = T.shift2.shape
-        depth = np.asarray([[_pow2_at_least(int(T.shift2[g, d]) + margin) for d in range(n_coarse)]
-                            for g in range(G)], np.int64)
+        depth = ((T.shift2.astype(np.int64) + margin + 31) // 32 * 32)
         seg_elems = depth * T.pitch.astype(np.int64)[:, None]
         self.seg_base = np.concatenate([[0], np.cumsum(seg_elems.reshape(-1))]).astype(np.int64)
-        self.seg_mask = (depth - 1).reshape(-1).astype(np.int32)
-        self.d_segbase, self.d_segmask = d(self.seg_base[:-1]), d(self.seg_mask)
+        self.seg_depth = depth.reshape(-1).astype(np.int32)
+        self.d_segbase, self.d_segdepth = d(self.seg_base[:-1]), d(self.seg_depth)
         # time-major rings: Y [time & (TY-1)][row]; D segmented as above
         self.Y = torch.zeros((self.TY, T.n_rows_y), dtype=torch.complex64, device=self.dev)
         self.D = torch.zeros(int(self.seg_base[-1]), dtype=torch.complex64, device=self.dev)
@@ -480,7 +480,7 @@ class SearchPipeline:
                 _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_ybase),
                 _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
-                _lib.ptr(self.d_segbase), _lib.ptr(self.d_segmask), j * C, C, cfg.coarse_dm.size,
+                _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
                 cfg.ceff, _lib.ptr(self.sky),
                 cfg.sky_window, self.sky_head, self.sky_count, sub, _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
@@ -500,7 +500,7 @@ class SearchPipeline:
         if out.shape != (n_f, n_t, N, N) or out.dtype != torch.float32 or not out.is_contiguous():
             raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
         _lib.check(_lib.lib().dsb_image_fft(
-            _lib.ptr(self.D), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segmask),
+            _lib.ptr(self.D), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
             cfg.coarse_dm.size, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq),
@@ -587,11 +587,14 @@ class SearchPipeline:
         compute = torch.cuda.current_stream(self.dev)
         copied = [torch.cuda.Event(), torch.cuda.Event()]
         free = [None, None]
+        t_submit = [0.0, 0.0]
+        self.block_latency_s: List[float] = []
 
         def submit(i: int, host: torch.Tensor) -> None:
             if host.dtype != torch.uint8 or host.numel() != self._stage[0].numel():
                 raise ValueError("raw must be uint8 (G, npkt, nant, nchan, 2, 2)")
             q = i % 2
+            t_submit[q] = time.perf_counter()
             with torch.cuda.stream(self._copy_stream):
                 if free[q] is not None:
                     self._copy_stream.wait_event(free[q])   # block i-2 is done with it
@@ -616,6 +619,9 @@ class SearchPipeline:
             out = self.process_block(self._stage[q], collect=collect)
             free[q] = torch.cuda.Event()
             free[q].record(compute)
+            # block-to-candidate latency: handed in -> its candidates on the host
+            # (process_block returns after the last chunk's candidate read-back)
+            self.block_latency_s.append(time.perf_counter() - t_submit[q])
             yield out
             i += 1
 
@@ -625,9 +631,9 @@ class SearchPipeline:
         nf = int(self.tab.n_filled[g])
         pitch = int(self.tab.pitch[g])
         gd = g * self.tab.shift2.shape[1] + d
-        base, msk = int(self.seg_base[gd]), int(self.seg_mask[gd])
-        seg = self.D[base:base + (msk + 1) * pitch].view(msk + 1, pitch)
-        rows = torch.as_tensor(np.asarray(times, np.int64) & msk, device=self.dev)
+        base, dep = int(self.seg_base[gd]), int(self.seg_depth[gd])
+        seg = self.D[base:base + dep * pitch].view(dep, pitch)
+        rows = torch.as_tensor(np.asarray(times, np.int64) % dep, device=self.dev)
         return seg[rows, :nf].cpu().numpy()
 
     def check_status(self) -> None:

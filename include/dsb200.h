@@ -127,9 +127,9 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264).
  * Rings are time-major with dense rows of even pitch p[g] per chgroup:
  *   Y[(t & y_mask)*y_rows + y_base[g] + s*p[g] + cell]   (subband s),
- *   D[seg_base[gd] + (t & seg_mask[gd])*p[g] + cell]     (gd = g*n_dm + d),
- * each (chgroup, coarse DM) its own ring segment of power-of-two depth
- * seg_mask + 1 (deep enough for its own stage-2 delay); the float64 sky ring
+ *   D[seg_base[gd] + (t mod seg_depth[gd])*p[g] + cell]  (gd = g*n_dm + d),
+ * each (chgroup, coarse DM) its own ring segment of seg_depth[gd] (>= 8)
+ * time slots, deep enough for its own stage-2 delay; the float64 sky ring
  * of (g, d, cell) is row d_base[g] + d*p[g] + cell.  y_base, seg_base, p,
  * y_rows even and Y, D 16-byte aligned (two cells per access; a pad cell at
  * nf[g] when nf[g] is odd).  Block b covers cells [blk_c0[b], +
@@ -137,7 +137,7 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
-                    void* D, const long long* seg_base, const int* seg_mask, long long t0,
+                    void* D, const long long* seg_base, const int* seg_depth, long long t0,
                     int n_t, int n_dm,
                     int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
                     int sky_subtract, cudaStream_t stream);
@@ -147,10 +147,10 @@ int dsb_stage1_block_size(void);
  * the Hermitian half-spectrum fold and fftshift checkerboard of
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
  * reads the segmented stage-2 ring directly (value of (g, coarse DM c,
- * cell) at time t: D[seg_base[g*n_coarse + c] + (t & seg_mask[...])*d_pitch[g]
+ * cell) at time t: D[seg_base[g*n_coarse + c] + (t mod seg_depth[...])*d_pitch[g]
  * + cell], as dsb_stage1_rows writes it), writes (n_f, n_t, N, N/2+1)
  * complex64. */
-int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
@@ -193,7 +193,7 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY is returned. */
 int dsb_image_fold(int n_grid);
 long long dsb_image_workspace_bytes(int n_grid, int n_s);
-int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_mask, int n_coarse,
+int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* corder, const int* so, const unsigned short* sq, int n_s,
                   const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,

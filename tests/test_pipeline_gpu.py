@@ -143,7 +143,7 @@ def test_image_fft_matches_combine_and_irfft2(dev, N):
     pipe.image(1, nf, t0, nt, out, max_blocks=3)
     gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
     _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), _lib.ptr(pipe.d_segbase),
-                                  _lib.ptr(pipe.d_segmask), len(kw["coarse_dm"]),
+                                  _lib.ptr(pipe.d_segdepth), len(kw["coarse_dm"]),
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
                                   _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_pitch),
                                   _lib.ptr(pipe.d_sfine), _lib.ptr(pipe.d_f2c), 1, nf,
