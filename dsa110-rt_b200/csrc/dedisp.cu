@@ -126,59 +126,99 @@ __global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int d
 //   D[seg_base[g*n_dm + d] + (t mod seg_depth[g*n_dm + d]) * pitch[g] + cell]
 // (each (chgroup, coarse DM) a ring segment as deep as its own stage-2 delay
 // needs); the sky ring is indexed by d_base[g] + d * pitch[g] + cell.
-// Rows are dense per (chgroup, subband) and (chgroup, coarse DM) with an
-// even pitch, so one thread owns two adjacent cells (16-byte loads and
-// stores) and the 32 lanes of a warp read 512 contiguous bytes.  Blocks
-// never straddle chgroups; one grid row per coarse DM.  Time is walked in
-// tiles of S1_TT samples: for each subband the tile's S1_TT loads are
-// independent.
+//
+// A CTA owns 4 adjacent cells of one chgroup and a group of S1_DG coarse
+// DMs, and walks the output times in tiles of S1_TT.  For each tile it
+// stages every subband's Y samples that any of its DMs needs (the tile plus
+// the spread of that subband's shifts over the DM group) in shared memory,
+// two planes of two cells, and then every (DM, time) output of the tile sums
+// its ceff subbands from there: each Y sample is read from L2 once per DM
+// group instead of once per DM.  Thread (dl, l8) = (tid / 8, tid % 8) owns
+// DM dl of the group and times l8, l8 + 8, ...; its D writes are whole
+// 32-byte sectors (4 cells).
 struct S1Args {
   const float2* Y;
   long long y_rows, y_mask;
   const int* blk_g;       // chgroup of each block
-  const int* blk_c0;      // first cell of each block (even)
-  const int* y_base;      // (G) first Y row of the chgroup (even)
-  const int* pitch;       // (G) even row pitch between subbands / coarse DMs
+  const int* blk_c0;      // first cell of each block (a multiple of 4)
+  const int* y_base;      // (G) first Y row of the chgroup (a multiple of 4)
+  const int* pitch;       // (G) row pitch between subbands / coarse DMs (a multiple of 4)
   const int* shift1;      // (G, ceff, n_dm)
   const int* shift2;      // (G, n_dm)
-  const int* d_base;      // (G) first sky-ring row of the chgroup (even)
+  const int* d_base;      // (G) first sky-ring row of the chgroup
   const int* n_filled;    // (G)
   float2* D;
   const long long* seg_base;  // (G * n_dm) first element of each ring segment (even)
   const int* seg_depth;       // (G * n_dm) time slots of each segment
   long long t0;           // absolute time of the first output
   int n_t, n_dm, ceff;
+  int win_len;            // S1_TT + largest shift spread over a DM group
   double2* sky_ring;      // (D rows, window) or null
   int sky_window, sky_head, sky_count, sky_subtract;
+  int* status;
 };
 
-constexpr int S1_THREADS = 128;
+constexpr int S1_THREADS = 256;
 constexpr int S1_MAX_C = 64;
-constexpr int S1_TT = 8;
+constexpr int S1_TT = 64;   // output times per tile
+constexpr int S1_DG = 32;   // coarse DMs per CTA (S1_THREADS / 8)
+
+__host__ __device__ inline size_t s1_smem_bytes(int ceff, int win_len) {
+  return (size_t)ceff * S1_DG * 4 + (size_t)S1_MAX_C * 8 + (size_t)ceff * win_len * 32 + 16;
+}
 
 __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
-  __shared__ int s_sh[S1_MAX_C];
-  const int g = A.blk_g[blockIdx.x];
-  const int d = blockIdx.y;
-  const int nf = A.n_filled[g];
-  const int pitch = A.pitch[g];
-  const int cl = A.blk_c0[blockIdx.x] + 2 * threadIdx.x;
+  extern __shared__ __align__(16) uint8_t s1_smem[];
   const int ceff = A.ceff;
-  for (int s = threadIdx.x; s < ceff; s += S1_THREADS)
-    s_sh[s] = A.shift1[(g * ceff + s) * A.n_dm + d];
+  int* s_sh = reinterpret_cast<int*>(s1_smem);              // [s][dl] shift - lo[s]
+  int* s_lo = s_sh + ceff * S1_DG;                          // [s] smallest shift
+  int* s_len = s_lo + S1_MAX_C;                             // [s] window length
+  float4* win0 = reinterpret_cast<float4*>(s1_smem + ((size_t)ceff * S1_DG * 4 +
+                                                      (size_t)S1_MAX_C * 8 + 15) / 16 * 16);
+  float4* win1 = win0 + (size_t)ceff * A.win_len;            // cells 2-3
+
+  const int g = A.blk_g[blockIdx.x];
+  const int c0 = A.blk_c0[blockIdx.x];
+  const int dg0 = blockIdx.y * S1_DG;
+  const int nd = min(S1_DG, A.n_dm - dg0);
+  const int pitch = A.pitch[g];
+  const int tid = threadIdx.x;
+  for (int sb = tid; sb < ceff; sb += S1_THREADS) {
+    const int* sh = A.shift1 + ((long long)g * ceff + sb) * A.n_dm + dg0;
+    int lo = sh[0], hi = sh[0];
+    for (int dl = 1; dl < nd; ++dl) {
+      lo = min(lo, sh[dl]);
+      hi = max(hi, sh[dl]);
+    }
+    s_lo[sb] = lo;
+    s_len[sb] = S1_TT + hi - lo;
+  }
   __syncthreads();
-  if (cl >= nf) return;  // cl + 1 <= pitch - 1: a pad cell at most
-  const float4* Y4 = reinterpret_cast<const float4*>(A.Y);
-  float4* D4 = reinterpret_cast<float4*>(A.D);
-  const long long y_rows2 = A.y_rows / 2;
-  const long long seg = (long long)A.seg_base[g * A.n_dm + d] + cl;
-  const long long dep = A.seg_depth[g * A.n_dm + d];
-  const long long ycol2 = (A.y_base[g] + cl) / 2;
-  const long long drow = (long long)A.d_base[g] + (long long)d * pitch + cl;
-  double mr[2] = {0.0, 0.0}, mi[2] = {0.0, 0.0};
+  // a window longer than the caller sized the shared memory for: flag, stop
+  bool fits = true;
+  for (int sb = 0; sb < ceff; ++sb) fits = fits && s_len[sb] <= A.win_len;
+  if (!fits) {
+    if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
+    return;
+  }
+  for (int i = tid; i < ceff * S1_DG; i += S1_THREADS) {
+    const int sb = i / S1_DG, dl = i % S1_DG;
+    s_sh[i] = dl < nd ? A.shift1[((long long)g * ceff + sb) * A.n_dm + dg0 + dl] - s_lo[sb] : 0;
+  }
+
+  const int dl = tid >> 3, l8 = tid & 7;
+  const bool active = dl < nd;
+  const int d = dg0 + (active ? dl : 0);
+  const int gd = g * A.n_dm + d;
+  const long long seg = A.seg_base[gd] + c0;
+  const long long dep = A.seg_depth[gd];
+  const int sh2 = A.shift2[gd];
+  const long long drow = (long long)A.d_base[g] + (long long)d * pitch + c0;
+  double mr[4] = {0, 0, 0, 0}, mi[4] = {0, 0, 0, 0};
   const bool sub = A.sky_ring && A.sky_subtract && A.sky_count > 0;
-  if (sub) {
-    for (int c = 0; c < 2; ++c) {
+  if (sub && active) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
       for (int w = 0; w < A.sky_count; ++w) {
         const double2 r = A.sky_ring[(drow + c) * A.sky_window + w];
         mr[c] += r.x;
@@ -188,49 +228,91 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
       mi[c] /= A.sky_count;
     }
   }
-  const int sh2 = A.shift2[g * A.n_dm + d];
-  double sr[2] = {0.0, 0.0}, si[2] = {0.0, 0.0};
-  for (int t = 0; t < A.n_t; t += S1_TT) {
-    const long long ta = A.t0 + t;
-    long long wpos = (ta + sh2) % dep;  // write slot of time ta (wraps below)
-    if (wpos < 0) wpos += dep;
-    float4 acc[S1_TT];
+  double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
+  const float4* Y4 = reinterpret_cast<const float4*>(A.Y);
+  const long long ycol = (long long)A.y_base[g] + c0;   // a multiple of 4
+  float4* D4 = reinterpret_cast<float4*>(A.D);
+
+  for (int tt = 0; tt < A.n_t; tt += S1_TT) {
+    __syncthreads();  // the previous tile's windows are no longer read
+    // stage the windows: entry (sb, tau) = Y at time t0 + tt + lo[sb] + tau,
+    // flattened over (sb, tau) so that each thread's loads are independent
+    {
+      constexpr int U = 4;
+      const int n_e = ceff * A.win_len;
+      for (int e0 = 0; e0 < n_e; e0 += U * S1_THREADS) {
+        float4 v0[U], v1[U];
+        int ei[U];
 #pragma unroll
-    for (int i = 0; i < S1_TT; ++i) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int s = 0; s < ceff; ++s) {
-      const long long col = ycol2 + (long long)s * (pitch / 2);
-      const long long p0 = ta + s_sh[s];
+        for (int q = 0; q < U; ++q) {
+          const int e = e0 + q * S1_THREADS + tid;
+          ei[q] = -1;
+          if (e < n_e) {
+            const int sb = e / A.win_len, tau = e - sb * A.win_len;
+            if (tau < s_len[sb]) {
+              const long long r2 = ((((A.t0 + tt + s_lo[sb] + tau) & A.y_mask) * A.y_rows) +
+                                    ycol + (long long)sb * pitch) / 2;
+              v0[q] = Y4[r2];
+              v1[q] = Y4[r2 + 1];
+              ei[q] = e;
+            }
+          }
+        }
 #pragma unroll
-      for (int i = 0; i < S1_TT; ++i) {
-        const float4 v = Y4[((p0 + i) & A.y_mask) * y_rows2 + col];
-        acc[i].x += v.x;
-        acc[i].y += v.y;
-        acc[i].z += v.z;
-        acc[i].w += v.w;
+        for (int q = 0; q < U; ++q) {
+          if (ei[q] >= 0) {
+            win0[ei[q]] = v0[q];
+            win1[ei[q]] = v1[q];
+          }
+        }
       }
     }
-#pragma unroll
-    for (int i = 0; i < S1_TT; ++i) {
-      if (t + i < A.n_t) {
-        const float4 a = acc[i];
-        sr[0] += a.x;
-        si[0] += a.y;
-        sr[1] += a.z;
-        si[1] += a.w;
-        float4 o = a;
-        if (sub)
-          o = make_float4((float)((double)a.x - mr[0]), (float)((double)a.y - mi[0]),
-                          (float)((double)a.z - mr[1]), (float)((double)a.w - mi[1]));
-        long long slot = wpos + i;
-        if (slot >= dep) slot -= dep;
-        D4[(seg + slot * pitch) / 2] = o;
+    __syncthreads();
+    if (!active) continue;
+    long long slot = (A.t0 + tt + l8 + sh2) % dep;
+    if (slot < 0) slot += dep;
+    for (int k = 0; k < S1_TT / 8; ++k, slot += 8) {
+      if (slot >= dep) slot -= dep;
+      const int tl = l8 + 8 * k;
+      if (tt + tl >= A.n_t) break;
+      float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+      for (int sb = 0; sb < ceff; ++sb) {
+        const int idx = sb * A.win_len + tl + s_sh[sb * S1_DG + dl];
+        const float4 v0 = win0[idx], v1 = win1[idx];
+        a0.x += v0.x; a0.y += v0.y; a0.z += v0.z; a0.w += v0.w;
+        a1.x += v1.x; a1.y += v1.y; a1.z += v1.z; a1.w += v1.w;
       }
+      sr[0] += a0.x; si[0] += a0.y; sr[1] += a0.z; si[1] += a0.w;
+      sr[2] += a1.x; si[2] += a1.y; sr[3] += a1.z; si[3] += a1.w;
+      float4 o0 = a0, o1 = a1;
+      if (sub) {
+        o0 = make_float4((float)((double)a0.x - mr[0]), (float)((double)a0.y - mi[0]),
+                         (float)((double)a0.z - mr[1]), (float)((double)a0.w - mi[1]));
+        o1 = make_float4((float)((double)a1.x - mr[2]), (float)((double)a1.y - mi[2]),
+                         (float)((double)a1.z - mr[3]), (float)((double)a1.w - mi[3]));
+      }
+      const long long o = (seg + slot * pitch) / 2;
+      D4[o] = o0;
+      D4[o + 1] = o1;
     }
   }
+  // sky: block mean of every (DM, cell) over the chunk, summed over the 8
+  // lanes that share the DM (lanes 8-aligned inside the warp)
   if (A.sky_ring) {
-    A.sky_ring[drow * A.sky_window + A.sky_head] = make_double2(sr[0] / A.n_t, si[0] / A.n_t);
-    A.sky_ring[(drow + 1) * A.sky_window + A.sky_head] =
-        make_double2(sr[1] / A.n_t, si[1] / A.n_t);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        sr[c] += __shfl_xor_sync(0xffffffffu, sr[c], o);
+        si[c] += __shfl_xor_sync(0xffffffffu, si[c], o);
+      }
+    }
+    if (active && l8 == 0) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        A.sky_ring[(drow + c) * A.sky_window + A.sky_head] =
+            make_double2(sr[c] / A.n_t, si[c] / A.n_t);
+    }
   }
 }
 
@@ -290,17 +372,21 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, const long long* seg_base, const int* seg_depth, long long t0,
-                    int n_t, int n_dm,
-                    int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
-                    int sky_subtract, cudaStream_t stream) {
+                    int n_t, int n_dm, int ceff, int max_spread, void* sky_ring, int sky_window,
+                    int sky_head, int sky_count, int sky_subtract, int* status,
+                    cudaStream_t stream) {
   if (!Y || !D || !blk_g || !blk_c0 || !y_base || !pitch || !shift1 || !shift2 ||
-      !d_base || !n_filled || !seg_base || !seg_depth || n_t <= 0 || n_dm <= 0 || ceff <= 0)
+      !d_base || !n_filled || !seg_base || !seg_depth || n_t <= 0 || n_dm <= 0 || ceff <= 0 ||
+      max_spread < 0)
     return DSB_E_ARG;
-  // two cells per 16-byte access: rings 16-byte aligned, row counts even
+  // four cells per 32-byte access: rings 16-byte aligned, row counts multiples of 4
   if ((reinterpret_cast<uintptr_t>(Y) & 15) || (reinterpret_cast<uintptr_t>(D) & 15) ||
-      (y_rows & 1))
+      (y_rows & 3))
     return DSB_E_ARG;
   if (ceff > S1_MAX_C) return DSB_E_CAPACITY;
+  const int win_len = S1_TT + max_spread;
+  const size_t smem = s1_smem_bytes(ceff, win_len);
+  if (smem > 227 * 1024) return DSB_E_CAPACITY;
   if (sky_ring && (sky_window <= 0 || sky_head < 0 || sky_head >= sky_window ||
                    sky_count < 0 || sky_count > sky_window))
     return DSB_E_ARG;
@@ -310,14 +396,18 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   A.blk_g = blk_g; A.blk_c0 = blk_c0; A.y_base = y_base; A.pitch = pitch;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
   A.D = (float2*)D; A.seg_base = seg_base; A.seg_depth = seg_depth;
-  A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff;
+  A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff; A.win_len = win_len;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
-  A.sky_count = sky_count; A.sky_subtract = sky_subtract;
-  dim3 grid(n_blocks, n_dm);
-  stage1_rows_kernel<<<grid, S1_THREADS, 0, stream>>>(A);
+  A.sky_count = sky_count; A.sky_subtract = sky_subtract; A.status = status;
+  if (cudaFuncSetAttribute(stage1_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return DSB_E_CUDA;
+  dim3 grid(n_blocks, (n_dm + S1_DG - 1) / S1_DG);
+  stage1_rows_kernel<<<grid, S1_THREADS, smem, stream>>>(A);
   return launch_status();
 }
 
-int dsb_stage1_block_size(void) { return 2 * S1_THREADS; }
+int dsb_stage1_block_size(void) { return 4; }
+int dsb_stage1_dm_group(void) { return S1_DG; }
 
 }  // extern "C"

@@ -131,6 +131,7 @@ class Tables:
     blk_c0: np.ndarray
     cell_base: np.ndarray           # (G,) first global cell of each chgroup
     shift1: np.ndarray              # (G, ceff, n_coarse) int32
+    max_spread: int                 # largest shift1 spread over a stage-1 DM group
     shift2: np.ndarray              # (G, n_coarse) int32
     d_base: np.ndarray              # (G,) first D row of each chgroup (even)
     n_rows_d: int
@@ -255,7 +256,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     # Y row of (g, s, cell) = y_base[g] + s*pitch[g] + cell, D row of
     # (g, coarse DM d, cell) = d_base[g] + d*pitch[g] + cell; the correlator's
     # group (g, s) writes every cell of its chgroup (0 where no baseline lands)
-    pitch = (n_filled + 1) // 2 * 2
+    pitch = (n_filled + 3) // 4 * 4
     y_base = np.concatenate([[0], np.cumsum(pitch * ceff)])
     n_rows_y = int(y_base[-1])
     yoff = np.zeros(G * ceff, np.int64)
@@ -283,6 +284,11 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     plan = DMPlan(dm_pc_cc=cfg.coarse_dm, t_int_fast_us=cfg.t_int_us, chan_sum_factor=cfg.csf,
                   band=band)
     shift1 = plan.delay_bins_all().astype(np.int32)
+    # largest spread of one subband's shifts over a group of coarse DMs (the
+    # shared time window of a stage-1 block)
+    dg = int(_lib.lib().dsb_stage1_dm_group())
+    s1 = shift1.reshape(G, ceff, -1)
+    max_spread = max(int(np.ptp(s1[:, :, k:k + dg], axis=2).max()) for k in range(0, s1.shape[2], dg))
     shift2 = np.stack([compute_stage2_shifts(chgroup=g, coarse_dm_pc_cm3=cfg.coarse_dm,
                                              t_int_corr_us=cfg.t_int_us,
                                              band=band).shifts_samples for g in range(G)])
@@ -312,7 +318,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     mask = compute_edge_mask(n_grid=N, kernel_support=1)
     e = np.arange(N)
     tw = np.exp(2j * np.pi * e / N).astype(np.complex64)
-    return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled,
+    return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled, max_spread=max_spread,
                   yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
                   row_off=row_off.astype(np.int32), row_bls=row_bls.astype(np.int32),
                   n_rows_y=n_rows_y, y_base=y_base[:-1].astype(np.int32),
@@ -481,8 +487,8 @@ class SearchPipeline:
                 _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
                 _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
-                cfg.ceff, _lib.ptr(self.sky),
-                cfg.sky_window, self.sky_head, self.sky_count, sub, _lib.stream_of(self.dev)),
+                cfg.ceff, T.max_spread, _lib.ptr(self.sky), cfg.sky_window, self.sky_head,
+                self.sky_count, sub, _lib.ptr(self.status), _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
         self.launches += 1
         if cfg.use_sky:

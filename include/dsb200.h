@@ -125,23 +125,30 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * subtraction fused, each output written at (t + shift2[g, d]) of the
  * stage-2 ring D, i.e. stage 1 + StaticSkyMean + the stage-2 FIFO
  * (corr_fast_integration.py:917, :1049; stage2_chgroup_alignment.py:264).
- * Rings are time-major with dense rows of even pitch p[g] per chgroup:
+ * Rings are time-major with dense rows of pitch p[g] (a multiple of 4) per
+ * chgroup:
  *   Y[(t & y_mask)*y_rows + y_base[g] + s*p[g] + cell]   (subband s),
  *   D[seg_base[gd] + (t mod seg_depth[gd])*p[g] + cell]  (gd = g*n_dm + d),
  * each (chgroup, coarse DM) its own ring segment of seg_depth[gd] (>= 8)
  * time slots, deep enough for its own stage-2 delay; the float64 sky ring
- * of (g, d, cell) is row d_base[g] + d*p[g] + cell.  y_base, seg_base, p,
- * y_rows even and Y, D 16-byte aligned (two cells per access; a pad cell at
- * nf[g] when nf[g] is odd).  Block b covers cells [blk_c0[b], +
- * dsb_stage1_block_size()) of chgroup blk_g[b]. */
+ * of (g, d, cell) is row d_base[g] + d*p[g] + cell.  y_base and y_rows are
+ * multiples of 4, seg_base even, Y and D 16-byte aligned (four cells per
+ * 32-byte access; pad cells up to the pitch).  Block b covers cells
+ * [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b] and one group
+ * of dsb_stage1_dm_group() coarse DMs (grid y). */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, const long long* seg_base, const int* seg_depth, long long t0,
-                    int n_t, int n_dm,
-                    int ceff, void* sky_ring, int sky_window, int sky_head, int sky_count,
-                    int sky_subtract, cudaStream_t stream);
+                    int n_t, int n_dm, int ceff, int max_spread, void* sky_ring, int sky_window,
+                    int sky_head, int sky_count, int sky_subtract, int* status,
+                    cudaStream_t stream);
+/* Cells per block (blk_c0 multiples of it) and coarse DMs per block; the
+ * caller passes max_spread = the largest (max - min) of shift1[g, s, d] over
+ * the DMs of one group (d in [k*group, (k+1)*group)), which sizes the shared
+ * time window of a block; a larger spread sets DSB_E_CAPACITY in *status. */
 int dsb_stage1_block_size(void);
+int dsb_stage1_dm_group(void);
 /* ---- a12: fine-DM combine ---------------------------------------------------
  * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
  * the Hermitian half-spectrum fold and fftshift checkerboard of
