@@ -6,23 +6,29 @@
 // which replaces fused_dequant_combine_per_fdm_half + torch.fft.irfft2
 // (src/dsart/image/fused_combine_cuda.py:560-620, image/imager_gpu.py:590).
 //
-// One CTA owns one image at a time (persistent loop over images), in three
-// steps that never leave the SM except for one small L2-resident scratch:
+// One CTA owns one image at a time (persistent loop over images); nothing
+// but the ring reads and the image writes leaves the SM:
 //
 //  1. Combine.  The non-zero half-spectrum cells S (the union of every
 //     chgroup's uv pattern, a few thousand cells) are summed in shared memory
 //     from the time-major stage-2 ring: one coalesced read of each chgroup's
-//     coarse-DM slice, shared-memory float atomics into S.  S is copied to
-//     this CTA's row of the workspace (it stays in L2).
+//     coarse-DM slice, shared-memory float atomics into S.  Each thread then
+//     moves its own range of S (at most IMG_MAXE entries, whole slots) into
+//     tensor memory, which this kernel uses as plain per-thread storage:
+//     TMEM is otherwise idle here and holds S across the passes below while
+//     the shared buffer is reused for the transforms.
 //  2. Column transforms by decimation in frequency.  Columns w = 0 and N/2
 //     of G_h are Hermitian in u, so their transforms are real: they ride
 //     together as one complex column (w = 0 + i * w = N/2), leaving N/2
 //     complex columns.  With N = FOLD * LC, output rows x = FOLD*m + p are
 //         A[FOLD m + p, w] = sum_n' W_LC^(n' m) W_N^(n' p)
 //                              sum_q i^(q p) G_h[n' + LC q, w]      (FOLD = 4)
-//     so pass p (p = 0..3) folds S into LC-point columns and transforms them
-//     in place: a shared buffer of LC x N/2 complex values (66 KB for
-//     N = 256), small enough for three CTAs per SM.
+//     so pass p (p = 0..3) folds S (read back from TMEM) into the occupied
+//     slots (n', w) of a shared LC x N/2 complex buffer (66 KB for N = 256,
+//     small enough for three CTAs per SM) and transforms its columns in
+//     place.  A column whose entries all sit at n' = 0 transforms to a
+//     constant, so it is broadcast instead (for the bench's array, half of
+//     the columns); a column without entries is zero.
 //  3. Row transforms of the pass's LC rows, two real rows per complex
 //     transform (x_a + i x_b), staged in shared memory and written as float4.
 //
@@ -134,11 +140,16 @@ struct ImgArgs {
   const int* cell_base;     // (G + 1) multiples of 32
   const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
   int n_c2;
-  const int* corder;        // (N/2) packed columns in work order (balanced over groups)
-  const int* so;            // (N/2 * C1 + 1) S entries of (packed column, lane j)
-  const uint16_t* sq;       // (n_s) q | packed << 2 | parity(u + w) << 3 | (u mod LC) << 4
-                            //       | last entry of its folded slot << 10
-  int n_s, ws_stride;       // ws_stride: float2 per workspace row (even, >= n_s)
+  const int* thr_b;         // (THREADS + 1) S range [thr_b[i], thr_b[i+1]) of thread i
+  const uint4* gmeta;       // (IMG_MAXE / 8, THREADS) 8 x uint16 per (chunk, thread): entry
+                            //   col | n' << 7 | q << 13 | last of its slot << 15
+  const unsigned long long* srot;  // (THREADS) 2 bits per entry: packed | parity(u+w) << 1
+  const int* dcols;         // (n_dense) packed columns that need the LC-point transform
+  const unsigned long long* dmask;  // (n_dense) occupied slots n' of each
+  int n_dense;
+  const int* kcols;         // (n_const) col | has entries << 16: every entry at n' = 0
+  int n_const;
+  int n_s, s_stride;        // s_stride: even, >= n_s (the split S arrays in shared memory)
   const int* d_pitch;       // (G) cells (row pitch) of each chgroup's segments
   const int* n_filled;      // (G) pattern cells of each chgroup
   const int* sfine;         // (n_fine, G)
@@ -149,12 +160,17 @@ struct ImgArgs {
   int n_t;
   int fftshift;
   float* out;               // (n_f, n_t, N, N)
-  float2* ws;               // (gridDim.x, ws_stride)
   int* status;
 };
 
 constexpr int IMG_MAX_G = 64;
 constexpr int IMG_MAX_CHUNKS = 2048;  // 32-entry chunks of c_meta (chunk -> chgroup table)
+constexpr int IMG_THREADS = 256;
+// TMEM: 128 columns per CTA (three CTAs per SM take 384 of 512).  Warps w
+// and w + 4 reach the same 32 lanes, so each takes 64 columns: 32 complex
+// S entries per thread.
+constexpr int IMG_TMEM_COLS = 128;
+constexpr int IMG_MAXE = IMG_TMEM_COLS / 4;
 
 template <int N>
 struct ImgGeom {
@@ -164,16 +180,18 @@ struct ImgGeom {
   static constexpr int NC = N / 2;                // packed columns
   static constexpr int P = NC + 2;                // buffer row pitch (float2), = 2 mod 16
   static constexpr int RR = (N == 256) ? 16 : 8;  // N = RR * RR
-  static constexpr int THREADS = 256;
+  static constexpr int THREADS = IMG_THREADS;
   static constexpr int CG = THREADS / C1;         // column groups
   static constexpr int RG = THREADS / RR;         // row groups
   static constexpr int BUF = LC * P;              // float2 slots
   static_assert(C1 * C1 == LC && RR * RR == N, "unsupported size");
   static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
-  // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases
+  static_assert(NC <= 128 && LC <= 64, "entry metadata holds 7 bits of column, 6 of n'");
+  // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases |
+  // pattern sizes | TMEM address | chunk -> chgroup
   static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
-                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + IMG_MAX_CHUNKS;
+                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + 16 + IMG_MAX_CHUNKS;
 };
 
 template <int N>
@@ -191,10 +209,12 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   const float2** s_slice = reinterpret_cast<const float2**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
   int* s_nf = s_cbase + IMG_MAX_G + 1;
-  uint8_t* s_chunkg = reinterpret_cast<uint8_t*>(s_nf + IMG_MAX_G);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_nf + IMG_MAX_G);
+  uint8_t* s_chunkg = reinterpret_cast<uint8_t*>(s_tmem + 4);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
+  const int warp = tid >> 5;
   for (int i = tid; i < N; i += THREADS) tw[i] = A.tw[i];
   for (int i = tid; i < RR * RR; i += THREADS)
     rtw[i] = A.tw[((i % RR) * (i / RR)) & (N - 1)];
@@ -202,9 +222,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     ctw[i] = A.tw[((i % C1) * (i / C1) * (N / LC)) & (N - 1)];
   for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
   for (int g = tid; g < A.G; g += THREADS) s_nf[g] = A.n_filled[g];
-  if (A.cell_base[A.G] > 32 * IMG_MAX_CHUNKS) {  // uniform: every thread leaves
+  // this thread's S entries [sb, sb + sn), whole slots
+  const int sb = __ldg(A.thr_b + tid);
+  const int sn = __ldg(A.thr_b + tid + 1) - sb;
+  const bool bad_range = sn < 0 || sn > IMG_MAXE || sb < 0 || sb + sn > A.n_s;
+  if (__syncthreads_or(bad_range || A.cell_base[A.G] > 32 * IMG_MAX_CHUNKS)) {
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
-    return;
+    return;  // every thread leaves, before any TMEM is taken
   }
   // chunk -> chgroup (each chgroup's run of c_meta is a whole number of chunks)
   for (int c = tid; c < A.cell_base[A.G] / 32; c += THREADS) {
@@ -212,8 +236,18 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     while (g + 1 < A.G && A.cell_base[g + 1] <= 32 * c) ++g;
     s_chunkg[c] = (uint8_t)g;
   }
+  const unsigned long long srot = __ldg(A.srot + tid);
+  const int nch = (__reduce_max_sync(0xffffffffu, sn) + 7) >> 3;  // 8-entry chunks, per warp
+  if (warp == 0) {
+    tmem_alloc(s_tmem, IMG_TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *s_tmem + ((uint32_t)((warp & 3) * 32) << 16) +
+                         (uint32_t)((warp >> 2) * (IMG_TMEM_COLS / 2));
 
-  float2* ws = A.ws + (size_t)blockIdx.x * A.ws_stride;
   const int n_tot = A.cell_base[A.G];
   const float scale = 0.5f / (float)(N * N);
   const int n_img = A.n_f * A.n_t;
@@ -241,7 +275,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
-      for (int i = tid; i < A.ws_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = tid; i < A.s_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
     // ---- 1. combine into S (shared-memory float atomics) ----
@@ -249,7 +283,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       // separate real and imaginary arrays: a warp's 32 atomics spread over
       // all 32 banks instead of the even (or odd) half
       float* s_re = reinterpret_cast<float*>(buf);
-      float* s_im = s_re + A.ws_stride;
+      float* s_im = s_re + A.s_stride;
       auto add = [&](unsigned m, float2 v) {
         const unsigned t = m & 0xffffu;
         atomicAdd(s_re + t, v.x);
@@ -285,46 +319,70 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       }
     }
     __syncthreads();
+    // ---- this thread's S entries into TMEM, with the rotation that does not
+    //      depend on the pass (i for the packed column N/2, -1 for the
+    //      fftshift checkerboard) already applied ----
     {
-      const float2* re2 = reinterpret_cast<const float2*>(buf);
-      const float2* im2 = re2 + A.ws_stride / 2;
-      float4* w4 = reinterpret_cast<float4*>(ws);
-      for (int i = tid; i < A.ws_stride / 2; i += THREADS) {
-        const float2 r = re2[i], m = im2[i];
-        w4[i] = make_float4(r.x, m.x, r.y, m.y);
+      const float* s_re = reinterpret_cast<const float*>(buf);
+      const float* s_im = s_re + A.s_stride;
+      for (int c = 0; c < nch; ++c) {
+        uint32_t r[16];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int i = 8 * c + j;
+          float2 v = make_float2(0.f, 0.f);
+          if (i < sn) {
+            const unsigned b = (unsigned)(srot >> (2 * i)) & 3u;
+            v = crot(make_float2(s_re[sb + i], s_im[sb + i]),
+                     (int)(b & 1u) + ((b & 2u) ? shift_rot : 0));
+          }
+          r[2 * j] = __float_as_uint(v.x);
+          r[2 * j + 1] = __float_as_uint(v.y);
+        }
+        tmem_st16(tbase + 16 * c, r);
       }
+      tmem_st_wait();
     }
-    __syncthreads();
+    __syncthreads();  // S is read: buf is free for the passes
 
     for (int p = 0; p < FOLD; ++p) {
-      // ---- 2. folded column transforms of pass p (in place in buf) ----
-      for (int ci = cgi; ci < NC; ci += Gm::CG) {
-        // fold column col's S entries into its LC slots of buf, lane j owning
-        // the slots n' = j (mod C1): its entries are one contiguous run
-        // sorted by slot, each slot written once (after its last entry)
-        const int col = __ldg(A.corder + ci);
-        float2* colp = buf + col;
+      // ---- 2a. fold S into the occupied slots (n', col) of buf: each slot's
+      //      entries are consecutive in one thread's range, written once
+      //      after the last of them ----
+      {
+        float2 acc = make_float2(0.f, 0.f);
+        for (int c = 0; c < nch; ++c) {
+          uint32_t r[16];
+          tmem_ld16_wait(tbase + 16 * c, r);
+          const uint4 md = __ldg(A.gmeta + c * THREADS + tid);
+          const unsigned mw[4] = {md.x, md.y, md.z, md.w};
 #pragma unroll
-        for (int k = 0; k < C1; ++k) colp[(cj + C1 * k) * P] = make_float2(0.f, 0.f);
-        {
-          const int e1 = __ldg(A.so + col * C1 + cj + 1);
-          float2 acc = make_float2(0.f, 0.f);
-#pragma unroll 4
-          for (int e = __ldg(A.so + col * C1 + cj); e < e1; ++e) {
-            const int qq = __ldg(A.sq + e);
-            const int rot = (qq & 3) * p + ((qq >> 2) & 1) + (((qq >> 3) & 1) ? shift_rot : 0);
-            acc = cadd(acc, crot(ws[e], rot));
-            if (qq & 1024) {
-              colp[((qq >> 4) & (LC - 1)) * P] = acc;
-              acc = make_float2(0.f, 0.f);
+          for (int j = 0; j < 8; ++j) {
+            if (8 * c + j < sn) {
+              const unsigned m = (mw[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+              const float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
+              acc = cadd(acc, crot(v, (int)((m >> 13) & 3u) * p));
+              if (m & 0x8000u) {
+                buf[((m >> 7) & (LC - 1)) * P + (m & (NC - 1))] = acc;
+                acc = make_float2(0.f, 0.f);
+              }
             }
           }
         }
+      }
+      __syncthreads();
+      // ---- 2b. column transforms of pass p (in place in buf); only the
+      //      occupied slots of a column are read ----
+      for (int di = cgi; di < A.n_dense; di += Gm::CG) {
+        const int col = __ldg(A.dcols + di) & (NC - 1);
+        const unsigned long long occ = __ldg(A.dmask + di);
+        float2* colp = buf + col;
         float2 y[C1];
 #pragma unroll
         for (int k = 0; k < C1; ++k) {
           const int n1 = cj + C1 * k;
-          y[k] = cmul(colp[n1 * P], tw[(n1 * p) & (N - 1)]);
+          y[k] = ((occ >> n1) & 1ull) ? cmul(colp[n1 * P], tw[(n1 * p) & (N - 1)])
+                                      : make_float2(0.f, 0.f);
         }
         idftR<C1>(y);
 #pragma unroll
@@ -339,6 +397,18 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         idftR<C1>(y);
 #pragma unroll
         for (int m2 = 0; m2 < C1; ++m2) colp[(cj + C1 * m2) * P] = y[m2];
+      }
+      // constant columns: every row holds the folded slot n' = 0 (row 0
+      // itself is already in place); columns without entries are zero
+      for (int i = tid; i < A.n_const * LC; i += THREADS) {
+        const int kc = __ldg(A.kcols + i / LC);
+        const int m = i & (LC - 1);
+        const int col = kc & (NC - 1);
+        if (kc >> 16) {
+          if (m) buf[m * P + col] = buf[col];
+        } else {
+          buf[m * P + col] = make_float2(0.f, 0.f);
+        }
       }
       __syncthreads();
       // ---- 3. row transforms: folded rows (2pr, 2pr + 1) are image rows
@@ -396,9 +466,20 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       __syncthreads();
     }
   }
+  // every tcgen05.ld above was waited for; give the columns back
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(*s_tmem, IMG_TMEM_COLS);
+  }
 }
 
 // Resident CTAs for image_kernel<N> on this device (the persistent grid).
+// The occupancy API answers 1 CTA per SM for any kernel that allocates
+// tensor memory (measured on B200 with CUDA 12.9), while the SM runs as many
+// as its shared memory, registers and 512 TMEM columns hold: three here.  So
+// the count is taken from those limits directly.
 template <int N>
 int image_grid(int* blocks) {
   using Gm = ImgGeom<N>;
@@ -407,13 +488,18 @@ int image_grid(int* blocks) {
     if (cudaFuncSetAttribute(image_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Gm::SMEM) != cudaSuccess)
       return DSB_E_CUDA;
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, image_kernel<N>, Gm::THREADS,
-                                                      Gm::SMEM) != cudaSuccess)
-      return DSB_E_CUDA;
-    int dev = 0, sms = 148;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, image_kernel<N>) != cudaSuccess) return DSB_E_CUDA;
+    int dev = 0, sms = 148, smem_sm = 0, smem_rsv = 0, regs_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    const int by_smem = smem_sm / ((int)Gm::SMEM + fa.sharedSizeBytes + smem_rsv);
+    const int regs_cta = (fa.numRegs + 7) / 8 * 8 * Gm::THREADS;
+    const int by_regs = regs_cta > 0 ? regs_sm / regs_cta : 1;
+    const int occ = std::min({3, by_smem, by_regs, 512 / IMG_TMEM_COLS});
     cached = std::max(1, occ) * sms;
   }
   *blocks = cached;
@@ -423,11 +509,11 @@ int image_grid(int* blocks) {
 template <int N>
 int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   using Gm = ImgGeom<N>;
-  if (A.ws_stride > Gm::BUF) return DSB_E_CAPACITY;
+  if (A.s_stride > Gm::BUF) return DSB_E_CAPACITY;
   int blocks = 0;
   const int rc = image_grid<N>(&blocks);
   if (rc != DSB_OK) return rc;
-  blocks = std::min(blocks, max_blocks);
+  if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   blocks = std::max(1, std::min(blocks, A.n_f * A.n_t));
   image_kernel<N><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
   return launch_status();
@@ -445,45 +531,35 @@ int dsb_image_fold(int n_grid) {
   }
 }
 
-long long dsb_image_workspace_bytes(int n_grid, int n_s) {
-  if (n_s <= 0) return -1;
-  int blocks = 0;
-  int rc = DSB_E_UNSUPPORTED;
-  switch (n_grid) {
-    case 64: rc = image_grid<64>(&blocks); break;
-    case 256: rc = image_grid<256>(&blocks); break;
-    default: break;
-  }
-  if (rc != DSB_OK) return -1;
-  return (long long)blocks * ((n_s + 1) & ~1) * 8;
-}
+int dsb_image_threads(void) { return IMG_THREADS; }
+
+int dsb_image_max_entries(void) { return IMG_MAXE; }
 
 int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
-                  const int* corder, const int* so, const unsigned short* sq, int n_s,
-                  const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,
-                  const void* twiddles, int f0, int n_f, int G, int N, long long t0, int n_t,
-                  int fftshift, void* out, void* workspace, long long workspace_bytes,
-                  int max_blocks, int* status, cudaStream_t stream) {
+                  const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
+                  const int* dcols, const unsigned long long* dmask, int n_dense,
+                  const int* kcols, int n_const, const int* d_pitch, const int* n_filled,
+                  const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
+                  int N, long long t0, int n_t, int fftshift, void* out, int max_blocks,
+                  int* status, cudaStream_t stream) {
   if (!D || !seg_base || !seg_depth || n_coarse <= 0 || !c_meta || !cell_base ||
-      (n_c2 > 0 && !c2) || n_c2 < 0 || !corder || !so || !sq || n_s <= 0 || n_s > 65536 ||
-      !d_pitch || !n_filled || !sfine || !f2c || !twiddles || !out || !workspace || n_f <= 0 ||
-      n_t <= 0 || G <= 0 || G > IMG_MAX_G)
+      (n_c2 > 0 && !c2) || n_c2 < 0 || !thr_b || !gmeta || !srot || n_s <= 0 ||
+      n_s > 65536 || n_dense < 0 || n_const < 0 || (n_dense > 0 && (!dcols || !dmask)) ||
+      (n_const > 0 && !kcols) || !d_pitch || !n_filled || !sfine || !f2c || !twiddles ||
+      !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
     return DSB_E_ARG;
-  if ((reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
+  if ((reinterpret_cast<uintptr_t>(gmeta) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
     return DSB_E_ARG;
+  if (n_dense + n_const != N / 2) return DSB_E_ARG;  // every packed column, once
   const int stride = (n_s + 1) & ~1;
-  const long long rows = workspace_bytes / ((long long)stride * 8);
-  if (rows <= 0) return DSB_E_CAPACITY;
-  int cap = (int)std::min<long long>(rows, 1 << 30);
-  if (max_blocks > 0) cap = std::min(cap, max_blocks);
   ImgArgs A{(const float2*)D, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
-            n_c2, corder, so, (const uint16_t*)sq, n_s, stride, d_pitch, n_filled, sfine, f2c,
-            (const float2*)twiddles, f0, n_f, G, t0, n_t, fftshift, (float*)out,
-            (float2*)workspace, status};
+            n_c2, thr_b, (const uint4*)gmeta, srot, dcols, dmask, n_dense, kcols, n_const,
+            n_s, stride, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
+            t0, n_t, fftshift, (float*)out, status};
   switch (N) {
-    case 64: return launch_image<64>(A, cap, stream);
-    case 256: return launch_image<256>(A, cap, stream);
+    case 64: return launch_image<64>(A, max_blocks, stream);
+    case 256: return launch_image<256>(A, max_blocks, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

@@ -41,10 +41,11 @@ _SIGNATURES = {
     "dsb_stage1_block_size": [],
     "dsb_stage1_dm_group": [],
     "dsb_image_fold": [_c_int],
-    "dsb_image_workspace_bytes": [_c_int, _c_int],
+    "dsb_image_threads": [],
+    "dsb_image_max_entries": [],
     "dsb_image_fft": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp,
-                      _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_int, _c_int,
-                      _vp, _vp, _c_ll, _c_int, _vp, _vp],
+                      _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
+                      _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],
     "dsb_combine_rows": [_vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
                          _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp],
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
@@ -64,7 +65,7 @@ _SIGNATURES = {
                          _vp, _vp],
 }
 
-_RESTYPES = {"dsb_image_workspace_bytes": _c_ll}
+_RESTYPES: dict = {}
 
 _lib: Optional[ctypes.CDLL] = None
 

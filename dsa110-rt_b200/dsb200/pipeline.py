@@ -146,15 +146,40 @@ class Tables:
 
 @dataclass
 class ImageTables:
-    """Tables of dsb_image_fft: the distinct non-zero half cells S and how
-    every pattern cell of every chgroup lands on them."""
+    """Tables of dsb_image_fft: the distinct non-zero half cells S, how every
+    pattern cell of every chgroup lands on them, and how the kernel's
+    threads and column groups split them."""
     n_s: int
     c_meta: np.ndarray      # uint32 s | conj << 16 | g << 17; chgroup runs padded to 32
     cell_base: np.ndarray   # (G + 1) int32
     c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
-    corder: np.ndarray      # (N/2) int32: packed columns in work order
-    so: np.ndarray          # (N/2 * C1 + 1) int32: S range of (packed column, n' mod C1)
-    sq: np.ndarray          # (n_s) uint16: q | packed << 2 | parity << 3 | n' << 4 | last << 10
+    thr_b: np.ndarray       # (threads + 1) int32: S range of each kernel thread
+    gmeta: np.ndarray       # (max_entries / 8, threads, 8) uint16: w' | n' << 7 | q << 13 | last << 15
+    srot: np.ndarray        # (threads,) uint64: 2 bits per entry: packed | parity << 1
+    dcols: np.ndarray       # (n_dense,) int32: packed columns with an entry off n' = 0
+    dmask: np.ndarray       # (n_dense,) uint64: their occupied n'
+    kcols: np.ndarray       # (n_const,) int32: w' | has entries << 16 (constant or zero columns)
+
+
+def _split_slots(sizes: np.ndarray, n_threads: int, cap: int) -> np.ndarray:
+    """Thread boundaries (n_threads + 1) over consecutive slots of the given
+    sizes: whole slots per thread, at most ``cap`` entries each, the
+    smallest such maximum found by greedy filling."""
+    total = int(sizes.sum())
+    lo = max(-(-total // n_threads), int(sizes.max()) if sizes.size else 0)
+    for m in range(lo, cap + 1):
+        b, cur = [0], 0
+        for sz in sizes.tolist():
+            if cur + sz > m:
+                b.append(b[-1] + cur)
+                cur = 0
+            cur += sz
+        b.append(b[-1] + cur)
+        if len(b) - 1 <= n_threads:
+            b += [total] * (n_threads + 1 - len(b))
+            return np.asarray(b, np.int64)
+    raise ValueError(f"dsb_image_fft: {total} half cells do not fit {n_threads} threads x "
+                     f"{cap} entries")
 
 
 def build_image_tables(pats, N: int) -> ImageTables:
@@ -162,9 +187,11 @@ def build_image_tables(pats, N: int) -> ImageTables:
     chgroup g adds to half cell (u, w) when w <= N/2 and, conjugated, to its
     mirror ((N-u) % N, (N-w) % N) when that column is <= N/2 (both for
     w = 0 and w = N/2): the Hermitian fold of fused_combine_cuda.py:560-620."""
-    fold = int(_lib.lib().dsb_image_fold(N))
+    L = _lib.lib()
+    fold = int(L.dsb_image_fold(N))
     if fold <= 0:
         raise ValueError(f"dsb_image_fft does not support N={N}")
+    n_thr, cap = int(L.dsb_image_threads()), int(L.dsb_image_max_entries())
     LC, NC = N // fold, N // 2
     G = len(pats)
     if G > 63:
@@ -191,39 +218,38 @@ def build_image_tables(pats, N: int) -> ImageTables:
     allw = np.concatenate([t1w, t2w])
     packed = (allw == N // 2).astype(np.int64)
     wp = np.where(packed == 1, 0, allw)
-    C1 = int(round(np.sqrt(LC)))
-    n1 = allu % LC
-    # slot order inside a column: lane j = n' mod C1 first, then n' div C1
-    lane_slot = (n1 % C1) * C1 + n1 // C1
-    key = ((wp * LC + lane_slot) * fold + allu // LC) * 2 + packed
+    key = ((wp * LC + allu % LC) * fold + allu // LC) * 2 + packed
     ukey, inv = np.unique(key, return_inverse=True)
     n_s = int(ukey.size)
     if n_s >= 1 << 16:
         raise ValueError("dsb_image_fft needs fewer than 65536 distinct half cells")
     s_pk = ukey & 1
     s_q = (ukey >> 1) % fold
-    s_slot = (ukey >> 1) // fold          # wp * LC + lane_slot
-    s_wp, s_ls = s_slot // LC, s_slot % LC
-    s_n = (s_ls % C1) * C1 + s_ls // C1   # back to n'
+    s_slot = (ukey >> 1) // fold          # w' * LC + n'
+    s_wp, s_n = s_slot // LC, s_slot % LC
     s_u = s_n + LC * s_q
     s_w = np.where(s_pk == 1, N // 2, s_wp)
     last = np.ones(n_s, np.int64)
     last[:-1] = (s_slot[1:] != s_slot[:-1]).astype(np.int64)
-    sq = (s_q | (s_pk << 2) | (((s_u + s_w) & 1) << 3) | (s_n << 4) | (last << 10)
-          ).astype(np.uint16)
-    so = np.zeros(NC * C1 + 1, np.int64)
-    so[1:] = np.cumsum(np.bincount(s_wp * C1 + s_ls // C1, minlength=NC * C1))
-    # work order: columns by entry count, dealt round-robin back and forth
-    # over the thread groups (group i takes corder[i], corder[i + n_groups], ...)
-    cnt = np.bincount(s_wp, minlength=NC)
-    n_groups = 256 // C1
-    by = np.argsort(-cnt, kind="stable")
-    corder = np.empty(NC, np.int64)
-    for r in range(0, NC, n_groups):
-        chunk = by[r:r + n_groups]
-        if (r // n_groups) % 2:
-            chunk = chunk[::-1]
-        corder[r:r + chunk.size] = chunk
+    # thread ranges: whole slots (a slot's entries are consecutive in S)
+    starts = np.flatnonzero(np.r_[True, s_slot[1:] != s_slot[:-1]])
+    thr_b = _split_slots(np.diff(np.r_[starts, n_s]), n_thr, cap)
+    owner = np.repeat(np.arange(n_thr), np.diff(thr_b))
+    idx = np.arange(n_s) - thr_b[owner]
+    gmeta = np.zeros((cap // 8, n_thr, 8), np.uint16)
+    gmeta[idx // 8, owner, idx % 8] = (s_wp | (s_n << 7) | (s_q << 13) | (last << 15)
+                                       ).astype(np.uint16)
+    srot = np.zeros(n_thr, np.uint64)
+    bits = (s_pk | (((s_u + s_w) & 1) << 1)).astype(np.uint64) << (2 * idx).astype(np.uint64)
+    np.bitwise_or.at(srot, owner, bits)
+    # columns: dense (an entry off n' = 0) get the LC-point transform; the
+    # rest are constant (every entry at n' = 0) or zero
+    occ = np.zeros(NC, np.uint64)
+    np.bitwise_or.at(occ, s_wp, np.left_shift(np.uint64(1), s_n.astype(np.uint64)))
+    dense = (occ & ~np.uint64(1)) != 0
+    dcols = np.flatnonzero(dense).astype(np.int32)
+    kc = np.flatnonzero(~dense)
+    kcols = (kc | ((occ[kc] != 0).astype(np.int64) << 16)).astype(np.int32)
     n1 = u.size
     # each chgroup's run padded with 0xffffffff to a whole number of 32-entry
     # chunks (the kernel finds an entry's chgroup from its chunk)
@@ -234,8 +260,9 @@ def build_image_tables(pats, N: int) -> ImageTables:
     c2 = np.stack([k[both] | (g[both] << 16), inv[n1:] | (1 << 16)], axis=1).astype(np.int32)
     cell_base = cell_base.astype(np.int32)
     return ImageTables(n_s=n_s, c_meta=c_meta, cell_base=cell_base,
-                       c2=np.ascontiguousarray(c2.reshape(-1, 2)), corder=corder.astype(np.int32),
-                       so=so.astype(np.int32), sq=sq)
+                       c2=np.ascontiguousarray(c2.reshape(-1, 2)),
+                       thr_b=thr_b.astype(np.int32), gmeta=gmeta, srot=srot, dcols=dcols,
+                       dmask=occ[dcols], kcols=kcols)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -358,12 +385,10 @@ class SearchPipeline:
         it = T.img
         self.d_img_cmeta = d(it.c_meta.view(np.int32))
         self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
-        self.d_img_corder, self.d_img_so = d(it.corder), d(it.so)
-        self.d_img_sq = d(it.sq.view(np.int16))
-        ws_bytes = int(_lib.lib().dsb_image_workspace_bytes(cfg.n_grid, it.n_s))
-        if ws_bytes <= 0:
-            raise ValueError(f"dsb_image_fft does not support N={cfg.n_grid}")
-        self.img_ws = torch.empty(ws_bytes // 4, dtype=torch.float32, device=self.dev)
+        self.d_img_thrb, self.d_img_gmeta = d(it.thr_b), d(it.gmeta.view(np.int16))
+        self.d_img_srot = d(it.srot.view(np.int64))
+        self.d_img_dcols, self.d_img_dmask = d(it.dcols), d(it.dmask.view(np.int64))
+        self.d_img_kcols = d(it.kcols)
         self.d_tw = d(T.twiddles)
         self.d_shift1, self.d_shift2 = d(T.shift1), d(T.shift2)
         self.d_dbase = d(T.d_base)
@@ -509,12 +534,12 @@ class SearchPipeline:
             _lib.ptr(self.D), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
             cfg.coarse_dm.size, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
-            _lib.ptr(self.d_img_corder), _lib.ptr(self.d_img_so), _lib.ptr(self.d_img_sq),
-            it.n_s, _lib.ptr(self.d_pitch), _lib.ptr(self.d_nfilled),
-            _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
+            _lib.ptr(self.d_img_thrb), _lib.ptr(self.d_img_gmeta), _lib.ptr(self.d_img_srot),
+            it.n_s, _lib.ptr(self.d_img_dcols), _lib.ptr(self.d_img_dmask), int(it.dcols.size),
+            _lib.ptr(self.d_img_kcols), int(it.kcols.size), _lib.ptr(self.d_pitch),
+            _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),
-            _lib.ptr(self.img_ws), self.img_ws.numel() * 4, max_blocks, _lib.ptr(self.status),
-            _lib.stream_of(self.dev)), "dsb_image_fft")
+            max_blocks, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_image_fft")
 
     def _search(self, jc: int, collect: bool = True) -> None:
         cfg, T = self.cfg, self.tab

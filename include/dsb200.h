@@ -181,32 +181,41 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * 1/N^2 normalisation (fftshifted when fftshift != 0).
  * Tables (built once per pattern set):
  *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
- *      (packed column w' = (w == N/2 ? 0 : w), n' mod C1, n' div C1, u div LC,
- *      w == N/2) with n' = u mod LC, LC = N / dsb_image_fold(N), C1*C1 = LC;
+ *      (packed column w' = (w == N/2 ? 0 : w), n', u div LC, w == N/2) with
+ *      n' = u mod LC, LC = N / dsb_image_fold(N); a slot is one (w', n');
  *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k <
  *      n_filled[g] of chgroup g adds its value (conjugated if conj) to S
  *      entry s; each chgroup's run is padded with 0xffffffff to a multiple
  *      of 32 entries (cell_base[g] multiples of 32, cell_base[G] <= 65536);
  *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
  *      w = N/2 that also land on their mirror);
- *   corder: (N/2) packed columns in the order the kernel's thread groups
- *      take them (any permutation; balance dense and sparse columns);
- *   so[w'*C1 + j .. + 1]: S range of packed column w', n' mod C1 = j;
- *   sq[s] = (u div LC) | (w == N/2) << 2 | ((u + w) & 1) << 3 | n' << 4 |
- *      (s is the last entry of its (w', n')) << 10.
- * workspace: >= dsb_image_workspace_bytes(N, n_s) bytes, 16-byte aligned (one
- * L2-resident row of S per resident CTA).  twiddles: (N) complex64
- * exp(+2 pi i e/N).  Supported N: 64, 256; n_s must fit the kernel's
- * shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY is returned. */
+ *   thr_b: (dsb_image_threads() + 1) S ranges, one per kernel thread, each
+ *      made of whole slots and at most dsb_image_max_entries() long;
+ *   gmeta: (max_entries / 8, threads, 8) uint16, 16-byte aligned: entry i
+ *      of thread t at [i / 8][t][i % 8] = w' | n' << 7 | (u div LC) << 13 |
+ *      (last entry of its slot) << 15;
+ *   srot: (threads) uint64, 2 bits per entry i at bit 2i: (w == N/2) |
+ *      ((u + w) & 1) << 1;
+ *   dcols/dmask: the n_dense packed columns with an entry off n' = 0 and
+ *      the bit mask of their occupied n';
+ *   kcols: the n_const other packed columns, w' | (has entries) << 16;
+ *      n_dense + n_const = N/2, every packed column once.
+ * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256; n_s must
+ * fit the kernel's shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY
+ * is returned.  status: a thread range longer than max_entries or
+ * cell_base[G] above 65536 sets DSB_E_CAPACITY and writes nothing.  Each
+ * CTA holds 128 columns of tensor memory while it runs. */
 int dsb_image_fold(int n_grid);
-long long dsb_image_workspace_bytes(int n_grid, int n_s);
+int dsb_image_threads(void);
+int dsb_image_max_entries(void);
 int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
-                  const int* corder, const int* so, const unsigned short* sq, int n_s,
-                  const int* d_pitch, const int* n_filled, const int* sfine, const int* f2c,
-                  const void* twiddles, int f0, int n_f, int G, int N, long long t0, int n_t,
-                  int fftshift, void* out, void* workspace, long long workspace_bytes,
-                  int max_blocks, int* status, cudaStream_t stream);
+                  const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
+                  const int* dcols, const unsigned long long* dmask, int n_dense,
+                  const int* kcols, int n_const, const int* d_pitch, const int* n_filled,
+                  const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
+                  int N, long long t0, int n_t, int fftshift, void* out, int max_blocks,
+                  int* status, cudaStream_t stream);
 
 /* ---- a13/a14: edge mask x Layer-1 normalisation into the detector cube -----
  * Replaces the mask multiply + cube write of GpuImager.process_cube

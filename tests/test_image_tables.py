@@ -35,6 +35,11 @@ def _patterns(N, n_g, seed):
 
 
 def _emulate(T, slices, N, fftshift):
+    """The kernel's steps, from its tables: combine into S, per-thread ranges
+    with the static rotation, the per-pass fold into slots, dense columns
+    transformed from their occupied slots only, constant columns broadcast,
+    then the row transforms.  Slots no thread writes in a pass are NaN, so a
+    read of one shows up in the result."""
     fold = 4
     LC, NC = N // fold, N // 2
     S = np.zeros(T.n_s, np.complex128)
@@ -47,20 +52,28 @@ def _emulate(T, slices, N, fftshift):
         S[sc & 0xFFFF] += np.conj(v) if (sc >> 16) & 1 else v
     A = np.zeros((N, NC), np.complex128)
     twN = np.exp(2j * np.pi * np.arange(N) / N)
-    q = (T.sq & 3).astype(np.int64)
-    pk = ((T.sq >> 2) & 1).astype(np.int64)
-    par = ((T.sq >> 3) & 1).astype(np.int64)
-    C1 = int(round(np.sqrt(LC)))
-    col = np.repeat(np.arange(NC * C1), np.diff(T.so)) // C1
-    slot = col * LC + ((T.sq >> 4) & (LC - 1)).astype(np.int64)
+    n_thr = T.thr_b.size - 1
     for p in range(fold):
-        rot = q * p + pk + (2 * par if fftshift else 0)
-        y = np.zeros(NC * LC, np.complex128)
-        np.add.at(y, slot, S * (1j) ** (rot % 4))
-        y = y.reshape(NC, LC).T                       # [n', col]
-        y = y * twN[(np.arange(LC) * p) % N][:, None]
-        X = np.fft.ifft(y, axis=0) * LC               # sum_n' y W_LC^(+n' m)
-        A[p::fold, :] = X
+        buf = np.full((LC, NC), np.nan, np.complex128)
+        for t in range(n_thr):
+            b, e = int(T.thr_b[t]), int(T.thr_b[t + 1])
+            acc = 0j
+            for i in range(e - b):
+                m = int(T.gmeta[i // 8, t, i % 8])
+                sr = (int(T.srot[t]) >> (2 * i)) & 3
+                rot = (sr & 1) + (2 if (sr & 2) and fftshift else 0) + ((m >> 13) & 3) * p
+                acc += S[b + i] * (1j) ** (rot % 4)
+                if m & 0x8000:
+                    buf[(m >> 7) & (LC - 1), m & (NC - 1)] = acc
+                    acc = 0j
+        out = np.full((LC, NC), np.nan, np.complex128)
+        for col, occ in zip(T.dcols.tolist(), T.dmask.tolist()):
+            y = np.array([buf[n, col] if (occ >> n) & 1 else 0j for n in range(LC)])
+            y = y * twN[(np.arange(LC) * p) % N]
+            out[:, col] = np.fft.ifft(y) * LC          # sum_n' y W_LC^(+n' m)
+        for kc in T.kcols.tolist():
+            out[:, kc & 0xFFFF] = buf[0, kc & 0xFFFF] if kc >> 16 else 0j
+        A[p::fold, :] = out
     img = np.zeros((N, N))
     for x in range(N):
         Y = np.zeros(N, np.complex128)
@@ -97,23 +110,37 @@ def test_image_tables_restate_irfft2(N, n_g, fftshift):
 
 
 def test_image_tables_layout():
+    from dsb200 import _lib
     N = 256
     pats = _patterns(N, 3, seed=3)
     T = build_image_tables(pats, N)
-    LC = N // 4
-    assert T.so[0] == 0 and T.so[-1] == T.n_s and np.all(np.diff(T.so) >= 0)
-    C1 = 8
-    assert T.so.size == N // 2 * C1 + 1
-    assert sorted(T.corder.tolist()) == list(range(N // 2))
-    # lane j = n' mod C1 of column w' owns exactly the entries of its run
-    lane = np.repeat(np.arange(N // 2 * C1), np.diff(T.so)) % C1
-    n1 = (T.sq >> 4) & (LC - 1)
-    assert np.array_equal(n1 % C1, lane)
-    # "last" marks the final entry of each (column, n') run of equal slots
-    col = np.repeat(np.arange(N // 2 * C1), np.diff(T.so)) // C1
-    slot = col * LC + n1
+    LC, NC = N // 4, N // 2
+    n_thr, cap = int(_lib.lib().dsb_image_threads()), int(_lib.lib().dsb_image_max_entries())
+    assert T.thr_b.size == n_thr + 1 and T.thr_b[0] == 0 and T.thr_b[-1] == T.n_s
+    cnt = np.diff(T.thr_b)
+    assert np.all(cnt >= 0) and cnt.max() <= cap
+    assert T.gmeta.shape == (cap // 8, n_thr, 8)
+    # entries in S order: slot (w', n') of each, and "last" on its final entry
+    owner = np.repeat(np.arange(n_thr), cnt)
+    idx = np.arange(T.n_s) - T.thr_b[owner]
+    m = T.gmeta[idx // 8, owner, idx % 8].astype(np.int64)
+    slot = (m & 127) * LC + ((m >> 7) & (LC - 1))
+    assert np.all(np.diff(slot) >= 0)                    # S is sorted by slot
     last = np.append(slot[1:] != slot[:-1], True)
-    assert np.array_equal(((T.sq >> 10) & 1).astype(bool), last)
+    assert np.array_equal((m >> 15).astype(bool), last)
+    # every thread range ends on a slot boundary (whole slots per thread)
+    ends = T.thr_b[1:][cnt > 0] - 1
+    assert np.all((m[ends] >> 15) == 1)
+    # columns: each packed column once; dense masks are the occupied n'
+    cols = np.concatenate([T.dcols, T.kcols & 0xFFFF])
+    assert sorted(cols.tolist()) == list(range(NC))
+    occ = {}
+    for sl in np.unique(slot).tolist():
+        occ[sl // LC] = occ.get(sl // LC, 0) | (1 << (sl % LC))
+    for c, msk in zip(T.dcols.tolist(), T.dmask.tolist()):
+        assert msk == occ[c] and msk & ~1
+    for kc in T.kcols.tolist():
+        assert occ.get(kc & 0xFFFF, 0) == (1 if kc >> 16 else 0)
     assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 32 == 0)
     for g, p in enumerate(pats):                # padding after each chgroup's run
         assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
