@@ -51,14 +51,14 @@ DSB_DEV float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 DSB_DEV float2 cmul_i(float2 a) { return make_float2(-a.y, a.x); }  // i * a
-// a * i^k
-DSB_DEV float2 crot(float2 a, int k) {
-  switch (k & 3) {
-    case 1: return make_float2(-a.y, a.x);
-    case 2: return make_float2(-a.x, -a.y);
-    case 3: return make_float2(a.y, -a.x);
-    default: return a;
-  }
+
+// a * i^k for a k known only at run time, without branches: swap the parts
+// for odd k, then flip the signs ((k+1) & 2 on the first, k & 2 on the second)
+DSB_DEV float2 crot_rt(float2 a, unsigned k) {
+  const bool sw = k & 1u;
+  const float u = sw ? a.y : a.x, v = sw ? a.x : a.y;
+  return make_float2(__uint_as_float(__float_as_uint(u) ^ (((k + 1u) & 2u) << 30)),
+                     __uint_as_float(__float_as_uint(v) ^ ((k & 2u) << 30)));
 }
 
 // cos/sin of multiples of pi/8 (exact mathematical constants, float-rounded)
@@ -164,7 +164,6 @@ struct ImgArgs {
 };
 
 constexpr int IMG_MAX_G = 64;
-constexpr int IMG_MAX_CHUNKS = 2048;  // 32-entry chunks of c_meta (chunk -> chgroup table)
 constexpr int IMG_THREADS = 256;
 // TMEM: 128 columns per CTA (three CTAs per SM take 384 of 512).  Warps w
 // and w + 4 reach the same 32 lanes, so each takes 64 columns: 32 complex
@@ -189,9 +188,9 @@ struct ImgGeom {
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
   static_assert(NC <= 128 && LC <= 64, "entry metadata holds 7 bits of column, 6 of n'");
   // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases |
-  // pattern sizes | TMEM address | chunk -> chgroup
+  // ends of the chgroups' cells | TMEM address
   static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
-                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + 16 + IMG_MAX_CHUNKS;
+                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + 16;
 };
 
 template <int N>
@@ -208,9 +207,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   float2* ctw = rtw + RR * RR;
   const float2** s_slice = reinterpret_cast<const float2**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
-  int* s_nf = s_cbase + IMG_MAX_G + 1;
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_nf + IMG_MAX_G);
-  uint8_t* s_chunkg = reinterpret_cast<uint8_t*>(s_tmem + 4);
+  int* s_end = s_cbase + IMG_MAX_G + 1;
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_end + IMG_MAX_G);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -221,20 +219,14 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   for (int i = tid; i < C1 * C1; i += THREADS)
     ctw[i] = A.tw[((i % C1) * (i / C1) * (N / LC)) & (N - 1)];
   for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
-  for (int g = tid; g < A.G; g += THREADS) s_nf[g] = A.n_filled[g];
+  for (int g = tid; g < A.G; g += THREADS) s_end[g] = A.cell_base[g] + A.n_filled[g];
   // this thread's S entries [sb, sb + sn), whole slots
   const int sb = __ldg(A.thr_b + tid);
   const int sn = __ldg(A.thr_b + tid + 1) - sb;
   const bool bad_range = sn < 0 || sn > IMG_MAXE || sb < 0 || sb + sn > A.n_s;
-  if (__syncthreads_or(bad_range || A.cell_base[A.G] > 32 * IMG_MAX_CHUNKS)) {
+  if (__syncthreads_or(bad_range || (A.cell_base[A.G] & 31))) {
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
     return;  // every thread leaves, before any TMEM is taken
-  }
-  // chunk -> chgroup (each chgroup's run of c_meta is a whole number of chunks)
-  for (int c = tid; c < A.cell_base[A.G] / 32; c += THREADS) {
-    int g = 0;
-    while (g + 1 < A.G && A.cell_base[g + 1] <= 32 * c) ++g;
-    s_chunkg[c] = (uint8_t)g;
   }
   const unsigned long long srot = __ldg(A.srot + tid);
   const int nch = (__reduce_max_sync(0xffffffffu, sn) + 7) >> 3;  // 8-entry chunks, per warp
@@ -289,23 +281,35 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         atomicAdd(s_re + t, v.x);
         atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
       };
-      // metadata and value loads of a step are independent (the chgroup of an
-      // entry comes from its chunk), 8 of each in flight per thread
-      constexpr int U = 8;
-      for (int e0 = 0; e0 < n_tot; e0 += U * THREADS) {
+      // warp w takes the 32-entry chunks w, w + 8, ... of c_meta in order;
+      // each chgroup's run is a whole number of chunks, so the chgroup, its
+      // first entry and its ring row stay in registers and change only at
+      // a run boundary (warp-uniform), and the shared-memory pipe is left to
+      // the atomics.  8 metadata and 8 value loads in flight per thread.
+      constexpr int U = 8, NW = THREADS / 32;
+      const int n_chunks = n_tot >> 5;
+      int g = -1, g_lo = 0, g_hi = 0, g_end = 0;
+      const float2* src = A.D;
+      for (int c0 = warp; c0 < n_chunks; c0 += NW * U) {
         unsigned m[U];
         float2 v[U];
 #pragma unroll
         for (int q = 0; q < U; ++q) {
-          const int e = e0 + q * THREADS + tid;
+          const int ch = c0 + NW * q;
           m[q] = 0xffffffffu;
           v[q] = make_float2(0.f, 0.f);
-          if (e < n_tot) {
-            const int g = s_chunkg[e >> 5];
-            const int k = e - s_cbase[g];
-            if (k < s_nf[g]) {
+          if (ch < n_chunks) {
+            while (32 * ch >= g_hi) {
+              ++g;
+              g_lo = s_cbase[g];
+              g_hi = s_cbase[g + 1];
+              g_end = s_end[g];
+              src = s_slice[g];
+            }
+            const int e = 32 * ch + lane;
+            if (e < g_end) {
               m[q] = __ldg(A.c_meta + e);
-              v[q] = s_slice[g][k];
+              v[q] = src[e - g_lo];
             }
           }
         }
@@ -333,8 +337,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
           float2 v = make_float2(0.f, 0.f);
           if (i < sn) {
             const unsigned b = (unsigned)(srot >> (2 * i)) & 3u;
-            v = crot(make_float2(s_re[sb + i], s_im[sb + i]),
-                     (int)(b & 1u) + ((b & 2u) ? shift_rot : 0));
+            v = crot_rt(make_float2(s_re[sb + i], s_im[sb + i]),
+                        (b & 1u) + ((b & 2u) ? (unsigned)shift_rot : 0u));
           }
           r[2 * j] = __float_as_uint(v.x);
           r[2 * j + 1] = __float_as_uint(v.y);
@@ -351,17 +355,19 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       //      after the last of them ----
       {
         float2 acc = make_float2(0.f, 0.f);
+        uint4 md_next = __ldg(A.gmeta + tid);
         for (int c = 0; c < nch; ++c) {
+          const uint4 md = md_next;  // next chunk's metadata loads under this one's
+          if (c + 1 < nch) md_next = __ldg(A.gmeta + (c + 1) * THREADS + tid);
           uint32_t r[16];
           tmem_ld16_wait(tbase + 16 * c, r);
-          const uint4 md = __ldg(A.gmeta + c * THREADS + tid);
           const unsigned mw[4] = {md.x, md.y, md.z, md.w};
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (8 * c + j < sn) {
               const unsigned m = (mw[j >> 1] >> (16 * (j & 1))) & 0xffffu;
               const float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
-              acc = cadd(acc, crot(v, (int)((m >> 13) & 3u) * p));
+              acc = cadd(acc, crot_rt(v, ((m >> 13) & 3u) * (unsigned)p));
               if (m & 0x8000u) {
                 buf[((m >> 7) & (LC - 1)) * P + (m & (NC - 1))] = acc;
                 acc = make_float2(0.f, 0.f);
