@@ -405,16 +405,16 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         for (int m2 = 0; m2 < C1; ++m2) colp[(cj + C1 * m2) * P] = y[m2];
       }
       // constant columns: every row holds the folded slot n' = 0 (row 0
-      // itself is already in place); columns without entries are zero
-      for (int i = tid; i < A.n_const * LC; i += THREADS) {
-        const int kc = __ldg(A.kcols + i / LC);
-        const int m = i & (LC - 1);
+      // itself is already in place); columns without entries are zero.  The
+      // lanes of a warp take consecutive columns of one row (no bank
+      // conflicts), the warps take rows m = warp (mod 8).
+      for (int k = lane; k < A.n_const; k += 32) {
+        const int kc = __ldg(A.kcols + k);
         const int col = kc & (NC - 1);
-        if (kc >> 16) {
-          if (m) buf[m * P + col] = buf[col];
-        } else {
-          buf[m * P + col] = make_float2(0.f, 0.f);
-        }
+        const bool has = kc >> 16;
+        const float2 y0 = has ? buf[col] : make_float2(0.f, 0.f);
+        for (int m = warp; m < LC; m += THREADS / 32)
+          if (m || !has) buf[m * P + col] = y0;
       }
       __syncthreads();
       // ---- 3. row transforms: folded rows (2pr, 2pr + 1) are image rows

@@ -314,9 +314,16 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   // x * 1.0f == x exactly, so an absent mask costs one exact multiply
   float mval = mask ? mask[fidx * mask_f_stride + p] : 1.0f;
   if (sig_f) mval = mval / sig_f[fidx];
-  float si[K];
+  float si[K], tau[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) si[k] = sinv[k];
+  for (int k = 0; k < K; ++k) {
+    si[k] = sinv[k];
+    // screen level of width k: a boxcar sum d can give fl(d * si) > thr only
+    // if d > thr / si up to two roundings (2^-23 relative), so a level
+    // lowered by 2^-20 of its magnitude never misses one
+    const float lv = thr / si[k];
+    tau[k] = lv - fabsf(lv) * 0x1p-20f;
+  }
   float ring[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) ring[q] = 0.f;
@@ -352,24 +359,24 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
     float xin[R];
     if (interior) {
       // steady state: every sample loaded, every time an output; the screen
-      // is the max over widths (fmaxf skips NaN, so it never hides a value
-      // the strict-'>' chain of emit() would report)
+      // compares each boxcar sum with its lowered level (a superset of what
+      // the exact strict-'>' chain of emit() reports, which decides)
 #pragma unroll
       for (int q = 0; q < R; ++q) xin[q] = ldf<T>(cube, (long long)(J0 + q - 1 - PL) * t_stride);
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         run += (double)(xin[q] * mval);
         ring[q] = (float)run;
-        float best = -INFINITY;
+        bool hit = false;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const int w = 1 << k;
           const int off = PL - w / 2;
           const int slo = ((q - MAXW + off) % R + R) % R;
           const int shi = ((q - MAXW + off + w) % R + R) % R;
-          best = fmaxf(best, (ring[shi] - ring[slo]) * si[k]);
+          hit |= (ring[shi] - ring[slo]) > tau[k];
         }
-        if (best > thr) emit(q, J0 + q - MAXW);
+        if (hit) emit(q, J0 + q - MAXW);
       }
       last = ring[R - 1];
       continue;
