@@ -125,10 +125,11 @@ class Clocks:
 # ---------------------------------------------------------------------------
 
 # DRAM traffic of image_kernel<256> measured by ncu (--set full, one launch)
-# on the medium workload: 302.19 MB written for 1152 images, 105.06 MB read
-# for 2 coarse DMs x 144 times
-IMAGE_DRAM_WRITE_PER_IMAGE = 302.187264e6 / 1152
-IMAGE_DRAM_READ_PER_SLICE_TIME = 105.063168e6 / (2 * 144)
+# on the medium workload: 249.12 MB written for 1152 images (the rest of the
+# images still sat in L2 when the kernel ended), 105.18 MB read for 2 coarse
+# DMs x 144 times
+IMAGE_DRAM_WRITE_PER_IMAGE = 249.123584e6 / 1152
+IMAGE_DRAM_READ_PER_SLICE_TIME = 105.180160e6 / (2 * 144)
 # ---------------------------------------------------------------------------
 
 
