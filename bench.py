@@ -70,7 +70,9 @@ def workload_desc(name, cfg):
                         f"({cfg.coarse_dm.size} coarse x {cfg.fine_per_coarse} fine) "
                         f"0-{cfg.coarse_dm.max():.0f}, boxcars 1..{1 << cfg.log_max_width}",
             "block_seconds": cfg.block_seconds, "l2": "inputs larger than L2 (19 GB/block)",
-            "chunk_tiles": cfg.chunk_tiles, "fdm_batch": cfg.fdm_batch}
+            "chunk_tiles": cfg.chunk_tiles, "fdm_batch": cfg.fdm_batch,
+            "stage2_ring": {"c64": "complex64", "bf16": "bf16 re/im pairs (BF16 storage form)"}[
+                cfg.ring_dtype]}
 
 
 class Clocks:
@@ -130,6 +132,10 @@ class Clocks:
 # DMs x 144 times
 IMAGE_DRAM_WRITE_PER_IMAGE = 249.123584e6 / 1152
 IMAGE_DRAM_READ_PER_SLICE_TIME = 105.180160e6 / (2 * 144)
+# the BF16 ring halves the ring reads: ncu dram__bytes_read.sum of the same
+# kernel on the medium workload, 49.49 MB (bf16 ring) against 99.22 MB
+# (complex64 ring) per launch, in one paired capture
+IMAGE_DRAM_READ_BF16_RATIO = 49.494272e6 / 99.225429e6
 # ---------------------------------------------------------------------------
 
 
@@ -142,15 +148,16 @@ def stage_work(pipe):
     nchan = cfg.band.n_chgroup * cfg.band.nchan
     half = N * (N // 2 + 1)
     coarse_per_batch = max(1, nb // cfg.fine_per_coarse) if cfg.fine_per_coarse else nb
+    esz = 4 if cfg.ring_dtype == "bf16" else 8   # bytes per stage-2 ring cell
     return {
         # tensor-core flops: 16 flops per (baseline, channel, native sample) (XX+YY complex MAC)
         "corr": ("tensor", 16.0 * nbase * nchan * C * cfg.t_int,
                  cfg.band.n_chgroup * C * cfg.t_int // 2 * cfg.nant * cfg.band.nchan * 4
                  + T.n_rows_y * C * 8),
-        "stage1": ("hbm", None, T.n_rows_y * C * 8 + T.n_rows_d * C * 8),
+        "stage1": ("hbm", None, T.n_rows_y * C * 8 + T.n_rows_d * C * esz),
         # fused combine + FFT: stage-2 ring slices of the batch's coarse DM(s)
         # read once, float32 images written once
-        "image": ("hbm", None, int(T.n_filled.sum()) * coarse_per_batch * nt * 8
+        "image": ("hbm", None, int(T.n_filled.sum()) * coarse_per_batch * nt * esz
                   + nb * nt * N * N * 4),
         "detect": ("hbm", None, nb * nt * N * N * 4),
         "layer1": ("hbm", None, nb * cfg.l1_times * cfg.l1_pixels * 4),
@@ -233,6 +240,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dsa110-2048dm")
+    ap.add_argument("--ring", default="bf16", choices=["c64", "bf16"],
+                    help="stage-2 ring element: the BF16 storage form (bf16 re/im, float32 "
+                         "accumulation; the precision form of the full DSA-110 shape), or "
+                         "complex64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stage-times", action="store_true", help="print per-stage device times")
@@ -243,6 +254,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     cfg = workload_config(a.workload)
+    cfg.ring_dtype = a.ring
 
     if a.impl == "reference":
         if rank != 0:
@@ -378,10 +390,13 @@ def main():
         nt = cfg_.chunk_tiles + 2 * cfg_.t_edge
         nb = cfg_.fdm_batch
         cpb = max(1, nb // cfg_.fine_per_coarse)
-        roof["traffic"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt
-                           + IMAGE_DRAM_READ_PER_SLICE_TIME * cpb * nt)
+        rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_BF16_RATIO
+                                                if cfg.ring_dtype == "bf16" else 1.0)
+        roof["traffic"] = IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt
         roof["traffic_note"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel on "
-                                "the medium workload (1152 images), scaled to this launch")
+                                "the medium workload (1152 images), scaled to this launch"
+                                + ("; ring reads x 0.499, the bf16/complex64 read ratio of a "
+                                   "paired capture" if cfg.ring_dtype == "bf16" else ""))
 
     if rank == 0:
         cb = None
@@ -390,7 +405,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "data-seconds/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "int8 (correlator) / f32", "data": "synthetic (seeded 4-bit Gaussian "
+                "dtype": ("int8 (correlator) / bf16 ring, f32 accumulate" if a.ring == "bf16"
+                          else "int8 (correlator) / f32"), "data": "synthetic (seeded 4-bit Gaussian "
                 "voltages, sigma 3, T-layout antennas)", "config": workload_desc(a.workload, cfg),
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
                 "cpu_baseline": cb,

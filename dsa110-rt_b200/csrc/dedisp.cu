@@ -147,8 +147,8 @@ struct S1Args {
   const int* shift2;      // (G, n_dm)
   const int* d_base;      // (G) first sky-ring row of the chgroup
   const int* n_filled;    // (G)
-  float2* D;
-  const long long* seg_base;  // (G * n_dm) first element of each ring segment (even)
+  void* D;                // complex64 elements, or (BF16) bf16 re/im pairs in 32 bits
+  const long long* seg_base;  // (G * n_dm) first element of each ring segment (a multiple of 4)
   const int* seg_depth;       // (G * n_dm) time slots of each segment
   long long t0;           // absolute time of the first output
   int n_t, n_dm, ceff;
@@ -167,6 +167,7 @@ __host__ __device__ inline size_t s1_smem_bytes(int ceff, int win_len) {
   return (size_t)ceff * S1_DG * 4 + (size_t)S1_MAX_C * 8 + (size_t)ceff * win_len * 32 + 16;
 }
 
+template <bool BF16>
 __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
   extern __shared__ __align__(16) uint8_t s1_smem[];
   const int ceff = A.ceff;
@@ -231,7 +232,6 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
   double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
   const float4* Y4 = reinterpret_cast<const float4*>(A.Y);
   const long long ycol = (long long)A.y_base[g] + c0;   // a multiple of 4
-  float4* D4 = reinterpret_cast<float4*>(A.D);
 
   for (int tt = 0; tt < A.n_t; tt += S1_TT) {
     __syncthreads();  // the previous tile's windows are no longer read
@@ -291,9 +291,16 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
         o1 = make_float4((float)((double)a1.x - mr[2]), (float)((double)a1.y - mi[2]),
                          (float)((double)a1.z - mr[3]), (float)((double)a1.w - mi[3]));
       }
-      const long long o = (seg + slot * pitch) / 2;
-      D4[o] = o0;
-      D4[o + 1] = o1;
+      const long long o = seg + slot * pitch;  // element of cell c0, a multiple of 4
+      if constexpr (BF16) {
+        reinterpret_cast<uint4*>(A.D)[o / 4] =
+            make_uint4(bf16_pair(o0.x, o0.y), bf16_pair(o0.z, o0.w), bf16_pair(o1.x, o1.y),
+                       bf16_pair(o1.z, o1.w));
+      } else {
+        float4* D4 = reinterpret_cast<float4*>(A.D);
+        D4[o / 2] = o0;
+        D4[o / 2 + 1] = o1;
+      }
     }
   }
   // sky: block mean of every (DM, cell) over the chunk, summed over the 8
@@ -371,7 +378,8 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
-                    void* D, const long long* seg_base, const int* seg_depth, long long t0,
+                    void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                    long long t0,
                     int n_t, int n_dm, int ceff, int max_spread, void* sky_ring, int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream) {
@@ -395,15 +403,16 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   A.Y = (const float2*)Y; A.y_rows = y_rows; A.y_mask = y_mask;
   A.blk_g = blk_g; A.blk_c0 = blk_c0; A.y_base = y_base; A.pitch = pitch;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
-  A.D = (float2*)D; A.seg_base = seg_base; A.seg_depth = seg_depth;
+  A.D = D; A.seg_base = seg_base; A.seg_depth = seg_depth;
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff; A.win_len = win_len;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
   A.sky_count = sky_count; A.sky_subtract = sky_subtract; A.status = status;
-  if (cudaFuncSetAttribute(stage1_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+  auto kern = d_bf16 ? stage1_rows_kernel<true> : stage1_rows_kernel<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
     return DSB_E_CUDA;
   dim3 grid(n_blocks, (n_dm + S1_DG - 1) / S1_DG);
-  stage1_rows_kernel<<<grid, S1_THREADS, smem, stream>>>(A);
+  kern<<<grid, S1_THREADS, smem, stream>>>(A);
   return launch_status();
 }
 

@@ -9,10 +9,22 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
+#include <cuda_bf16.h>
 
 #include "../../include/dsb200.h"
 
 #define DSB_DEV __device__ __forceinline__
+
+// Stage-2 ring element in the BF16 storage form: one 32-bit word per cell,
+// the real part (bf16, nearest-even from float32) in the low half and the
+// imaginary part in the high half.
+DSB_DEV uint32_t bf16_pair(float re, float im) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);  // .x = re (low), .y = im (high)
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+DSB_DEV float2 bf16_pair_to_f2(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
 
 // Iteration limit for every mbarrier spin (each try_wait may itself suspend
 // for a hardware-chosen interval, so this bounds the wait to well under a

@@ -130,8 +130,23 @@ DSB_DEV void idftR(float2 (&a)[R]) {
   else idft4(a[0], a[1], a[2], a[3]);
 }
 
+// Stage-2 ring elements: complex64, or the BF16 storage form (bf16 re/im
+// pairs in 32 bits, decoded to float32 before any arithmetic).
+template <bool BF16> struct RingElem {
+  using T = float2;
+  static DSB_DEV T zero() { return make_float2(0.f, 0.f); }
+  static DSB_DEV float2 dec(T w) { return w; }
+  static DSB_DEV float2 get(const T* p) { return *p; }
+};
+template <> struct RingElem<true> {
+  using T = uint32_t;
+  static DSB_DEV T zero() { return 0u; }
+  static DSB_DEV float2 dec(T w) { return bf16_pair_to_f2(w); }
+  static DSB_DEV float2 get(const T* p) { return bf16_pair_to_f2(*p); }
+};
+
 struct ImgArgs {
-  const float2* D;
+  const void* D;            // ring: complex64, or bf16 pairs when the kernel's BF16 is set
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
@@ -193,8 +208,9 @@ struct ImgGeom {
                                  (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + 16;
 };
 
-template <int N>
+template <int N, bool BF16>
 __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
+  using Elem = typename RingElem<BF16>::T;
   using Gm = ImgGeom<N>;
   constexpr int FOLD = Gm::FOLD, LC = Gm::LC, C1 = Gm::C1, NC = Gm::NC, P = Gm::P,
                 RR = Gm::RR, THREADS = Gm::THREADS;
@@ -205,7 +221,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   // rtw[x1*RR + j] = W_N^(j x1), ctw[m1*C1 + j] = W_LC^(j m1)
   float2* rtw = tw + N;
   float2* ctw = rtw + RR * RR;
-  const float2** s_slice = reinterpret_cast<const float2**>(ctw + C1 * C1);
+  const Elem** s_slice = reinterpret_cast<const Elem**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
   int* s_end = s_cbase + IMG_MAX_G + 1;
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_end + IMG_MAX_G);
@@ -263,7 +279,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       const long long dep = A.seg_depth[gc];
       long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
       if (slot < 0) slot += dep;
-      s_slice[g] = A.D + A.seg_base[gc] + slot * A.d_pitch[g];
+      s_slice[g] = static_cast<const Elem*>(A.D) + A.seg_base[gc] + slot * A.d_pitch[g];
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
@@ -289,15 +305,17 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       constexpr int U = 8, NW = THREADS / 32;
       const int n_chunks = n_tot >> 5;
       int g = -1, g_lo = 0, g_hi = 0, g_end = 0;
-      const float2* src = A.D;
+      const Elem* src = static_cast<const Elem*>(A.D);
       for (int c0 = warp; c0 < n_chunks; c0 += NW * U) {
+        // raw ring words: decoded only in the add loop below, so that no
+        // instruction waits on a load before the batch's other loads issue
         unsigned m[U];
-        float2 v[U];
+        Elem v[U];
 #pragma unroll
         for (int q = 0; q < U; ++q) {
           const int ch = c0 + NW * q;
           m[q] = 0xffffffffu;
-          v[q] = make_float2(0.f, 0.f);
+          v[q] = RingElem<BF16>::zero();
           if (ch < n_chunks) {
             while (32 * ch >= g_hi) {
               ++g;
@@ -315,11 +333,12 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         }
 #pragma unroll
         for (int q = 0; q < U; ++q)
-          if (m[q] != 0xffffffffu) add(m[q], v[q]);
+          if (m[q] != 0xffffffffu) add(m[q], RingElem<BF16>::dec(v[q]));
       }
       for (int i = tid; i < A.n_c2; i += THREADS) {
         const int2 cm = __ldg(A.c2 + i);
-        add((unsigned)cm.y, s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)][cm.x & 0xffff]);
+        add((unsigned)cm.y,
+            RingElem<BF16>::get(s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)] + (cm.x & 0xffff)));
       }
     }
     __syncthreads();
@@ -481,21 +500,21 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   }
 }
 
-// Resident CTAs for image_kernel<N> on this device (the persistent grid).
+// Resident CTAs for image_kernel<N, BF16> on this device (the persistent grid).
 // The occupancy API answers 1 CTA per SM for any kernel that allocates
 // tensor memory (measured on B200 with CUDA 12.9), while the SM runs as many
 // as its shared memory, registers and 512 TMEM columns hold: three here.  So
 // the count is taken from those limits directly.
-template <int N>
+template <int N, bool BF16>
 int image_grid(int* blocks) {
   using Gm = ImgGeom<N>;
   static int cached = 0;
   if (!cached) {
-    if (cudaFuncSetAttribute(image_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(image_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Gm::SMEM) != cudaSuccess)
       return DSB_E_CUDA;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, image_kernel<N>) != cudaSuccess) return DSB_E_CUDA;
+    if (cudaFuncGetAttributes(&fa, image_kernel<N, BF16>) != cudaSuccess) return DSB_E_CUDA;
     int dev = 0, sms = 148, smem_sm = 0, smem_rsv = 0, regs_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -512,16 +531,16 @@ int image_grid(int* blocks) {
   return DSB_OK;
 }
 
-template <int N>
+template <int N, bool BF16>
 int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   using Gm = ImgGeom<N>;
   if (A.s_stride > Gm::BUF) return DSB_E_CAPACITY;
   int blocks = 0;
-  const int rc = image_grid<N>(&blocks);
+  const int rc = image_grid<N, BF16>(&blocks);
   if (rc != DSB_OK) return rc;
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   blocks = std::max(1, std::min(blocks, A.n_f * A.n_t));
-  image_kernel<N><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
+  image_kernel<N, BF16><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
   return launch_status();
 }
 
@@ -541,7 +560,8 @@ int dsb_image_threads(void) { return IMG_THREADS; }
 
 int dsb_image_max_entries(void) { return IMG_MAXE; }
 
-int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
+int dsb_image_fft(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                  int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   const int* dcols, const unsigned long long* dmask, int n_dense,
@@ -559,13 +579,17 @@ int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth
     return DSB_E_ARG;
   if (n_dense + n_const != N / 2) return DSB_E_ARG;  // every packed column, once
   const int stride = (n_s + 1) & ~1;
-  ImgArgs A{(const float2*)D, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
+  ImgArgs A{D, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
             n_c2, thr_b, (const uint4*)gmeta, srot, dcols, dmask, n_dense, kcols, n_const,
             n_s, stride, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
             t0, n_t, fftshift, (float*)out, status};
   switch (N) {
-    case 64: return launch_image<64>(A, max_blocks, stream);
-    case 256: return launch_image<256>(A, max_blocks, stream);
+    case 64:
+      return d_bf16 ? launch_image<64, true>(A, max_blocks, stream)
+                    : launch_image<64, false>(A, max_blocks, stream);
+    case 256:
+      return d_bf16 ? launch_image<256, true>(A, max_blocks, stream)
+                    : launch_image<256, false>(A, max_blocks, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

@@ -33,7 +33,7 @@ __global__ void uv_cells_kernel(const double* __restrict__ du, const double* __r
 // that chgroup's pattern, and whether it is the conjugate mirror.
 // ===========================================================================
 struct CombArgs {
-  const float2* D;
+  const void* D;         // ring: complex64, or bf16 re/im pairs in 32 bits (BF16)
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
@@ -55,6 +55,7 @@ struct CombArgs {
 // output time is written coalesced across the half cells of a warp.
 constexpr int CB_T = 8;
 
+template <bool BF16>
 __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
   const int nh = A.N / 2 + 1;
   const int n_hc = A.N * nh;
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
       if (mirror) cell = ~cell;
       const int gc = g * A.n_coarse + c;
       const long long ts0 = A.t0 + tt - A.sfine[(long long)f * A.G + g];
-      const float2* src = A.D + A.seg_base[gc] + cell;
+      const long long e0 = A.seg_base[gc] + cell;
       const long long dep = A.seg_depth[gc];
       const long long pitch = A.d_pitch[g];
       long long slot0 = ts0 % dep;
@@ -87,7 +88,11 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
       for (int i = 0; i < CB_T; ++i) {
         long long slot = slot0 + i;
         if (slot >= dep) slot -= dep;
-        const float2 x = src[slot * pitch];
+        float2 x;
+        if constexpr (BF16)
+          x = bf16_pair_to_f2(static_cast<const uint32_t*>(A.D)[e0 + slot * pitch]);
+        else
+          x = static_cast<const float2*>(A.D)[e0 + slot * pitch];
         re[i] += x.x;
         im[i] += mirror ? -(double)x.y : (double)x.y;
       }
@@ -540,7 +545,8 @@ int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_
   return launch_status();
 }
 
-int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
+int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                     int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
@@ -548,11 +554,14 @@ int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_de
       !d_pitch || !sfine || !f2c || !out)
     return DSB_E_ARG;
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
-  CombArgs A{(const float2*)D, seg_base, seg_depth, n_coarse, hc_off, e_g, e_cell, d_pitch,
+  CombArgs A{D, seg_base, seg_depth, n_coarse, hc_off, e_g, e_cell, d_pitch,
              sfine, f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
   const int n_hc = N * (N / 2 + 1);
   dim3 grid((n_hc + 127) / 128, n_f);
-  combine_rows_kernel<<<grid, 128, 0, stream>>>(A);
+  if (d_bf16)
+    combine_rows_kernel<true><<<grid, 128, 0, stream>>>(A);
+  else
+    combine_rows_kernel<false><<<grid, 128, 0, stream>>>(A);
   return launch_status();
 }
 

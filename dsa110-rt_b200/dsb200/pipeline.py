@@ -76,8 +76,13 @@ class PipelineConfig:
     l1_times: int = 16
     l1_pixels: int = 256
     cand_capacity: int = 1 << 22
+    # stage-2 ring element: "c64" (complex64) or "bf16" (the BF16 storage form:
+    # each part rounded to nearest-even bf16, accumulated in float32 on read)
+    ring_dtype: str = "c64"
 
     def __post_init__(self):
+        if self.ring_dtype not in ("c64", "bf16"):
+            raise ValueError(f"ring_dtype must be 'c64' or 'bf16', got {self.ring_dtype!r}")
         self.coarse_dm = np.asarray(self.coarse_dm, np.float64)
         if self.fine_dm is None:
             # fine DMs spread evenly around each coarse DM (v2 plan: coarse at the
@@ -421,7 +426,11 @@ class SearchPipeline:
         self.d_segbase, self.d_segdepth = d(self.seg_base[:-1]), d(self.seg_depth)
         # time-major rings: Y [time & (TY-1)][row]; D segmented as above
         self.Y = torch.zeros((self.TY, T.n_rows_y), dtype=torch.complex64, device=self.dev)
-        self.D = torch.zeros(int(self.seg_base[-1]), dtype=torch.complex64, device=self.dev)
+        # D: complex64 elements, or one int32 word of bf16 (re low, im high) per cell
+        self.ring_bf16 = cfg.ring_dtype == "bf16"
+        self.D = torch.zeros(int(self.seg_base[-1]),
+                             dtype=torch.int32 if self.ring_bf16 else torch.complex64,
+                             device=self.dev)
         self.sky = (torch.zeros((T.n_rows_d, cfg.sky_window), dtype=torch.complex128,
                                 device=self.dev) if cfg.use_sky else None)
         self.sky_count = self.sky_head = self.sky_seen = 0
@@ -511,7 +520,7 @@ class SearchPipeline:
                 _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_ybase),
                 _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
-                _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
+                int(self.ring_bf16), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
                 cfg.ceff, T.max_spread, _lib.ptr(self.sky), cfg.sky_window, self.sky_head,
                 self.sky_count, sub, _lib.ptr(self.status), _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
@@ -531,7 +540,7 @@ class SearchPipeline:
         if out.shape != (n_f, n_t, N, N) or out.dtype != torch.float32 or not out.is_contiguous():
             raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
         _lib.check(_lib.lib().dsb_image_fft(
-            _lib.ptr(self.D), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
+            _lib.ptr(self.D), int(self.ring_bf16), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
             cfg.coarse_dm.size, _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_thrb), _lib.ptr(self.d_img_gmeta), _lib.ptr(self.d_img_srot),
@@ -665,7 +674,12 @@ class SearchPipeline:
         base, dep = int(self.seg_base[gd]), int(self.seg_depth[gd])
         seg = self.D[base:base + dep * pitch].view(dep, pitch)
         rows = torch.as_tensor(np.asarray(times, np.int64) % dep, device=self.dev)
-        return seg[rows, :nf].cpu().numpy()
+        vals = seg[rows, :nf].cpu().numpy()
+        if not self.ring_bf16:
+            return vals
+        w = vals.view(np.uint32)
+        return ((w << 16).view(np.float32) + 1j * (w & 0xFFFF0000).view(np.float32)
+                ).astype(np.complex64)
 
     def check_status(self) -> None:
         _lib.check_status(self.status, "pipeline")

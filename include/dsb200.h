@@ -132,15 +132,20 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * each (chgroup, coarse DM) its own ring segment of seg_depth[gd] (>= 8)
  * time slots, deep enough for its own stage-2 delay; the float64 sky ring
  * of (g, d, cell) is row d_base[g] + d*p[g] + cell.  y_base and y_rows are
- * multiples of 4, seg_base even, Y and D 16-byte aligned (four cells per
- * 32-byte access; pad cells up to the pitch).  Block b covers cells
+ * multiples of 4, seg_base multiples of 4, Y and D 16-byte aligned (four
+ * cells per access; pad cells up to the pitch).  d_bf16 selects the ring's
+ * element: 0 = complex64; 1 = the BF16 storage form, one 32-bit word per
+ * cell holding the real part (bf16, rounded to nearest even from the float32
+ * sum) in the low half and the imaginary part in the high half; sums and the
+ * sky statistics stay float32/float64.  Block b covers cells
  * [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b] and one group
  * of dsb_stage1_dm_group() coarse DMs (grid y). */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
-                    void* D, const long long* seg_base, const int* seg_depth, long long t0,
-                    int n_t, int n_dm, int ceff, int max_spread, void* sky_ring, int sky_window,
+                    void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                    long long t0, int n_t, int n_dm, int ceff, int max_spread, void* sky_ring,
+                    int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream);
 /* Cells per block (blk_c0 multiples of it) and coarse DMs per block; the
@@ -155,9 +160,10 @@ int dsb_stage1_dm_group(void);
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
  * reads the segmented stage-2 ring directly (value of (g, coarse DM c,
  * cell) at time t: D[seg_base[g*n_coarse + c] + (t mod seg_depth[...])*d_pitch[g]
- * + cell], as dsb_stage1_rows writes it), writes (n_f, n_t, N, N/2+1)
- * complex64. */
-int dsb_combine_rows(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
+ * + cell], as dsb_stage1_rows writes it, in the element form d_bf16 names),
+ * writes (n_f, n_t, N, N/2+1) complex64. */
+int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                     int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
@@ -209,7 +215,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
 int dsb_image_fold(int n_grid);
 int dsb_image_threads(void);
 int dsb_image_max_entries(void);
-int dsb_image_fft(const void* D, const long long* seg_base, const int* seg_depth, int n_coarse,
+int dsb_image_fft(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
+                  int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   const int* dcols, const unsigned long long* dmask, int n_dense,

@@ -780,12 +780,35 @@ def pipeline_tables(band: Band, antpos_e, antpos_n, *, nant, csf, n_grid, coarse
     return dict(cell=cell, pats=pats, cims=cims, sh1=sh1, sh2=sh2, sf=sf)
 
 
+def round_bf16(x: np.ndarray) -> np.ndarray:
+    """float32 values rounded to the nearest bfloat16 (ties to even), returned
+    as float32: the conversion of torch ``.to(torch.bfloat16)`` and of the
+    stage-2 ring's BF16 storage form.  Keep the top 16 bits of the float32
+    pattern after adding 0x7FFF plus the lowest kept bit; NaN stays NaN."""
+    f = np.ascontiguousarray(x, np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    r = (((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16).astype(np.uint32)
+    out = r.view(np.float32).copy()
+    nan = np.isnan(f)
+    out[nan] = f[nan]
+    return out
+
+
+def round_bf16_complex(z: np.ndarray) -> np.ndarray:
+    """complex64 with both parts rounded to bfloat16 (the BF16 ring element)."""
+    z = np.asarray(z, np.complex64)
+    return (round_bf16(z.real) + 1j * round_bf16(z.imag)).astype(np.complex64)
+
+
 def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block, t_int, csf,
                  n_grid, coarse_dm, fine_dm, fine_to_coarse, log_max_width, threshold, chunk,
                  use_sky=True, sky_window=8, sky_warmup=8, n_top=256, r_t=4, r_f=5, r_lm=3,
-                 l1_times=16, l1_pixels=256, keep=None):
+                 l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None):
     """Oracle of the CUDA streaming pipeline; returns candidate tuples
-    ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates."""
+    ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates.
+    ``ring_dtype="bf16"`` stores the stage-2 streams in the BF16 form (each
+    part rounded to bfloat16 after the sky subtraction), as the pipeline's
+    precision form does."""
     keep = {} if keep is None else keep
     G = band.n_chgroup
     tb = pipeline_tables(band, antpos_e, antpos_n, nant=nant, csf=csf, n_grid=n_grid,
@@ -826,6 +849,8 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
                 x = (o_re[d] + 1j * o_im[d]).astype(np.complex64)
                 if sky is not None:
                     x = sky.apply(x, dm_slot=g * n_coarse + d)
+                if ring_dtype == "bf16":
+                    x = round_bf16_complex(x)
                 D1[g][d][j * chunk:(j + 1) * chunk] = x
     keep["D1"] = D1
     # search cubes

@@ -49,14 +49,19 @@ def _setup(n_blocks=8, amp=1.0):
     return band, ob, e, n, blocks, kw
 
 
-def test_pipeline_matches_oracle(dev):
+@pytest.mark.parametrize("ring", ["c64", "bf16"])
+def test_pipeline_matches_oracle(dev, ring):
+    """Both ring forms against the oracle pipeline with the same ring form:
+    the BF16 ring is the complex64 one rounded to bfloat16 part by part,
+    bit-exact; candidates as for the complex64 ring."""
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup()
     cfg = PipelineConfig(band=band, nant=kw["nant"], npkt_block=kw["npkt_block"],
                          t_int=kw["t_int"], csf=kw["csf"], n_grid=kw["n_grid"],
                          coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
                          fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, threshold=6.0,
-                         sky_window=2, sky_warmup=1, chunk_tiles=32, fdm_batch=3)
+                         sky_window=2, sky_warmup=1, chunk_tiles=32, fdm_batch=3,
+                         ring_dtype=ring)
     pipe = SearchPipeline(cfg, e, n, device=dev)
     got = []
     for b in blocks:
@@ -64,7 +69,8 @@ def test_pipeline_matches_oracle(dev):
     torch.cuda.synchronize()
     pipe.check_status()
     keep = {}
-    want = O.run_pipeline(blocks, ob, e, n, chunk=32, sky_window=2, sky_warmup=1, keep=keep, **kw)
+    want = O.run_pipeline(blocks, ob, e, n, chunk=32, sky_window=2, sky_warmup=1, keep=keep,
+                          ring_dtype=ring, **kw)
     assert len(want) >= 1, "oracle found no burst candidate"
 
     # stage-2 ring vs oracle stage-1 streams (last emitted chunk), bit-exact
@@ -122,28 +128,38 @@ def test_pipeline_rejects_wrong_raw_size(dev):
         pipe.process_block(torch.zeros(100, dtype=torch.uint8, device=dev))
 
 
+@pytest.mark.parametrize("ring", ["c64", "bf16"])
 @pytest.mark.parametrize("N", [64, 256])
-def test_image_fft_matches_combine_and_irfft2(dev, N):
+def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     """Fused combine + 2-D c2r FFT == dsb_combine_rows + torch.fft.irfft2 on
-    the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale."""
+    the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale,
+    for both ring element forms."""
     from dsb200 import _lib
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
     cfg = PipelineConfig(band=band, nant=16, npkt_block=256, t_int=8, csf=4, n_grid=N,
                          coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
-                         fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, chunk_tiles=32)
+                         fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, chunk_tiles=32,
+                         ring_dtype=ring)
     pipe = SearchPipeline(cfg, e, n, device=dev)
     T = pipe.tab
     g = torch.Generator(device=dev)
     g.manual_seed(3)
-    pipe.D.copy_(torch.randn(pipe.D.shape, dtype=torch.complex64, device=dev, generator=g))
+    if ring == "bf16":
+        # random bf16 parts: real in the low 16 bits, imaginary in the high
+        parts = torch.randn((2,) + tuple(pipe.D.shape), device=dev, generator=g)
+        bits = parts.to(torch.bfloat16).view(torch.int16).to(torch.int32) & 0xFFFF
+        pipe.D.copy_(bits[0] | (bits[1] << 16))
+    else:
+        pipe.D.copy_(torch.randn(pipe.D.shape, dtype=torch.complex64, device=dev, generator=g))
     nf, nt, t0 = 5, 20, 37
     out = torch.empty((nf, nt, N, N), dtype=torch.float32, device=dev)
     L = _lib.lib()
     pipe.image(1, nf, t0, nt, out, max_blocks=3)
     gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
-    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), _lib.ptr(pipe.d_segbase),
-                                  _lib.ptr(pipe.d_segdepth), len(kw["coarse_dm"]),
+    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), int(pipe.ring_bf16),
+                                  _lib.ptr(pipe.d_segbase), _lib.ptr(pipe.d_segdepth),
+                                  len(kw["coarse_dm"]),
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
                                   _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_pitch),
                                   _lib.ptr(pipe.d_sfine), _lib.ptr(pipe.d_f2c), 1, nf,
