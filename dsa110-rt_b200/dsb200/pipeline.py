@@ -494,12 +494,12 @@ class SearchPipeline:
             out[k] = {"n": len(ts), "total_ms": float(sum(ts)), "mean_ms": float(np.mean(ts))}
         return out
 
-    def _corr(self, raw: torch.Tensor, p0: int) -> None:
+    def _corr(self, raw: torch.Tensor, p0: int, npkt: int) -> None:
         cfg, T = self.cfg, self.tab
         C = cfg.chunk_tiles
         ppfv = cfg.t_int // 2
         row_bytes = cfg.nant * cfg.band.nchan * 4
-        page = cfg.npkt_block * row_bytes
+        page = npkt * row_bytes
         base = raw.data_ptr() + p0 * row_bytes
         with self._mark("corr"):
             _lib.check(_lib.lib().dsb_corr_tc_grid(
@@ -584,24 +584,37 @@ class SearchPipeline:
                 self.out.append(StreamCandidate(t_first + t, f, l_, m_, v, self.widths[k]))
             self._pending = []
 
+    def block_packets(self, raw: torch.Tensor) -> int:
+        """Packets per chgroup page of a raw block ``(G, npkt, nant, nchan,
+        2, 2)`` uint8; a block may hold any whole number of chunks
+        (``chunk_tiles * t_int / 2`` packets each), so streams can deliver
+        blocks of uneven length."""
+        cfg = self.cfg
+        row = cfg.band.n_chgroup * cfg.nant * cfg.band.nchan * 4
+        per_chunk = cfg.chunk_tiles * (cfg.t_int // 2)
+        if raw.dtype != torch.uint8 or raw.numel() == 0 or raw.numel() % (row * per_chunk):
+            raise ValueError("raw must be uint8 (G, npkt, nant, nchan, 2, 2) with npkt a "
+                             f"multiple of {per_chunk} packets")
+        return raw.numel() // row
+
     def process_block(self, raw: torch.Tensor, *, collect: bool = True) -> List[StreamCandidate]:
         """Push one block of raw pages ``(G, npkt, nant, nchan, 2, 2)`` uint8
         (device tensor, or host tensor copied here) through the pipeline;
-        returns the candidates whose detector cubes completed."""
+        returns the candidates whose detector cubes completed.  ``npkt`` is
+        any whole number of chunks (``npkt_block`` for the fixed-size
+        stream)."""
         cfg = self.cfg
+        npkt = self.block_packets(raw)
         if raw.device.type != "cuda":
             raw = raw.to(self.dev, non_blocking=True)
-        if raw.dtype != torch.uint8 or raw.numel() != cfg.band.n_chgroup * cfg.npkt_block * \
-                cfg.nant * cfg.band.nchan * 4:
-            raise ValueError("raw must be uint8 (G, npkt, nant, nchan, 2, 2)")
         raw = raw.contiguous()
         self.out = []
         self._pending = []
         self.last_d2h_bytes = 0
         C = cfg.chunk_tiles
         ppfv = cfg.t_int // 2
-        for ci in range(cfg.n_fv_block // C):
-            self._corr(raw, ci * C * ppfv)
+        for ci in range(npkt // (C * ppfv)):
+            self._corr(raw, ci * C * ppfv, npkt)
             j = self.chunk - self.depth1
             if j >= 0:
                 self._stage1(j)
