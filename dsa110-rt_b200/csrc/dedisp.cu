@@ -13,6 +13,7 @@
 #include "dsb_common.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace {
 
@@ -127,14 +128,17 @@ __global__ void stage2_roll_kernel(const float2* const* __restrict__ hist, int d
 // (each (chgroup, coarse DM) a ring segment as deep as its own stage-2 delay
 // needs); the sky ring is indexed by d_base[g] + d * pitch[g] + cell.
 //
-// A CTA owns 4 adjacent cells of one chgroup and a group of S1_DG coarse
+// A CTA owns 4 adjacent cells of one chgroup and a group of DG coarse
 // DMs, and walks the output times in tiles of S1_TT.  For each tile it
 // stages every subband's Y samples that any of its DMs needs (the tile plus
 // the spread of that subband's shifts over the DM group) in shared memory,
 // two planes of two cells, and then every (DM, time) output of the tile sums
 // its ceff subbands from there: each Y sample is read from L2 once per DM
-// group instead of once per DM.  Thread (dl, l8) = (tid / 8, tid % 8) owns
-// DM dl of the group and times l8, l8 + 8, ...; its D writes are whole
+// group instead of once per DM.  Thread (dl, ln) = (tid / L, tid % L), with
+// L = 256 / DG lanes per DM, owns DM dl of the group and times ln, ln + L,
+// ...; DG is 32, 16 or 8: the largest whose windows fit in shared memory
+// (a wide DM spread per group, as with few coarse DMs over a wide range,
+// needs a smaller group); its D writes are whole
 // 32-byte sectors (4 cells).
 struct S1Args {
   const float2* Y;
@@ -161,27 +165,29 @@ struct S1Args {
 constexpr int S1_THREADS = 256;
 constexpr int S1_MAX_C = 64;
 constexpr int S1_TT = 64;   // output times per tile
-constexpr int S1_DG = 32;   // coarse DMs per CTA (S1_THREADS / 8)
+constexpr int S1_DG = 32;   // largest DM group (coarse DMs per CTA)
 
-__host__ __device__ inline size_t s1_smem_bytes(int ceff, int win_len) {
-  return (size_t)ceff * S1_DG * 4 + (size_t)S1_MAX_C * 8 + (size_t)ceff * win_len * 32 + 16;
+__host__ __device__ inline size_t s1_smem_bytes(int ceff, int dg, int win_len) {
+  return (size_t)ceff * dg * 4 + (size_t)S1_MAX_C * 8 + (size_t)ceff * win_len * 32 + 16;
 }
 
-template <bool BF16>
+template <bool BF16, int DG>
 __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A) {
+  constexpr int L = S1_THREADS / DG;  // time lanes per DM
+  static_assert(L >= 8 && L <= 32 && S1_TT % L == 0, "unsupported DM group");
   extern __shared__ __align__(16) uint8_t s1_smem[];
   const int ceff = A.ceff;
   int* s_sh = reinterpret_cast<int*>(s1_smem);              // [s][dl] shift - lo[s]
-  int* s_lo = s_sh + ceff * S1_DG;                          // [s] smallest shift
+  int* s_lo = s_sh + ceff * DG;                             // [s] smallest shift
   int* s_len = s_lo + S1_MAX_C;                             // [s] window length
-  float4* win0 = reinterpret_cast<float4*>(s1_smem + ((size_t)ceff * S1_DG * 4 +
+  float4* win0 = reinterpret_cast<float4*>(s1_smem + ((size_t)ceff * DG * 4 +
                                                       (size_t)S1_MAX_C * 8 + 15) / 16 * 16);
   float4* win1 = win0 + (size_t)ceff * A.win_len;            // cells 2-3
 
   const int g = A.blk_g[blockIdx.x];
   const int c0 = A.blk_c0[blockIdx.x];
-  const int dg0 = blockIdx.y * S1_DG;
-  const int nd = min(S1_DG, A.n_dm - dg0);
+  const int dg0 = blockIdx.y * DG;
+  const int nd = min(DG, A.n_dm - dg0);
   const int pitch = A.pitch[g];
   const int tid = threadIdx.x;
   for (int sb = tid; sb < ceff; sb += S1_THREADS) {
@@ -202,12 +208,12 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
     return;
   }
-  for (int i = tid; i < ceff * S1_DG; i += S1_THREADS) {
-    const int sb = i / S1_DG, dl = i % S1_DG;
+  for (int i = tid; i < ceff * DG; i += S1_THREADS) {
+    const int sb = i / DG, dl = i % DG;
     s_sh[i] = dl < nd ? A.shift1[((long long)g * ceff + sb) * A.n_dm + dg0 + dl] - s_lo[sb] : 0;
   }
 
-  const int dl = tid >> 3, l8 = tid & 7;
+  const int dl = tid / L, ln = tid % L;
   const bool active = dl < nd;
   const int d = dg0 + (active ? dl : 0);
   const int gd = g * A.n_dm + d;
@@ -269,15 +275,15 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
     }
     __syncthreads();
     if (!active) continue;
-    long long slot = (A.t0 + tt + l8 + sh2) % dep;
+    long long slot = (A.t0 + tt + ln + sh2) % dep;
     if (slot < 0) slot += dep;
-    for (int k = 0; k < S1_TT / 8; ++k, slot += 8) {
+    for (int k = 0; k < S1_TT / L; ++k, slot += L) {
       if (slot >= dep) slot -= dep;
-      const int tl = l8 + 8 * k;
+      const int tl = ln + L * k;
       if (tt + tl >= A.n_t) break;
       float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
       for (int sb = 0; sb < ceff; ++sb) {
-        const int idx = sb * A.win_len + tl + s_sh[sb * S1_DG + dl];
+        const int idx = sb * A.win_len + tl + s_sh[sb * DG + dl];
         const float4 v0 = win0[idx], v1 = win1[idx];
         a0.x += v0.x; a0.y += v0.y; a0.z += v0.z; a0.w += v0.w;
         a1.x += v1.x; a1.y += v1.y; a1.z += v1.z; a1.w += v1.w;
@@ -303,18 +309,18 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
       }
     }
   }
-  // sky: block mean of every (DM, cell) over the chunk, summed over the 8
-  // lanes that share the DM (lanes 8-aligned inside the warp)
+  // sky: block mean of every (DM, cell) over the chunk, summed over the L
+  // lanes that share the DM (L-aligned inside the warp)
   if (A.sky_ring) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
 #pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
+      for (int o = 1; o < L; o <<= 1) {
         sr[c] += __shfl_xor_sync(0xffffffffu, sr[c], o);
         si[c] += __shfl_xor_sync(0xffffffffu, si[c], o);
       }
     }
-    if (active && l8 == 0) {
+    if (active && ln == 0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c)
         A.sky_ring[(drow + c) * A.sky_window + A.sky_head] =
@@ -379,13 +385,13 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                    long long t0,
-                    int n_t, int n_dm, int ceff, int max_spread, void* sky_ring, int sky_window,
+                    long long t0, int n_t, int n_dm, int ceff, int dm_group, int max_spread,
+                    void* sky_ring, int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream) {
   if (!Y || !D || !blk_g || !blk_c0 || !y_base || !pitch || !shift1 || !shift2 ||
       !d_base || !n_filled || !seg_base || !seg_depth || n_t <= 0 || n_dm <= 0 || ceff <= 0 ||
-      max_spread < 0)
+      max_spread < 0 || (dm_group != 32 && dm_group != 16 && dm_group != 8))
     return DSB_E_ARG;
   // four cells per 32-byte access: rings 16-byte aligned, row counts multiples of 4
   if ((reinterpret_cast<uintptr_t>(Y) & 15) || (reinterpret_cast<uintptr_t>(D) & 15) ||
@@ -393,7 +399,7 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
     return DSB_E_ARG;
   if (ceff > S1_MAX_C) return DSB_E_CAPACITY;
   const int win_len = S1_TT + max_spread;
-  const size_t smem = s1_smem_bytes(ceff, win_len);
+  const size_t smem = s1_smem_bytes(ceff, dm_group, win_len);
   if (smem > 227 * 1024) return DSB_E_CAPACITY;
   if (sky_ring && (sky_window <= 0 || sky_head < 0 || sky_head >= sky_window ||
                    sky_count < 0 || sky_count > sky_window))
@@ -407,16 +413,28 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff; A.win_len = win_len;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
   A.sky_count = sky_count; A.sky_subtract = sky_subtract; A.status = status;
-  auto kern = d_bf16 ? stage1_rows_kernel<true> : stage1_rows_kernel<false>;
+  auto pick = [&](auto bf) {
+    constexpr bool B = decltype(bf)::value;
+    return dm_group == 32 ? stage1_rows_kernel<B, 32>
+         : dm_group == 16 ? stage1_rows_kernel<B, 16> : stage1_rows_kernel<B, 8>;
+  };
+  auto kern = d_bf16 ? pick(std::true_type{}) : pick(std::false_type{});
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return DSB_E_CUDA;
-  dim3 grid(n_blocks, (n_dm + S1_DG - 1) / S1_DG);
+  dim3 grid(n_blocks, (n_dm + dm_group - 1) / dm_group);
   kern<<<grid, S1_THREADS, smem, stream>>>(A);
   return launch_status();
 }
 
 int dsb_stage1_block_size(void) { return 4; }
 int dsb_stage1_dm_group(void) { return S1_DG; }
+
+long long dsb_stage1_smem_bytes(int ceff, int dm_group, int max_spread) {
+  if (ceff <= 0 || ceff > S1_MAX_C || max_spread < 0 ||
+      (dm_group != 32 && dm_group != 16 && dm_group != 8))
+    return -1;
+  return (long long)s1_smem_bytes(ceff, dm_group, S1_TT + max_spread);
+}
 
 }  // extern "C"

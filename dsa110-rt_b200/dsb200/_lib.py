@@ -36,10 +36,11 @@ _SIGNATURES = {
     "dsb_static_sky": [_vp, _vp, _c_int, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_stage2_roll": [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_ll, _vp, _vp],
     "dsb_stage1_rows": [_vp, _c_ll, _c_ll, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                        _vp, _c_int, _vp, _vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _vp,
-                        _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+                        _vp, _c_int, _vp, _vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int,
+                        _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
     "dsb_stage1_block_size": [],
     "dsb_stage1_dm_group": [],
+    "dsb_stage1_smem_bytes": [_c_int, _c_int, _c_int],
     "dsb_image_fold": [_c_int],
     "dsb_image_threads": [],
     "dsb_image_max_entries": [],
@@ -65,7 +66,7 @@ _SIGNATURES = {
                          _vp, _vp],
 }
 
-_RESTYPES: dict = {}
+_RESTYPES = {"dsb_stage1_smem_bytes": _c_ll}
 
 _lib: Optional[ctypes.CDLL] = None
 

@@ -79,6 +79,9 @@ class PipelineConfig:
     # stage-2 ring element: "c64" (complex64) or "bf16" (the BF16 storage form:
     # each part rounded to nearest-even bf16, accumulated in float32 on read)
     ring_dtype: str = "c64"
+    # coarse DMs per stage-1 block: None picks the largest of 32, 16, 8 whose
+    # shared time window fits; a value forces that group
+    stage1_dm_group: Optional[int] = None
 
     def __post_init__(self):
         if self.ring_dtype not in ("c64", "bf16"):
@@ -137,6 +140,7 @@ class Tables:
     cell_base: np.ndarray           # (G,) first global cell of each chgroup
     shift1: np.ndarray              # (G, ceff, n_coarse) int32
     max_spread: int                 # largest shift1 spread over a stage-1 DM group
+    dm_group: int                   # coarse DMs per stage-1 block (32, 16 or 8)
     shift2: np.ndarray              # (G, n_coarse) int32
     d_base: np.ndarray              # (G,) first D row of each chgroup (even)
     n_rows_d: int
@@ -316,11 +320,24 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     plan = DMPlan(dm_pc_cc=cfg.coarse_dm, t_int_fast_us=cfg.t_int_us, chan_sum_factor=cfg.csf,
                   band=band)
     shift1 = plan.delay_bins_all().astype(np.int32)
-    # largest spread of one subband's shifts over a group of coarse DMs (the
-    # shared time window of a stage-1 block)
-    dg = int(_lib.lib().dsb_stage1_dm_group())
+    # stage-1 DM group: the largest (32, 16, 8 coarse DMs) whose shared time
+    # window (the largest spread of one subband's shifts over the group) fits
+    # a block's shared memory
+    L = _lib.lib()
     s1 = shift1.reshape(G, ceff, -1)
-    max_spread = max(int(np.ptp(s1[:, :, k:k + dg], axis=2).max()) for k in range(0, s1.shape[2], dg))
+    dg = max_spread = None
+    cands = (int(L.dsb_stage1_dm_group()), 16, 8) if cfg.stage1_dm_group is None \
+        else (int(cfg.stage1_dm_group),)
+    for cand in cands:
+        spread = max(int(np.ptp(s1[:, :, k:k + cand], axis=2).max())
+                     for k in range(0, s1.shape[2], cand))
+        need = int(L.dsb_stage1_smem_bytes(ceff, cand, spread))
+        if 0 < need <= 227 * 1024:
+            dg, max_spread = cand, spread
+            break
+    if dg is None:
+        raise ValueError("stage 1: the DM plan's shift spread does not fit shared memory even "
+                         "with 8 coarse DMs per block; use more coarse DMs over the range")
     shift2 = np.stack([compute_stage2_shifts(chgroup=g, coarse_dm_pc_cm3=cfg.coarse_dm,
                                              t_int_corr_us=cfg.t_int_us,
                                              band=band).shifts_samples for g in range(G)])
@@ -351,6 +368,7 @@ def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None
     e = np.arange(N)
     tw = np.exp(2j * np.pi * e / N).astype(np.complex64)
     return Tables(cell_lambda=cell, patterns=pats, n_filled=n_filled, max_spread=max_spread,
+                  dm_group=dg,
                   yoff=yoff.astype(np.int32), ycnt=ycnt.astype(np.int32),
                   row_off=row_off.astype(np.int32), row_bls=row_bls.astype(np.int32),
                   n_rows_y=n_rows_y, y_base=y_base[:-1].astype(np.int32),
@@ -521,7 +539,8 @@ class SearchPipeline:
                 _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
                 int(self.ring_bf16), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
-                cfg.ceff, T.max_spread, _lib.ptr(self.sky), cfg.sky_window, self.sky_head,
+                cfg.ceff, T.dm_group, T.max_spread, _lib.ptr(self.sky), cfg.sky_window,
+                self.sky_head,
                 self.sky_count, sub, _lib.ptr(self.status), _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
         self.launches += 1

@@ -139,21 +139,27 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * sum) in the low half and the imaginary part in the high half; sums and the
  * sky statistics stay float32/float64.  Block b covers cells
  * [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b] and one group
- * of dsb_stage1_dm_group() coarse DMs (grid y). */
+ * of dm_group coarse DMs (grid y). */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                    long long t0, int n_t, int n_dm, int ceff, int max_spread, void* sky_ring,
-                    int sky_window,
+                    long long t0, int n_t, int n_dm, int ceff, int dm_group, int max_spread,
+                    void* sky_ring, int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream);
-/* Cells per block (blk_c0 multiples of it) and coarse DMs per block; the
- * caller passes max_spread = the largest (max - min) of shift1[g, s, d] over
- * the DMs of one group (d in [k*group, (k+1)*group)), which sizes the shared
- * time window of a block; a larger spread sets DSB_E_CAPACITY in *status. */
+/* Cells per block (blk_c0 multiples of it); the largest DM group (coarse
+ * DMs per block: 32, 16 or 8, grid y = ceil(n_dm / dm_group)); and the
+ * shared memory a block needs for a DM group whose largest shift spread is
+ * max_spread = the largest (max - min) of shift1[g, s, d] over the DMs of
+ * one group (d in [k*group, (k+1)*group)).  The caller picks the largest
+ * group that fits the device's 227 KB per block (a wide DM range over few
+ * coarse DMs needs a smaller group); a spread larger than the one passed
+ * sets DSB_E_CAPACITY in *status.  dsb_stage1_smem_bytes returns -1 for an
+ * unsupported group or ceff. */
 int dsb_stage1_block_size(void);
 int dsb_stage1_dm_group(void);
+long long dsb_stage1_smem_bytes(int ceff, int dm_group, int max_spread);
 /* ---- a12: fine-DM combine ---------------------------------------------------
  * Pipeline form of combine_chgroups (src/dsart/fine_dm/combiner.py:548) with
  * the Hermitian half-spectrum fold and fftshift checkerboard of

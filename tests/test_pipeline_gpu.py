@@ -49,11 +49,13 @@ def _setup(n_blocks=8, amp=1.0):
     return band, ob, e, n, blocks, kw
 
 
-@pytest.mark.parametrize("ring", ["c64", "bf16"])
-def test_pipeline_matches_oracle(dev, ring):
+@pytest.mark.parametrize("ring,dm_group", [("c64", None), ("bf16", None), ("bf16", 8),
+                                           ("c64", 16)])
+def test_pipeline_matches_oracle(dev, ring, dm_group):
     """Both ring forms against the oracle pipeline with the same ring form:
     the BF16 ring is the complex64 one rounded to bfloat16 part by part,
-    bit-exact; candidates as for the complex64 ring."""
+    bit-exact; candidates as for the complex64 ring.  Stage 1 runs with its
+    chosen DM group and with the smaller groups forced."""
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup()
     cfg = PipelineConfig(band=band, nant=kw["nant"], npkt_block=kw["npkt_block"],
@@ -61,7 +63,7 @@ def test_pipeline_matches_oracle(dev, ring):
                          coarse_dm=kw["coarse_dm"], fine_dm=kw["fine_dm"],
                          fine_to_coarse=kw["fine_to_coarse"], log_max_width=2, threshold=6.0,
                          sky_window=2, sky_warmup=1, chunk_tiles=32, fdm_batch=3,
-                         ring_dtype=ring)
+                         ring_dtype=ring, stage1_dm_group=dm_group)
     pipe = SearchPipeline(cfg, e, n, device=dev)
     got = []
     for b in blocks:
