@@ -2,6 +2,8 @@
 // noise estimate, and the FP64 uv-cell geometry kernel (sm_100a).
 #include "dsb_common.cuh"
 
+#include <type_traits>
+
 #include <algorithm>
 
 namespace {
@@ -113,9 +115,12 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
 
 // ===========================================================================
 // Reference-layout dense cint8 combine (image/fused_combine_cuda.py:210-300,
-// 560-700): streams [G, T_stream, 2, N, N] int8.
+// 560-700): streams [G, T_stream, 2, N, N] int8.  Calibrated forms add
+// scale * q + offset per chgroup term, with one scale/offset per chgroup or
+// (PER_T) per (chgroup, source time) [G, T_stream] -- the wire's per-tile
+// scales (fused_combine_cuda.py:431-505).
 // ===========================================================================
-template <bool HALF, bool CALIB, bool OUT_F16>
+template <bool HALF, bool CALIB, bool OUT_F16, bool PER_T>
 __global__ void combine_dense_kernel(const int8_t* __restrict__ streams,
                                      const int* __restrict__ shifts,
                                      const float* __restrict__ scales,
@@ -161,7 +166,8 @@ __global__ void combine_dense_kernel(const int8_t* __restrict__ streams,
       const int ts = t - shifts[g];
       if (ts >= 0 && ts < t_stream) {
         const long long b = g * g_stride + ts * t_stride;
-        const float sc = scales[g], orr = off_re[g], oii = off_im[g];
+        const int gt = PER_T ? g * t_stream + ts : g;
+        const float sc = scales[gt], orr = off_re[gt], oii = off_im[gt];
         ar = fmaf(sc, (float)streams[b + off_cell], ar) + orr;
         ai = fmaf(sc, (float)streams[b + off_cell + nsq], ai) + oii;
         if (HALF) {
@@ -566,7 +572,8 @@ int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const
 }
 
 int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
-                      const float* off_re, const float* off_im, void* out, int out_f16, int half,
+                      const float* off_re, const float* off_im, int per_t, void* out,
+                      int out_f16, int half,
                       int G, int t_stream, int t_det, int N, int t_lo, int fftshift,
                       cudaStream_t stream) {
   if (!streams || !shifts || !out || G <= 0 || N <= 0 || t_det <= t_lo || t_lo < 0) return DSB_E_ARG;
@@ -577,18 +584,20 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
   dim3 block(32, 4, 8);
   dim3 grid((nw + 31) / 32, (N + 3) / 4, (t_det - t_lo + 7) / 8);
   const int8_t* s = (const int8_t*)streams;
-#define DSB_CD(H, C, F)                                                                       \
-  combine_dense_kernel<H, C, F><<<grid, block, 0, stream>>>(s, shifts, scales, off_re, off_im, \
-                                                            out, G, t_stream, t_det, N, t_lo, \
-                                                            fftshift)
-  if (half) {
-    if (calib) { if (out_f16) DSB_CD(true, true, true); else DSB_CD(true, true, false); }
-    else { if (out_f16) DSB_CD(true, false, true); else DSB_CD(true, false, false); }
-  } else {
-    if (calib) { if (out_f16) DSB_CD(false, true, true); else DSB_CD(false, true, false); }
-    else { if (out_f16) DSB_CD(false, false, true); else DSB_CD(false, false, false); }
-  }
-#undef DSB_CD
+  auto go = [&](auto h, auto c, auto f, auto pt) {
+    combine_dense_kernel<decltype(h)::value, decltype(c)::value, decltype(f)::value,
+                         decltype(pt)::value><<<grid, block, 0, stream>>>(
+        s, shifts, scales, off_re, off_im, out, G, t_stream, t_det, N, t_lo, fftshift);
+  };
+  using T = std::true_type;
+  using F = std::false_type;
+  auto by_f = [&](auto h, auto c, auto pt) { out_f16 ? go(h, c, T{}, pt) : go(h, c, F{}, pt); };
+  auto by_c = [&](auto h) {
+    if (!calib) by_f(h, F{}, F{});
+    else if (per_t) by_f(h, T{}, T{});
+    else by_f(h, T{}, F{});
+  };
+  half ? by_c(T{}) : by_c(F{});
   return launch_status();
 }
 

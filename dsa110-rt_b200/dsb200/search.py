@@ -42,16 +42,23 @@ def _combine_dense(streams_cint8, shifts, output, *, half, scales, offsets_re, o
     if output.dtype not in (torch.complex32, torch.complex64):
         raise RuntimeError(f"output dtype {output.dtype} not in (complex32, complex64)")
     calib = scales is not None
+    # per-(chgroup, source time) scales [G, T] (the wire's per-tile scales) when
+    # all three are 2-D, as fused_combine_cuda.py:1299-1330 decides
+    per_t = calib and all(t is not None and t.dim() == 2
+                          for t in (scales, offsets_re, offsets_im))
     if calib:
+        want = (G, T) if per_t else (G,)
         for t, nm in ((scales, "scales"), (offsets_re, "offsets_re"), (offsets_im, "offsets_im")):
-            if t is None or t.dtype != torch.float32 or t.numel() != G:
-                raise RuntimeError(f"{nm} must be float32 ({G},)")
+            if t is None or t.dtype != torch.float32 or tuple(t.shape) != want:
+                raise RuntimeError(f"{nm} must be float32 {want}")
             _lib.require_cuda(t, nm)
+            if not t.is_contiguous():
+                raise RuntimeError(f"{nm} must be contiguous")
     t_det = int(t_lo) + int(output.shape[0])
     _lib.check(_lib.lib().dsb_combine_dense(
         _lib.ptr(streams_cint8), _lib.ptr(shifts), _lib.ptr(scales if calib else None),
         _lib.ptr(offsets_re if calib else None), _lib.ptr(offsets_im if calib else None),
-        _lib.ptr(output), int(output.dtype == torch.complex32), int(half), G, T, t_det, N,
+        int(per_t), _lib.ptr(output), int(output.dtype == torch.complex32), int(half), G, T, t_det, N,
         int(t_lo), int(bool(fftshift)), _lib.stream_of(output.device)), "dsb_combine_dense")
 
 

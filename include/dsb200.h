@@ -177,9 +177,26 @@ int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const
 /* Reference-layout combine on dense cint8 streams [G, T, 2, N, N]: replaces
  * fused_dequant_combine_per_fdm[_half] and the calibrated variants
  * (src/dsart/image/fused_combine_cuda.py:1104, :1359; kernels :210-700).
- * scales/off_* null -> integer path; out complex32 (out_f16) or complex64. */
+ * scales/off_* null -> integer path; otherwise each term is scale * q +
+ * offset (float32 fma, then add) with one value per chgroup [G], or, when
+ * per_t != 0, per (chgroup, source time) [G, t_stream]: the per-tile scales
+ * of the wire format (fused_combine_cuda.py:431-505).  out complex32
+ * (out_f16) or complex64. */
+
+/* ---- next row: wire encoding of dedispersed rows ------------------------------
+ * Replaces TransportTx._encode_rows (src/dsart/transport/tx.py:825-873).
+ * rows: n_rows x n_filled complex64 cells, row r at rows + r*row_stride
+ * (elements).  bits_per_cell 16: payload int8 (n_rows, n_filled, 2), per-row
+ * scale = float32(amax / 127) over |re|, |im| (1 for an all-zero row),
+ * q = clip(rint(x * float32(1 / scale)), -128, 127), ties to even.
+ * bits_per_cell 32: payload half (n_rows, n_filled, 2), nearest-even,
+ * scale 1.  Rows holding NaN or infinity are outside the reference's pinned
+ * behaviour (its float-to-int8 conversion of them is platform-defined). */
+int dsb_encode_rows(const void* rows, long long row_stride, int n_rows, int n_filled,
+                    int bits_per_cell, void* payload, float* scales, cudaStream_t stream);
 int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
-                      const float* off_re, const float* off_im, void* out, int out_f16, int half,
+                      const float* off_re, const float* off_im, int per_t, void* out,
+                      int out_f16, int half,
                       int G, int t_stream, int t_det, int N, int t_lo, int fftshift,
                       cudaStream_t stream);
 

@@ -586,6 +586,89 @@ def combine_half(streams: np.ndarray, shifts: np.ndarray, t_det: int, t_lo: int 
     return h
 
 
+def _fma32(a, b, c):
+    """float32 fma: a*b + c rounded once (a*b is exact in float64 for the
+    float32 x int8 products used here, and so is the sum at these ranges)."""
+    return (np.asarray(a, np.float64) * np.asarray(b, np.float64)
+            + np.asarray(c, np.float64)).astype(np.float32)
+
+
+def combine_dequant(q: np.ndarray, shifts: np.ndarray, scales, off_re, off_im, t_det: int,
+                    t_lo: int = 0, half: bool = False, fftshift: bool = True) -> np.ndarray:
+    """Calibrated cint8 combine (fused_combine_cuda.py:431-505, :681): each
+    chgroup term adds ``fma(scale, q, acc) + offset`` in float32, scale and
+    offsets per chgroup ``[G]`` or per (chgroup, source time) ``[G, T]``;
+    the half form sums the mirror term the same way and takes
+    ``0.5 (direct + conj mirror)``.  ``q``: int8 ``[G, T, 2, N, N]``."""
+    G, Ts, _, N, _ = q.shape
+    per_t = np.ndim(scales) == 2
+    nw = N // 2 + 1 if half else N
+    u = np.arange(N)[:, None]
+    w = np.arange(nw)[None, :]
+    um, wm = (N - u) % N, (N - w) % N
+    out = np.zeros((t_det - t_lo, N, nw), np.complex64)
+    for t in range(t_lo, t_det):
+        ar = np.zeros((N, nw), np.float32)
+        ai = np.zeros_like(ar)
+        mr = np.zeros_like(ar)
+        mi = np.zeros_like(ar)
+        for g in range(G):
+            ts = t - int(shifts[g])
+            if not 0 <= ts < Ts:
+                continue
+            idx = (g, ts) if per_t else (g,)
+            sc = np.float32(np.asarray(scales)[idx])
+            orr = np.float32(np.asarray(off_re)[idx])
+            oii = np.float32(np.asarray(off_im)[idx])
+            re, im = q[g, ts, 0].astype(np.float32), q[g, ts, 1].astype(np.float32)
+            ar = (_fma32(sc, re[u, w], ar) + orr).astype(np.float32)
+            ai = (_fma32(sc, im[u, w], ai) + oii).astype(np.float32)
+            if half:
+                mr = (_fma32(sc, re[um, wm], mr) + orr).astype(np.float32)
+                mi = (_fma32(sc, im[um, wm], mi) + oii).astype(np.float32)
+        if half:
+            o_re = (np.float32(0.5) * (ar + mr)).astype(np.float32)
+            o_im = (np.float32(0.5) * (ai - mi)).astype(np.float32)
+        else:
+            o_re, o_im = ar, ai
+        if fftshift:
+            flip = ((u + w) & 1).astype(bool)
+            o_re = np.where(flip, -o_re, o_re)
+            o_im = np.where(flip, -o_im, o_im)
+        out[t - t_lo] = o_re + 1j * o_im
+    return out
+
+
+# ---------------------------------------------------------------------------
+# wire encoding of dedispersed rows (transport/tx.py:803-873)
+# ---------------------------------------------------------------------------
+
+
+def encode_rows(row: np.ndarray, bits_per_cell: int):
+    """``TransportTx._encode_rows`` (tx.py:825-873): one DM row ``(n_fv,
+    n_filled)`` complex encoded tile by tile.  16 bits per cell: cint8 with
+    scale = float32(float64(amax) / 127) over |re|, |im| (1 for an all-zero
+    tile) and q = clip(round-half-even(x * float32(1 / scale)), -128, 127);
+    32 bits: float16 parts, scale 1.  Returns ``(payloads (n_fv, n_filled,
+    2), scales (n_fv,) float32)``."""
+    arr = np.asarray(row).astype(np.complex64, copy=False)
+    n_fv, n_filled = arr.shape
+    re_im = np.empty((n_fv, n_filled, 2), np.float32)
+    re_im[:, :, 0] = arr.real
+    re_im[:, :, 1] = arr.imag
+    if bits_per_cell == 16:
+        amax = (np.abs(re_im).reshape(n_fv, -1).max(axis=1) if n_filled
+                else np.zeros(n_fv, np.float32))
+        scales = (amax.astype(np.float64) / 127.0).astype(np.float32)
+        scales[amax == 0.0] = np.float32(1.0)
+        inv = (1.0 / scales.astype(np.float64)).astype(np.float32)
+        q = np.clip(np.round(re_im * inv[:, None, None]), -128.0, 127.0).astype(np.int8)
+        return q, scales
+    if bits_per_cell == 32:
+        return re_im.astype(np.float16), np.ones(n_fv, np.float32)
+    raise AssertionError(f"unhandled bits_per_cell={bits_per_cell}")
+
+
 def compact_to_dense(values: np.ndarray, ix_row, ix_col, n_grid: int) -> np.ndarray:
     """Scatter ``(..., n_filled)`` cell values into ``(..., N, N)``."""
     out = np.zeros(values.shape[:-1] + (n_grid, n_grid), values.dtype)

@@ -310,6 +310,36 @@ def make_image_detector():
     np.savez_compressed(os.path.join(HERE, "image_detector.npz"), **out)
 
 
+TRANSPORT_SEED = 880
+
+
+def transport_rows(seed: int = TRANSPORT_SEED) -> np.ndarray:
+    """Seeded DM rows (n_fv 24, n_filled 300): Gaussian tiles of spread
+    magnitudes, an all-zero tile, and tiles with amax 127 whose values sit
+    on half-integers (exact ties of the rounding)."""
+    rng = np.random.default_rng(seed)
+    n_fv, nf = 24, 300
+    mag = 10.0 ** rng.uniform(-3, 6, n_fv)
+    row = (rng.standard_normal((n_fv, nf)) + 1j * rng.standard_normal((n_fv, nf))) * mag[:, None]
+    row[5] = 0
+    for t in (7, 8):
+        re = rng.integers(-127, 127, nf) + 0.5
+        im = rng.integers(-127, 127, nf) + 0.5
+        re[0], im[0] = 127.0, -127.0
+        row[t] = re + 1j * im
+    return row.astype(np.complex64)
+
+
+def make_transport():
+    """TransportTx._encode_rows (transport/tx.py:825-873) on seeded rows."""
+    from dsart.transport.tx import TransportTx
+    rows = transport_rows()
+    q16, s16 = TransportTx._encode_rows(rows, 16)
+    q32, s32 = TransportTx._encode_rows(rows, 32)
+    np.savez_compressed(os.path.join(HERE, "transport.npz"), q16=np.asarray(q16),
+                        s16=np.asarray(s16), q32=np.asarray(q32), s32=np.asarray(s32))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DSART_REFERENCE", ""))
@@ -319,7 +349,7 @@ def main():
         sys.exit("need --reference <dsa110-rt>/src")
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
-            make_image_detector]
+            make_image_detector, make_transport]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
