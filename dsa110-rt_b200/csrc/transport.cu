@@ -73,7 +73,7 @@ extern "C" {
 
 int dsb_encode_rows(const void* rows, long long row_stride, int n_rows, int n_filled,
                     int bits_per_cell, void* payload, float* scales, cudaStream_t stream) {
-  if (!rows || (!payload && n_filled > 0) || !scales || n_rows < 0 || n_filled < 0 ||
+  if (((!rows || !payload) && n_filled > 0) || !scales || n_rows < 0 || n_filled < 0 ||
       row_stride < n_filled)
     return DSB_E_ARG;
   if (bits_per_cell != 16 && bits_per_cell != 32) return DSB_E_UNSUPPORTED;
