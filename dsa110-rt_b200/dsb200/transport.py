@@ -24,8 +24,10 @@ BITS_CFP16_COMPLEX = 32
 
 
 def encode_rows(row: torch.Tensor, bits_per_cell: int):
-    """Encode all tiles of one DM row ``(n_fv, n_filled)`` complex64 (CUDA)."""
-    _lib.require_cuda(row, "row")
+    """Encode all tiles of one DM row ``(n_fv, n_filled)`` complex64 (CUDA);
+    tiles may be strided (a view of every k-th tile), cells must be dense."""
+    if not isinstance(row, torch.Tensor) or row.device.type != "cuda":
+        raise ValueError("row must be a CUDA tensor (dsb200 has no CPU path)")
     if row.dim() != 2:
         raise ValueError(f"row must be (n_fv, n_filled); got {tuple(row.shape)}")
     if bits_per_cell not in (BITS_CINT8_COMPLEX, BITS_CFP16_COMPLEX):
