@@ -132,16 +132,21 @@ DSB_DEV void idftR(float2 (&a)[R]) {
 
 // Stage-2 ring elements: complex64, or the BF16 storage form (bf16 re/im
 // pairs in 32 bits, decoded to float32 before any arithmetic).
+// T2 holds two adjacent cells (one 8- or 16-byte load).
 template <bool BF16> struct RingElem {
   using T = float2;
-  static DSB_DEV T zero() { return make_float2(0.f, 0.f); }
-  static DSB_DEV float2 dec(T w) { return w; }
+  using T2 = float4;
+  static DSB_DEV T2 zero2() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  static DSB_DEV float2 lo(T2 w) { return make_float2(w.x, w.y); }
+  static DSB_DEV float2 hi(T2 w) { return make_float2(w.z, w.w); }
   static DSB_DEV float2 get(const T* p) { return *p; }
 };
 template <> struct RingElem<true> {
   using T = uint32_t;
-  static DSB_DEV T zero() { return 0u; }
-  static DSB_DEV float2 dec(T w) { return bf16_pair_to_f2(w); }
+  using T2 = uint2;
+  static DSB_DEV T2 zero2() { return make_uint2(0u, 0u); }
+  static DSB_DEV float2 lo(T2 w) { return bf16_pair_to_f2(w.x); }
+  static DSB_DEV float2 hi(T2 w) { return bf16_pair_to_f2(w.y); }
   static DSB_DEV float2 get(const T* p) { return bf16_pair_to_f2(*p); }
 };
 
@@ -151,8 +156,8 @@ struct ImgArgs {
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
   const unsigned* c_meta;   // (cell_base[G]) per pattern cell: tgt | conj << 16 | g << 17;
-                            // 0xffffffff pads each chgroup's run to a multiple of 32
-  const int* cell_base;     // (G + 1) multiples of 32
+                            // 0xffffffff pads each chgroup's run to a multiple of 64
+  const int* cell_base;     // (G + 1) multiples of 64
   const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
   int n_c2;
   const int* thr_b;         // (THREADS + 1) S range [thr_b[i], thr_b[i+1]) of thread i
@@ -240,7 +245,9 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   const int sb = __ldg(A.thr_b + tid);
   const int sn = __ldg(A.thr_b + tid + 1) - sb;
   const bool bad_range = sn < 0 || sn > IMG_MAXE || sb < 0 || sb + sn > A.n_s;
-  if (__syncthreads_or(bad_range || (A.cell_base[A.G] & 31))) {
+  bool bad_base = false;  // each chgroup's run: whole 64-entry pairs of chunks
+  for (int g = tid; g <= A.G; g += THREADS) bad_base |= (A.cell_base[g] & 63) != 0;
+  if (__syncthreads_or(bad_range || bad_base)) {
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
     return;  // every thread leaves, before any TMEM is taken
   }
@@ -297,43 +304,50 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         atomicAdd(s_re + t, v.x);
         atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
       };
-      // warp w takes the 32-entry chunks w, w + 8, ... of c_meta in order;
-      // each chgroup's run is a whole number of chunks, so the chgroup, its
-      // first entry and its ring row stay in registers and change only at
-      // a run boundary (warp-uniform), and the shared-memory pipe is left to
-      // the atomics.  8 metadata and 8 value loads in flight per thread.
-      constexpr int U = 8, NW = THREADS / 32;
-      const int n_chunks = n_tot >> 5;
+      // warp w takes the 64-entry double chunks w, w + 8, ... of c_meta in
+      // order, each lane two adjacent cells with one metadata and one ring
+      // load; each chgroup's run is a whole number of double chunks, so the
+      // chgroup, its first entry and its ring row stay in registers and
+      // change only at a run boundary (warp-uniform), and the shared-memory
+      // pipe is left to the atomics.  8 cells in flight per thread.
+      using Elem2 = typename RingElem<BF16>::T2;
+      constexpr int U = 4, NW = THREADS / 32;
+      const int n_dch = n_tot >> 6;
+      const uint2* cm2 = reinterpret_cast<const uint2*>(A.c_meta);
       int g = -1, g_lo = 0, g_hi = 0, g_end = 0;
       const Elem* src = static_cast<const Elem*>(A.D);
-      for (int c0 = warp; c0 < n_chunks; c0 += NW * U) {
+      for (int c0 = warp; c0 < n_dch; c0 += NW * U) {
         // raw ring words: decoded only in the add loop below, so that no
         // instruction waits on a load before the batch's other loads issue
-        unsigned m[U];
-        Elem v[U];
+        uint2 m[U];
+        Elem2 v[U];
 #pragma unroll
         for (int q = 0; q < U; ++q) {
           const int ch = c0 + NW * q;
-          m[q] = 0xffffffffu;
-          v[q] = RingElem<BF16>::zero();
-          if (ch < n_chunks) {
-            while (32 * ch >= g_hi) {
+          m[q] = make_uint2(0xffffffffu, 0xffffffffu);
+          v[q] = RingElem<BF16>::zero2();
+          if (ch < n_dch) {
+            while (64 * ch >= g_hi) {
               ++g;
               g_lo = s_cbase[g];
               g_hi = s_cbase[g + 1];
               g_end = s_end[g];
               src = s_slice[g];
             }
-            const int e = 32 * ch + lane;
+            // cells e, e + 1 (e even): both inside the row's pitch whenever
+            // e is a pattern cell (the pitch is n_filled rounded up to 4)
+            const int e = 64 * ch + 2 * lane;
             if (e < g_end) {
-              m[q] = __ldg(A.c_meta + e);
-              v[q] = src[e - g_lo];
+              m[q] = __ldg(cm2 + (e >> 1));
+              v[q] = *reinterpret_cast<const Elem2*>(src + (e - g_lo));
             }
           }
         }
 #pragma unroll
-        for (int q = 0; q < U; ++q)
-          if (m[q] != 0xffffffffu) add(m[q], RingElem<BF16>::dec(v[q]));
+        for (int q = 0; q < U; ++q) {
+          if (m[q].x != 0xffffffffu) add(m[q].x, RingElem<BF16>::lo(v[q]));
+          if (m[q].y != 0xffffffffu) add(m[q].y, RingElem<BF16>::hi(v[q]));
+        }
       }
       for (int i = tid; i < A.n_c2; i += THREADS) {
         const int2 cm = __ldg(A.c2 + i);

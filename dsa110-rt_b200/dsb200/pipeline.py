@@ -159,7 +159,7 @@ class ImageTables:
     pattern cell of every chgroup lands on them, and how the kernel's
     threads and column groups split them."""
     n_s: int
-    c_meta: np.ndarray      # uint32 s | conj << 16 | g << 17; chgroup runs padded to 32
+    c_meta: np.ndarray      # uint32 s | conj << 16 | g << 17; chgroup runs padded to 64
     cell_base: np.ndarray   # (G + 1) int32
     c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
     thr_b: np.ndarray       # (threads + 1) int32: S range of each kernel thread
@@ -260,10 +260,10 @@ def build_image_tables(pats, N: int) -> ImageTables:
     kc = np.flatnonzero(~dense)
     kcols = (kc | ((occ[kc] != 0).astype(np.int64) << 16)).astype(np.int32)
     n1 = u.size
-    # each chgroup's run padded with 0xffffffff to a whole number of 32-entry
-    # chunks (the kernel finds an entry's chgroup from its chunk)
+    # each chgroup's run padded with 0xffffffff to a whole number of 64-entry
+    # double chunks (the kernel's warps walk the runs 64 cells at a time)
     nfs = np.asarray([p.ix_row.size for p in pats], np.int64)
-    cell_base = np.concatenate([[0], np.cumsum((nfs + 31) // 32 * 32)])
+    cell_base = np.concatenate([[0], np.cumsum((nfs + 63) // 64 * 64)])
     c_meta = np.full(int(cell_base[-1]), 0xFFFFFFFF, np.uint32)
     c_meta[cell_base[g] + k] = (inv[:n1] | (t1c << 16) | (g << 17)).astype(np.uint32)
     c2 = np.stack([k[both] | (g[both] << 16), inv[n1:] | (1 << 16)], axis=1).astype(np.int32)

@@ -215,7 +215,7 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k <
  *      n_filled[g] of chgroup g adds its value (conjugated if conj) to S
  *      entry s; each chgroup's run is padded with 0xffffffff to a multiple
- *      of 32 entries (cell_base[g] multiples of 32);
+ *      of 64 entries (cell_base[g] multiples of 64);
  *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
  *      w = N/2 that also land on their mirror);
  *   thr_b: (dsb_image_threads() + 1) S ranges, one per kernel thread, each
@@ -232,7 +232,7 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256; n_s must
  * fit the kernel's shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY
  * is returned.  status: a thread range longer than max_entries or a
- * cell_base[G] that is not a multiple of 32 sets DSB_E_CAPACITY and writes
+ * cell_base[g] that is not a multiple of 64 sets DSB_E_CAPACITY and writes
  * nothing.  Each
  * CTA holds 128 columns of tensor memory while it runs. */
 int dsb_image_fold(int n_grid);

@@ -141,7 +141,7 @@ def test_image_tables_layout():
         assert msk == occ[c] and msk & ~1
     for kc in T.kcols.tolist():
         assert occ.get(kc & 0xFFFF, 0) == (1 if kc >> 16 else 0)
-    assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 32 == 0)
+    assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 64 == 0)
     for g, p in enumerate(pats):                # padding after each chgroup's run
         assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
     assert T.n_s <= LC * (N // 2 + 2)          # fits the kernel's shared buffer
