@@ -40,6 +40,7 @@
 #include "dsb_common.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace {
 
@@ -386,7 +387,10 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       // ---- 2a. fold S into the occupied slots (n', col) of buf: each slot's
       //      entries are consecutive in one thread's range, written once
       //      after the last of them ----
-      {
+      // (one copy of the loop per pass, so that the rotation i^(q p) is
+      // nothing for p = 0, a sign for p = 2 and needs no multiply otherwise)
+      auto fold = [&](auto pass) {
+        constexpr unsigned PP = decltype(pass)::value;
         float2 acc = make_float2(0.f, 0.f);
         uint4 md_next = __ldg(A.gmeta + tid);
         for (int c = 0; c < nch; ++c) {
@@ -399,8 +403,16 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
           for (int j = 0; j < 8; ++j) {
             if (8 * c + j < sn) {
               const unsigned m = (mw[j >> 1] >> (16 * (j & 1))) & 0xffffu;
-              const float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
-              acc = cadd(acc, crot_rt(v, ((m >> 13) & 3u) * (unsigned)p));
+              float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
+              const unsigned q = (m >> 13) & 3u;
+              if constexpr (PP == 2) {
+                const unsigned sgn = (q & 1u) << 31;  // i^(2q) = (-1)^q
+                v = make_float2(__uint_as_float(__float_as_uint(v.x) ^ sgn),
+                                __uint_as_float(__float_as_uint(v.y) ^ sgn));
+              } else if constexpr (PP != 0) {
+                v = crot_rt(v, q * PP);
+              }
+              acc = cadd(acc, v);
               if (m & 0x8000u) {
                 buf[((m >> 7) & (LC - 1)) * P + (m & (NC - 1))] = acc;
                 acc = make_float2(0.f, 0.f);
@@ -408,6 +420,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
             }
           }
         }
+      };
+      static_assert(FOLD == 4, "the fold is instantiated for four passes");
+      switch (p) {
+        case 0: fold(std::integral_constant<unsigned, 0>{}); break;
+        case 1: fold(std::integral_constant<unsigned, 1>{}); break;
+        case 2: fold(std::integral_constant<unsigned, 2>{}); break;
+        default: fold(std::integral_constant<unsigned, 3>{}); break;
       }
       __syncthreads();
       // ---- 2b. column transforms of pass p (in place in buf); only the
