@@ -52,6 +52,7 @@ _SIGNATURES = {
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                           _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_encode_rows": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp, _vp],
+    "dsb_rfi_zero_fill": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_int, _vp],
     "dsb_mask_to_cube": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _c_int, _c_int,
                          _vp],
     "dsb_padded_cumsum": [_vp, _c_int, _c_int, _c_ll, _c_int, _vp, _vp],

@@ -75,6 +75,57 @@ def unpack_int4_split(
     return re, im
 
 
+def apply_rfi_mask_to_raw(raw: torch.Tensor, rfi_mask: Optional[torch.Tensor] = None, *,
+                          time_chan_mask: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Zero flagged voltages in raw on-wire pages, in place: the RFI
+    excision of ``apply_rfi_mask_to_voltages``
+    (services/corr_fast_integration.py:1249-1370) moved ahead of the unpack,
+    so the correlator never sees a flagged sample (a zero byte is 0 + 0i).
+
+    ``raw``: uint8 ``(G, npkt, nant, nchan, 2, 2)`` (or one page without G)
+    on the GPU.  ``rfi_mask``: bool ``(G, nant, nchan, 2)`` (or ``(nant,
+    nchan, 2)`` for one page), True == flagged.  ``time_chan_mask``: bool
+    ``(G, n_acc, nchan, 2)`` (or 3-D), True == flagged for that accumulation
+    of ``npkt / n_acc`` packets on every antenna.  Raises TypeError for a
+    non-bool mask and ValueError for a shape mismatch or an ``n_acc`` that
+    does not divide the packets, as the reference does."""
+    _lib.require_cuda(raw, "raw")
+    if raw.dtype != torch.uint8 or raw.dim() not in (5, 6) or raw.shape[-2:] != (2, 2):
+        raise ValueError(f"raw must be uint8 (G, npkt, nant, nchan, 2, 2); got "
+                         f"{raw.dtype} {tuple(raw.shape)}")
+    pages = raw if raw.dim() == 6 else raw.unsqueeze(0)
+    G, npkt, nant, nchan = pages.shape[:4]
+
+    def prep(m, name):
+        # one flag byte per entry, a leading page axis (added for one page)
+        if m is None:
+            return None
+        if m.dtype != torch.bool:
+            raise TypeError(f"{name} must be bool; got {m.dtype}")
+        if m.dim() != 3 + (raw.dim() == 6):
+            raise ValueError(f"{name} shape {tuple(m.shape)} does not match the pages")
+        return m.reshape((G,) + tuple(m.shape[-3:])).to(raw.device, torch.uint8).contiguous()
+
+    m = prep(rfi_mask, "rfi_mask")
+    if m is not None and tuple(m.shape) != (G, nant, nchan, 2):
+        raise ValueError(f"rfi_mask shape {tuple(rfi_mask.shape)} != (G, NANTS, NCHAN, NPOL) = "
+                         f"({G}, {nant}, {nchan}, 2)")
+    tm = prep(time_chan_mask, "time_chan_mask")
+    n_acc = 0
+    if tm is not None:
+        n_acc = int(tm.shape[1])
+        if tuple(tm.shape[2:]) != (nchan, 2):
+            raise ValueError(f"time_chan_mask shape {tuple(time_chan_mask.shape)} != "
+                             f"(n_acc, NCHAN, NPOL) = (*, {nchan}, 2)")
+        if n_acc <= 0 or npkt % n_acc:
+            raise ValueError(f"time_chan_mask has n_acc={n_acc}, which does not divide the "
+                             f"packet axis {npkt}")
+    _lib.check(_lib.lib().dsb_rfi_zero_fill(_lib.ptr(raw), G, npkt, nant, nchan, _lib.ptr(m),
+                                            _lib.ptr(tm), n_acc, _lib.stream_of(raw.device)),
+               "dsb_rfi_zero_fill")
+    return raw
+
+
 def validate_fast_voltage_shape(real_v, imag_v, *, t_int_fast_native: int, nants: int = NANTS,
                                 nchan: int = NCHAN_PER_CHGROUP, nvolt_pol: int = NPOL
                                 ) -> Tuple[int, int]:

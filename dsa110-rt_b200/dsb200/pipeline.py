@@ -40,6 +40,7 @@ import torch
 
 from . import _lib
 from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
+from .corr import apply_rfi_mask_to_raw
 from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
 from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
 from .search import (CandidateBuffer, _nms, compute_edge_mask, detect_images, irfft2_image,
@@ -616,17 +617,24 @@ class SearchPipeline:
                              f"multiple of {per_chunk} packets")
         return raw.numel() // row
 
-    def process_block(self, raw: torch.Tensor, *, collect: bool = True) -> List[StreamCandidate]:
+    def process_block(self, raw: torch.Tensor, *, collect: bool = True,
+                      rfi_mask: Optional[torch.Tensor] = None,
+                      time_chan_mask: Optional[torch.Tensor] = None) -> List[StreamCandidate]:
         """Push one block of raw pages ``(G, npkt, nant, nchan, 2, 2)`` uint8
         (device tensor, or host tensor copied here) through the pipeline;
         returns the candidates whose detector cubes completed.  ``npkt`` is
         any whole number of chunks (``npkt_block`` for the fixed-size
-        stream)."""
+        stream).  ``rfi_mask`` ``(G, nant, nchan, 2)`` and ``time_chan_mask``
+        ``(G, n_acc, nchan, 2)`` (bool, True == flagged) zero the flagged
+        voltages before the correlator (``apply_rfi_mask_to_raw``; a device
+        block is changed in place, as the reference's voltages are)."""
         cfg = self.cfg
         npkt = self.block_packets(raw)
         if raw.device.type != "cuda":
             raw = raw.to(self.dev, non_blocking=True)
         raw = raw.contiguous()
+        if rfi_mask is not None or time_chan_mask is not None:
+            apply_rfi_mask_to_raw(raw, rfi_mask, time_chan_mask=time_chan_mask)
         self.out = []
         self._pending = []
         self.last_d2h_bytes = 0

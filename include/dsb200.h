@@ -183,6 +183,19 @@ int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const
  * of the wire format (fused_combine_cuda.py:431-505).  out complex32
  * (out_f16) or complex64. */
 
+/* ---- next row: RFI excision hook -------------------------------------------
+ * Replaces apply_rfi_mask_to_voltages (src/dsart/services/
+ * corr_fast_integration.py:1249-1370), applied to the raw on-wire pages
+ * before the correlator instead of to the unpacked voltages: in raw
+ * (n_pages, npkt, nant, nchan, 2t, 2p) uint8 (4-byte aligned), every sample
+ * flagged in mask (n_pages, nant, nchan, 2) or, for packets of accumulation
+ * a = pkt / (npkt / n_acc), in time_mask (n_pages, n_acc, nchan, 2) is set
+ * to 0 (0 + 0i); nonzero flag bytes mean flagged; either mask may be null.
+ * In place. */
+int dsb_rfi_zero_fill(void* raw, int n_pages, int npkt, int nant, int nchan,
+                      const unsigned char* mask, const unsigned char* time_mask, int n_acc,
+                      cudaStream_t stream);
+
 /* ---- next row: wire encoding of dedispersed rows ------------------------------
  * Replaces TransportTx._encode_rows (src/dsart/transport/tx.py:825-873).
  * rows: n_rows x n_filled complex64 cells, row r at rows + r*row_stride

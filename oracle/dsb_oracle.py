@@ -147,6 +147,30 @@ def unpack_int4_gemm_layout(raw: np.ndarray, npkt: int, nant: int, nchan: int
             np.ascontiguousarray(im.transpose(perm)))
 
 
+def rfi_zero_fill_raw(page: np.ndarray, rfi_mask: Optional[np.ndarray],
+                      time_chan_mask: Optional[np.ndarray] = None) -> np.ndarray:
+    """RFI excision by voltage zero-fill (apply_rfi_mask_to_voltages,
+    services/corr_fast_integration.py:1249-1370) applied to one on-wire page
+    ``(npkt, nant, nchan, 2t, 2p)`` uint8: every sample of a flagged (antenna,
+    channel, pol) of ``rfi_mask (nant, nchan, 2)``, and of a flagged (chan,
+    pol) in accumulation a of ``time_chan_mask (n_acc, nchan, 2)`` (packets
+    [a * npkt / n_acc, (a + 1) * npkt / n_acc), every antenna), becomes 0:
+    both nibbles zero is the voltage 0 + 0i.  True == flagged.  Returns a
+    copy."""
+    out = np.array(page, np.uint8, copy=True)
+    npkt, nant, nchan = out.shape[:3]
+    keep = np.ones((npkt, nant, nchan, 1, 2), bool)
+    if rfi_mask is not None:
+        keep &= ~np.asarray(rfi_mask, bool)[None, :, :, None, :]
+    if time_chan_mask is not None:
+        tm = np.asarray(time_chan_mask, bool)
+        n_acc = tm.shape[0]
+        per = npkt // n_acc
+        keep &= ~np.repeat(tm, per, axis=0)[:, None, :, None, :]
+    out[~np.broadcast_to(keep, out.shape)] = 0
+    return out
+
+
 # ---------------------------------------------------------------------------
 # a4: fast correlator (services/corr_fast_kernel.py:364-755)
 # ---------------------------------------------------------------------------

@@ -310,6 +310,31 @@ def make_image_detector():
     np.savez_compressed(os.path.join(HERE, "image_detector.npz"), **out)
 
 
+RFI_SEED = 515
+
+
+def rfi_masks(seed: int = RFI_SEED):
+    """Seeded flags for a full page (96 ant, 384 ch, 2 pol; 64 accumulations
+    of 32 packets): about 2 % of (ant, chan, pol) and 1 % of (acc, chan, pol)."""
+    rng = np.random.default_rng(seed)
+    return rng.random((96, 384, 2)) < 0.02, rng.random((64, 384, 2)) < 0.01
+
+
+def make_rfi():
+    """apply_rfi_mask_to_voltages (services/corr_fast_integration.py:1249) on
+    the unpacked reference page, both masks."""
+    import torch
+    from dsart.services.corr_fast_integration import apply_rfi_mask_to_voltages
+    from dsart.services.slow_corr_kernel import unpack_int4_split
+    raw = unpack_raw()
+    re, im = unpack_int4_split(raw, device="cpu", scale=1.0, out_dtype=torch.float32)
+    m, tm = rfi_masks()
+    apply_rfi_mask_to_voltages(re, im, torch.from_numpy(m), time_chan_mask=torch.from_numpy(tm))
+    re8, im8 = re.numpy().astype(np.int8), im.numpy().astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, "rfi.npz"), sha_re=sha(re8), sha_im=sha(im8),
+                        zeros=np.asarray([(re8 == 0).sum(), (im8 == 0).sum()]))
+
+
 TRANSPORT_SEED = 880
 
 
@@ -349,7 +374,7 @@ def main():
         sys.exit("need --reference <dsa110-rt>/src")
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
-            make_image_detector, make_transport]
+            make_image_detector, make_transport, make_rfi]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
