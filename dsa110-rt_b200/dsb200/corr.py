@@ -269,3 +269,50 @@ class FastCorrKernel:
             _lib.ptr(st), _lib.stream_of(self.device)), "dsb_corr_tc")
         self._last_status = st
         return out if raw.ndim == 6 else out[0]
+
+
+@dataclass
+class SlowCorrKernel:
+    """Slow correlator product (slow_corr_kernel.py:576-720): one full-block
+    integration per (baseline, channel, pol), ``(NBASE, NCHAN, nbada_pol)``
+    complex64, stored at ``bls(a, b)`` as ``conj(E_b) E_a`` (F18).  The same
+    X-engine as ``FastCorrKernel.compute_split`` with the tile as long as the
+    block and the pols kept apart; the block is summed whole, so
+    ``half_fac`` (the reference's sub-batching of the packet axis) does not
+    change the result.  Integer codes correlate exactly."""
+
+    device: torch.device
+    nants: int = NANTS
+    nchan: int = NCHAN_PER_CHGROUP
+    nvolt_pol: int = NPOL
+    nbada_pol: int = BADA_NPOL
+    n_time_samples: int = NPACKETS_PER_BLOCK * NTIMES_PER_PACKET
+    half_fac: int = 1
+    accum_dtype: torch.dtype = torch.float32
+    _fast: FastCorrKernel = field(init=False)
+
+    def __post_init__(self) -> None:
+        if self.nbada_pol > self.nvolt_pol:
+            raise ValueError(f"nbada_pol ({self.nbada_pol}) > nvolt_pol ({self.nvolt_pol})")
+        if self.half_fac <= 0 or self.n_time_samples % self.half_fac != 0:
+            raise ValueError(f"n_time_samples ({self.n_time_samples}) not divisible by "
+                             f"half_fac ({self.half_fac})")
+        self._fast = FastCorrKernel(self.device, t_int_fast_native=self.n_time_samples,
+                                    nants=self.nants, nchan=self.nchan)
+        self.device = self._fast.device
+
+    def compute_split(self, real_v: torch.Tensor, imag_v: torch.Tensor) -> torch.Tensor:
+        """Correlate one block of GEMM-layout voltages ``(NCHAN, 2, NPOL,
+        n_time_samples / 2, NANTS)`` -> ``(NBASE, NCHAN, nbada_pol)``."""
+        want = (self.nchan, NTIMES_PER_PACKET, self.nvolt_pol,
+                self.n_time_samples // NTIMES_PER_PACKET, self.nants)
+        for name, t in (("real_v", real_v), ("imag_v", imag_v)):
+            if t.device != self.device:
+                raise ValueError(f"{name} on {t.device}, kernel on {self.device}")
+            if tuple(t.shape) != want:
+                raise ValueError(f"{name} shape {tuple(t.shape)}, expected {want}")
+        if real_v.dtype != imag_v.dtype:
+            raise ValueError(f"real_v dtype {real_v.dtype} != imag_v dtype {imag_v.dtype}")
+        vis = self._fast.compute_split(real_v, imag_v, fuse_stokes_i=False)
+        return vis[0, :, :, : self.nbada_pol]
+

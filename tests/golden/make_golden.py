@@ -335,6 +335,22 @@ def make_rfi():
                         zeros=np.asarray([(re8 == 0).sum(), (im8 == 0).sum()]))
 
 
+def make_slow_corr():
+    """SlowCorrKernel.compute_split (services/slow_corr_kernel.py:576-720) on
+    the unpacked reference page in float32 (scale 1: integer codes, exact
+    sums), full block, both pols."""
+    import torch
+    from dsart.services.slow_corr_kernel import SlowCorrKernel, unpack_int4_split
+    raw = unpack_raw()
+    re, im = unpack_int4_split(raw, device="cpu", scale=1.0, out_dtype=torch.float32)
+    vis = SlowCorrKernel(device="cpu").compute_split(re, im).numpy()
+    v = np.ascontiguousarray(vis.astype(np.complex64))
+    rng = np.random.default_rng(2)
+    idx = rng.integers(0, v.size, 4096)
+    np.savez_compressed(os.path.join(HERE, "slow_corr.npz"), shape=np.asarray(v.shape),
+                        sha=sha(v.view(np.float32)), idx=idx, samples=v.reshape(-1)[idx])
+
+
 TRANSPORT_SEED = 880
 
 
@@ -374,7 +390,7 @@ def main():
         sys.exit("need --reference <dsa110-rt>/src")
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
-            make_image_detector, make_transport, make_rfi]
+            make_image_detector, make_transport, make_rfi, make_slow_corr]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
