@@ -351,6 +351,53 @@ def make_slow_corr():
                         sha=sha(v.view(np.float32)), idx=idx, samples=v.reshape(-1)[idx])
 
 
+POSTPROC_SEED = 6060
+
+
+def postproc_fields(seed: int = POSTPROC_SEED, n: int = 500):
+    """Seeded candidate fields, clustered so that the mergers suppress: one
+    row per candidate (l, m, dm_idx, event_specnum, width, snr, flags,
+    kernel index); dm_fine carries the row index."""
+    rng = np.random.default_rng(seed)
+    centre = rng.integers(0, 12, n)
+    l = np.round(rng.normal(centre * 7.0, 2.0), 1)
+    m = np.round(rng.normal((centre % 5) * 9.0, 2.0), 1)
+    dm_idx = np.maximum(0, centre * 3 + rng.integers(-4, 5, n))
+    t = np.maximum(0, centre * 400 + rng.integers(-300, 300, n))
+    width = 1 << rng.integers(0, 6, n)
+    snr = np.round(rng.uniform(6.0, 30.0, n), 2)
+    snr[:20] = snr[20:40]                     # exact SNR ties
+    flags = np.where(rng.random(n) < 0.05, 1 << 3, 0)
+    kern = rng.integers(0, 4, n)
+    return l, m, dm_idx, t, width, snr, flags, kern
+
+
+def make_postproc():
+    """merge_across_kernels_c1 / merge_across_kernels (detector/merger.py)
+    and filter_to_canonical (detector/decoder.py:541) on seeded candidates."""
+    from dsart.common.contracts import Candidate
+    from dsart.detector.decoder import filter_to_canonical
+    from dsart.detector.merger import MergerConfig, merge_across_kernels, merge_across_kernels_c1
+    l, m, d, t, w, snr, flags, kern = postproc_fields()
+    cands = [Candidate(l=float(l[i]), m=float(m[i]), dm_fine=float(i), dm_idx=int(d[i]),
+                       event_specnum=int(t[i]), width_samples=int(w[i]),
+                       kernel_id=f"unit:d1:b{1 << int(kern[i])}", snr=float(snr[i]),
+                       detector_version="v1", flags=int(flags[i]), search_node_id=0, gpu_half=0)
+             for i in range(len(l))]
+    ids = lambda cs: np.asarray([int(c.dm_fine) for c in cs], np.int64)  # noqa: E731
+    out = dict(c1_default=ids(merge_across_kernels_c1(cands, MergerConfig())),
+               c1_custom=ids(merge_across_kernels_c1(cands, MergerConfig(
+                   lm_max_cells=5, dm_max_trials=1, t_frac=0.5, sample_period_specnum=4))),
+               legacy=ids(merge_across_kernels(cands)),
+               legacy_custom=ids(merge_across_kernels(cands, merge_radius_lm=2,
+                                                      merge_radius_fdm=3, merge_radius_t=50)))
+    emit, dropped = filter_to_canonical(cands, dm_idx_canonical_lo=5, dm_idx_canonical_hi=25,
+                                        t_det=4000, n_kernel_max_t=128, cube_t_offset=100)
+    out.update(emit=ids(emit), dropped=ids(dropped),
+               dropped_flags=np.asarray([c.flags for c in dropped], np.int64))
+    np.savez_compressed(os.path.join(HERE, "postproc.npz"), **out)
+
+
 TRANSPORT_SEED = 880
 
 
@@ -390,7 +437,7 @@ def main():
         sys.exit("need --reference <dsa110-rt>/src")
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
-            make_image_detector, make_transport, make_rfi, make_slow_corr]
+            make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
