@@ -71,8 +71,9 @@ def workload_desc(name, cfg):
                         f"0-{cfg.coarse_dm.max():.0f}, boxcars 1..{1 << cfg.log_max_width}",
             "block_seconds": cfg.block_seconds, "l2": "inputs larger than L2 (19 GB/block)",
             "chunk_tiles": cfg.chunk_tiles, "fdm_batch": cfg.fdm_batch,
-            "stage2_ring": {"c64": "complex64", "bf16": "bf16 re/im pairs (BF16 storage form)"}[
-                cfg.ring_dtype]}
+            "stage2_ring": {"c64": "complex64", "bf16": "bf16 re/im pairs (BF16 storage form)",
+                            "cint8": "int8 re/im pairs with an amax/127 scale per row "
+                                     "(cint8 wire form)"}[cfg.ring_dtype]}
 
 
 class Clocks:
@@ -148,13 +149,15 @@ def stage_work(pipe):
     nchan = cfg.band.n_chgroup * cfg.band.nchan
     half = N * (N // 2 + 1)
     coarse_per_batch = max(1, nb // cfg.fine_per_coarse) if cfg.fine_per_coarse else nb
-    esz = 4 if cfg.ring_dtype == "bf16" else 8   # bytes per stage-2 ring cell
+    esz = {"c64": 8, "bf16": 4, "cint8": 2}[cfg.ring_dtype]   # bytes per stage-2 ring cell
+    # cint8: stage 1 writes complex64 rows that the quantiser reads back
+    s1_out = 8 + 8 + 2 if cfg.ring_dtype == "cint8" else esz
     return {
         # tensor-core flops: 16 flops per (baseline, channel, native sample) (XX+YY complex MAC)
         "corr": ("tensor", 16.0 * nbase * nchan * C * cfg.t_int,
                  cfg.band.n_chgroup * C * cfg.t_int // 2 * cfg.nant * cfg.band.nchan * 4
                  + T.n_rows_y * C * 8),
-        "stage1": ("hbm", None, T.n_rows_y * C * 8 + T.n_rows_d * C * esz),
+        "stage1": ("hbm", None, T.n_rows_y * C * 8 + T.n_rows_d * C * s1_out),
         # fused combine + FFT: stage-2 ring slices of the batch's coarse DM(s)
         # read once, float32 images written once
         "image": ("hbm", None, int(T.n_filled.sum()) * coarse_per_batch * nt * esz
@@ -322,10 +325,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dsa110-2048dm")
-    ap.add_argument("--ring", default="bf16", choices=["c64", "bf16"],
+    ap.add_argument("--ring", default="bf16", choices=["c64", "bf16", "cint8"],
                     help="stage-2 ring element: the BF16 storage form (bf16 re/im, float32 "
-                         "accumulation; the precision form of the full DSA-110 shape), or "
-                         "complex64")
+                         "accumulation; the precision form of the full DSA-110 shape), "
+                         "complex64, or the cint8 wire form (int8 re/im, a scale per row)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stage-times", action="store_true", help="print per-stage device times")
@@ -483,7 +486,8 @@ def main():
         cpb = max(1, nb // cfg_.fine_per_coarse)
         rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_BF16_RATIO
                                                 if cfg.ring_dtype == "bf16" else 1.0)
-        roof["traffic"] = IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt
+        roof["traffic"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt
+                           if cfg.ring_dtype != "cint8" else None)
         roof["traffic_note"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel on "
                                 "the medium workload (1152 images), scaled to this launch"
                                 + ("; ring reads x 0.499, the bf16/complex64 read ratio of a "

@@ -131,28 +131,40 @@ DSB_DEV void idftR(float2 (&a)[R]) {
   else idft4(a[0], a[1], a[2], a[3]);
 }
 
-// Stage-2 ring elements: complex64, or the BF16 storage form (bf16 re/im
-// pairs in 32 bits, decoded to float32 before any arithmetic).
-// T2 holds two adjacent cells (one 8- or 16-byte load).
-template <bool BF16> struct RingElem {
+// Stage-2 ring elements (FMT): 0 complex64; 1 the BF16 storage form (bf16
+// re/im pairs in 32 bits); 2 the cint8 wire form (int8 re/im pairs in 16
+// bits, value = the row's scale x q).  Decoded to float32 before any
+// arithmetic; T2 holds two adjacent cells (one 4-, 8- or 16-byte load).
+template <int FMT> struct RingElem {
   using T = float2;
   using T2 = float4;
   static DSB_DEV T2 zero2() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-  static DSB_DEV float2 lo(T2 w) { return make_float2(w.x, w.y); }
-  static DSB_DEV float2 hi(T2 w) { return make_float2(w.z, w.w); }
-  static DSB_DEV float2 get(const T* p) { return *p; }
+  static DSB_DEV float2 lo(T2 w, float) { return make_float2(w.x, w.y); }
+  static DSB_DEV float2 hi(T2 w, float) { return make_float2(w.z, w.w); }
+  static DSB_DEV float2 get(const T* p, float) { return *p; }
 };
-template <> struct RingElem<true> {
+template <> struct RingElem<1> {
   using T = uint32_t;
   using T2 = uint2;
   static DSB_DEV T2 zero2() { return make_uint2(0u, 0u); }
-  static DSB_DEV float2 lo(T2 w) { return bf16_pair_to_f2(w.x); }
-  static DSB_DEV float2 hi(T2 w) { return bf16_pair_to_f2(w.y); }
-  static DSB_DEV float2 get(const T* p) { return bf16_pair_to_f2(*p); }
+  static DSB_DEV float2 lo(T2 w, float) { return bf16_pair_to_f2(w.x); }
+  static DSB_DEV float2 hi(T2 w, float) { return bf16_pair_to_f2(w.y); }
+  static DSB_DEV float2 get(const T* p, float) { return bf16_pair_to_f2(*p); }
+};
+template <> struct RingElem<2> {
+  using T = uint16_t;
+  using T2 = uint32_t;
+  static DSB_DEV float s8(uint32_t w, int b) { return (float)(int)(int8_t)(uint8_t)(w >> (8 * b)); }
+  static DSB_DEV T2 zero2() { return 0u; }
+  static DSB_DEV float2 lo(T2 w, float sc) { return make_float2(sc * s8(w, 0), sc * s8(w, 1)); }
+  static DSB_DEV float2 hi(T2 w, float sc) { return make_float2(sc * s8(w, 2), sc * s8(w, 3)); }
+  static DSB_DEV float2 get(const T* p, float sc) { return lo(*p, sc); }
 };
 
 struct ImgArgs {
-  const void* D;            // ring: complex64, or bf16 pairs when the kernel's BF16 is set
+  const void* D;            // ring in the element form FMT of the kernel
+  const float* scales;      // FMT 2: scale of each (chgroup, coarse DM, slot) row,
+  const long long* sc_base; //   at scales[sc_base[g*n_coarse + c] + slot]
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
@@ -209,14 +221,14 @@ struct ImgGeom {
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
   static_assert(NC <= 128 && LC <= 64, "entry metadata holds 7 bits of column, 6 of n'");
   // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases |
-  // ends of the chgroups' cells | TMEM address
+  // ends of the chgroups' cells | slice scales | TMEM address
   static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
-                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + 16;
+                                 (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + IMG_MAX_G * 4 + 16;
 };
 
-template <int N, bool BF16>
+template <int N, int FMT>
 __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
-  using Elem = typename RingElem<BF16>::T;
+  using Elem = typename RingElem<FMT>::T;
   using Gm = ImgGeom<N>;
   constexpr int FOLD = Gm::FOLD, LC = Gm::LC, C1 = Gm::C1, NC = Gm::NC, P = Gm::P,
                 RR = Gm::RR, THREADS = Gm::THREADS;
@@ -230,7 +242,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   const Elem** s_slice = reinterpret_cast<const Elem**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
   int* s_end = s_cbase + IMG_MAX_G + 1;
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_end + IMG_MAX_G);
+  float* s_scale = reinterpret_cast<float*>(s_end + IMG_MAX_G);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_scale + IMG_MAX_G);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -288,6 +301,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
       if (slot < 0) slot += dep;
       s_slice[g] = static_cast<const Elem*>(A.D) + A.seg_base[gc] + slot * A.d_pitch[g];
+      s_scale[g] = FMT == 2 ? A.scales[A.sc_base[gc] + slot] : 1.f;
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
@@ -311,22 +325,25 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       // chgroup, its first entry and its ring row stay in registers and
       // change only at a run boundary (warp-uniform), and the shared-memory
       // pipe is left to the atomics.  8 cells in flight per thread.
-      using Elem2 = typename RingElem<BF16>::T2;
+      using Elem2 = typename RingElem<FMT>::T2;
       constexpr int U = 4, NW = THREADS / 32;
       const int n_dch = n_tot >> 6;
       const uint2* cm2 = reinterpret_cast<const uint2*>(A.c_meta);
       int g = -1, g_lo = 0, g_hi = 0, g_end = 0;
+      float g_sc = 1.f;
       const Elem* src = static_cast<const Elem*>(A.D);
       for (int c0 = warp; c0 < n_dch; c0 += NW * U) {
         // raw ring words: decoded only in the add loop below, so that no
         // instruction waits on a load before the batch's other loads issue
         uint2 m[U];
         Elem2 v[U];
+        float sc[U];
 #pragma unroll
         for (int q = 0; q < U; ++q) {
           const int ch = c0 + NW * q;
           m[q] = make_uint2(0xffffffffu, 0xffffffffu);
-          v[q] = RingElem<BF16>::zero2();
+          v[q] = RingElem<FMT>::zero2();
+          sc[q] = 1.f;
           if (ch < n_dch) {
             while (64 * ch >= g_hi) {
               ++g;
@@ -334,6 +351,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
               g_hi = s_cbase[g + 1];
               g_end = s_end[g];
               src = s_slice[g];
+              g_sc = s_scale[g];
             }
             // cells e, e + 1 (e even): both inside the row's pitch whenever
             // e is a pattern cell (the pitch is n_filled rounded up to 4)
@@ -341,19 +359,21 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
             if (e < g_end) {
               m[q] = __ldg(cm2 + (e >> 1));
               v[q] = *reinterpret_cast<const Elem2*>(src + (e - g_lo));
+              sc[q] = g_sc;
             }
           }
         }
 #pragma unroll
         for (int q = 0; q < U; ++q) {
-          if (m[q].x != 0xffffffffu) add(m[q].x, RingElem<BF16>::lo(v[q]));
-          if (m[q].y != 0xffffffffu) add(m[q].y, RingElem<BF16>::hi(v[q]));
+          if (m[q].x != 0xffffffffu) add(m[q].x, RingElem<FMT>::lo(v[q], sc[q]));
+          if (m[q].y != 0xffffffffu) add(m[q].y, RingElem<FMT>::hi(v[q], sc[q]));
         }
       }
       for (int i = tid; i < A.n_c2; i += THREADS) {
         const int2 cm = __ldg(A.c2 + i);
         add((unsigned)cm.y,
-            RingElem<BF16>::get(s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)] + (cm.x & 0xffff)));
+            RingElem<FMT>::get(s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)] + (cm.x & 0xffff),
+                               s_scale[(cm.x >> 16) & (IMG_MAX_G - 1)]));
       }
     }
     __syncthreads();
@@ -533,21 +553,21 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   }
 }
 
-// Resident CTAs for image_kernel<N, BF16> on this device (the persistent grid).
+// Resident CTAs for image_kernel<N, FMT> on this device (the persistent grid).
 // The occupancy API answers 1 CTA per SM for any kernel that allocates
 // tensor memory (measured on B200 with CUDA 12.9), while the SM runs as many
 // as its shared memory, registers and 512 TMEM columns hold: three here.  So
 // the count is taken from those limits directly.
-template <int N, bool BF16>
+template <int N, int FMT>
 int image_grid(int* blocks) {
   using Gm = ImgGeom<N>;
   static int cached = 0;
   if (!cached) {
-    if (cudaFuncSetAttribute(image_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(image_kernel<N, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Gm::SMEM) != cudaSuccess)
       return DSB_E_CUDA;
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, image_kernel<N, BF16>) != cudaSuccess) return DSB_E_CUDA;
+    if (cudaFuncGetAttributes(&fa, image_kernel<N, FMT>) != cudaSuccess) return DSB_E_CUDA;
     int dev = 0, sms = 148, smem_sm = 0, smem_rsv = 0, regs_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -564,16 +584,16 @@ int image_grid(int* blocks) {
   return DSB_OK;
 }
 
-template <int N, bool BF16>
+template <int N, int FMT>
 int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   using Gm = ImgGeom<N>;
   if (A.s_stride > Gm::BUF) return DSB_E_CAPACITY;
   int blocks = 0;
-  const int rc = image_grid<N, BF16>(&blocks);
+  const int rc = image_grid<N, FMT>(&blocks);
   if (rc != DSB_OK) return rc;
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   blocks = std::max(1, std::min(blocks, A.n_f * A.n_t));
-  image_kernel<N, BF16><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
+  image_kernel<N, FMT><<<blocks, Gm::THREADS, Gm::SMEM, stream>>>(A);
   return launch_status();
 }
 
@@ -593,8 +613,8 @@ int dsb_image_threads(void) { return IMG_THREADS; }
 
 int dsb_image_max_entries(void) { return IMG_MAXE; }
 
-int dsb_image_fft(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                  int n_coarse,
+int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
+                  const float* scales, const long long* sc_base, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   const int* dcols, const unsigned long long* dmask, int n_dense,
@@ -606,23 +626,28 @@ int dsb_image_fft(const void* D, int d_bf16, const long long* seg_base, const in
       (n_c2 > 0 && !c2) || n_c2 < 0 || !thr_b || !gmeta || !srot || n_s <= 0 ||
       n_s > 65536 || n_dense < 0 || n_const < 0 || (n_dense > 0 && (!dcols || !dmask)) ||
       (n_const > 0 && !kcols) || !d_pitch || !n_filled || !sfine || !f2c || !twiddles ||
-      !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G)
+      !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G ||
+      d_format < 0 || d_format > 2 || (d_format == 2 && (!scales || !sc_base)))
     return DSB_E_ARG;
+  // two adjacent cells per load: 4-byte aligned cint8 pairs
+  if (d_format == 2 && (reinterpret_cast<uintptr_t>(D) & 3)) return DSB_E_ARG;
   if ((reinterpret_cast<uintptr_t>(gmeta) & 15) || (reinterpret_cast<uintptr_t>(out) & 15))
     return DSB_E_ARG;
   if (n_dense + n_const != N / 2) return DSB_E_ARG;  // every packed column, once
   const int stride = (n_s + 1) & ~1;
-  ImgArgs A{D, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
+  ImgArgs A{D, scales, sc_base, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
             n_c2, thr_b, (const uint4*)gmeta, srot, dcols, dmask, n_dense, kcols, n_const,
             n_s, stride, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
             t0, n_t, fftshift, (float*)out, status};
   switch (N) {
     case 64:
-      return d_bf16 ? launch_image<64, true>(A, max_blocks, stream)
-                    : launch_image<64, false>(A, max_blocks, stream);
+      return d_format == 2   ? launch_image<64, 2>(A, max_blocks, stream)
+             : d_format == 1 ? launch_image<64, 1>(A, max_blocks, stream)
+                             : launch_image<64, 0>(A, max_blocks, stream);
     case 256:
-      return d_bf16 ? launch_image<256, true>(A, max_blocks, stream)
-                    : launch_image<256, false>(A, max_blocks, stream);
+      return d_format == 2   ? launch_image<256, 2>(A, max_blocks, stream)
+             : d_format == 1 ? launch_image<256, 1>(A, max_blocks, stream)
+                             : launch_image<256, 0>(A, max_blocks, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

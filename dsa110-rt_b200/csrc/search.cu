@@ -35,7 +35,10 @@ __global__ void uv_cells_kernel(const double* __restrict__ du, const double* __r
 // that chgroup's pattern, and whether it is the conjugate mirror.
 // ===========================================================================
 struct CombArgs {
-  const void* D;         // ring: complex64, or bf16 re/im pairs in 32 bits (BF16)
+  const void* D;         // ring: complex64 (FMT 0), bf16 re/im pairs in 32 bits (1),
+                         // or int8 re/im pairs in 16 bits (2) times the row's scale
+  const float* scales;   // FMT 2: scales[sc_base[gc] + slot] of each ring row
+  const long long* sc_base;
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
@@ -57,7 +60,7 @@ struct CombArgs {
 // output time is written coalesced across the half cells of a warp.
 constexpr int CB_T = 8;
 
-template <bool BF16>
+template <int FMT>
 __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
   const int nh = A.N / 2 + 1;
   const int n_hc = A.N * nh;
@@ -91,7 +94,11 @@ __global__ void __launch_bounds__(128) combine_rows_kernel(const CombArgs A) {
         long long slot = slot0 + i;
         if (slot >= dep) slot -= dep;
         float2 x;
-        if constexpr (BF16)
+        if constexpr (FMT == 2) {
+          const char2 q = static_cast<const char2*>(A.D)[e0 + slot * pitch];
+          const float sc = A.scales[A.sc_base[gc] + slot];
+          x = make_float2(sc * (float)q.x, sc * (float)q.y);
+        } else if constexpr (FMT == 1)
           x = bf16_pair_to_f2(static_cast<const uint32_t*>(A.D)[e0 + slot * pitch]);
         else
           x = static_cast<const float2*>(A.D)[e0 + slot * pitch];
@@ -551,23 +558,26 @@ int dsb_uv_cells(const double* du, const double* dv, int n_bl, const double* nu_
   return launch_status();
 }
 
-int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                     int n_coarse,
+int dsb_combine_rows(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
+                     const float* scales, const long long* sc_base, int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream) {
   if (!D || !seg_base || !seg_depth || n_coarse <= 0 || !hc_off || !e_g || !e_cell ||
-      !d_pitch || !sfine || !f2c || !out)
+      !d_pitch || !sfine || !f2c || !out || d_format < 0 || d_format > 2 ||
+      (d_format == 2 && (!scales || !sc_base)))
     return DSB_E_ARG;
   if (N <= 0 || (N & 1) || n_f <= 0 || n_t <= 0 || G <= 0) return DSB_E_ARG;
-  CombArgs A{D, seg_base, seg_depth, n_coarse, hc_off, e_g, e_cell, d_pitch,
+  CombArgs A{D, scales, sc_base, seg_base, seg_depth, n_coarse, hc_off, e_g, e_cell, d_pitch,
              sfine, f2c, f0, n_f, G, N, t0, n_t, fftshift, (float2*)out};
   const int n_hc = N * (N / 2 + 1);
   dim3 grid((n_hc + 127) / 128, n_f);
-  if (d_bf16)
-    combine_rows_kernel<true><<<grid, 128, 0, stream>>>(A);
+  if (d_format == 2)
+    combine_rows_kernel<2><<<grid, 128, 0, stream>>>(A);
+  else if (d_format == 1)
+    combine_rows_kernel<1><<<grid, 128, 0, stream>>>(A);
   else
-    combine_rows_kernel<false><<<grid, 128, 0, stream>>>(A);
+    combine_rows_kernel<0><<<grid, 128, 0, stream>>>(A);
   return launch_status();
 }
 

@@ -44,14 +44,16 @@ _SIGNATURES = {
     "dsb_image_fold": [_c_int],
     "dsb_image_threads": [],
     "dsb_image_max_entries": [],
-    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp,
+    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp,
                       _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
                       _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],
-    "dsb_combine_rows": [_vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
+    "dsb_combine_rows": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,
                          _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp],
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                           _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_encode_rows": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp, _vp],
+    "dsb_ring_encode_cint8": [_vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _vp, _c_ll, _vp, _vp,
+                              _vp, _vp, _vp, _vp, _vp],
     "dsb_rfi_zero_fill": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_int, _vp],
     "dsb_mask_to_cube": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _c_int, _c_int,
                          _vp],

@@ -77,16 +77,19 @@ class PipelineConfig:
     l1_times: int = 16
     l1_pixels: int = 256
     cand_capacity: int = 1 << 22
-    # stage-2 ring element: "c64" (complex64) or "bf16" (the BF16 storage form:
+    # stage-2 ring element: "c64" (complex64), "bf16" (the BF16 storage form:
     # each part rounded to nearest-even bf16, accumulated in float32 on read)
+    # or "cint8" (the reference's cint8 wire form: every (chgroup, coarse DM,
+    # time) row quantised with its own amax/127 scale, dequantised on read)
     ring_dtype: str = "c64"
     # coarse DMs per stage-1 block: None picks the largest of 32, 16, 8 whose
     # shared time window fits; a value forces that group
     stage1_dm_group: Optional[int] = None
 
     def __post_init__(self):
-        if self.ring_dtype not in ("c64", "bf16"):
-            raise ValueError(f"ring_dtype must be 'c64' or 'bf16', got {self.ring_dtype!r}")
+        if self.ring_dtype not in RING_FORMATS:
+            raise ValueError(f"ring_dtype must be one of {sorted(RING_FORMATS)}, "
+                             f"got {self.ring_dtype!r}")
         self.coarse_dm = np.asarray(self.coarse_dm, np.float64)
         if self.fine_dm is None:
             # fine DMs spread evenly around each coarse DM (v2 plan: coarse at the
@@ -120,6 +123,10 @@ class PipelineConfig:
     @property
     def block_seconds(self) -> float:
         return self.npkt_block * 2 * NATIVE_SAMPLE_US * 1e-6
+
+
+# element form of the stage-2 ring -> the kernels' format code
+RING_FORMATS = {"c64": 0, "bf16": 1, "cint8": 2}
 
 
 @dataclass
@@ -445,11 +452,28 @@ class SearchPipeline:
         self.d_segbase, self.d_segdepth = d(self.seg_base[:-1]), d(self.seg_depth)
         # time-major rings: Y [time & (TY-1)][row]; D segmented as above
         self.Y = torch.zeros((self.TY, T.n_rows_y), dtype=torch.complex64, device=self.dev)
-        # D: complex64 elements, or one int32 word of bf16 (re low, im high) per cell
-        self.ring_bf16 = cfg.ring_dtype == "bf16"
+        # D: complex64 elements, one int32 word of bf16 (re low, im high) or
+        # one int16 word of int8 (re low, im high) per cell
+        self.ring_fmt = RING_FORMATS[cfg.ring_dtype]
+        self.ring_bf16 = self.ring_fmt == 1
         self.D = torch.zeros(int(self.seg_base[-1]),
-                             dtype=torch.int32 if self.ring_bf16 else torch.complex64,
+                             dtype=(torch.complex64, torch.int32, torch.int16)[self.ring_fmt],
                              device=self.dev)
+        # cint8: the scale of every ring row (one per segment slot), and the
+        # chunk's stage-1 rows in complex64 before they are quantised (one
+        # segment of C slots per (chgroup, coarse DM), written without delay)
+        self.sc_base = np.concatenate([[0], np.cumsum(depth.reshape(-1))]).astype(np.int64)
+        self.d_scbase = d(self.sc_base[:-1])
+        if self.ring_fmt == 2:
+            self.scales = torch.ones(int(self.sc_base[-1]), dtype=torch.float32, device=self.dev)
+            x_elems = np.broadcast_to(C * T.pitch.astype(np.int64)[:, None], depth.shape)
+            x_base = np.concatenate([[0], np.cumsum(x_elems.reshape(-1))]).astype(np.int64)
+            self.d_xbase = d(x_base[:-1])
+            self.d_xdepth = d(np.full(depth.size, C, np.int32))
+            self.d_zero2 = d(np.zeros(depth.size, np.int32))
+            self.X = torch.empty(int(x_base[-1]), dtype=torch.complex64, device=self.dev)
+        else:
+            self.scales = None
         self.sky = (torch.zeros((T.n_rows_d, cfg.sky_window), dtype=torch.complex128,
                                 device=self.dev) if cfg.use_sky else None)
         self.sky_count = self.sky_head = self.sky_seen = 0
@@ -533,18 +557,32 @@ class SearchPipeline:
         cfg, T = self.cfg, self.tab
         C = cfg.chunk_tiles
         sub = int(cfg.use_sky and self.sky_count > 0 and self.sky_seen >= cfg.sky_warmup)
+        q8 = self.ring_fmt == 2
+        # cint8: stage 1 writes the chunk's rows to X (slot t of C, no delay);
+        # the quantiser then moves them into the ring at t + shift2
         with self._mark("stage1"):
             _lib.check(_lib.lib().dsb_stage1_rows(
                 _lib.ptr(self.Y), T.n_rows_y, self.TY - 1, int(T.blk_g.size),
                 _lib.ptr(self.d_blk_g), _lib.ptr(self.d_blk_c0), _lib.ptr(self.d_ybase),
-                _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1), _lib.ptr(self.d_shift2),
-                _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled), _lib.ptr(self.D),
-                int(self.ring_bf16), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth), j * C, C, cfg.coarse_dm.size,
+                _lib.ptr(self.d_pitch), _lib.ptr(self.d_shift1),
+                _lib.ptr(self.d_zero2 if q8 else self.d_shift2),
+                _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled),
+                _lib.ptr(self.X if q8 else self.D), 0 if q8 else self.ring_fmt,
+                _lib.ptr(self.d_xbase if q8 else self.d_segbase),
+                _lib.ptr(self.d_xdepth if q8 else self.d_segdepth), j * C, C, cfg.coarse_dm.size,
                 cfg.ceff, T.dm_group, T.max_spread, _lib.ptr(self.sky), cfg.sky_window,
                 self.sky_head,
                 self.sky_count, sub, _lib.ptr(self.status), _lib.stream_of(self.dev)),
                 "dsb_stage1_rows")
-        self.launches += 1
+            self.launches += 1
+            if q8:
+                _lib.check(_lib.lib().dsb_ring_encode_cint8(
+                    _lib.ptr(self.X), _lib.ptr(self.d_xbase), C, _lib.ptr(self.d_pitch),
+                    _lib.ptr(self.d_nfilled), cfg.band.n_chgroup, cfg.coarse_dm.size,
+                    _lib.ptr(self.d_shift2), j * C, _lib.ptr(self.D), _lib.ptr(self.d_segbase),
+                    _lib.ptr(self.d_segdepth), _lib.ptr(self.scales), _lib.ptr(self.d_scbase),
+                    _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_ring_encode_cint8")
+                self.launches += 1
         if cfg.use_sky:
             self.sky_count = min(self.sky_count + 1, cfg.sky_window)
             self.sky_head = (self.sky_head + 1) % cfg.sky_window
@@ -560,8 +598,9 @@ class SearchPipeline:
         if out.shape != (n_f, n_t, N, N) or out.dtype != torch.float32 or not out.is_contiguous():
             raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
         _lib.check(_lib.lib().dsb_image_fft(
-            _lib.ptr(self.D), int(self.ring_bf16), _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
-            cfg.coarse_dm.size, _lib.ptr(self.d_img_cmeta),
+            _lib.ptr(self.D), self.ring_fmt, _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
+            _lib.ptr(self.scales), _lib.ptr(self.d_scbase), cfg.coarse_dm.size,
+            _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_thrb), _lib.ptr(self.d_img_gmeta), _lib.ptr(self.d_img_srot),
             it.n_s, _lib.ptr(self.d_img_dcols), _lib.ptr(self.d_img_dmask), int(it.dcols.size),
@@ -713,10 +752,15 @@ class SearchPipeline:
         gd = g * self.tab.shift2.shape[1] + d
         base, dep = int(self.seg_base[gd]), int(self.seg_depth[gd])
         seg = self.D[base:base + dep * pitch].view(dep, pitch)
-        rows = torch.as_tensor(np.asarray(times, np.int64) % dep, device=self.dev)
+        slots = np.asarray(times, np.int64) % dep
+        rows = torch.as_tensor(slots, device=self.dev)
         vals = seg[rows, :nf].cpu().numpy()
-        if not self.ring_bf16:
+        if self.ring_fmt == 0:
             return vals
+        if self.ring_fmt == 2:
+            q = vals.view(np.int8).reshape(len(slots), nf, 2).astype(np.float32)
+            sc = self.scales[int(self.sc_base[gd]) + rows].cpu().numpy()[:, None]
+            return (sc * q[..., 0] + 1j * (sc * q[..., 1])).astype(np.complex64)
         w = vals.view(np.uint32)
         return ((w << 16).view(np.float32) + 1j * (w & 0xFFFF0000).view(np.float32)
                 ).astype(np.complex64)

@@ -166,10 +166,14 @@ long long dsb_stage1_smem_bytes(int ceff, int dm_group, int max_spread);
  * fused_dequant_combine_per_fdm_half (src/dsart/image/fused_combine_cuda.py:560-620):
  * reads the segmented stage-2 ring directly (value of (g, coarse DM c,
  * cell) at time t: D[seg_base[g*n_coarse + c] + (t mod seg_depth[...])*d_pitch[g]
- * + cell], as dsb_stage1_rows writes it, in the element form d_bf16 names),
- * writes (n_f, n_t, N, N/2+1) complex64. */
-int dsb_combine_rows(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                     int n_coarse,
+ * + cell]) and writes (n_f, n_t, N, N/2+1) complex64.  d_format names the
+ * ring's element: 0 complex64 and 1 the BF16 storage form, as dsb_stage1_rows
+ * writes them; 2 the cint8 wire form as dsb_ring_encode_cint8 writes it (int8
+ * re in the low byte, im in the high byte of 16 bits; value float32(scale *
+ * q) with the row's scale at scales[sc_base[g*n_coarse + c] + slot], slot the
+ * time's ring slot).  scales and sc_base may be null for formats 0 and 1. */
+int dsb_combine_rows(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
+                     const float* scales, const long long* sc_base, int n_coarse,
                      const int* hc_off, const int* e_g, const int* e_cell, const int* d_pitch,
                      const int* sfine, const int* f2c, int f0, int n_f, int G, int N,
                      long long t0, int n_t, int fftshift, void* out, cudaStream_t stream);
@@ -207,6 +211,22 @@ int dsb_rfi_zero_fill(void* raw, int n_pages, int npkt, int nant, int nchan,
  * behaviour (its float-to-int8 conversion of them is platform-defined). */
 int dsb_encode_rows(const void* rows, long long row_stride, int n_rows, int n_filled,
                     int bits_per_cell, void* payload, float* scales, cudaStream_t stream);
+/* The same cint8 encoder applied to one chunk of stage-1 output, written
+ * straight into the stage-2 ring, so that the ring holds what the search
+ * side of the reference receives (TransportTx._encode_rows, tx.py:825-873,
+ * per (chgroup, coarse DM, time) row, then the stage-2 FIFO).
+ * X: complex64 (16-byte aligned); row (g, d, t), t in [0, n_t), at
+ * X + x_base[g*n_dm + d] + t * pitch[g] with n_filled[g] pattern cells.
+ * D: int8 pairs (4-byte aligned), row written at slot (t0 + t +
+ * shift2[gd]) mod seg_depth[gd] of segment seg_base[gd] (cells past
+ * n_filled set to 0); the row's scale at scales[sc_base[gd] + slot].
+ * pitch, x_base and seg_base even (two cells per access); a row that breaks
+ * this sets DSB_E_ARG in *status and is skipped. */
+int dsb_ring_encode_cint8(const void* X, const long long* x_base, int n_t, const int* pitch,
+                          const int* n_filled, int G, int n_dm, const int* shift2, long long t0,
+                          void* D, const long long* seg_base, const int* seg_depth,
+                          float* scales, const long long* sc_base, int* status,
+                          cudaStream_t stream);
 int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
                       const float* off_re, const float* off_im, int per_t, void* out,
                       int out_f16, int half,
@@ -218,7 +238,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * GpuImager.process_cube (src/dsart/image/fused_combine_cuda.py:1359,
  * src/dsart/image/imager_gpu.py:575-605): for each (fine DM f0+fl, time t0+t)
  * the Hermitian half spectrum is combined from the segmented stage-2 ring
- * (as dsb_combine_rows reads it) and
+ * (as dsb_combine_rows reads it, in any of its three element forms; cint8
+ * needs D 4-byte aligned) and
  * transformed on chip; out (n_f, n_t, N, N) float32 = irfft2(G_h) with
  * 1/N^2 normalisation (fftshifted when fftshift != 0).
  * Tables (built once per pattern set):
@@ -251,8 +272,8 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
 int dsb_image_fold(int n_grid);
 int dsb_image_threads(void);
 int dsb_image_max_entries(void);
-int dsb_image_fft(const void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                  int n_coarse,
+int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
+                  const float* scales, const long long* sc_base, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   const int* dcols, const unsigned long long* dmask, int n_dense,

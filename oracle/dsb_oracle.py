@@ -693,6 +693,15 @@ def encode_rows(row: np.ndarray, bits_per_cell: int):
     raise AssertionError(f"unhandled bits_per_cell={bits_per_cell}")
 
 
+def decode_cint8(q: np.ndarray, scales: np.ndarray) -> np.ndarray:
+    """Receiver side of the cint8 form: ``(n_fv, n_filled, 2)`` int8 payload
+    and ``(n_fv,)`` scales -> complex64 rows, each part float32(scale * q)
+    (the per-tile dequantisation of image/fused_combine_cuda.py:431-505)."""
+    sc = np.asarray(scales, np.float32)[:, None]
+    qf = np.asarray(q).astype(np.float32)
+    return (sc * qf[..., 0] + 1j * (sc * qf[..., 1])).astype(np.complex64)
+
+
 def compact_to_dense(values: np.ndarray, ix_row, ix_col, n_grid: int) -> np.ndarray:
     """Scatter ``(..., n_filled)`` cell values into ``(..., N, N)``."""
     out = np.zeros(values.shape[:-1] + (n_grid, n_grid), values.dtype)
@@ -915,7 +924,10 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
     ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates.
     ``ring_dtype="bf16"`` stores the stage-2 streams in the BF16 form (each
     part rounded to bfloat16 after the sky subtraction), as the pipeline's
-    precision form does."""
+    precision form does; ``"cint8"`` sends every time row of every (chgroup,
+    coarse DM) stream through the cint8 wire encoder (``encode_rows``, one
+    tile per row) and stores what the receiver dequantises, float32(scale *
+    q) per part."""
     keep = {} if keep is None else keep
     G = band.n_chgroup
     tb = pipeline_tables(band, antpos_e, antpos_n, nant=nant, csf=csf, n_grid=n_grid,
@@ -958,6 +970,8 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
                     x = sky.apply(x, dm_slot=g * n_coarse + d)
                 if ring_dtype == "bf16":
                     x = round_bf16_complex(x)
+                elif ring_dtype == "cint8":
+                    x = decode_cint8(*encode_rows(x, 16))
                 D1[g][d][j * chunk:(j + 1) * chunk] = x
     keep["D1"] = D1
     # search cubes

@@ -50,12 +50,13 @@ def _setup(n_blocks=8, amp=1.0):
 
 
 @pytest.mark.parametrize("ring,dm_group", [("c64", None), ("bf16", None), ("bf16", 8),
-                                           ("c64", 16)])
+                                           ("c64", 16), ("cint8", None)])
 def test_pipeline_matches_oracle(dev, ring, dm_group):
-    """Both ring forms against the oracle pipeline with the same ring form:
-    the BF16 ring is the complex64 one rounded to bfloat16 part by part,
-    bit-exact; candidates as for the complex64 ring.  Stage 1 runs with its
-    chosen DM group and with the smaller groups forced."""
+    """Every ring form against the oracle pipeline with the same ring form:
+    the BF16 ring is the complex64 one rounded to bfloat16 part by part, the
+    cint8 ring the wire encoder's payload dequantised with each row's scale,
+    both bit-exact; candidates as for the complex64 ring.  Stage 1 runs with
+    its chosen DM group and with the smaller groups forced."""
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup()
     cfg = PipelineConfig(band=band, nant=kw["nant"], npkt_block=kw["npkt_block"],
@@ -130,12 +131,12 @@ def test_pipeline_rejects_wrong_raw_size(dev):
         pipe.process_block(torch.zeros(100, dtype=torch.uint8, device=dev))
 
 
-@pytest.mark.parametrize("ring", ["c64", "bf16"])
+@pytest.mark.parametrize("ring", ["c64", "bf16", "cint8"])
 @pytest.mark.parametrize("N", [64, 256])
 def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     """Fused combine + 2-D c2r FFT == dsb_combine_rows + torch.fft.irfft2 on
     the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale,
-    for both ring element forms."""
+    for every ring element form (cint8 with a random scale per ring row)."""
     from dsb200 import _lib
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
@@ -152,6 +153,10 @@ def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
         parts = torch.randn((2,) + tuple(pipe.D.shape), device=dev, generator=g)
         bits = parts.to(torch.bfloat16).view(torch.int16).to(torch.int32) & 0xFFFF
         pipe.D.copy_(bits[0] | (bits[1] << 16))
+    elif ring == "cint8":
+        pipe.D.copy_(torch.randint(-32768, 32768, pipe.D.shape, dtype=torch.int32, device=dev,
+                                   generator=g).to(torch.int16))
+        pipe.scales.copy_(torch.rand(pipe.scales.shape, device=dev, generator=g) + 0.01)
     else:
         pipe.D.copy_(torch.randn(pipe.D.shape, dtype=torch.complex64, device=dev, generator=g))
     nf, nt, t0 = 5, 20, 37
@@ -159,8 +164,9 @@ def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     L = _lib.lib()
     pipe.image(1, nf, t0, nt, out, max_blocks=3)
     gh = torch.empty((nf, nt, N, N // 2 + 1), dtype=torch.complex64, device=dev)
-    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), int(pipe.ring_bf16),
+    _lib.check(L.dsb_combine_rows(_lib.ptr(pipe.D), pipe.ring_fmt,
                                   _lib.ptr(pipe.d_segbase), _lib.ptr(pipe.d_segdepth),
+                                  _lib.ptr(pipe.scales), _lib.ptr(pipe.d_scbase),
                                   len(kw["coarse_dm"]),
                                   _lib.ptr(pipe.d_hc_off), _lib.ptr(pipe.d_eg),
                                   _lib.ptr(pipe.d_ecell), _lib.ptr(pipe.d_pitch),

@@ -95,3 +95,73 @@ def test_per_tile_dequant_combine_matches_oracle(half):
     want = O.combine_dequant(q, shifts, scales[:, 0], off_re[:, 0], off_im[:, 0], t_det, t_lo,
                              half=half)
     np.testing.assert_array_equal(out.cpu().numpy(), want)
+
+
+def test_oracle_decode_cint8_within_half_step():
+    """Receiver side: float32(scale * q) is within half a quantisation step
+    of every part (no part clips: |x| <= amax = 127 scale)."""
+    rows = MG.transport_rows()
+    q, s = O.encode_rows(rows, 16)
+    back = O.decode_cint8(q, s)
+    err = np.maximum(np.abs(back.real - rows.real), np.abs(back.imag - rows.imag))
+    assert np.all(err <= 0.5 * s[:, None] * (1 + 1e-6))
+
+
+@pytest.mark.gpu
+def test_ring_encode_cint8_matches_oracle():
+    """dsb_ring_encode_cint8 == the oracle encoder per (chgroup, coarse DM,
+    time) row, bit for bit: payload at slot (t0 + t + shift2) mod depth, the
+    pitch padding zeroed (and ignored in X), the row's scale beside it;
+    all-zero and tie rows included."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dsb200 import _lib
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(21)
+    G, n_dm, n_t, t0 = 3, 2, 5, 17
+    pitch = np.array([8, 12, 4], np.int32)
+    nfill = np.array([7, 12, 3], np.int32)
+    shift2 = rng.integers(0, 10, G * n_dm).astype(np.int32)
+    depth = (shift2 + n_t + 3).astype(np.int32)
+    gd_pitch = np.repeat(pitch, n_dm).astype(np.int64)
+    x_base = np.concatenate([[0], np.cumsum(n_t * gd_pitch)]).astype(np.int64)
+    seg_base = np.concatenate([[0], np.cumsum(depth * gd_pitch)]).astype(np.int64)
+    sc_base = np.concatenate([[0], np.cumsum(depth)]).astype(np.int64)
+    X = np.full(int(x_base[-1]), 1e6 + 1e6j, np.complex64)   # padding: must be ignored
+    tie = MG.transport_rows()[7]
+    rows = {}
+    for gd in range(G * n_dm):
+        g = gd // n_dm
+        nf, pt = int(nfill[g]), int(pitch[g])
+        for t in range(n_t):
+            r = (rng.standard_normal(nf) * 30 + 1j * rng.standard_normal(nf) * 3).astype(
+                np.complex64)
+            if (gd, t) == (1, 2):
+                r[:] = 0
+            if (gd, t) == (2, 4):
+                r = tie[:nf].copy()
+            rows[gd, t] = r
+            X[x_base[gd] + t * pt: x_base[gd] + t * pt + nf] = r
+    D = torch.full((int(seg_base[-1]),), 0x5555, dtype=torch.int16, device=dev)
+    scales = torch.full((int(sc_base[-1]),), -1.0, dtype=torch.float32, device=dev)
+    st = _lib.status_word(dev)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    keep = [d(X), d(x_base[:-1]), d(pitch), d(nfill), d(shift2), d(seg_base[:-1]), d(depth),
+            d(sc_base[:-1])]
+    _lib.check(_lib.lib().dsb_ring_encode_cint8(
+        _lib.ptr(keep[0]), _lib.ptr(keep[1]), n_t, _lib.ptr(keep[2]), _lib.ptr(keep[3]), G, n_dm,
+        _lib.ptr(keep[4]), t0, _lib.ptr(D), _lib.ptr(keep[5]), _lib.ptr(keep[6]),
+        _lib.ptr(scales), _lib.ptr(keep[7]), _lib.ptr(st), _lib.stream_of(dev)), "ring encode")
+    torch.cuda.synchronize()
+    _lib.check_status(st, "ring encode")
+    Dh = D.cpu().numpy().view(np.int8).reshape(-1, 2)
+    sh = scales.cpu().numpy()
+    for (gd, t), r in rows.items():
+        g = gd // n_dm
+        nf, pt = int(nfill[g]), int(pitch[g])
+        wq, ws = O.encode_rows(r[None], 16)
+        slot = (t0 + t + int(shift2[gd])) % int(depth[gd])
+        e0 = int(seg_base[gd]) + slot * pt
+        assert np.array_equal(Dh[e0:e0 + nf], wq[0])
+        assert np.all(Dh[e0 + nf:e0 + pt] == 0)
+        assert sh[int(sc_base[gd]) + slot].view(np.uint32) == ws[0].view(np.uint32)
