@@ -428,6 +428,91 @@ def make_transport():
                         s16=np.asarray(s16), q32=np.asarray(q32), s32=np.asarray(s32))
 
 
+CLUSTER_SEED = 7171
+
+
+def cluster_fields(seed: int = CLUSTER_SEED, n: int = 400):
+    """Seeded per-cube candidates: clumps around a few bursts in (l, m,
+    fine DM, time, width) plus scattered noise detections.  Rows of (l, m,
+    dm_fine, event_specnum, width, snr, search_node_id, gpu_half); the
+    geometry is ``cluster_geometry()``."""
+    rng = np.random.default_rng(seed)
+    grid = cluster_geometry()["fine_dm_pc_cc"]
+    n_b = 6
+    bl, bm = rng.integers(20, 236, n_b), rng.integers(20, 236, n_b)
+    bd, bt = rng.integers(3, 60, n_b), rng.integers(10, 240, n_b)
+    which = rng.integers(-1, n_b, n)               # -1: scattered noise
+    l = np.where(which >= 0, bl[which] + rng.integers(-3, 4, n), rng.integers(0, 256, n))
+    m = np.where(which >= 0, bm[which] + rng.integers(-3, 4, n), rng.integers(0, 256, n))
+    d = np.where(which >= 0, np.clip(bd[which] + rng.integers(-3, 4, n), 0, 63),
+                 rng.integers(0, 64, n))
+    t = np.where(which >= 0, bt[which] + rng.integers(-4, 5, n), rng.integers(0, 256, n))
+    # dm_fine near (not on) the grid value, some beyond the grid's ends
+    dm = grid[d] + rng.uniform(-4.0, 4.0, n)
+    dm[:3] = [grid[0] - 30.0, grid[-1] + 30.0, 0.5 * (grid[10] + grid[11])]
+    width = 1 << rng.integers(0, 6, n)
+    snr = np.round(rng.uniform(6.0, 40.0, n), 3)
+    # sub-pixel positions, exact .5 included (round half to even)
+    lf = l + np.where(rng.random(n) < 0.1, 0.5, np.round(rng.uniform(-0.4, 0.4, n), 2))
+    mf = m + np.round(rng.uniform(-0.4, 0.4, n), 2)
+    return (lf.astype(np.float64), mf.astype(np.float64), dm, 1024 + t, width, snr,
+            rng.integers(0, 8, n), rng.integers(0, 2, n))
+
+
+def cluster_geometry():
+    return dict(cube_id=3, specnum_start=1024, sample_period_specnum=16, t_det=256, n_grid=256,
+                n_fdm_in_cube=64, sample_period_us=131.072, cell_l_rad=1.5e-4,
+                cell_m_rad=1.4e-4, l0_rad=0.001, m0_rad=-0.002,
+                fine_dm_pc_cc=np.linspace(50.0, 800.0, 64), mjd_start=60942.5)
+
+
+RECORD_FIELDS = ("cluster_id", "cube_id", "cntc", "cntb_lm", "cntb_dm", "peak_candidate_idx",
+                 "l_rad", "m_rad", "l_pix", "m_pix", "dm_fine_pc_cc", "fine_dm_idx", "t_in_cube",
+                 "t_seconds", "width_samples", "snr", "event_specnum", "search_node_id",
+                 "gpu_half")
+
+
+def make_cluster():
+    """cluster/features.py and cluster/forward.py (DBSCAN backend) on
+    seeded candidates.  The reference's HDBSCAN backend needs the
+    ``hdbscan`` package, which this environment lacks: its labels are
+    taken from scikit-learn's HDBSCAN on the same weighted features, with
+    min_samples + 1 (scikit-learn counts the point itself)."""
+    import warnings
+
+    from sklearn.cluster import HDBSCAN
+
+    from dsart.cluster.features import candidates_to_features, candidates_to_real_coords
+    from dsart.cluster.forward import ClustererConfig, cluster_candidates
+    from dsart.common.contracts import Candidate, CubeGeometry
+    l, m, dm, t, w, snr, node, half = cluster_fields()
+    geom = CubeGeometry(**cluster_geometry())
+    cands = [Candidate(l=float(l[i]), m=float(m[i]), dm_fine=float(dm[i]), dm_idx=0,
+                       event_specnum=int(t[i]), width_samples=int(w[i]),
+                       kernel_id=f"unit:d1:b{int(w[i])}", snr=float(snr[i]),
+                       detector_version="v1", flags=0, search_node_id=int(node[i]),
+                       gpu_half=int(half[i])) for i in range(len(l))]
+    out = dict(feat_int=candidates_to_features(cands, geom),
+               feat_real=candidates_to_features(cands, geom, mode="real",
+                                                weights=(1.0, 0.5, 2.0, 3e3, 3e3)),
+               coords=np.asarray(candidates_to_real_coords(cands, geom), np.float64))
+    for name, cfg in (("db", ClustererConfig(backend="dbscan")),
+                      ("dbreal", ClustererConfig(backend="dbscan", feature_mode="real",
+                                                 weights=(1.0, 0.02, 20.0, 3e3, 3e3),
+                                                 dbscan_eps=2.5, dbscan_min_samples=3))):
+        labels, recs = cluster_candidates(cands, geom, config=cfg)
+        out[name + "_labels"] = labels
+        out[name + "_records"] = np.asarray([[float(getattr(r, f)) for f in RECORD_FIELDS]
+                                             for r in recs], np.float64)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        for name, X in (("hdb_int", out["feat_int"]), ("hdb_real", out["feat_real"])):
+            out[name] = HDBSCAN(min_cluster_size=2, min_samples=2, cluster_selection_epsilon=10.0,
+                                metric="manhattan", allow_single_cluster=True,
+                                copy=True).fit_predict(X)
+    np.savez_compressed(os.path.join(HERE, "cluster.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DSART_REFERENCE", ""))
@@ -437,7 +522,8 @@ def main():
         sys.exit("need --reference <dsa110-rt>/src")
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
-            make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc]
+            make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
+            make_cluster]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
