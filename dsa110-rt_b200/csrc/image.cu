@@ -183,6 +183,7 @@ struct ImgArgs {
   const int* kcols;         // (n_const) col | has entries << 16: every entry at n' = 0
   int n_const;
   int n_s, s_stride;        // s_stride: even, >= n_s (the split S arrays in shared memory)
+  int s_mult_log2;          // ceil(log2) of the most contributions to one S entry
   const int* d_pitch;       // (G) cells (row pitch) of each chgroup's segments
   const int* n_filled;      // (G) pattern cells of each chgroup
   const int* sfine;         // (n_fine, G)
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   int* s_end = s_cbase + IMG_MAX_G + 1;
   float* s_scale = reinterpret_cast<float*>(s_end + IMG_MAX_G);
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_scale + IMG_MAX_G);
+  int* s_fixk = reinterpret_cast<int*>(s_tmem + 1);  // FMT 2: S holds S * 2^k as int32
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -294,14 +296,30 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     const int c = A.f2c[f];
     const long long ta = A.t0 + t;
     __syncthreads();  // the previous image is done with buf and s_slice
-    for (int g = tid; g < A.G; g += THREADS)
-    {
-      const int gc = g * A.n_coarse + c;
-      const long long dep = A.seg_depth[gc];
-      long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
-      if (slot < 0) slot += dep;
-      s_slice[g] = static_cast<const Elem*>(A.D) + A.seg_base[gc] + slot * A.d_pitch[g];
-      s_scale[g] = FMT == 2 ? A.scales[A.sc_base[gc] + slot] : 1.f;
+    if (warp == 0) {
+      float smax = 0.f;
+      for (int g = lane; g < A.G; g += 32) {
+        const int gc = g * A.n_coarse + c;
+        const long long dep = A.seg_depth[gc];
+        long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
+        if (slot < 0) slot += dep;
+        s_slice[g] = static_cast<const Elem*>(A.D) + A.seg_base[gc] + slot * A.d_pitch[g];
+        const float sc = FMT == 2 ? A.scales[A.sc_base[gc] + slot] : 1.f;
+        s_scale[g] = sc;
+        smax = fmaxf(smax, sc);
+      }
+      if constexpr (FMT == 2) {
+        // fixed point: every part is |q| <= 127 times its row's scale, so
+        // with 2^k = 2^(22 - ilogb(max scale) - s_mult_log2) a part is
+        // below 2^(30 - s_mult_log2) and any S entry's sum below 2^30
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        const bool ok = smax > 0.f && smax <= 3.0e38f;
+        const int k = ok ? min(100, 22 - ilogbf(smax) - A.s_mult_log2) : 0;
+        if (!ok && lane == 0) dsb_flag(A.status, DSB_E_ARG);
+        for (int g = lane; g < A.G; g += 32) s_scale[g] = ldexpf(ok ? s_scale[g] : 0.f, k);
+        if (lane == 0) *s_fixk = k;
+      }
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
@@ -316,8 +334,16 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       float* s_im = s_re + A.s_stride;
       auto add = [&](unsigned m, float2 v) {
         const unsigned t = m & 0xffffu;
-        atomicAdd(s_re + t, v.x);
-        atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
+        if constexpr (FMT == 2) {
+          // v is already scaled by 2^k: integer atomics (native, no
+          // compare-and-swap loop) and an order-independent exact sum
+          const int re = __float2int_rn(v.x), im = __float2int_rn(v.y);
+          atomicAdd(reinterpret_cast<int*>(s_re) + t, re);
+          atomicAdd(reinterpret_cast<int*>(s_im) + t, ((m >> 16) & 1u) ? -im : im);
+        } else {
+          atomicAdd(s_re + t, v.x);
+          atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
+        }
       };
       // warp w takes the 64-entry double chunks w, w + 8, ... of c_meta in
       // order, each lane two adjacent cells with one metadata and one ring
@@ -383,6 +409,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     {
       const float* s_re = reinterpret_cast<const float*>(buf);
       const float* s_im = s_re + A.s_stride;
+      const float unfix = FMT == 2 ? ldexpf(1.f, -*s_fixk) : 1.f;
       for (int c = 0; c < nch; ++c) {
         uint32_t r[16];
 #pragma unroll
@@ -391,8 +418,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
           float2 v = make_float2(0.f, 0.f);
           if (i < sn) {
             const unsigned b = (unsigned)(srot >> (2 * i)) & 3u;
-            v = crot_rt(make_float2(s_re[sb + i], s_im[sb + i]),
-                        (b & 1u) + ((b & 2u) ? (unsigned)shift_rot : 0u));
+            float2 x;
+            if constexpr (FMT == 2)
+              x = make_float2(__int2float_rn(__float_as_int(s_re[sb + i])) * unfix,
+                              __int2float_rn(__float_as_int(s_im[sb + i])) * unfix);
+            else
+              x = make_float2(s_re[sb + i], s_im[sb + i]);
+            v = crot_rt(x, (b & 1u) + ((b & 2u) ? (unsigned)shift_rot : 0u));
           }
           r[2 * j] = __float_as_uint(v.x);
           r[2 * j + 1] = __float_as_uint(v.y);
@@ -617,7 +649,7 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
                   const float* scales, const long long* sc_base, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
-                  const int* dcols, const unsigned long long* dmask, int n_dense,
+                  int s_mult, const int* dcols, const unsigned long long* dmask, int n_dense,
                   const int* kcols, int n_const, const int* d_pitch, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, int max_blocks,
@@ -627,7 +659,8 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
       n_s > 65536 || n_dense < 0 || n_const < 0 || (n_dense > 0 && (!dcols || !dmask)) ||
       (n_const > 0 && !kcols) || !d_pitch || !n_filled || !sfine || !f2c || !twiddles ||
       !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G ||
-      d_format < 0 || d_format > 2 || (d_format == 2 && (!scales || !sc_base)))
+      d_format < 0 || d_format > 2 || (d_format == 2 && (!scales || !sc_base)) ||
+      s_mult < 1 || s_mult > (1 << 20))
     return DSB_E_ARG;
   // two adjacent cells per load: 4-byte aligned cint8 pairs
   if (d_format == 2 && (reinterpret_cast<uintptr_t>(D) & 3)) return DSB_E_ARG;
@@ -635,9 +668,11 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
     return DSB_E_ARG;
   if (n_dense + n_const != N / 2) return DSB_E_ARG;  // every packed column, once
   const int stride = (n_s + 1) & ~1;
+  int mult_log2 = 0;
+  while ((1 << mult_log2) < s_mult) ++mult_log2;
   ImgArgs A{D, scales, sc_base, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
             n_c2, thr_b, (const uint4*)gmeta, srot, dcols, dmask, n_dense, kcols, n_const,
-            n_s, stride, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
+            n_s, stride, mult_log2, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
             t0, n_t, fftshift, (float*)out, status};
   switch (N) {
     case 64:

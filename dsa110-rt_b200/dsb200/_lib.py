@@ -44,7 +44,8 @@ _SIGNATURES = {
     "dsb_image_fold": [_c_int],
     "dsb_image_threads": [],
     "dsb_image_max_entries": [],
-    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp,
+    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int,
+                      _c_int, _vp,
                       _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
                       _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],
     "dsb_combine_rows": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int,

@@ -176,6 +176,7 @@ class ImageTables:
     dcols: np.ndarray       # (n_dense,) int32: packed columns with an entry off n' = 0
     dmask: np.ndarray       # (n_dense,) uint64: their occupied n'
     kcols: np.ndarray       # (n_const,) int32: w' | has entries << 16 (constant or zero columns)
+    s_mult: int = 1         # most contributions (pattern cells, both targets) to one S entry
 
 
 def _split_slots(sizes: np.ndarray, n_threads: int, cap: int) -> np.ndarray:
@@ -279,7 +280,8 @@ def build_image_tables(pats, N: int) -> ImageTables:
     return ImageTables(n_s=n_s, c_meta=c_meta, cell_base=cell_base,
                        c2=np.ascontiguousarray(c2.reshape(-1, 2)),
                        thr_b=thr_b.astype(np.int32), gmeta=gmeta, srot=srot, dcols=dcols,
-                       dmask=occ[dcols], kcols=kcols)
+                       dmask=occ[dcols], kcols=kcols,
+                       s_mult=int(np.bincount(inv, minlength=n_s).max()))
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -603,7 +605,7 @@ class SearchPipeline:
             _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_thrb), _lib.ptr(self.d_img_gmeta), _lib.ptr(self.d_img_srot),
-            it.n_s, _lib.ptr(self.d_img_dcols), _lib.ptr(self.d_img_dmask), int(it.dcols.size),
+            it.n_s, it.s_mult, _lib.ptr(self.d_img_dcols), _lib.ptr(self.d_img_dmask), int(it.dcols.size),
             _lib.ptr(self.d_img_kcols), int(it.kcols.size), _lib.ptr(self.d_pitch),
             _lib.ptr(self.d_nfilled), _lib.ptr(self.d_sfine), _lib.ptr(self.d_f2c),
             _lib.ptr(self.d_tw), f0, n_f, cfg.band.n_chgroup, N, t0, n_t, 1, _lib.ptr(out),

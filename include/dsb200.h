@@ -263,6 +263,13 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  *      the bit mask of their occupied n';
  *   kcols: the n_const other packed columns, w' | (has entries) << 16;
  *      n_dense + n_const = N/2, every packed column once.
+ *   s_mult: the most contributions (c_meta and c2 entries) to one S entry.
+ * Sums: float32 atomics for forms 0 and 1.  For the cint8 form S is summed
+ * exactly in int32 fixed point: each part scale * q is taken times 2^k,
+ * k = 22 - ilogb(max scale of the image's rows) - ceil(log2(s_mult)), and
+ * rounded to an integer (an error of at most 2^-(k+1) per part, below
+ * 2^(s_mult_log2 - 31) of the largest possible part); the sum does not
+ * depend on the order of the adds.
  * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256; n_s must
  * fit the kernel's shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY
  * is returned.  status: a thread range longer than max_entries or a
@@ -276,7 +283,7 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
                   const float* scales, const long long* sc_base, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
-                  const int* dcols, const unsigned long long* dmask, int n_dense,
+                  int s_mult, const int* dcols, const unsigned long long* dmask, int n_dense,
                   const int* kcols, int n_const, const int* d_pitch, const int* n_filled,
                   const int* sfine, const int* f2c, const void* twiddles, int f0, int n_f, int G,
                   int N, long long t0, int n_t, int fftshift, void* out, int max_blocks,
