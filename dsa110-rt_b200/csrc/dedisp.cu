@@ -154,6 +154,7 @@ struct S1Args {
   void* D;                // complex64 elements, or (BF16) bf16 re/im pairs in 32 bits
   const long long* seg_base;  // (G * n_dm) first element of each ring segment (a multiple of 4)
   const int* seg_depth;       // (G * n_dm) time slots of each segment
+  float* amax;            // (G * n_dm) or null: raised to the largest |part| written
   long long t0;           // absolute time of the first output
   int n_t, n_dm, ceff;
   int win_len;            // S1_TT + largest shift spread over a DM group
@@ -236,6 +237,7 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
     }
   }
   double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
+  float amax = 0.f;  // largest |part| this thread writes
   const float4* Y4 = reinterpret_cast<const float4*>(A.Y);
   const long long ycol = (long long)A.y_base[g] + c0;   // a multiple of 4
 
@@ -297,6 +299,8 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
         o1 = make_float4((float)((double)a1.x - mr[2]), (float)((double)a1.y - mi[2]),
                          (float)((double)a1.z - mr[3]), (float)((double)a1.w - mi[3]));
       }
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(o0.x), fabsf(o0.y)), fmaxf(fabsf(o0.z), fabsf(o0.w))));
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(o1.x), fabsf(o1.y)), fmaxf(fabsf(o1.z), fabsf(o1.w))));
       const long long o = seg + slot * pitch;  // element of cell c0, a multiple of 4
       if constexpr (BF16) {
         reinterpret_cast<uint4*>(A.D)[o / 4] =
@@ -308,6 +312,13 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
         D4[o / 2 + 1] = o1;
       }
     }
+  }
+  // the bound of the (chgroup, DM) rows: max over the L lanes that share
+  // the DM, one atomic per DM and block (non-negative floats order as ints)
+  if (A.amax) {
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if (active && ln == 0) atomicMax(reinterpret_cast<int*>(A.amax) + gd, __float_as_int(amax));
   }
   // sky: block mean of every (DM, cell) over the chunk, summed over the L
   // lanes that share the DM (L-aligned inside the warp)
@@ -385,7 +396,7 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                    long long t0, int n_t, int n_dm, int ceff, int dm_group, int max_spread,
+                    float* amax, long long t0, int n_t, int n_dm, int ceff, int dm_group, int max_spread,
                     void* sky_ring, int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream) {
@@ -409,7 +420,7 @@ int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blo
   A.Y = (const float2*)Y; A.y_rows = y_rows; A.y_mask = y_mask;
   A.blk_g = blk_g; A.blk_c0 = blk_c0; A.y_base = y_base; A.pitch = pitch;
   A.shift1 = shift1; A.shift2 = shift2; A.d_base = d_base; A.n_filled = n_filled;
-  A.D = D; A.seg_base = seg_base; A.seg_depth = seg_depth;
+  A.D = D; A.seg_base = seg_base; A.seg_depth = seg_depth; A.amax = amax;
   A.t0 = t0; A.n_t = n_t; A.n_dm = n_dm; A.ceff = ceff; A.win_len = win_len;
   A.sky_ring = (double2*)sky_ring; A.sky_window = sky_window; A.sky_head = sky_head;
   A.sky_count = sky_count; A.sky_subtract = sky_subtract; A.status = status;

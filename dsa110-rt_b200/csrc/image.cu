@@ -133,23 +133,32 @@ DSB_DEV void idftR(float2 (&a)[R]) {
 
 // Stage-2 ring elements (FMT): 0 complex64; 1 the BF16 storage form (bf16
 // re/im pairs in 32 bits); 2 the cint8 wire form (int8 re/im pairs in 16
-// bits, value = the row's scale x q).  Decoded to float32 before any
-// arithmetic; T2 holds two adjacent cells (one 4-, 8- or 16-byte load).
+// bits, value = the row's scale x q).  Decoded to float32 and multiplied by
+// the slice's factor sc (a power of two for forms 0 and 1, the row's scale
+// times one for form 2); T2 holds two adjacent cells (one 4-, 8- or 16-byte
+// load).
 template <int FMT> struct RingElem {
   using T = float2;
   using T2 = float4;
   static DSB_DEV T2 zero2() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-  static DSB_DEV float2 lo(T2 w, float) { return make_float2(w.x, w.y); }
-  static DSB_DEV float2 hi(T2 w, float) { return make_float2(w.z, w.w); }
-  static DSB_DEV float2 get(const T* p, float) { return *p; }
+  static DSB_DEV float2 lo(T2 w, float sc) { return make_float2(w.x * sc, w.y * sc); }
+  static DSB_DEV float2 hi(T2 w, float sc) { return make_float2(w.z * sc, w.w * sc); }
+  static DSB_DEV float2 get(const T* p, float sc) {
+    const float2 v = *p;
+    return make_float2(v.x * sc, v.y * sc);
+  }
 };
 template <> struct RingElem<1> {
   using T = uint32_t;
   using T2 = uint2;
+  static DSB_DEV float2 f(uint32_t w, float sc) {
+    const float2 v = bf16_pair_to_f2(w);
+    return make_float2(v.x * sc, v.y * sc);
+  }
   static DSB_DEV T2 zero2() { return make_uint2(0u, 0u); }
-  static DSB_DEV float2 lo(T2 w, float) { return bf16_pair_to_f2(w.x); }
-  static DSB_DEV float2 hi(T2 w, float) { return bf16_pair_to_f2(w.y); }
-  static DSB_DEV float2 get(const T* p, float) { return bf16_pair_to_f2(*p); }
+  static DSB_DEV float2 lo(T2 w, float sc) { return f(w.x, sc); }
+  static DSB_DEV float2 hi(T2 w, float sc) { return f(w.y, sc); }
+  static DSB_DEV float2 get(const T* p, float sc) { return f(*p, sc); }
 };
 template <> struct RingElem<2> {
   using T = uint16_t;
@@ -165,6 +174,11 @@ struct ImgArgs {
   const void* D;            // ring in the element form FMT of the kernel
   const float* scales;      // FMT 2: scale of each (chgroup, coarse DM, slot) row,
   const long long* sc_base; //   at scales[sc_base[g*n_coarse + c] + slot]
+  const float* amax;        // FMT 0, 1: (amax_rows, G * n_coarse) bound of every |part|
+                            //   stage 1 wrote for (chgroup, coarse DM) in a chunk of
+                            //   amax_chunk stage-1 times, row (chunk mod amax_rows)
+  const int* shift2;        // (G * n_coarse) stage-2 delays: ring time - stage-1 time
+  int amax_chunk, amax_rows;
   const long long* seg_base;  // (G * n_coarse) ring segment of (chgroup, coarse DM)
   const int* seg_depth;       // (G * n_coarse) time slots of each segment
   int n_coarse;
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   int* s_end = s_cbase + IMG_MAX_G + 1;
   float* s_scale = reinterpret_cast<float*>(s_end + IMG_MAX_G);
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(s_scale + IMG_MAX_G);
-  int* s_fixk = reinterpret_cast<int*>(s_tmem + 1);  // FMT 2: S holds S * 2^k as int32
+  int* s_fixk = reinterpret_cast<int*>(s_tmem + 1);  // S holds S * 2^k as int32
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -304,22 +318,36 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         long long slot = (ta - A.sfine[(long long)f * A.G + g]) % dep;
         if (slot < 0) slot += dep;
         s_slice[g] = static_cast<const Elem*>(A.D) + A.seg_base[gc] + slot * A.d_pitch[g];
-        const float sc = FMT == 2 ? A.scales[A.sc_base[gc] + slot] : 1.f;
+        float sc = 1.f, bound;
+        if constexpr (FMT == 2) {
+          sc = A.scales[A.sc_base[gc] + slot];
+          bound = sc;
+        } else {
+          // stage-1 time of the value read, its chunk's bound row
+          const long long t1 = ta - A.sfine[(long long)f * A.G + g] - A.shift2[gc];
+          const long long ch = t1 >= 0 ? t1 / A.amax_chunk
+                                       : -((A.amax_chunk - 1 - t1) / A.amax_chunk);
+          long long row = ch % A.amax_rows;
+          if (row < 0) row += A.amax_rows;
+          bound = A.amax[row * (long long)A.G * A.n_coarse + gc];
+        }
         s_scale[g] = sc;
-        smax = fmaxf(smax, sc);
+        smax = fmaxf(smax, bound);
       }
-      if constexpr (FMT == 2) {
-        // fixed point: every part is |q| <= 127 times its row's scale, so
-        // with 2^k = 2^(22 - ilogb(max scale) - s_mult_log2) a part is
-        // below 2^(30 - s_mult_log2) and any S entry's sum below 2^30
+      // Fixed point, S summed as S * 2^k in int32.  Every part is at most
+      // 128 x its row's scale (FMT 2) or its row's bound x (1 + 2^-8) (the
+      // bf16 rounding; FMT 0, 1), so with 2^k = 2^(22 or 28 - ilogb(max) -
+      // s_mult_log2) a part stays below 2^(30 - s_mult_log2) and any S
+      // entry's sum below 2^30.
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-        const bool ok = smax > 0.f && smax <= 3.0e38f;
-        const int k = ok ? min(100, 22 - ilogbf(smax) - A.s_mult_log2) : 0;
-        if (!ok && lane == 0) dsb_flag(A.status, DSB_E_ARG);
-        for (int g = lane; g < A.G; g += 32) s_scale[g] = ldexpf(ok ? s_scale[g] : 0.f, k);
-        if (lane == 0) *s_fixk = k;
-      }
+      for (int o = 16; o > 0; o >>= 1) smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+      const bool ok = smax >= 0.f && smax <= 3.0e38f;
+      const int k = (ok && smax > 0.f)
+                        ? min(100, (FMT == 2 ? 22 : 28) - ilogbf(smax) - A.s_mult_log2)
+                        : 0;
+      if (!ok && lane == 0) dsb_flag(A.status, DSB_E_ARG);
+      for (int g = lane; g < A.G; g += 32) s_scale[g] = ldexpf(ok ? s_scale[g] : 0.f, k);
+      if (lane == 0) *s_fixk = k;
     }
     {
       float4* b4 = reinterpret_cast<float4*>(buf);
@@ -334,16 +362,11 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       float* s_im = s_re + A.s_stride;
       auto add = [&](unsigned m, float2 v) {
         const unsigned t = m & 0xffffu;
-        if constexpr (FMT == 2) {
-          // v is already scaled by 2^k: integer atomics (native, no
-          // compare-and-swap loop) and an order-independent exact sum
-          const int re = __float2int_rn(v.x), im = __float2int_rn(v.y);
-          atomicAdd(reinterpret_cast<int*>(s_re) + t, re);
-          atomicAdd(reinterpret_cast<int*>(s_im) + t, ((m >> 16) & 1u) ? -im : im);
-        } else {
-          atomicAdd(s_re + t, v.x);
-          atomicAdd(s_im + t, ((m >> 16) & 1u) ? -v.y : v.y);
-        }
+        // v is already scaled by 2^k: integer atomics (native, no
+        // compare-and-swap loop) and a sum that does not depend on order
+        const int re = __float2int_rn(v.x), im = __float2int_rn(v.y);
+        atomicAdd(reinterpret_cast<int*>(s_re) + t, re);
+        atomicAdd(reinterpret_cast<int*>(s_im) + t, ((m >> 16) & 1u) ? -im : im);
       };
       // warp w takes the 64-entry double chunks w, w + 8, ... of c_meta in
       // order, each lane two adjacent cells with one metadata and one ring
@@ -409,7 +432,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     {
       const float* s_re = reinterpret_cast<const float*>(buf);
       const float* s_im = s_re + A.s_stride;
-      const float unfix = FMT == 2 ? ldexpf(1.f, -*s_fixk) : 1.f;
+      const float unfix = ldexpf(1.f, -*s_fixk);
       for (int c = 0; c < nch; ++c) {
         uint32_t r[16];
 #pragma unroll
@@ -418,12 +441,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
           float2 v = make_float2(0.f, 0.f);
           if (i < sn) {
             const unsigned b = (unsigned)(srot >> (2 * i)) & 3u;
-            float2 x;
-            if constexpr (FMT == 2)
-              x = make_float2(__int2float_rn(__float_as_int(s_re[sb + i])) * unfix,
-                              __int2float_rn(__float_as_int(s_im[sb + i])) * unfix);
-            else
-              x = make_float2(s_re[sb + i], s_im[sb + i]);
+            const float2 x = make_float2(__int2float_rn(__float_as_int(s_re[sb + i])) * unfix,
+                                         __int2float_rn(__float_as_int(s_im[sb + i])) * unfix);
             v = crot_rt(x, (b & 1u) + ((b & 2u) ? (unsigned)shift_rot : 0u));
           }
           r[2 * j] = __float_as_uint(v.x);
@@ -646,7 +665,8 @@ int dsb_image_threads(void) { return IMG_THREADS; }
 int dsb_image_max_entries(void) { return IMG_MAXE; }
 
 int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
-                  const float* scales, const long long* sc_base, int n_coarse,
+                  const float* scales, const long long* sc_base, const float* amax,
+                  const int* shift2, int amax_chunk, int amax_rows, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   int s_mult, const int* dcols, const unsigned long long* dmask, int n_dense,
@@ -660,6 +680,7 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
       (n_const > 0 && !kcols) || !d_pitch || !n_filled || !sfine || !f2c || !twiddles ||
       !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G ||
       d_format < 0 || d_format > 2 || (d_format == 2 && (!scales || !sc_base)) ||
+      (d_format != 2 && (!amax || !shift2 || amax_chunk <= 0 || amax_rows <= 0)) ||
       s_mult < 1 || s_mult > (1 << 20))
     return DSB_E_ARG;
   // two adjacent cells per load: 4-byte aligned cint8 pairs
@@ -670,7 +691,7 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
   const int stride = (n_s + 1) & ~1;
   int mult_log2 = 0;
   while ((1 << mult_log2) < s_mult) ++mult_log2;
-  ImgArgs A{D, scales, sc_base, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
+  ImgArgs A{D, scales, sc_base, amax, shift2, amax_chunk, amax_rows, seg_base, seg_depth, n_coarse, c_meta, cell_base, (const int2*)c2,
             n_c2, thr_b, (const uint4*)gmeta, srot, dcols, dmask, n_dense, kcols, n_const,
             n_s, stride, mult_log2, d_pitch, n_filled, sfine, f2c, (const float2*)twiddles, f0, n_f, G,
             t0, n_t, fftshift, (float*)out, status};

@@ -36,15 +36,15 @@ _SIGNATURES = {
     "dsb_static_sky": [_vp, _vp, _c_int, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_stage2_roll": [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_ll, _vp, _vp],
     "dsb_stage1_rows": [_vp, _c_ll, _c_ll, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                        _vp, _c_int, _vp, _vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int,
-                        _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+                        _vp, _c_int, _vp, _vp, _vp, _c_ll, _c_int, _c_int, _c_int, _c_int,
+                        _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
     "dsb_stage1_block_size": [],
     "dsb_stage1_dm_group": [],
     "dsb_stage1_smem_bytes": [_c_int, _c_int, _c_int],
     "dsb_image_fold": [_c_int],
     "dsb_image_threads": [],
     "dsb_image_max_entries": [],
-    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int,
+    "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int,
                       _c_int, _vp,
                       _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
                       _c_int, _c_ll, _c_int, _c_int, _vp, _c_int, _vp, _vp],

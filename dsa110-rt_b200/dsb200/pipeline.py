@@ -464,6 +464,13 @@ class SearchPipeline:
         # cint8: the scale of every ring row (one per segment slot), and the
         # chunk's stage-1 rows in complex64 before they are quantised (one
         # segment of C slots per (chgroup, coarse DM), written without delay)
+        # bound rows (formats c64, bf16): the largest |part| stage 1 wrote to
+        # each (chgroup, coarse DM) in a chunk, one row per chunk kept alive
+        # in the ring (reset when its row comes round again); the image
+        # kernel sums in fixed point under it
+        self.amax_rows = int(-(-int(depth.max()) // C)) + 2
+        self.amax = torch.zeros((self.amax_rows, depth.size), dtype=torch.float32,
+                                device=self.dev)
         self.sc_base = np.concatenate([[0], np.cumsum(depth.reshape(-1))]).astype(np.int64)
         self.d_scbase = d(self.sc_base[:-1])
         if self.ring_fmt == 2:
@@ -562,6 +569,10 @@ class SearchPipeline:
         q8 = self.ring_fmt == 2
         # cint8: stage 1 writes the chunk's rows to X (slot t of C, no delay);
         # the quantiser then moves them into the ring at t + shift2
+        arow = None
+        if not q8:
+            arow = self.amax[j % self.amax_rows]
+            arow.zero_()
         with self._mark("stage1"):
             _lib.check(_lib.lib().dsb_stage1_rows(
                 _lib.ptr(self.Y), T.n_rows_y, self.TY - 1, int(T.blk_g.size),
@@ -571,7 +582,8 @@ class SearchPipeline:
                 _lib.ptr(self.d_dbase), _lib.ptr(self.d_nfilled),
                 _lib.ptr(self.X if q8 else self.D), 0 if q8 else self.ring_fmt,
                 _lib.ptr(self.d_xbase if q8 else self.d_segbase),
-                _lib.ptr(self.d_xdepth if q8 else self.d_segdepth), j * C, C, cfg.coarse_dm.size,
+                _lib.ptr(self.d_xdepth if q8 else self.d_segdepth), _lib.ptr(arow), j * C, C,
+                cfg.coarse_dm.size,
                 cfg.ceff, T.dm_group, T.max_spread, _lib.ptr(self.sky), cfg.sky_window,
                 self.sky_head,
                 self.sky_count, sub, _lib.ptr(self.status), _lib.stream_of(self.dev)),
@@ -601,7 +613,8 @@ class SearchPipeline:
             raise ValueError("out must be contiguous float32 (n_f, n_t, N, N)")
         _lib.check(_lib.lib().dsb_image_fft(
             _lib.ptr(self.D), self.ring_fmt, _lib.ptr(self.d_segbase), _lib.ptr(self.d_segdepth),
-            _lib.ptr(self.scales), _lib.ptr(self.d_scbase), cfg.coarse_dm.size,
+            _lib.ptr(self.scales), _lib.ptr(self.d_scbase), _lib.ptr(self.amax),
+            _lib.ptr(self.d_shift2), cfg.chunk_tiles, self.amax_rows, cfg.coarse_dm.size,
             _lib.ptr(self.d_img_cmeta),
             _lib.ptr(self.d_img_cbase), _lib.ptr(self.d_img_c2), int(it.c2.shape[0]),
             _lib.ptr(self.d_img_thrb), _lib.ptr(self.d_img_gmeta), _lib.ptr(self.d_img_srot),

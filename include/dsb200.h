@@ -137,14 +137,18 @@ int dsb_stage2_roll(const void* const* hist, int depth, const int* kblk, const i
  * element: 0 = complex64; 1 = the BF16 storage form, one 32-bit word per
  * cell holding the real part (bf16, rounded to nearest even from the float32
  * sum) in the low half and the imaginary part in the high half; sums and the
- * sky statistics stay float32/float64.  Block b covers cells
+ * sky statistics stay float32/float64.  amax, when not null, holds one
+ * float per (chgroup g, coarse DM d) at g*n_dm + d, each raised (atomic
+ * max) to the largest |part| of the float32 values written for it (the
+ * bound dsb_image_fft sums under).  Block b covers cells
  * [blk_c0[b], + dsb_stage1_block_size()) of chgroup blk_g[b] and one group
  * of dm_group coarse DMs (grid y). */
 int dsb_stage1_rows(const void* Y, long long y_rows, long long y_mask, int n_blocks,
                     const int* blk_g, const int* blk_c0, const int* y_base, const int* pitch,
                     const int* shift1, const int* shift2, const int* d_base, const int* n_filled,
                     void* D, int d_bf16, const long long* seg_base, const int* seg_depth,
-                    long long t0, int n_t, int n_dm, int ceff, int dm_group, int max_spread,
+                    float* amax, long long t0, int n_t, int n_dm, int ceff, int dm_group,
+                    int max_spread,
                     void* sky_ring, int sky_window,
                     int sky_head, int sky_count, int sky_subtract, int* status,
                     cudaStream_t stream);
@@ -264,12 +268,19 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  *   kcols: the n_const other packed columns, w' | (has entries) << 16;
  *      n_dense + n_const = N/2, every packed column once.
  *   s_mult: the most contributions (c_meta and c2 entries) to one S entry.
- * Sums: float32 atomics for forms 0 and 1.  For the cint8 form S is summed
- * exactly in int32 fixed point: each part scale * q is taken times 2^k,
- * k = 22 - ilogb(max scale of the image's rows) - ceil(log2(s_mult)), and
- * rounded to an integer (an error of at most 2^-(k+1) per part, below
- * 2^(s_mult_log2 - 31) of the largest possible part); the sum does not
- * depend on the order of the adds.
+ * Sums: S is summed in int32 fixed point, each part times 2^k rounded to an
+ * integer, so the sum does not depend on the order of the adds.  k comes
+ * from a bound on the image's parts: for the cint8 form the rows' scales
+ * (k = 22 - ilogb(max scale) - ceil(log2(s_mult))); for forms 0 and 1 the
+ * bound rows stage 1 keeps (dsb_stage1_rows' amax), row (floor(t1 /
+ * amax_chunk) mod amax_rows) of (amax_rows, G * n_coarse) floats for the
+ * value of stage-1 time t1 = t - sfine - shift2[g*n_coarse + c]
+ * (k = 28 - ilogb(max bound) - ceil(log2(s_mult))).  A part's rounding
+ * error is at most 2^-(k+1), below 2^(ceil(log2(s_mult)) - 29) of the bound;
+ * bf16 parts above 2^-16 of it are exact.  The bound must cover every value
+ * read: the caller keeps a row alive while the ring holds its chunk and
+ * zeroes it before stage 1 writes a new chunk into it.  A non-finite bound
+ * sets DSB_E_ARG in *status.
  * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256; n_s must
  * fit the kernel's shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY
  * is returned.  status: a thread range longer than max_entries or a
@@ -280,7 +291,8 @@ int dsb_image_fold(int n_grid);
 int dsb_image_threads(void);
 int dsb_image_max_entries(void);
 int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
-                  const float* scales, const long long* sc_base, int n_coarse,
+                  const float* scales, const long long* sc_base, const float* amax,
+                  const int* shift2, int amax_chunk, int amax_rows, int n_coarse,
                   const unsigned* c_meta, const int* cell_base, const void* c2, int n_c2,
                   const int* thr_b, const void* gmeta, const unsigned long long* srot, int n_s,
                   int s_mult, const int* dcols, const unsigned long long* dmask, int n_dense,
