@@ -127,16 +127,16 @@ class Clocks:
 # algorithmic work per launch (for the roofline of the dominant kernel)
 # ---------------------------------------------------------------------------
 
-# DRAM traffic of image_kernel<256> measured by ncu (--set full, one launch)
-# on the medium workload: 249.12 MB written for 1152 images (the rest of the
-# images still sat in L2 when the kernel ended), 105.18 MB read for 2 coarse
-# DMs x 144 times
-IMAGE_DRAM_WRITE_PER_IMAGE = 249.123584e6 / 1152
-IMAGE_DRAM_READ_PER_SLICE_TIME = 105.180160e6 / (2 * 144)
-# the BF16 ring halves the ring reads: ncu dram__bytes_read.sum of the same
-# kernel on the medium workload, 49.49 MB (bf16 ring) against 99.22 MB
-# (complex64 ring) per launch, in one paired capture
-IMAGE_DRAM_READ_BF16_RATIO = 49.494272e6 / 99.225429e6
+# DRAM traffic of image_kernel<256, 1> (bf16 ring) measured by ncu (--set
+# full, one launch) on the medium workload: 244.01 MB written for 1152
+# images (the rest of the images still sat in L2 when the kernel ended),
+# 52.67 MB read for 2 coarse DMs x 144 times
+IMAGE_DRAM_WRITE_PER_IMAGE = 244.012544e6 / 1152
+IMAGE_DRAM_READ_PER_SLICE_TIME = 52.672768e6 / (2 * 144)
+# ring reads of the complex64 ring against the bf16 ring: ncu
+# dram__bytes_read.sum of the same kernel on the medium workload, 99.22 MB
+# (complex64) against 49.49 MB (bf16) per launch, in one paired capture
+IMAGE_DRAM_READ_C64_RATIO = 99.225429e6 / 49.494272e6
 # ---------------------------------------------------------------------------
 
 
@@ -484,14 +484,17 @@ def main():
         nt = cfg_.chunk_tiles + 2 * cfg_.t_edge
         nb = cfg_.fdm_batch
         cpb = max(1, nb // cfg_.fine_per_coarse)
-        rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_BF16_RATIO
-                                                if cfg.ring_dtype == "bf16" else 1.0)
+        rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_C64_RATIO
+                                                if cfg.ring_dtype == "c64" else 1.0)
         roof["traffic"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt
                            if cfg.ring_dtype != "cint8" else None)
         roof["traffic_note"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel on "
-                                "the medium workload (1152 images), scaled to this launch"
-                                + ("; ring reads x 0.499, the bf16/complex64 read ratio of a "
-                                   "paired capture" if cfg.ring_dtype == "bf16" else ""))
+                                "the medium workload (1152 images, bf16 ring), scaled to this "
+                                "launch"
+                                + ("; ring reads x 2.005, the complex64/bf16 read ratio of a "
+                                   "paired capture" if cfg.ring_dtype == "c64" else "")
+                                + ("; not captured for the cint8 ring"
+                                   if cfg.ring_dtype == "cint8" else ""))
 
     if rank == 0:
         cb = None

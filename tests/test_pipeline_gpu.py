@@ -136,7 +136,8 @@ def test_pipeline_rejects_wrong_raw_size(dev):
 def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     """Fused combine + 2-D c2r FFT == dsb_combine_rows + torch.fft.irfft2 on
     the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale,
-    for every ring element form (cint8 with a random scale per ring row)."""
+    for every ring element form (cint8 with a random scale per ring row), and
+    bit-identical for two grid sizes."""
     from dsb200 import _lib
     from dsb200.pipeline import PipelineConfig, SearchPipeline
     band, ob, e, n, blocks, kw = _setup(n_blocks=1, amp=0.0)
@@ -183,3 +184,9 @@ def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     pipe.check_status()
     err = (out.double() - want).abs().max().item()
     assert err <= 2e-6 * want.abs().max().item(), err
+    # the fixed-point sums do not depend on the order of the atomics: another
+    # grid size gives the same bits
+    out2 = torch.empty_like(out)
+    pipe.image(1, nf, t0, nt, out2, max_blocks=0)
+    torch.cuda.synchronize()
+    assert torch.equal(out, out2)
