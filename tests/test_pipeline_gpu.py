@@ -84,6 +84,19 @@ def test_pipeline_matches_oracle(dev, ring, dm_group):
         for d in range(len(kw["coarse_dm"])):
             got_d = pipe.ring_values(g, d, t1 + T.shift2[g, d])
             np.testing.assert_array_equal(got_d, keep["D1"][g][d][t1].astype(np.complex64))
+    # the bound row of that chunk (the image kernel's fixed-point scale): the
+    # largest |part| stage 1 wrote, before the bf16 rounding
+    if ring != "cint8":
+        row = pipe.amax[(T1 // 32 - 1) % pipe.amax_rows].cpu().numpy()
+        for g in range(band.n_chgroup):
+            for d in range(len(kw["coarse_dm"])):
+                x = keep["D1"][g][d][t1].astype(np.complex64)
+                top = max(np.abs(x.real).max(), np.abs(x.imag).max())
+                b = row[g * len(kw["coarse_dm"]) + d]
+                if ring == "c64":
+                    assert b == top, (g, d, b, top)
+                else:
+                    assert top * (1 - 2.0 ** -8) <= b <= top * (1 + 2.0 ** -8), (g, d, b, top)
 
     key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
     g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
