@@ -39,7 +39,7 @@ def workload_config(name: str):
         return PipelineConfig(nant=96, band=DSA110_BAND, npkt_block=8192, t_int=8, csf=16,
                               n_grid=256, coarse_dm=np.linspace(0.0, 2000.0, 128),
                               fine_per_coarse=16, log_max_width=4, threshold=7.0,
-                              chunk_tiles=512, fdm_batch=8)
+                              chunk_tiles=512, fdm_batch=32)
     if name == "dsa110-512dm":
         # the full DSA-110 shape as given: 512 DMs over 0-2000
         return PipelineConfig(nant=96, band=DSA110_BAND, npkt_block=8192, t_int=8, csf=16,

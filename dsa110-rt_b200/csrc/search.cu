@@ -434,6 +434,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
 // ===========================================================================
 constexpr int L1_MAX = 4096;
 constexpr int L1_THREADS = 1024;
+static_assert(L1_MAX % L1_THREADS == 0, "each thread stages a whole number of samples");
 
 // Where a row's samples come from: a [rows, m] matrix, or (GATHER) the
 // images themselves, sample i of row f = img[f*f_stride + times[i / n_pix] *
@@ -451,40 +452,90 @@ template <bool GATHER>
 __global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const L1Src src, int m,
                                                                  float n_sigma, int n_iter,
                                                                  float* __restrict__ out) {
-  __shared__ float v[L1_MAX];
+  __shared__ __align__(16) float v[L1_MAX];
   __shared__ double red[L1_THREADS / 32];
   __shared__ int s_lo, s_hi;
   const float* row = src.x + (long long)blockIdx.x * (GATHER ? src.f_stride : m);
   int P = 1;
   while (P < m) P <<= 1;
-  for (int i = threadIdx.x; i < P; i += L1_THREADS) {
-    float a = __int_as_float(0x7f800000);
+  // Thread t holds samples 4t .. 4t + 3 in registers (every load issues
+  // before the first is used); the padding past m is +inf.  The bitonic
+  // network sorts all L1_MAX entries: its stages with partner distance j < 4
+  // run inside the thread, 4 <= j <= 64 across the warp by shuffles, and only
+  // j >= 128 through shared memory with a barrier (15 of the 78 stages).
+  // The smallest P entries are the P entries of the P-padded sort, so the
+  // result is the same as sorting P.
+  static_assert(L1_MAX == 4 * L1_THREADS, "four samples per thread");
+  float r[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = 4 * threadIdx.x + q;
+    r[q] = __int_as_float(0x7f800000);
     if (i < m) {
       if constexpr (GATHER)
-        a = row[src.times[i / src.n_pix] * src.t_stride + src.pix[i % src.n_pix]];
+        r[q] = row[src.times[i / src.n_pix] * src.t_stride + src.pix[i % src.n_pix]];
       else
-        a = row[i];
+        r[q] = row[i];
     }
-    if (!(a == a) || isinf(a)) a = __int_as_float(0x7f800000);  // non-finite -> +inf (dropped)
-    v[i] = a;
   }
-  __syncthreads();
-  for (int k = 2; k <= P; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < P; i += L1_THREADS) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const bool up = (i & k) == 0;
-          const float a = v[i], b = v[ixj];
-          if ((a > b) == up) {
-            v[i] = b;
-            v[ixj] = a;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (!(r[q] == r[q]) || isinf(r[q])) r[q] = __int_as_float(0x7f800000);  // non-finite -> +inf
+  const int i0 = 4 * threadIdx.x;
+  float4* v4 = reinterpret_cast<float4*>(v);
+  // compare-exchange of positions (i, i ^ j), i the lower: ascending where
+  // (i & k) == 0
+  auto cx = [](float& lo, float& hi, bool up) {
+    if ((lo > hi) == up) {
+      const float t = lo;
+      lo = hi;
+      hi = t;
+    }
+  };
+  for (int k = 2; k <= L1_MAX; k <<= 1) {
+    const bool up = (i0 & k) == 0;  // for k >= 4 the same for all four samples
+    int j = k >> 1;
+    if (j >= 128) {
+      v4[threadIdx.x] = make_float4(r[0], r[1], r[2], r[3]);
+      __syncthreads();
+      for (; j >= 128; j >>= 1) {
+        for (int i = threadIdx.x; i < L1_MAX; i += L1_THREADS) {
+          const int ixj = i ^ j;
+          if (ixj > i) {
+            const bool u = (i & k) == 0;
+            const float a = v[i], b = v[ixj];
+            if ((a > b) == u) {
+              v[i] = b;
+              v[ixj] = a;
+            }
           }
         }
+        __syncthreads();
       }
-      __syncthreads();
+      const float4 w = v4[threadIdx.x];
+      r[0] = w.x; r[1] = w.y; r[2] = w.z; r[3] = w.w;
+    }
+    for (; j >= 4; j >>= 1) {
+      const bool lower = (i0 & j) == 0;  // this thread's samples are the lower positions
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float o = __shfl_xor_sync(0xffffffffu, r[q], j >> 2);
+        // the lower position keeps the smaller value where ascending
+        const bool keep_small = lower == up;
+        r[q] = keep_small ? (o < r[q] ? o : r[q]) : (o > r[q] ? o : r[q]);
+      }
+    }
+    if (k >= 4) {  // j = 2: pairs (0, 2), (1, 3)
+      cx(r[0], r[2], up);
+      cx(r[1], r[3], up);
+    }
+    {  // j = 1: pairs (0, 1), (2, 3); for k = 2 the direction alternates per pair
+      cx(r[0], r[1], k == 2 ? ((i0 & 2) == 0) : up);
+      cx(r[2], r[3], k == 2 ? (((i0 + 2) & 2) == 0) : up);
     }
   }
+  v4[threadIdx.x] = make_float4(r[0], r[1], r[2], r[3]);
+  __syncthreads();
   // finite count
   if (threadIdx.x == 0) {
     int n_fin = 0;

@@ -230,6 +230,27 @@ def test_layer1_vs_reference(dev, golden_dir):
     np.testing.assert_allclose(got, O.sigma_clipped_std_batched(z["l1_in"]), rtol=2e-6)
 
 
+@pytest.mark.parametrize("m", [4096, 4000, 1000, 37, 2])
+def test_layer1_sort_edge_cases(dev, m):
+    """The clipped std's in-register / shuffle / shared-memory bitonic sort
+    on rows of every fill (power of two or not), with non-finite values,
+    signed zeros, heavy ties and outliers, against the oracle."""
+    from dsb200.search import sigma_clipped_std_batched
+    rng = np.random.default_rng(m)
+    rows = rng.standard_normal((6, m)).astype(np.float32)
+    rows[1] = np.round(rows[1] * 2) / 2             # many exact ties
+    rows[2, ::7] = np.nan
+    rows[2, 3::11] = np.inf
+    rows[2, 5::13] = -np.inf
+    rows[3] = 0.0
+    rows[3, ::2] = -0.0
+    rows[3, :min(m, 5)] = [1.0, -1.0, 2.0, 0.5, 3.0][:min(m, 5)]
+    rows[4, :max(1, m // 50)] = 1e4                 # outliers the clip removes
+    rows[5] = np.nan                                # nothing finite
+    got = sigma_clipped_std_batched(torch.from_numpy(rows).to(dev)).cpu().numpy()
+    np.testing.assert_allclose(got, O.sigma_clipped_std_batched(rows), rtol=2e-6)
+
+
 def test_uv_cells_fp64_gpu_equals_numpy(dev):
     from dsb200.grid import per_baseline_uv_meters, uv_cells_gpu
     e, n = MG.t_layout_antpos(96, seed=3)
