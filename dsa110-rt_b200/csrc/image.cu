@@ -12,7 +12,8 @@
 //  1. Combine.  The non-zero half-spectrum cells S (the union of every
 //     chgroup's uv pattern, a few thousand cells) are summed in shared memory
 //     from the time-major stage-2 ring: one coalesced read of each chgroup's
-//     coarse-DM slice, shared-memory float atomics into S.  Each thread then
+//     coarse-DM slice, shared-memory int32 atomics into S held in fixed
+//     point (S * 2^k, k from a bound on the image's parts).  Each thread then
 //     moves its own range of S (at most IMG_MAXE entries, whole slots) into
 //     tensor memory, which this kernel uses as plain per-thread storage:
 //     TMEM is otherwise idle here and holds S across the passes below while
@@ -35,8 +36,8 @@
 // Every transform of length L = R*R runs on a group of R threads: an R-point
 // DFT in registers, the twiddles W_L^(j*x1), one XOR-swizzled shared-memory
 // transpose, and a second R-point DFT (the classic two-step factorisation).
-// The shared-memory atomics of step 1 add in no fixed order, so an image can
-// differ from run to run in the last bits of a float32 sum.
+// The shared-memory atomics of step 1 add integers, so an image does not
+// depend on the order in which they land: it is the same from run to run.
 #include "dsb_common.cuh"
 
 #include <algorithm>
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       for (int i = tid; i < A.s_stride / 2; i += THREADS) b4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
-    // ---- 1. combine into S (shared-memory float atomics) ----
+    // ---- 1. combine into S (shared-memory int32 atomics, fixed point) ----
     {
       // separate real and imaginary arrays: a warp's 32 atomics spread over
       // all 32 banks instead of the even (or odd) half
