@@ -287,8 +287,8 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
       for (int sb = 0; sb < ceff; ++sb) {
         const int idx = sb * A.win_len + tl + s_sh[sb * DG + dl];
         const float4 v0 = win0[idx], v1 = win1[idx];
-        a0.x += v0.x; a0.y += v0.y; a0.z += v0.z; a0.w += v0.w;
-        a1.x += v1.x; a1.y += v1.y; a1.z += v1.z; a1.w += v1.w;
+        a0 = f4_add(a0, v0);  // packed pairs: 4 adds instead of 8
+        a1 = f4_add(a1, v1);
       }
       sr[0] += a0.x; si[0] += a0.y; sr[1] += a0.z; si[1] += a0.w;
       sr[2] += a1.x; si[2] += a1.y; sr[3] += a1.z; si[3] += a1.w;

@@ -26,6 +26,35 @@ DSB_DEV float2 bf16_pair_to_f2(uint32_t w) {
   return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
 }
 
+// Packed float32 pairs (sm_100 add.rn.f32x2 / sub.rn.f32x2): one
+// instruction for two independent float32 adds, each part rounded to
+// nearest as the scalar add rounds it.
+DSB_DEV unsigned long long f2_pack(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+DSB_DEV float2 f2_unpack(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+DSB_DEV float2 f2_add(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+  return f2_unpack(r);
+}
+DSB_DEV float2 f2_sub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+  return f2_unpack(r);
+}
+DSB_DEV float4 f4_add(float4 a, float4 b) {
+  const float2 lo = f2_add(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  const float2 hi = f2_add(make_float2(a.z, a.w), make_float2(b.z, b.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+
 // Iteration limit for every mbarrier spin (each try_wait may itself suspend
 // for a hardware-chosen interval, so this bounds the wait to well under a
 // few seconds on a healthy GPU).

@@ -47,31 +47,11 @@ namespace {
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? DSB_OK : DSB_E_CUDA; }
 
-// Complex add / subtract as one packed float32-pair instruction (sm_100
-// add.rn.f32x2 / sub.rn.f32x2): each part rounded to nearest as the scalar
-// operation rounds it.  Against two scalar adds this took the image kernel
-// from 896 to 863 ms per block at the bench workload (the transforms are
-// mostly butterflies).
-DSB_DEV unsigned long long f2_pack(float2 a) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
-  return r;
-}
-DSB_DEV float2 f2_unpack(unsigned long long r) {
-  float2 a;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
-  return a;
-}
-DSB_DEV float2 cadd(float2 a, float2 b) {
-  unsigned long long r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
-  return f2_unpack(r);
-}
-DSB_DEV float2 csub(float2 a, float2 b) {
-  unsigned long long r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
-  return f2_unpack(r);
-}
+// Complex add / subtract as one packed float32-pair instruction.  Against
+// two scalar adds this took the image kernel from 896 to 863 ms per block at
+// the bench workload (the transforms are mostly butterflies).
+DSB_DEV float2 cadd(float2 a, float2 b) { return f2_add(a, b); }
+DSB_DEV float2 csub(float2 a, float2 b) { return f2_sub(a, b); }
 DSB_DEV float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
