@@ -128,11 +128,11 @@ class Clocks:
 # ---------------------------------------------------------------------------
 
 # DRAM traffic of image_kernel<256, 1> (bf16 ring) measured by ncu (--set
-# full, one launch) on the medium workload: 244.01 MB written for 1152
+# full, one launch) on the medium workload: 242.73 MB written for 1152
 # images (the rest of the images still sat in L2 when the kernel ended),
-# 52.67 MB read for 2 coarse DMs x 144 times
-IMAGE_DRAM_WRITE_PER_IMAGE = 244.012544e6 / 1152
-IMAGE_DRAM_READ_PER_SLICE_TIME = 52.672768e6 / (2 * 144)
+# 49.53 MB read for 2 coarse DMs x 144 times
+IMAGE_DRAM_WRITE_PER_IMAGE = 242.731776e6 / 1152
+IMAGE_DRAM_READ_PER_SLICE_TIME = 49.525504e6 / (2 * 144)
 # ring reads of the complex64 ring against the bf16 ring: ncu
 # dram__bytes_read.sum of the same kernel on the medium workload, 99.22 MB
 # (complex64) against 49.49 MB (bf16) per launch, in one paired capture

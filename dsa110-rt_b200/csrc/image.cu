@@ -301,7 +301,12 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
                          (uint32_t)((warp >> 2) * (IMG_TMEM_COLS / 2));
 
   const int n_tot = A.cell_base[A.G];
+  // 0.5 / N^2 is a power of two, applied to S on its way into TMEM: scaling
+  // every input of the transforms by a power of two scales every rounded
+  // intermediate exactly, so the images are the bits the scale at the end
+  // would give, without 2 N^2 multiplies per image
   const float scale = 0.5f / (float)(N * N);
+  static_assert((N & (N - 1)) == 0, "0.5 / N^2 must be a power of two");
   const int n_img = A.n_f * A.n_t;
   // column groups: C1 lanes; row groups: RR lanes (groups never straddle warps)
   const int cgi = tid / C1, cj = tid % C1;
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     {
       const float* s_re = reinterpret_cast<const float*>(buf);
       const float* s_im = s_re + A.s_stride;
-      const float unfix = ldexpf(1.f, -*s_fixk);
+      const float unfix = ldexpf(scale, -*s_fixk);  // 2^-k x 0.5 / N^2
       for (int c = 0; c < nch; ++c) {
         uint32_t r[16];
 #pragma unroll
@@ -589,8 +594,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         float* stage = reinterpret_cast<float*>(reg);
 #pragma unroll
         for (int x2 = 0; x2 < RR; ++x2) {
-          stage[rj + RR * x2] = a[x2].x * scale;
-          stage[N + rj + RR * x2] = a[x2].y * scale;
+          stage[rj + RR * x2] = a[x2].x;
+          stage[N + rj + RR * x2] = a[x2].y;
         }
         __syncwarp(rmask);
         const size_t ibase = ((size_t)fl * A.n_t + t) * N;
