@@ -184,10 +184,15 @@ def test_cumsum_boxcars_argmax_vs_reference(dev, golden_dir):
 
 @pytest.mark.parametrize("log_w", [2, 4])
 @pytest.mark.parametrize("f16", [False, True])
-def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16):
+@pytest.mark.parametrize("hw", [(12, 10), (11, 9)])
+def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16, hw):
+    """Candidates of the streaming detector == every cell above threshold of
+    the padded cumsum + boxcar argmax, bit for bit, for even and odd pixel
+    counts and float or half cubes."""
     from dsb200.search import CandidateBuffer, detect_cube
     rng = np.random.default_rng(10 + log_w)
-    T, F, H, W = 70, 3, 12, 10
+    T, F = 70, 3
+    H, W = hw
     x = rng.normal(size=(T, F, H, W)).astype(np.float16 if f16 else np.float32)
     x[30:34, 1, 5, 5] += 6.0
     widths = [1 << k for k in range(log_w + 1)]
