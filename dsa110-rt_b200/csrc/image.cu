@@ -321,7 +321,9 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
     const int f = A.f0 + fl;
     const int c = A.f2c[f];
     const long long ta = A.t0 + t;
-    __syncthreads();  // the previous image is done with buf and s_slice
+    // (the previous image is done with buf and s_slice: its last pass ended
+    // with a barrier, and the first image follows the one after the TMEM
+    // allocation)
     if (warp == 0) {
       float smax = 0.f;
       for (int g = lane; g < A.G; g += 32) {
