@@ -30,6 +30,12 @@ sys.path[:0] = [os.path.join(ROOT, "dsa110-rt_b200"), os.path.join(ROOT, "oracle
 METRIC = "real-time factor at 96-ant/6144-ch/2048-DM (data-seconds per second)"
 
 
+def metric_for(cfg) -> str:
+    """The metric's name with the workload's DM count (2048 for the default
+    workload, the name above)."""
+    return METRIC.replace("2048-DM", f"{cfg.fine_dm.size}-DM")
+
+
 def workload_config(name: str):
     from dsb200.constants import DSA110_BAND
     from dsb200.pipeline import PipelineConfig
@@ -358,7 +364,7 @@ def main():
         v = float(np.median([r["value"] for r in res]))
         cb = dict(res[0])
         cb["value"] = v
-        line = {"metric": METRIC, "value": v, "unit": "data-seconds/s", "n_gpus": a.gpus,
+        line = {"metric": metric_for(cfg), "value": v, "unit": "data-seconds/s", "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": cfg.block_seconds / v * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": workload_desc(a.workload, cfg), "impl": "reference",
@@ -500,7 +506,7 @@ def main():
         cb = None
         if not a.no_cpu:
             cb = cpu_baseline(cfg, threads=os.cpu_count() or 1)
-        line = {"metric": METRIC, "value": value, "unit": "data-seconds/s", "n_gpus": world,
+        line = {"metric": metric_for(cfg), "value": value, "unit": "data-seconds/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": ("int8 (correlator) / bf16 ring, f32 accumulate" if a.ring == "bf16"
