@@ -38,6 +38,18 @@ def test_binding_covers_header():
     assert sorted(_lib.declared_symbols()) == _declared()
 
 
+def test_binding_argument_counts_match_header():
+    """Every ctypes signature has as many arguments as the header's
+    prototype (ctypes itself does not check)."""
+    from dsb200 import _lib
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    for name, args in _lib._SIGNATURES.items():
+        m = re.search(r"\b" + name + r"\s*\(([^;]*?)\)\s*;", src, re.S)
+        assert m, name
+        params = [q for q in m.group(1).split(",") if q.strip() and q.strip() != "void"]
+        assert len(params) == len(args), (name, len(params), len(args))
+
+
 def test_strerror_without_gpu():
     from dsb200 import _lib
     if not os.path.exists(_lib.SO_PATH):
