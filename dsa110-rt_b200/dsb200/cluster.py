@@ -263,24 +263,28 @@ def _bfs_hierarchy(Z: np.ndarray, root: int, n: int) -> List[int]:
     return out
 
 
-def _single_linkage(M: np.ndarray) -> np.ndarray:
-    """Minimum spanning tree of the dense graph M (Prim) turned into a
-    single-linkage hierarchy ``(n - 1, 4)``: left, right, distance, size;
-    node n + i is row i."""
-    n = M.shape[0]
-    in_tree = np.zeros(n, bool)
-    in_tree[0] = True
-    best = M[0].copy()
-    src = np.zeros(n, np.int64)
+def mst_edges(X: np.ndarray, min_samples: int) -> np.ndarray:
+    """Prim's minimum spanning tree over the mutual-reachability graph of the
+    rows of X (cityblock distance, core distance to the ``min_samples``-th
+    other point), from the library's host code (``dsb_cluster_mst``):
+    ``(n - 1, 3)`` rows (source, point, distance) in the order added."""
+    from . import _lib
+    X = np.ascontiguousarray(X, np.float64)
+    n = X.shape[0]
+    core = np.empty(n, np.float64)
     edges = np.empty((n - 1, 3), np.float64)
-    for k in range(n - 1):
-        cand = np.where(in_tree, np.inf, best)
-        j = int(np.argmin(cand))
-        edges[k] = (src[j], j, best[j])
-        in_tree[j] = True
-        upd = (M[j] < best) & ~in_tree
-        best[upd] = M[j][upd]
-        src[upd] = j
+    _lib.check(_lib.lib().dsb_cluster_mst(
+        X.ctypes.data_as(_lib.ctypes.c_void_p), n, X.shape[1], int(min_samples),
+        core.ctypes.data_as(_lib.ctypes.c_void_p), edges.ctypes.data_as(_lib.ctypes.c_void_p)),
+        "dsb_cluster_mst")
+    return edges
+
+
+def _single_linkage(edges: np.ndarray, n: int) -> np.ndarray:
+    """MST edges turned into a single-linkage hierarchy ``(n - 1, 4)``:
+    left, right, distance, size; node n + i is row i.  Equal weights keep
+    the order numpy's default argsort gives them (as scikit-learn's
+    implementation does)."""
     edges = edges[np.argsort(edges[:, 2], kind="quicksort")]
     parent = np.arange(2 * n - 1)
     size = np.ones(2 * n - 1, np.int64)
@@ -390,11 +394,7 @@ def hdbscan_labels(X: np.ndarray, *, min_cluster_size: int = 2, min_samples: int
         raise ValueError(f"min_cluster_size={min_cluster_size}, expected >= 2")
     if n < 2:
         return np.full(n, -1, np.int64)
-    D = cityblock_matrix(X)
-    k = max(1, min(n - 1, int(min_samples)))
-    core = np.partition(D, k, axis=1)[:, k]
-    M = np.maximum(D, np.maximum(core[:, None], core[None, :]))
-    Z = _single_linkage(M)
+    Z = _single_linkage(mst_edges(X, min_samples), n)
     tree = _condense(Z, n, int(min_cluster_size))
     par, chi, lam, sz = tree[:, 0].astype(np.int64), tree[:, 1].astype(np.int64), tree[:, 2], \
         tree[:, 3].astype(np.int64)

@@ -375,6 +375,18 @@ int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, i
                      const int* times, int n_times, const int* pix, int n_pix, float n_sigma,
                      int n_iter, float* sigma, cudaStream_t stream);
 
+/* ---- next row: per-cube clusterer (host) ------------------------------------
+ * The minimum spanning tree of the HDBSCAN backend that cluster/forward.py:103
+ * runs through the hdbscan package: X (n, d) float64 row-major feature rows,
+ * cityblock distances (summed over the columns in order), core[a] = the
+ * min_samples-th smallest distance from a counting a itself as the 0-th
+ * (min_samples clamped to [1, n - 1]), mutual reachability max(D, core_a,
+ * core_b), Prim's algorithm from point 0 (first index on a tie, strict
+ * improvement to update).  edges: (n - 1) x 3 doubles (source, point,
+ * distance) in the order added.  Host code, no stream; n >= 2. */
+int dsb_cluster_mst(const double* X, int n, int d, int min_samples, double* core,
+                    double* edges);
+
 #ifdef __cplusplus
 }
 #endif
