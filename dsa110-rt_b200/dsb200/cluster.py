@@ -484,6 +484,9 @@ def cluster_candidates(cands: Sequence, geom, *, config: Optional[ClustererConfi
                        ) -> Tuple[np.ndarray, List[ClusterRecord]]:
     """``(labels, records)`` of one cube's candidates (forward.py:153-238)."""
     cfg = config or ClustererConfig()
+    if cfg.metric not in ("manhattan", "cityblock", "l1"):
+        raise ValueError(f"metric={cfg.metric!r}: only the cityblock (manhattan) distance "
+                         f"of the reference's configuration is implemented")
     if not cands:
         return np.zeros(0, np.int64), []
     X = candidates_to_features(cands, geom, mode=cfg.feature_mode, weights=cfg.weights)

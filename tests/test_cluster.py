@@ -195,6 +195,8 @@ def test_feature_errors_and_clamps():
         CL.candidates_to_features([_cand(width=0)], g)
     with pytest.raises(ValueError):
         CL.cluster_candidates([_cand(), _cand()], g, config=CL.ClustererConfig(backend="x"))
+    with pytest.raises(ValueError):
+        CL.cluster_candidates([_cand(), _cand()], g, config=CL.ClustererConfig(metric="euclidean"))
     assert CL.candidates_to_features([], g).shape == (0, 5)
     lo = Cand(10.0, 20.0, 1.0, 1024, 4, 9.0)
     hi = Cand(10.0, 20.0, 9999.0, 1024, 4, 9.0)
