@@ -419,6 +419,9 @@ def main():
     clk = clocks.stop()
     barrier()
     ms = ev0.elapsed_time(ev1)
+    # a kernel that flagged an error (capacity, bound, bounded wait) makes the
+    # run fail here rather than report a number
+    pipe.check_status()
     launches = (pipe.launches - launches0) // max(1, a.steps)
     stages = pipe.stage_times_ms()
     if world > 1:
@@ -448,6 +451,7 @@ def main():
             pass
         ev1.record()
         torch.cuda.synchronize()
+        pipe.check_status()
         ms_e = ev0.elapsed_time(ev1)
         if world > 1:
             t = torch.tensor([ms_e], device=dev)
