@@ -401,6 +401,18 @@ def main():
             pipe.process_block(blocks[i % len(blocks)])
         pipe.timing = False
 
+    def check_all(p):
+        """The device status word, agreed on by every rank before any raises."""
+        code = int(p.status.item())
+        if world > 1:
+            t = torch.tensor([code], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            code = int(t.item())
+        if code:
+            from dsb200 import _lib
+            raise _lib.DsbError(f"pipeline: {_lib.lib().dsb_strerror(code).decode()} "
+                                f"(code {code})")
+
     # warm-up
     run(a.warmup)
     torch.cuda.synchronize()
@@ -420,8 +432,8 @@ def main():
     barrier()
     ms = ev0.elapsed_time(ev1)
     # a kernel that flagged an error (capacity, bound, bounded wait) makes the
-    # run fail here rather than report a number
-    pipe.check_status()
+    # run fail here rather than report a number (on every rank alike)
+    check_all(pipe)
     launches = (pipe.launches - launches0) // max(1, a.steps)
     stages = pipe.stage_times_ms()
     if world > 1:
@@ -451,7 +463,7 @@ def main():
             pass
         ev1.record()
         torch.cuda.synchronize()
-        pipe.check_status()
+        check_all(pipe)
         ms_e = ev0.elapsed_time(ev1)
         if world > 1:
             t = torch.tensor([ms_e], device=dev)
