@@ -30,6 +30,24 @@ sys.path[:0] = [os.path.join(ROOT, "dsa110-rt_b200"), os.path.join(ROOT, "oracle
 METRIC = "real-time factor at 96-ant/6144-ch/2048-DM (data-seconds per second)"
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """x on this rank -> the largest x of all ranks (every rank calls it at
+    the same point; one rank returns x itself)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def agreed_status(code: int, world: int, device) -> int:
+    """A device status code agreed on by every rank (the largest), so that
+    all ranks raise together or none does."""
+    return int(max_over_ranks(code, world, device))
+
+
 def metric_for(cfg) -> str:
     """The metric's name with the workload's DM count (2048 for the default
     workload, the name above)."""
@@ -403,11 +421,7 @@ def main():
 
     def check_all(p):
         """The device status word, agreed on by every rank before any raises."""
-        code = int(p.status.item())
-        if world > 1:
-            t = torch.tensor([code], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            code = int(t.item())
+        code = agreed_status(int(p.status.item()), world, dev)
         if code:
             from dsb200 import _lib
             raise _lib.DsbError(f"pipeline: {_lib.lib().dsb_strerror(code).decode()} "
@@ -436,10 +450,7 @@ def main():
     check_all(pipe)
     launches = (pipe.launches - launches0) // max(1, a.steps)
     stages = pipe.stage_times_ms()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dev)
     ms_step = ms / a.steps
     value = world * cfg.block_seconds * a.steps / (ms / 1e3)
 
@@ -465,10 +476,7 @@ def main():
         torch.cuda.synchronize()
         check_all(pipe)
         ms_e = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms_e], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e = float(t.item())
+        ms_e = max_over_ranks(ms_e, world, dev)
         lat = np.asarray(pipe.block_latency_s) * 1e3
         e2e = {"value": world * cfg.block_seconds * a.steps / (ms_e / 1e3),
                "unit": "data-seconds/s", "h2d_bytes_per_step": int(block_bytes),
