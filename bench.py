@@ -110,7 +110,10 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples: DSB_CLOCKS_DIR when set, else the temp directory
+        import tempfile
+        self.path = os.path.join(os.environ.get("DSB_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
