@@ -54,6 +54,8 @@ _SIGNATURES = {
                           _c_int, _c_int, _c_int, _c_int, _vp],
     "dsb_encode_rows": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp, _vp],
     "dsb_cluster_mst": [_vp, _c_int, _c_int, _c_int, _vp, _vp],
+    "dsb_cal_apply": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                      _vp, _vp, _vp],
     "dsb_ring_encode_cint8": [_vp, _vp, _c_int, _vp, _vp, _c_int, _c_int, _vp, _c_ll, _vp, _vp,
                               _vp, _vp, _vp, _vp, _vp],
     "dsb_rfi_zero_fill": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_int, _vp],

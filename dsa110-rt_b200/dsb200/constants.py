@@ -6,6 +6,7 @@ defaults of a parametric ``Band`` and of the kernel geometry arguments.
 
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -20,6 +21,8 @@ NCHAN_PER_CHGROUP = 384                   # constants.py:70
 N_CHGROUP = 16                            # constants.py:67
 K_DM_MS_GHZ2_PC = 4.148808                # constants.py:163
 SPEED_OF_LIGHT_M_S = 299_792_458.0        # constants.py:178
+PHI_LAT_OVRO_DEG = 37.234                 # constants.py:187
+PHI_LAT_OVRO_RAD = math.radians(PHI_LAT_OVRO_DEG)
 LEGACY_FLUFF_SCALE = 0.05                 # constants.py:373
 T_INT_FAST_NATIVE = 8
 

@@ -75,6 +75,82 @@ def unpack_int4_split(
     return re, im
 
 
+def apply_cal_split(real_v: torch.Tensor, imag_v: torch.Tensor, cal_real_fine: torch.Tensor,
+                    cal_imag_fine: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Per-(antenna, fine channel, pol) complex gain on split voltages
+    (slow_corr_kernel.py:459-528): ``real*g_re - imag*g_im``,
+    ``real*g_im + imag*g_re`` on the GEMM layout ``(nchan, 2, 2, npkt,
+    nant)``, gains ``(1 or nchan, 1, 2, 1, nant)``; float16 or float32, the
+    reference's eager rounding; new output tensors."""
+    if real_v.shape != imag_v.shape:
+        raise ValueError(f"real_v shape {tuple(real_v.shape)} != imag_v shape "
+                         f"{tuple(imag_v.shape)}")
+    if real_v.dim() != 5 or real_v.shape[1] != NTIMES_PER_PACKET or real_v.shape[2] != NPOL:
+        raise ValueError(f"voltage shape {tuple(real_v.shape)} is not the GEMM layout "
+                         f"(nchan, {NTIMES_PER_PACKET}, {NPOL}, npkt, nant)")
+    if real_v.dtype != imag_v.dtype:
+        raise ValueError(f"real_v dtype {real_v.dtype} != imag_v dtype {imag_v.dtype}")
+    if cal_real_fine.dtype != real_v.dtype or cal_imag_fine.dtype != real_v.dtype:
+        raise ValueError(f"cal dtypes ({cal_real_fine.dtype}, {cal_imag_fine.dtype}) != "
+                         f"voltage dtype {real_v.dtype}")
+    if cal_real_fine.device != real_v.device or cal_imag_fine.device != real_v.device:
+        raise ValueError(f"cal devices ({cal_real_fine.device}, {cal_imag_fine.device}) != "
+                         f"voltage device {real_v.device}")
+    if real_v.dtype not in (torch.float16, torch.float32):
+        raise ValueError(f"voltage dtype {real_v.dtype}: float16 or float32 expected")
+    nchan, nt, npol, npkt, nant = real_v.shape
+    gsh = tuple(cal_real_fine.shape)
+    if cal_imag_fine.shape != cal_real_fine.shape or gsh not in (
+            (1, 1, npol, 1, nant), (nchan, 1, npol, 1, nant)):
+        raise ValueError(f"cal shape {gsh}: (1 or {nchan}, 1, {npol}, 1, {nant}) expected")
+    dev = _lib.cuda_device(real_v.device)
+    args = [t.contiguous() for t in (real_v, imag_v, cal_real_fine, cal_imag_fine)]
+    out_re = torch.empty_like(args[0])
+    out_im = torch.empty_like(args[0])
+    _lib.check(_lib.lib().dsb_cal_apply(
+        _lib.ptr(args[0]), _lib.ptr(args[1]), _lib.ptr(args[2]), _lib.ptr(args[3]),
+        int(real_v.dtype == torch.float16), nchan, nt, npol, npkt, nant, gsh[0],
+        _lib.ptr(out_re), _lib.ptr(out_im), _lib.stream_of(dev)), "dsb_cal_apply")
+    return out_re, out_im
+
+
+def make_cal_broadcast_tensors(gains_fine: np.ndarray, *, device="cuda",
+                               dtype: torch.dtype = torch.float16
+                               ) -> Tuple[torch.Tensor, torch.Tensor]:
+    """``(nant, nchan, npol)`` complex gains -> ``(cal_real, cal_imag)`` of
+    shape ``(nchan, 1, npol, 1, nant)`` (slow_corr_kernel.py:531-569): the
+    float64 parts converted to ``dtype`` once, then permuted."""
+    g = np.asarray(gains_fine)
+    if g.ndim != 3 or g.shape[2] != NPOL:
+        raise ValueError(f"gains_fine shape {g.shape}, expected (nant, nchan, {NPOL})")
+    out = []
+    for part in (np.ascontiguousarray(g.real), np.ascontiguousarray(g.imag)):
+        t = torch.from_numpy(part).to(device=device, dtype=dtype)
+        out.append(t.permute(1, 2, 0).contiguous().unsqueeze(1).unsqueeze(3))
+    return out[0], out[1]
+
+
+def compute_dec_phase(*, chgroup: int, obs_dec_rad: float, antpos_n: np.ndarray,
+                      band=None) -> np.ndarray:
+    """DEC-only fringe-stop phase per (antenna, channel), complex128
+    (cal/cal_loader.py:209-290): exp(-2 pi i f sin(dec - lat) N_a / c),
+    cos and sin taken separately, in the reference's order of operations."""
+    import math
+
+    from .constants import DSA110_BAND, PHI_LAT_OVRO_RAD, SPEED_OF_LIGHT_M_S
+    band = DSA110_BAND if band is None else band
+    if not 0 <= chgroup < band.n_chgroup:
+        raise ValueError(f"chgroup={chgroup}, expected 0..{band.n_chgroup - 1}")
+    n_a = np.asarray(antpos_n)
+    if n_a.ndim != 1:
+        raise ValueError(f"antpos_n shape {n_a.shape}, expected (nants,)")
+    sin_delta = math.sin(obs_dec_rad - PHI_LAT_OVRO_RAD)
+    f_hz = band.freq_table()[chgroup].astype(np.float64) * 1.0e9
+    arg = (-2.0 * math.pi * sin_delta / SPEED_OF_LIGHT_M_S
+           * f_hz[None, :] * n_a.astype(np.float64, copy=False)[:, None])
+    return (np.cos(arg) + 1j * np.sin(arg)).astype(np.complex128)
+
+
 def apply_rfi_mask_to_raw(raw: torch.Tensor, rfi_mask: Optional[torch.Tensor] = None, *,
                           time_chan_mask: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Zero flagged voltages in raw on-wire pages, in place: the RFI

@@ -375,6 +375,19 @@ int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, i
                      const int* times, int n_times, const int* pix, int n_pix, float n_sigma,
                      int n_iter, float* sigma, cudaStream_t stream);
 
+/* ---- a3: per-antenna complex gains on split voltages ---------------------------
+ * Replaces apply_cal_split (src/dsart/services/slow_corr_kernel.py:459-528,
+ * eager form :417-423): out_re = re*g_re - im*g_im, out_im = re*g_im + im*g_re
+ * on voltages (nchan, ntimes, npol, npkt, nant) with gains (gain_nchan, 1,
+ * npol, 1, nant), gain_nchan 1 or nchan (broadcast), all contiguous, float16
+ * (dtype_f16 = 1) or float32.  Rounded as the reference's eager tensor ops:
+ * half products rounded to half, their sum / difference taken in float32
+ * and rounded to half; float32 without fused multiply-adds.  Writes new
+ * out_re, out_im (not in place). */
+int dsb_cal_apply(const void* re, const void* im, const void* gain_re, const void* gain_im,
+                  int dtype_f16, int nchan, int ntimes, int npol, int npkt, int nant,
+                  int gain_nchan, void* out_re, void* out_im, cudaStream_t stream);
+
 /* ---- next row: per-cube clusterer (host) ------------------------------------
  * The minimum spanning tree of the HDBSCAN backend that cluster/forward.py:103
  * runs through the hdbscan package: X (n, d) float64 row-major feature rows,

@@ -172,6 +172,43 @@ def rfi_zero_fill_raw(page: np.ndarray, rfi_mask: Optional[np.ndarray],
 
 
 # ---------------------------------------------------------------------------
+# a3: per-antenna complex gains (services/slow_corr_kernel.py:417-569,
+# cal/cal_loader.py:209-290)
+# ---------------------------------------------------------------------------
+
+
+def apply_cal_split(re: np.ndarray, im: np.ndarray, g_re: np.ndarray, g_im: np.ndarray
+                    ) -> Tuple[np.ndarray, np.ndarray]:
+    """``_apply_cal_split_eager`` (slow_corr_kernel.py:417-423) one array op
+    at a time in the arrays' dtype: numpy's float16 arithmetic, like torch's,
+    computes each op in float32 and rounds the result to half."""
+    out_re = re * g_re - im * g_im
+    out_im = re * g_im + im * g_re
+    return out_re, out_im
+
+
+def make_cal_broadcast(gains_fine: np.ndarray, dtype=np.float16) -> Tuple[np.ndarray, np.ndarray]:
+    """``make_cal_broadcast_tensors`` (slow_corr_kernel.py:531-569): parts
+    of ``(nant, nchan, npol)`` gains -> ``(nchan, 1, npol, 1, nant)``."""
+    out = []
+    for part in (np.ascontiguousarray(gains_fine.real), np.ascontiguousarray(gains_fine.imag)):
+        out.append(part.astype(dtype).transpose(1, 2, 0)[:, None, :, None, :].copy())
+    return out[0], out[1]
+
+
+def dec_phase(band: Band, chgroup: int, obs_dec_rad: float, antpos_n: np.ndarray,
+              lat_rad: float, c_m_s: float = 299_792_458.0) -> np.ndarray:
+    """``compute_dec_phase`` (cal_loader.py:209-290): exp(-2 pi i f sin(dec -
+    lat) N_a / c) per (antenna, channel), complex128."""
+    import math
+    sin_delta = math.sin(obs_dec_rad - lat_rad)
+    f_hz = band.freq_table()[chgroup].astype(np.float64) * 1.0e9
+    arg = -2.0 * math.pi * sin_delta / c_m_s * f_hz[None, :] * np.asarray(
+        antpos_n, np.float64)[:, None]
+    return (np.cos(arg) + 1j * np.sin(arg)).astype(np.complex128)
+
+
+# ---------------------------------------------------------------------------
 # a4: fast correlator (services/corr_fast_kernel.py:364-755)
 # ---------------------------------------------------------------------------
 

@@ -428,6 +428,54 @@ def make_transport():
                         s16=np.asarray(s16), q32=np.asarray(q32), s32=np.asarray(s32))
 
 
+CAL_SEED = 4242
+
+
+def cal_inputs(seed: int = CAL_SEED):
+    """Seeded split voltages (nchan 8, 2, 2, npkt 4, nant 96) float16 (the
+    fluffed int4 values x 0.05), complex gains (96, 8, 2) of spread
+    magnitude and phase, and N-S antenna positions (96,) m."""
+    rng = np.random.default_rng(seed)
+    shape = (8, 2, 2, 4, 96)
+    re = (rng.integers(-8, 8, shape) * 0.05).astype(np.float16)
+    im = (rng.integers(-8, 8, shape) * 0.05).astype(np.float16)
+    amp = 10.0 ** rng.uniform(-1, 1, (96, 8, 2))
+    gains = amp * np.exp(1j * rng.uniform(-np.pi, np.pi, (96, 8, 2)))
+    gains[0] = 1.0                                # one antenna at unit gain
+    antpos_n = rng.uniform(-800.0, 800.0, 96)
+    return re, im, gains, antpos_n
+
+
+def make_cal():
+    """apply_cal_split's eager form (slow_corr_kernel.py:417-423) on CPU
+    float16 and float32 tensors, per-channel and broadcast (1-channel) gains,
+    make_cal_broadcast_tensors (:531-569), and compute_dec_phase
+    (cal/cal_loader.py:209) for chgroup 5 at two declinations."""
+    import torch
+
+    from dsart.cal.cal_loader import compute_dec_phase
+    from dsart.services.slow_corr_kernel import _apply_cal_split_eager
+    re, im, gains, antpos_n = cal_inputs()
+    out = {}
+    for dt, name in ((torch.float16, "f16"), (torch.float32, "f32")):
+        r = torch.from_numpy(re.astype(np.float32)).to(dt)
+        i = torch.from_numpy(im.astype(np.float32)).to(dt)
+        gr = torch.from_numpy(np.ascontiguousarray(gains.real)).to(dt)
+        gi = torch.from_numpy(np.ascontiguousarray(gains.imag)).to(dt)
+        gr = gr.permute(1, 2, 0).contiguous().unsqueeze(1).unsqueeze(3)   # (8, 1, 2, 1, 96)
+        gi = gi.permute(1, 2, 0).contiguous().unsqueeze(1).unsqueeze(3)
+        out[f"g_re_{name}"], out[f"g_im_{name}"] = gr.numpy(), gi.numpy()
+        o_re, o_im = _apply_cal_split_eager(r, i, gr, gi)
+        out[f"out_re_{name}"], out[f"out_im_{name}"] = o_re.numpy(), o_im.numpy()
+        b_re, b_im = _apply_cal_split_eager(r, i, gr[5:6], gi[5:6])      # one channel's gains
+        out[f"bout_re_{name}"], out[f"bout_im_{name}"] = b_re.numpy(), b_im.numpy()
+    for k, dec in enumerate((0.2, 1.3)):
+        ph = compute_dec_phase(chgroup=5, obs_dec_rad=dec, antpos_n=antpos_n)
+        out[f"dec_phase_sha_{k}"] = np.asarray(sha(ph.view(np.float64)))
+        out[f"dec_phase_cols_{k}"] = ph[:, ::16]
+    np.savez_compressed(os.path.join(HERE, "cal.npz"), **out)
+
+
 CLUSTER_SEED = 7171
 
 
@@ -523,7 +571,7 @@ def main():
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
             make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
-            make_cluster]
+            make_cluster, make_cal]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
