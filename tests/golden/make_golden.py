@@ -428,6 +428,54 @@ def make_transport():
                         s16=np.asarray(s16), q32=np.asarray(q32), s32=np.asarray(s32))
 
 
+LAYER2_SEED = 5353
+
+LAYER2_CONFIGS = (
+    dict(n_burnin=5),
+    dict(n_burnin=3, sigma_floor=0.9, sigma_max_ratio=1.5, clamp_escape_cubes=4),
+    dict(n_burnin=2, sigma_floor=(0.5, 0.8, 1.1, 0.2, 0.0), sigma_max_ratio=2.0,
+         clamp_escape_cubes=0, tau_s=3.0),
+)
+
+
+def layer2_sequence(seed: int = LAYER2_SEED, n_cubes: int = 60, n_k: int = 5):
+    """Seeded per-kernel σ estimates for ``n_cubes`` cubes: noise around 1,
+    some zeros (no estimate), a two-cube spike and a lasting level rise on
+    kernel 2 (clamp and escape), and invalid cubes."""
+    rng = np.random.default_rng(seed)
+    sig = (1.0 + 0.05 * rng.standard_normal((n_cubes, n_k))).astype(np.float32)
+    sig[rng.random((n_cubes, n_k)) < 0.05] = 0.0
+    sig[10:12, 1] *= 3.0
+    sig[20:, 2] *= 2.5
+    valid = rng.random(n_cubes) > 0.1
+    return sig, valid
+
+
+def make_layer2():
+    """Layer2State.update_and_query(per_kernel_sigma=) (noise_norm/layer2.py:
+    113-452) on CPU over a seeded sequence, for three configurations."""
+    import torch
+
+    from dsart.noise_norm.layer2 import Layer2State
+    sig, valid = layer2_sequence()
+    out = {}
+    for ci, cfg in enumerate(LAYER2_CONFIGS):
+        st = Layer2State(sig.shape[1], **cfg)
+        s_k, warm = [], []
+        for c in range(sig.shape[0]):
+            s, w = st.update_and_query(per_kernel_sigma=torch.from_numpy(sig[c]),
+                                       valid=bool(valid[c]))
+            s_k.append(s.numpy())
+            warm.append(w)
+        out[f"s_k_{ci}"] = np.asarray(s_k, np.float32)
+        out[f"warm_{ci}"] = np.asarray(warm, bool)
+        out[f"counters_{ci}"] = np.asarray([st.n_clamped_high, st.n_clamp_escapes, st.cube_count])
+        out[f"per_kernel_{ci}"] = np.stack([st.per_kernel_clamped_high.numpy(),
+                                            st.per_kernel_clamp_escapes.numpy(),
+                                            st.per_kernel_clamp_streak.numpy()])
+    np.savez_compressed(os.path.join(HERE, "layer2.npz"), **out)
+
+
 CAL_SEED = 4242
 
 
@@ -571,7 +619,7 @@ def main():
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
             make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
-            make_cluster, make_cal]
+            make_cluster, make_cal, make_layer2]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
