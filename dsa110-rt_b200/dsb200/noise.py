@@ -1,4 +1,11 @@
-"""Layer-2 per-kernel noise state (noise_norm/layer2.py:113-452 of the
+"""Noise-state trackers of the detector's normalisation.
+
+Layer-1 (noise_norm/layer1.py:342-600): per fine DM, a ring of the last
+``n_burnin_cubes`` σ values; during the first ``n_burnin_cubes`` cubes the
+σ used is the median of the ring so far, afterwards the cube's own σ; an
+optional floor.
+
+Layer-2 per-kernel noise state (noise_norm/layer2.py:113-452 of the
 reference): one σ_k per detector kernel, a Welford running mean over the
 first ``n_burnin`` cubes, then an EMA with γ = 1 − exp(−cube_cadence_s /
 τ_s).  Each cube's σ_k estimate comes in through
@@ -20,15 +27,80 @@ materialises per-kernel score cubes; callers pass ``per_kernel_sigma``.
 from __future__ import annotations
 
 import math
+from collections import deque
 from typing import Optional, Tuple
 
+import numpy as np
 import torch
+
+NOISE_LAYER1_N_BURNIN_CUBES_DEFAULT = 5         # constants.py:556
 
 T_INT_SEARCH_US_DEFAULT = 16 * 32.768         # constants.py:533
 CUBE_CADENCE_S_DEFAULT = 256 * T_INT_SEARCH_US_DEFAULT * 1e-6   # constants.py:538-548
 NOISE_LAYER2_TAU_S_DEFAULT = 30.0              # constants.py:564
 NOISE_LAYER2_N_BURNIN_DEFAULT = 30             # constants.py:571
 N_KERNEL_MAX_T_DEFAULT = 128                   # constants.py:550
+
+
+class Layer1State:
+    """Per-fine-DM Layer-1 σ with the cold-start burn-in (layer1.py:342)."""
+
+    def __init__(self, n_fdm: int, *, n_burnin_cubes: int = NOISE_LAYER1_N_BURNIN_CUBES_DEFAULT,
+                 sigma_floor: float = 0.0):
+        if n_fdm < 1:
+            raise ValueError(f"n_fdm={n_fdm}, expected ≥ 1")
+        if n_burnin_cubes < 1:
+            raise ValueError(f"n_burnin_cubes={n_burnin_cubes}, expected ≥ 1")
+        if sigma_floor < 0.0:
+            raise ValueError(f"sigma_floor={sigma_floor}, expected ≥ 0")
+        self.n_fdm = int(n_fdm)
+        self.n_burnin_cubes = int(n_burnin_cubes)
+        self.sigma_floor = float(sigma_floor)
+        self._history = [deque(maxlen=self.n_burnin_cubes) for _ in range(self.n_fdm)]
+        self._cube_count = 0
+
+    @property
+    def cube_count(self) -> int:
+        return self._cube_count
+
+    @property
+    def is_warming_up(self) -> bool:
+        return self._cube_count < self.n_burnin_cubes
+
+    def reset(self) -> None:
+        for d in self._history:
+            d.clear()
+        self._cube_count = 0
+
+    def update_and_query(self, cube: Optional[torch.Tensor] = None, *,
+                         per_fdm_sigma: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Push this cube's per-fine-DM σ (``dsb200.search.layer1_sigma``
+        computes it from the images) and return the σ to normalise this
+        cube with (layer1.py:537-600)."""
+        if cube is not None:
+            raise NotImplementedError(
+                "pass per_fdm_sigma (dsb200.search.layer1_sigma gathers it from the images)")
+        if per_fdm_sigma is None:
+            raise ValueError("pass exactly one of cube= or per_fdm_sigma=")
+        sig = per_fdm_sigma.to(torch.float32)
+        if sig.shape != (self.n_fdm,):
+            raise ValueError(f"per-fdm sigma shape {tuple(sig.shape)} != (n_fdm={self.n_fdm},)")
+        device = sig.device
+        vals = sig.detach().cpu().numpy()
+        for f in range(self.n_fdm):
+            self._history[f].append(float(vals[f]))
+        if self._cube_count < self.n_burnin_cubes:
+            out = np.empty(self.n_fdm, dtype=np.float32)
+            for f in range(self.n_fdm):
+                out[f] = float(np.median(list(self._history[f])))
+            self._cube_count += 1
+            out_t = torch.from_numpy(out).to(device)
+        else:
+            self._cube_count += 1
+            out_t = sig
+        if self.sigma_floor > 0.0:
+            out_t = out_t.clamp_min(float(self.sigma_floor))
+        return out_t
 
 
 class Layer2State:

@@ -451,6 +451,22 @@ def layer2_sequence(seed: int = LAYER2_SEED, n_cubes: int = 60, n_k: int = 5):
     return sig, valid
 
 
+def make_layer1_state():
+    """Layer1State.update_and_query(per_fdm_sigma=) (noise_norm/layer1.py:
+    342-600) over the first 12 cubes of the seeded sequence (its 5 columns
+    as fine DMs), with and without a floor."""
+    import torch
+
+    from dsart.noise_norm.layer1 import Layer1State
+    sig, _ = layer2_sequence()
+    out = {}
+    for ci, kw in enumerate((dict(), dict(n_burnin_cubes=3, sigma_floor=0.97))):
+        st = Layer1State(sig.shape[1], **kw)
+        out[f"l1_{ci}"] = np.asarray([st.update_and_query(
+            per_fdm_sigma=torch.from_numpy(sig[c])).numpy() for c in range(12)], np.float32)
+    np.savez_compressed(os.path.join(HERE, "layer1_state.npz"), **out)
+
+
 def make_layer2():
     """Layer2State.update_and_query(per_kernel_sigma=) (noise_norm/layer2.py:
     113-452) on CPU over a seeded sequence, for three configurations."""
@@ -619,7 +635,7 @@ def main():
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
             make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
-            make_cluster, make_cal, make_layer2]
+            make_cluster, make_cal, make_layer2, make_layer1_state]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue

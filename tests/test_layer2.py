@@ -1,4 +1,5 @@
-"""Layer-2 per-kernel noise state (noise_norm/layer2.py:113-452): the
+"""Layer-1 burn-in and Layer-2 per-kernel noise state (noise_norm/layer1.py:
+342-600, noise_norm/layer2.py:113-452).  Layer-2: the
 Welford burn-in, the EMA, zero estimates, invalid cubes, the clamp above
 ``sigma_max_ratio`` with its escape hatch, and scalar and per-kernel floors
 equal the reference's state on CPU bit for bit over a seeded sequence of
@@ -53,3 +54,19 @@ def test_layer2_arguments_and_reset():
     assert torch.equal(s, torch.tensor([2.0, 3.0, 4.0])) and w
     st.reset()
     assert st.cube_count == 0 and torch.equal(st.s_k, torch.ones(3))
+
+
+@pytest.mark.parametrize("ci,kw", [(0, dict()), (1, dict(n_burnin_cubes=3, sigma_floor=0.97))])
+def test_layer1_state_matches_reference(golden_dir, ci, kw):
+    """Layer1State (noise_norm/layer1.py:342-600): burn-in medians, then the
+    cube's own σ, and the floor, bit for bit."""
+    from dsb200.noise import Layer1State
+    z = np.load(os.path.join(golden_dir, "layer1_state.npz"))
+    sig, _ = MG.layer2_sequence()
+    st = Layer1State(sig.shape[1], **kw)
+    got = np.asarray([st.update_and_query(per_fdm_sigma=torch.from_numpy(sig[c])).numpy()
+                      for c in range(12)], np.float32)
+    assert np.array_equal(got.view(np.uint32), z[f"l1_{ci}"].view(np.uint32))
+    assert not st.is_warming_up and st.cube_count == 12
+    with pytest.raises(ValueError):
+        st.update_and_query(per_fdm_sigma=torch.ones(2))
