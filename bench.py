@@ -58,10 +58,11 @@ def workload_config(name: str):
     from dsb200.constants import DSA110_BAND
     from dsb200.pipeline import PipelineConfig
     if name == "dsa110-2048dm":
-        # the metric's 96 antennas / 6144 channels / 2048 DMs, with the full
-        # DSA-110 shape's imaging: 256^2 grid, 0-2000 pc/cm^3, boxcars 1..16
+        # the metric's 96 antennas / 6144 channels / 2048 DMs over its 0-3000
+        # pc/cm^3, with the full DSA-110 shape's imaging: 256^2 grid,
+        # boxcars 1..16
         return PipelineConfig(nant=96, band=DSA110_BAND, npkt_block=8192, t_int=8, csf=16,
-                              n_grid=256, coarse_dm=np.linspace(0.0, 2000.0, 128),
+                              n_grid=256, coarse_dm=np.linspace(0.0, 3000.0, 128),
                               fine_per_coarse=16, log_max_width=4, threshold=7.0,
                               chunk_tiles=512, fdm_batch=32)
     if name == "dsa110-512dm":
