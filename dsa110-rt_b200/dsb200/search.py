@@ -135,6 +135,118 @@ def mask_into_cube(img: torch.Tensor, mask: torch.Tensor, cube: torch.Tensor, f0
         _lib.stream_of(img.device)), "dsb_mask_to_cube")
 
 
+@dataclass
+class GpuImagerConfig:
+    """GPU imager geometry (image/imager_gpu.py:74-117 defaults).  The
+    spectrum is complex64 and the transform float32 here (the reference's
+    default is complex32); ``cube_dtype`` is the output cube's."""
+
+    n_grid: int = 256
+    t_det: int = 256
+    n_fdm: int = 32
+    n_chgroup: int = 16
+    kernel_support: int = 5
+    sigma_l_pix: Optional[float] = None
+    envelope_threshold: float = 0.5
+    drop_dc: bool = True
+    cube_dtype: torch.dtype = torch.float16
+    complex_dtype: torch.dtype = torch.complex64
+    device: Optional[torch.device] = None
+    imager_uv_prescale: float = 1.0
+
+    def resolved_device(self) -> torch.device:
+        return _lib.cuda_device(self.device if self.device is not None else "cuda")
+
+
+class GpuImager:
+    """Stateful imager for one cube of dense cint8 streams
+    (image/imager_gpu.py:123-790): per fine DM the half-spectrum combine
+    (``fused_dequant_combine_per_fdm_half``, fftshift folded in), the
+    inverse real FFT, and the edge mask (or the per-fine-DM mask of
+    ``set_edge_mask_per_fdm``) into ``output_cube [t_det, n_fdm, N, N]``;
+    two output cubes alternate, so a returned cube stays valid until the
+    next-but-one call.  The streaming pipeline itself uses the fused
+    ``dsb_image_fft`` path instead."""
+
+    def __init__(self, config: GpuImagerConfig, device: torch.device, edge_mask_real, output_cube,
+                 output_cube_alt, uv_slab):
+        self.config = config
+        self.device = device
+        self.edge_mask_real = edge_mask_real
+        self.edge_mask_per_fdm: Optional[torch.Tensor] = None
+        self.output_cube = output_cube
+        self.output_cube_alt = output_cube_alt
+        self.uv_slab = uv_slab
+        self._flip = False
+
+    @classmethod
+    def build(cls, config: GpuImagerConfig) -> "GpuImager":
+        """Allocate the persistent buffers and the edge mask (no compute)."""
+        if config.complex_dtype != torch.complex64:
+            raise ValueError("this imager transforms in float32: complex_dtype must be complex64")
+        dev = config.resolved_device()
+        N = config.n_grid
+        edge = compute_edge_mask(n_grid=N, kernel_support=config.kernel_support,
+                                 sigma_l_pix=config.sigma_l_pix,
+                                 envelope_threshold=config.envelope_threshold,
+                                 drop_dc=config.drop_dc)
+        edge_t = torch.from_numpy(edge).to(device=dev, dtype=torch.float32)
+        shape = (config.t_det, config.n_fdm, N, N)
+        out = torch.empty(shape, dtype=config.cube_dtype, device=dev)
+        out_alt = torch.empty(shape, dtype=config.cube_dtype, device=dev)
+        uv = torch.empty((config.t_det, N, N // 2 + 1), dtype=torch.complex64, device=dev)
+        return cls(config, dev, edge_t, out, out_alt, uv)
+
+    def set_edge_mask_per_fdm(self, sigma_inv: Optional[torch.Tensor]) -> None:
+        """``edge_mask * sigma_inv[f]`` per fine DM (the Layer-1 divide fused
+        into the mask), or back to the common mask with None
+        (imager_gpu.py:724-790)."""
+        if sigma_inv is None:
+            self.edge_mask_per_fdm = None
+            return
+        if sigma_inv.shape != (self.config.n_fdm,):
+            raise ValueError(f"sigma_inv.shape={tuple(sigma_inv.shape)}, expected "
+                             f"({self.config.n_fdm},)")
+        self.edge_mask_per_fdm = (self.edge_mask_real[None, :, :] *
+                                  sigma_inv.to(self.device, torch.float32)[:, None, None]
+                                  ).contiguous()
+
+    def process_cube(self, *, streams_cint8: torch.Tensor, time_shifts_gpu: torch.Tensor,
+                     chgroup_scales: Optional[torch.Tensor] = None,
+                     chgroup_offsets_re: Optional[torch.Tensor] = None,
+                     chgroup_offsets_im: Optional[torch.Tensor] = None, t_lo: int = 0,
+                     compact_inv_lut: Optional[torch.Tensor] = None, compact_t_stream: int = 0,
+                     compact_shift_bounds: Optional[tuple] = None) -> torch.Tensor:
+        """One cube: ``streams_cint8 [G, T_stream, 2, N, N]`` int8 and
+        ``time_shifts_gpu [n_fdm, G]`` int32 -> ``[t_det, n_fdm, N, N]``
+        (imager_gpu.py:217-657).  The compact-layout combine is not built."""
+        cfg = self.config
+        if compact_inv_lut is not None:
+            raise NotImplementedError("the compact-layout combine is not built; pass dense streams")
+        if time_shifts_gpu.shape != (cfg.n_fdm, streams_cint8.shape[0]):
+            raise ValueError(f"time_shifts_gpu shape {tuple(time_shifts_gpu.shape)}, expected "
+                             f"({cfg.n_fdm}, {streams_cint8.shape[0]})")
+        N = cfg.n_grid
+        n_t = cfg.t_det - t_lo
+        uv = self.uv_slab[:n_t]
+        cube = self.output_cube_alt if self._flip else self.output_cube
+        self._flip = not self._flip
+        shifts = time_shifts_gpu.to(torch.int32).contiguous()
+        for f in range(cfg.n_fdm):
+            fused_dequant_combine_per_fdm_half(streams_cint8, shifts[f], uv,
+                                               scales=chgroup_scales,
+                                               offsets_re=chgroup_offsets_re,
+                                               offsets_im=chgroup_offsets_im, t_lo=t_lo,
+                                               fftshift=True)
+            if cfg.imager_uv_prescale != 1.0:
+                uv.mul_(cfg.imager_uv_prescale)
+            img = irfft2_image(uv, N)[None]                    # (1, n_t, N, N)
+            mask = (self.edge_mask_real if self.edge_mask_per_fdm is None
+                    else self.edge_mask_per_fdm[f:f + 1])
+            mask_into_cube(img.contiguous(), mask, cube[t_lo:] if t_lo else cube, f)
+        return cube
+
+
 # ---------------------------------------------------------------------------
 # detector
 # ---------------------------------------------------------------------------
