@@ -33,7 +33,7 @@ from __future__ import annotations
 import math
 import time
 from dataclasses import dataclass, field
-from typing import Iterable, Iterator, List, Optional, Tuple
+from typing import Iterable, Iterator, List, Optional
 
 import numpy as np
 import torch
@@ -43,8 +43,7 @@ from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
 from .corr import apply_rfi_mask_to_raw
 from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
 from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
-from .search import (CandidateBuffer, _nms, compute_edge_mask, detect_images, irfft2_image,
-                     layer1_sigma)
+from .search import CandidateBuffer, _nms, compute_edge_mask, detect_images, layer1_sigma
 
 
 def _pow2_at_least(n: int) -> int:

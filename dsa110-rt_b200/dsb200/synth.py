@@ -16,7 +16,7 @@ conventions (V_ab = conj(E_b) E_a, u = -(e_a - e_b)/lambda, row = v).
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import List, Sequence
+from typing import Sequence
 
 import numpy as np
 import torch

@@ -33,7 +33,7 @@ Geometry is parametric (the reference hard-codes 96 antennas and
 from __future__ import annotations
 
 from collections import deque
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np

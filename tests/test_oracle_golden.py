@@ -12,7 +12,6 @@ import os
 import sys
 
 import numpy as np
-import pytest
 
 import dsb_oracle as O
 

@@ -13,8 +13,6 @@ inputs.  The file sorts last so that it also runs after every other test
 has used the library on the same device.
 """
 
-import ctypes
-
 import numpy as np
 import pytest
 import torch
