@@ -277,7 +277,9 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * value of stage-1 time t1 = t - sfine - shift2[g*n_coarse + c]
  * (k = 28 - ilogb(max bound) - ceil(log2(s_mult))).  A part's rounding
  * error is at most 2^-(k+1), below 2^(ceil(log2(s_mult)) - 29) of the bound;
- * bf16 parts above 2^-16 of it are exact.  The bound must cover every value
+ * bf16 parts above 2^-16 of it are exact.  k is clamped at 100 (so that
+ * 2^-k x 0.5/N^2 stays a normal float): bounds below about 2^-72 get a
+ * coarser grid.  The bound must cover every value
  * read: the caller keeps a row alive while the ring holds its chunk and
  * zeroes it before stage 1 writes a new chunk into it.  A non-finite bound
  * sets DSB_E_ARG in *status.
