@@ -4,7 +4,8 @@ seeded raw pages (small array, two chgroups, one dispersed burst).
 * per-subband gridded rows and the stage-2 ring (stage 1 + static sky):
   bit-exact (integer sums; float64 sky mean, one rounding);
 * candidate lists: identical (time, fine DM, pixel, width); S/N within
-  1e-4 relative (cuFFT float32 images vs the float64 oracle images).  The
+  1e-5 relative (float32 images vs the float64 oracle images; measured
+  about 3e-7 on every ring form).  The
   only allowed difference is a candidate whose S/N lies within 1e-3 of
   the threshold (the epsilon band stated in the design notes).
 """
@@ -101,12 +102,15 @@ def test_pipeline_matches_oracle(dev, ring, dm_group):
     key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
     g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
     w_map = {key(c): c[4] for c in want}
+    worst = 0.0
     for k in set(g_map) | set(w_map):
         if k in g_map and k in w_map:
-            assert abs(g_map[k] - w_map[k]) <= 1e-4 * abs(w_map[k]), (k, g_map[k], w_map[k])
+            worst = max(worst, abs(g_map[k] - w_map[k]) / abs(w_map[k]))
+            assert abs(g_map[k] - w_map[k]) <= 1e-5 * abs(w_map[k]), (k, g_map[k], w_map[k])
         else:
             v = g_map.get(k, w_map.get(k))
             assert abs(v - 6.0) < EPS_BAND * 6.0, f"unmatched candidate {k} snr={v}"
+    print(f"ring {ring}: largest S/N relative difference {worst:.2e}")
     # the injected burst is recovered at its pixel
     assert any(c.l == 32 + 3 and c.m == 32 - 5 for c in got)
 
