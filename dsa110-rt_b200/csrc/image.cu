@@ -14,7 +14,7 @@
 //     from the time-major stage-2 ring: one coalesced read of each chgroup's
 //     coarse-DM slice, shared-memory int32 atomics into S held in fixed
 //     point (S * 2^k, k from a bound on the image's parts).  Each thread then
-//     moves its own range of S (at most IMG_MAXE entries, whole slots) into
+//     moves its own range of S (at most MAXE entries, whole slots) into
 //     tensor memory, which this kernel uses as plain per-thread storage:
 //     TMEM is otherwise idle here and holds S across the passes below while
 //     the shared buffer is reused for the transforms.
@@ -128,12 +128,55 @@ DSB_DEV void idft16(float2 (&a)[16]) {
   for (int i = 0; i < 16; ++i) a[i] = x[i];
 }
 
+// W_32^j = exp(+2 pi i j / 32), j = 0..15 (cos and sin of j pi / 16, exact
+// mathematical values rounded to float)
+__device__ __constant__ float2 kW32[16] = {
+    {1.0f, 0.0f},
+    {0.98078528040323043f, 0.19509032201612825f},
+    {0.92387953251128674f, 0.38268343236508978f},
+    {0.83146961230254524f, 0.55557023301960218f},
+    {0.70710678118654752f, 0.70710678118654752f},
+    {0.55557023301960218f, 0.83146961230254524f},
+    {0.38268343236508978f, 0.92387953251128674f},
+    {0.19509032201612825f, 0.98078528040323043f},
+    {0.0f, 1.0f},
+    {-0.19509032201612825f, 0.98078528040323043f},
+    {-0.38268343236508978f, 0.92387953251128674f},
+    {-0.55557023301960218f, 0.83146961230254524f},
+    {-0.70710678118654752f, 0.70710678118654752f},
+    {-0.83146961230254524f, 0.55557023301960218f},
+    {-0.92387953251128674f, 0.38268343236508978f},
+    {-0.98078528040323043f, 0.19509032201612825f}};
+
+// Inverse 32-point DFT, natural order out: two 16-point transforms of the
+// even and odd samples, then one radix-2 stage with the twiddles W_32^m.
+DSB_DEV void idft32(float2 (&a)[32]) {
+  float2 e[16], o[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    e[k] = a[2 * k];
+    o[k] = a[2 * k + 1];
+  }
+  idft16(e);
+  idft16(o);
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const float2 t = m ? cmul(o[m], kW32[m]) : o[m];
+    a[m] = cadd(e[m], t);
+    a[m + 16] = csub(e[m], t);
+  }
+}
+
 template <int R>
 DSB_DEV void idftR(float2 (&a)[R]) {
-  if constexpr (R == 16) idft16(a);
+  if constexpr (R == 32) idft32(a);
+  else if constexpr (R == 16) idft16(a);
   else if constexpr (R == 8) idft8(a);
   else idft4(a[0], a[1], a[2], a[3]);
 }
+
+// a * W_8 = a * (1 + i) / sqrt(2)
+DSB_DEV float2 cmul_w8(float2 a) { return make_float2(R2 * (a.x - a.y), R2 * (a.x + a.y)); }
 
 // Stage-2 ring elements (FMT): 0 complex64; 1 the BF16 storage form (bf16
 // re/im pairs in 32 bits); 2 the cint8 wire form (int8 re/im pairs in 16
@@ -192,9 +235,12 @@ struct ImgArgs {
   const int2* c2;           // (n_c2) second targets: {cell | g << 16, tgt | conj << 16}
   int n_c2;
   const int* thr_b;         // (THREADS + 1) S range [thr_b[i], thr_b[i+1]) of thread i
-  const uint4* gmeta;       // (IMG_MAXE / 8, THREADS) 8 x uint16 per (chunk, thread): entry
-                            //   col | n' << 7 | q << 13 | last of its slot << 15
-  const unsigned long long* srot;  // (THREADS) 2 bits per entry: packed | parity(u+w) << 1
+  const uint4* gmeta;       // (MAXE / EPV, THREADS) 16 bytes per (chunk, thread): EPV
+                            //   entries col | n' << NP_SH | q << Q_SH | last of its slot
+                            //   << LAST_SH (the 32-bit form also packed | parity(u+w) << 1
+                            //   at ROT_SH); ImgGeom gives the form of each N
+  const unsigned long long* srot;  // 16-bit form: (THREADS) 2 bits per entry, packed |
+                                   // parity(u+w) << 1; unused (may be null) at N = 512
   const int* dcols;         // (n_dense) packed columns that need the LC-point transform
   const unsigned long long* dmask;  // (n_dense) occupied slots n' of each
   int n_dense;
@@ -219,48 +265,92 @@ constexpr int IMG_MAX_G = 64;
 #ifndef IMG_COMBINE_U
 #define IMG_COMBINE_U 8   // 64-entry double chunks per warp in flight in the combine
 #endif
-constexpr int IMG_THREADS = 256;
-// TMEM: 128 columns per CTA (three CTAs per SM take 384 of 512).  Warps w
-// and w + 4 reach the same 32 lanes, so each takes 64 columns: 32 complex
-// S entries per thread.
-constexpr int IMG_TMEM_COLS = 128;
-constexpr int IMG_MAXE = IMG_TMEM_COLS / 4;
 
+// Geometry of image_kernel<N>.
+//  * Column pass: N = FOLD * LC output rows in FOLD passes of LC rows; an
+//    LC-point column transform is two C1-point steps (LC = C1 * C1).
+//  * Row transforms: N = R1 * R2 on a group of R1 threads, each holding R2
+//    points (an R2-point step, a transpose, R2 / R1 R1-point steps).
+//  * N = 512: FOLD 8 (64-row passes), 512 threads, one CTA per SM with all
+//    512 TMEM columns, 32-bit entry metadata (8 bits of column); the combine's
+//    S arrays (int32 real and imaginary parts) take 192 KB of shared memory.
+//  * N = 64, 256: FOLD 4, 256 threads, three CTAs per SM with 128 TMEM
+//    columns each, 16-bit entry metadata.
+// TMEM: warps w, w + 4, w + 8, ... reach the same 32 lanes; each takes an
+// equal share of the CTA's columns, two 32-bit columns per complex S entry.
 template <int N>
 struct ImgGeom {
-  static constexpr int FOLD = 4;
+  static constexpr int FOLD = (N == 512) ? 8 : 4;
   static constexpr int LC = N / FOLD;             // folded column length
   static constexpr int C1 = (LC == 64) ? 8 : 4;    // LC = C1 * C1
   static constexpr int NC = N / 2;                // packed columns
   static constexpr int P = NC + 2;                // buffer row pitch (float2), = 2 mod 16
-  static constexpr int RR = (N == 256) ? 16 : 8;  // N = RR * RR
-  static constexpr int THREADS = IMG_THREADS;
+  static constexpr int R1 = (N == 64) ? 8 : 16;   // threads per row transform
+  static constexpr int R2 = N / R1;               // points per thread
+  static constexpr int THREADS = (N == 512) ? 512 : 256;
+  static constexpr int CTAS = (N == 512) ? 1 : 3; // resident CTAs per SM
+  static constexpr int TMEM_COLS = (N == 512) ? 512 : 128;
+  static constexpr int WARP_COLS = TMEM_COLS / (THREADS / 128);  // columns per warp
+  static constexpr int MAXE = WARP_COLS / 2;      // S entries per thread
+  static constexpr bool META32 = (N == 512);
+  // entry metadata fields: column | n' << NP_SH | q << Q_SH | last << LAST_SH
+  // (32-bit form also: packed << ROT_SH | parity(u + w) << ROT_SH + 1)
+  static constexpr int NP_SH = META32 ? 8 : 7;
+  static constexpr int Q_SH = META32 ? 14 : 13;
+  static constexpr int LAST_SH = META32 ? 17 : 15;
+  static constexpr int ROT_SH = 18;
   static constexpr int CG = THREADS / C1;         // column groups
-  static constexpr int RG = THREADS / RR;         // row groups
-  static constexpr int BUF = LC * P;              // float2 slots
-  static_assert(C1 * C1 == LC && RR * RR == N, "unsupported size");
+  static constexpr int RG = THREADS / R1;         // row groups
+  static constexpr int BUF = LC * P;              // float2 slots of the column buffer
+  // S entries the combine's split int32 arrays hold
+  static constexpr int SCAP = (N == 512) ? 24576 : BUF;
+  static constexpr size_t BUFB = (size_t)(BUF > SCAP ? BUF : SCAP) * 8;
+  static_assert(C1 * C1 == LC && R1 * R2 == N && R2 % R1 == 0, "unsupported size");
   static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
-  static_assert(NC <= 128 && LC <= 64, "entry metadata holds 7 bits of column, 6 of n'");
-  // buf | tw (N) | rtw (RR*RR) | ctw (C1*C1) | slice pointers | cell bases |
-  // ends of the chgroups' cells | slice scales | TMEM address
-  static constexpr size_t SMEM = (size_t)(BUF + N + RR * RR + C1 * C1) * 8 + IMG_MAX_G * 8 +
+  static_assert(META32 ? (NC <= 256 && LC <= 64 && FOLD <= 8)
+                       : (NC <= 128 && LC <= 64 && FOLD <= 4),
+                "entry metadata field widths");
+  static_assert(MAXE % 8 == 0 && MAXE <= 64, "whole 8-entry chunks, 64-bit rotation masks");
+  static_assert(LC <= 64, "one 64-bit occupancy mask per column");
+  // buf | tw (N) | rtw (R1*R2) | ctw (C1*C1) | slice pointers | cell bases |
+  // ends of the chgroups' cells | slice scales | TMEM address | k
+  static constexpr size_t SMEM = BUFB + (size_t)(N + R1 * R2 + C1 * C1) * 8 + IMG_MAX_G * 8 +
                                  (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + IMG_MAX_G * 4 + 16;
+  static_assert(SMEM <= 227 * 1024, "shared memory of one CTA");
 };
 
+// The 8 metadata entries of chunk c of this thread (entries 8c .. 8c + 7).
+template <int N>
+DSB_DEV void load_meta8(const uint4* gm, int c, int tid, unsigned (&m)[8]) {
+  using Gm = ImgGeom<N>;
+  if constexpr (Gm::META32) {
+    const uint4 a = __ldg(gm + (2 * c) * Gm::THREADS + tid);
+    const uint4 b = __ldg(gm + (2 * c + 1) * Gm::THREADS + tid);
+    m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+    m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+  } else {
+    const uint4 a = __ldg(gm + c * Gm::THREADS + tid);
+    const unsigned w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) m[j] = (w[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+  }
+}
+
 template <int N, int FMT>
-__global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
+__global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
+    image_kernel(const ImgArgs A) {
   using Elem = typename RingElem<FMT>::T;
   using Gm = ImgGeom<N>;
   constexpr int FOLD = Gm::FOLD, LC = Gm::LC, C1 = Gm::C1, NC = Gm::NC, P = Gm::P,
-                RR = Gm::RR, THREADS = Gm::THREADS;
+                R1 = Gm::R1, R2 = Gm::R2, THREADS = Gm::THREADS, MAXE = Gm::MAXE;
   extern __shared__ __align__(16) uint8_t smem_raw[];
   float2* buf = reinterpret_cast<float2*>(smem_raw);  // S in step 1, columns in 2-3
-  float2* tw = buf + Gm::BUF;
+  float2* tw = reinterpret_cast<float2*>(smem_raw + Gm::BUFB);
   // twiddles laid out so that the lanes of a group read consecutive slots:
-  // rtw[x1*RR + j] = W_N^(j x1), ctw[m1*C1 + j] = W_LC^(j m1)
+  // rtw[m2*R1 + j] = W_N^(j m2), ctw[m1*C1 + j] = W_LC^(j m1)
   float2* rtw = tw + N;
-  float2* ctw = rtw + RR * RR;
+  float2* ctw = rtw + R1 * R2;
   const Elem** s_slice = reinterpret_cast<const Elem**>(ctw + C1 * C1);
   int* s_cbase = reinterpret_cast<int*>(s_slice + IMG_MAX_G);
   int* s_end = s_cbase + IMG_MAX_G + 1;
@@ -272,8 +362,8 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   const int lane = tid & 31;
   const int warp = tid >> 5;
   for (int i = tid; i < N; i += THREADS) tw[i] = A.tw[i];
-  for (int i = tid; i < RR * RR; i += THREADS)
-    rtw[i] = A.tw[((i % RR) * (i / RR)) & (N - 1)];
+  for (int i = tid; i < R1 * R2; i += THREADS)
+    rtw[i] = A.tw[((i % R1) * (i / R1)) & (N - 1)];
   for (int i = tid; i < C1 * C1; i += THREADS)
     ctw[i] = A.tw[((i % C1) * (i / C1) * (N / LC)) & (N - 1)];
   for (int g = tid; g <= A.G; g += THREADS) s_cbase[g] = A.cell_base[g];
@@ -281,24 +371,25 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   // this thread's S entries [sb, sb + sn), whole slots
   const int sb = __ldg(A.thr_b + tid);
   const int sn = __ldg(A.thr_b + tid + 1) - sb;
-  const bool bad_range = sn < 0 || sn > IMG_MAXE || sb < 0 || sb + sn > A.n_s;
+  const bool bad_range = sn < 0 || sn > MAXE || sb < 0 || sb + sn > A.n_s;
   bool bad_base = false;  // each chgroup's run: whole 64-entry pairs of chunks
   for (int g = tid; g <= A.G; g += THREADS) bad_base |= (A.cell_base[g] & 63) != 0;
   if (__syncthreads_or(bad_range || bad_base)) {
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
     return;  // every thread leaves, before any TMEM is taken
   }
-  const unsigned long long srot = __ldg(A.srot + tid);
+  // rotation bits of the 16-bit form: 2 per entry (packed | parity << 1)
+  const unsigned long long srot = Gm::META32 ? 0ull : __ldg(A.srot + tid);
   const int nch = (__reduce_max_sync(0xffffffffu, sn) + 7) >> 3;  // 8-entry chunks, per warp
   if (warp == 0) {
-    tmem_alloc(s_tmem, IMG_TMEM_COLS);
+    tmem_alloc(s_tmem, Gm::TMEM_COLS);
     tmem_relinquish();
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *s_tmem + ((uint32_t)((warp & 3) * 32) << 16) +
-                         (uint32_t)((warp >> 2) * (IMG_TMEM_COLS / 2));
+                         (uint32_t)((warp >> 2) * Gm::WARP_COLS);
 
   const int n_tot = A.cell_base[A.G];
   // 0.5 / N^2 is a power of two, applied to S on its way into TMEM: scaling
@@ -308,12 +399,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   const float scale = 0.5f / (float)(N * N);
   static_assert((N & (N - 1)) == 0, "0.5 / N^2 must be a power of two");
   const int n_img = A.n_f * A.n_t;
-  // column groups: C1 lanes; row groups: RR lanes (groups never straddle warps)
+  // column groups: C1 lanes; row groups: R1 lanes (groups never straddle warps)
   const int cgi = tid / C1, cj = tid % C1;
   const unsigned cmask = ((1u << C1) - 1u) << (lane / C1 * C1);
-  const int rgi = tid / RR, rj = tid % RR;
-  const unsigned rmask = ((1u << RR) - 1u) << (lane / RR * RR);
+  const int rgi = tid / R1, rj = tid % R1;
+  const unsigned rmask = ((1u << R1) - 1u) << (lane / R1 * R1);
   const int shift_rot = A.fftshift ? 2 : 0;
+  const uint4* gmeta = A.gmeta;
 
   for (int img = blockIdx.x; img < n_img; img += gridDim.x) {
     // fine DM fastest: CTAs that run together share coarse-DM slices in L2
@@ -382,13 +474,13 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         atomicAdd(reinterpret_cast<int*>(s_re) + t, re);
         atomicAdd(reinterpret_cast<int*>(s_im) + t, ((m >> 16) & 1u) ? -im : im);
       };
-      // warp w takes the 64-entry double chunks w, w + 8, ... of c_meta in
+      // warp w takes the 64-entry double chunks w, w + NW, ... of c_meta in
       // order, each lane two adjacent cells with one metadata and one ring
       // load; each chgroup's run is a whole number of double chunks, so the
       // chgroup, its first entry and its ring row stay in registers and
       // change only at a run boundary (warp-uniform), and the shared-memory
       // pipe is left to the atomics.  16 cells in flight per thread (8 was
-      // 1.4 % slower over the whole kernel at the bench workload).
+      // 1.4 % slower over the whole kernel at the 256^2 workload).
       using Elem2 = typename RingElem<FMT>::T2;
       constexpr int U = IMG_COMBINE_U, NW = THREADS / 32;
       const int n_dch = n_tot >> 6;
@@ -452,13 +544,17 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       const float* s_im = s_re + A.s_stride;
       const float unfix = ldexpf(scale, -*s_fixk);  // 2^-k x 0.5 / N^2
       for (int c = 0; c < nch; ++c) {
+        unsigned md[8];
+        if constexpr (Gm::META32) load_meta8<N>(gmeta, c, tid, md);
         uint32_t r[16];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int i = 8 * c + j;
           float2 v = make_float2(0.f, 0.f);
           if (i < sn) {
-            const unsigned b = (unsigned)(srot >> (2 * i)) & 3u;
+            unsigned b;
+            if constexpr (Gm::META32) b = (md[j] >> Gm::ROT_SH) & 3u;
+            else b = (unsigned)(srot >> (2 * i)) & 3u;
             const float2 x = make_float2(__int2float_rn(__float_as_int(s_re[sb + i])) * unfix,
                                          __int2float_rn(__float_as_int(s_im[sb + i])) * unfix);
             v = crot_rt(x, (b & 1u) + ((b & 2u) ? (unsigned)shift_rot : 0u));
@@ -476,46 +572,71 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       // ---- 2a. fold S into the occupied slots (n', col) of buf: each slot's
       //      entries are consecutive in one thread's range, written once
       //      after the last of them ----
-      // (one copy of the loop per pass, so that the rotation i^(q p) is
-      // nothing for p = 0, a sign for p = 2 and needs no multiply otherwise)
+      // (one copy of the loop per pass, so that the rotation W_FOLD^(q p)
+      // needs as little work as the pass allows: none for p = 0, a sign for
+      // p = FOLD/2, a swap and signs for the other even multiples, and one
+      // multiply by W_8 for the odd ones)
       auto fold = [&](auto pass) {
         constexpr unsigned PP = decltype(pass)::value;
         float2 acc = make_float2(0.f, 0.f);
-        uint4 md_next = __ldg(A.gmeta + tid);
+        unsigned md_next[8];
+        load_meta8<N>(gmeta, 0, tid, md_next);
         for (int c = 0; c < nch; ++c) {
-          const uint4 md = md_next;  // next chunk's metadata loads under this one's
-          if (c + 1 < nch) md_next = __ldg(A.gmeta + (c + 1) * THREADS + tid);
+          unsigned mw[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) mw[j] = md_next[j];
+          // next chunk's metadata loads under this one's
+          if (c + 1 < nch) load_meta8<N>(gmeta, c + 1, tid, md_next);
           uint32_t r[16];
           tmem_ld16_wait(tbase + 16 * c, r);
-          const unsigned mw[4] = {md.x, md.y, md.z, md.w};
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             if (8 * c + j < sn) {
-              const unsigned m = (mw[j >> 1] >> (16 * (j & 1))) & 0xffffu;
+              const unsigned m = mw[j];
               float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
-              const unsigned q = (m >> 13) & 3u;
-              if constexpr (PP == 2) {
-                const unsigned sgn = (q & 1u) << 31;  // i^(2q) = (-1)^q
-                v = make_float2(__uint_as_float(__float_as_uint(v.x) ^ sgn),
-                                __uint_as_float(__float_as_uint(v.y) ^ sgn));
-              } else if constexpr (PP != 0) {
-                v = crot_rt(v, q * PP);
+              const unsigned q = (m >> Gm::Q_SH) & (FOLD - 1);
+              if constexpr (PP != 0) {
+                if constexpr (FOLD == 4) {
+                  if constexpr (PP == 2) {
+                    const unsigned sgn = (q & 1u) << 31;  // i^(2q) = (-1)^q
+                    v = make_float2(__uint_as_float(__float_as_uint(v.x) ^ sgn),
+                                    __uint_as_float(__float_as_uint(v.y) ^ sgn));
+                  } else {
+                    v = crot_rt(v, q * PP);
+                  }
+                } else {
+                  // W_8^k = i^(k >> 1) x (W_8 if k is odd), k = q p mod 8
+                  const unsigned k = (q * PP) & 7u;
+                  if constexpr (PP & 1u) {
+                    if (k & 1u) v = cmul_w8(v);
+                  }
+                  v = crot_rt(v, k >> 1);
+                }
               }
               acc = cadd(acc, v);
-              if (m & 0x8000u) {
-                buf[((m >> 7) & (LC - 1)) * P + (m & (NC - 1))] = acc;
+              if ((m >> Gm::LAST_SH) & 1u) {
+                buf[((m >> Gm::NP_SH) & (LC - 1)) * P + (m & (NC - 1))] = acc;
                 acc = make_float2(0.f, 0.f);
               }
             }
           }
         }
       };
-      static_assert(FOLD == 4, "the fold is instantiated for four passes");
       switch (p) {
         case 0: fold(std::integral_constant<unsigned, 0>{}); break;
         case 1: fold(std::integral_constant<unsigned, 1>{}); break;
         case 2: fold(std::integral_constant<unsigned, 2>{}); break;
-        default: fold(std::integral_constant<unsigned, 3>{}); break;
+        case 3: fold(std::integral_constant<unsigned, 3>{}); break;
+        default:
+          if constexpr (FOLD == 8) {
+            switch (p) {
+              case 4: fold(std::integral_constant<unsigned, 4>{}); break;
+              case 5: fold(std::integral_constant<unsigned, 5>{}); break;
+              case 6: fold(std::integral_constant<unsigned, 6>{}); break;
+              default: fold(std::integral_constant<unsigned, 7>{}); break;
+            }
+          }
+          break;
       }
       __syncthreads();
       // ---- 2b. column transforms of pass p (in place in buf); only the
@@ -548,7 +669,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       // constant columns: every row holds the folded slot n' = 0 (row 0
       // itself is already in place); columns without entries are zero.  The
       // lanes of a warp take consecutive columns of one row (no bank
-      // conflicts), the warps take rows m = warp (mod 8).
+      // conflicts), the warps take rows m = warp (mod warps).
       for (int k = lane; k < A.n_const; k += 32) {
         const int kc = __ldg(A.kcols + k);
         const int col = kc & (NC - 1);
@@ -559,15 +680,19 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
       }
       __syncthreads();
       // ---- 3. row transforms: folded rows (2pr, 2pr + 1) are image rows
-      //      FOLD*2pr + p and FOLD*(2pr+1) + p ----
+      //      FOLD*2pr + p and FOLD*(2pr+1) + p.  N = R1 * R2: thread rj holds
+      //      points rj + R1 k2 (k2 < R2), takes their R2-point transform,
+      //      twiddles it by W_N^(rj m2), and after the transpose owns the
+      //      R1-point transforms of columns m2 = rj + R1 h, which give the
+      //      outputs m2 + R2 m1 ----
       for (int pr = rgi; pr < LC / 2; pr += Gm::RG) {
         float2* reg = buf + 2 * pr * P;
         const float2* ra = reg;
         const float2* rb = reg + P;
-        float2 a[RR];
+        float2 a[R2];
 #pragma unroll
-        for (int k = 0; k < RR; ++k) {
-          const int i = rj + RR * k;
+        for (int k = 0; k < R2; ++k) {
+          const int i = rj + R1 * k;
           float2 z;
           if (i == 0) {
             z = make_float2(ra[0].x, rb[0].x);
@@ -582,22 +707,32 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
           }
           a[k] = z;
         }
-        idftR<RR>(a);
+        idftR<R2>(a);
 #pragma unroll
-        for (int x1 = 1; x1 < RR; ++x1) a[x1] = cmul(a[x1], rtw[x1 * RR + rj]);
+        for (int m2 = 1; m2 < R2; ++m2) a[m2] = cmul(a[m2], rtw[m2 * R1 + rj]);
         __syncwarp(rmask);  // every lane has read the pair's rows
 #pragma unroll
-        for (int x1 = 0; x1 < RR; ++x1) reg[rj * RR + (x1 ^ rj)] = a[x1];
+        for (int m2 = 0; m2 < R2; ++m2) reg[m2 * R1 + (rj ^ (m2 & (R1 - 1)))] = a[m2];
         __syncwarp(rmask);
+        constexpr int H = R2 / R1;
+        float2 b[H][R1];
 #pragma unroll
-        for (int jj = 0; jj < RR; ++jj) a[jj] = reg[jj * RR + (rj ^ jj)];
+        for (int h = 0; h < H; ++h) {
+          const int m2 = rj + R1 * h;
+#pragma unroll
+          for (int jj = 0; jj < R1; ++jj) b[h][jj] = reg[m2 * R1 + (jj ^ rj)];
+        }
         __syncwarp(rmask);
-        idftR<RR>(a);
         float* stage = reinterpret_cast<float*>(reg);
 #pragma unroll
-        for (int x2 = 0; x2 < RR; ++x2) {
-          stage[rj + RR * x2] = a[x2].x;
-          stage[N + rj + RR * x2] = a[x2].y;
+        for (int h = 0; h < H; ++h) {
+          idftR<R1>(b[h]);
+#pragma unroll
+          for (int m1 = 0; m1 < R1; ++m1) {
+            const int x = rj + R1 * h + R2 * m1;
+            stage[x] = b[h][m1].x;
+            stage[N + x] = b[h][m1].y;
+          }
         }
         __syncwarp(rmask);
         const size_t ibase = ((size_t)fl * A.n_t + t) * N;
@@ -605,7 +740,7 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
         float4* ob = reinterpret_cast<float4*>(A.out + (ibase + FOLD * (2 * pr + 1) + p) * N);
         const float4* s4 = reinterpret_cast<const float4*>(stage);
 #pragma unroll
-        for (int q = rj; q < N / 4; q += RR) {
+        for (int q = rj; q < N / 4; q += R1) {
           oa[q] = s4[q];
           ob[q] = s4[N / 4 + q];
         }
@@ -618,15 +753,16 @@ __global__ void __launch_bounds__(256, 3) image_kernel(const ImgArgs A) {
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(*s_tmem, IMG_TMEM_COLS);
+    tmem_dealloc(*s_tmem, Gm::TMEM_COLS);
   }
 }
 
 // Resident CTAs for image_kernel<N, FMT> on this device (the persistent grid).
 // The occupancy API answers 1 CTA per SM for any kernel that allocates
 // tensor memory (measured on B200 with CUDA 12.9), while the SM runs as many
-// as its shared memory, registers and 512 TMEM columns hold: three here.  So
-// the count is taken from those limits directly.
+// as its shared memory, registers and 512 TMEM columns hold (three at
+// N <= 256, one at N = 512).  So the count is taken from those limits
+// directly.
 template <int N, int FMT>
 int image_grid(int* blocks) {
   using Gm = ImgGeom<N>;
@@ -646,7 +782,7 @@ int image_grid(int* blocks) {
     const int by_smem = smem_sm / ((int)Gm::SMEM + fa.sharedSizeBytes + smem_rsv);
     const int regs_cta = (fa.numRegs + 7) / 8 * 8 * Gm::THREADS;
     const int by_regs = regs_cta > 0 ? regs_sm / regs_cta : 1;
-    const int occ = std::min({3, by_smem, by_regs, 512 / IMG_TMEM_COLS});
+    const int occ = std::min({Gm::CTAS, by_smem, by_regs, 512 / Gm::TMEM_COLS});
     cached = std::max(1, occ) * sms;
   }
   *blocks = cached;
@@ -656,7 +792,8 @@ int image_grid(int* blocks) {
 template <int N, int FMT>
 int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   using Gm = ImgGeom<N>;
-  if (A.s_stride > Gm::BUF) return DSB_E_CAPACITY;
+  if (A.s_stride > Gm::SCAP) return DSB_E_CAPACITY;
+  if (!Gm::META32 && !A.srot) return DSB_E_ARG;
   int blocks = 0;
   const int rc = image_grid<N, FMT>(&blocks);
   if (rc != DSB_OK) return rc;
@@ -666,21 +803,30 @@ int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   return launch_status();
 }
 
+template <int N>
+int image_geometry(int* g) {
+  using Gm = ImgGeom<N>;
+  g[0] = Gm::FOLD;
+  g[1] = Gm::THREADS;
+  g[2] = Gm::MAXE;
+  g[3] = Gm::META32 ? 32 : 16;
+  g[4] = Gm::SCAP;
+  return DSB_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
-int dsb_image_fold(int n_grid) {
+int dsb_image_geometry(int n_grid, int* geom) {
+  if (!geom) return DSB_E_ARG;
   switch (n_grid) {
-    case 64:
-    case 256: return ImgGeom<256>::FOLD;
-    default: return 0;
+    case 64: return image_geometry<64>(geom);
+    case 256: return image_geometry<256>(geom);
+    case 512: return image_geometry<512>(geom);
+    default: return DSB_E_UNSUPPORTED;
   }
 }
-
-int dsb_image_threads(void) { return IMG_THREADS; }
-
-int dsb_image_max_entries(void) { return IMG_MAXE; }
 
 int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
                   const float* scales, const long long* sc_base, const float* amax,
@@ -693,7 +839,7 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
                   int N, long long t0, int n_t, int fftshift, void* out, int max_blocks,
                   int* status, cudaStream_t stream) {
   if (!D || !seg_base || !seg_depth || n_coarse <= 0 || !c_meta || !cell_base ||
-      (n_c2 > 0 && !c2) || n_c2 < 0 || !thr_b || !gmeta || !srot || n_s <= 0 ||
+      (n_c2 > 0 && !c2) || n_c2 < 0 || !thr_b || !gmeta || n_s <= 0 ||
       n_s > 65536 || n_dense < 0 || n_const < 0 || (n_dense > 0 && (!dcols || !dmask)) ||
       (n_const > 0 && !kcols) || !d_pitch || !n_filled || !sfine || !f2c || !twiddles ||
       !out || !status || n_f <= 0 || n_t <= 0 || G <= 0 || G > IMG_MAX_G ||
@@ -722,6 +868,10 @@ int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const 
       return d_format == 2   ? launch_image<256, 2>(A, max_blocks, stream)
              : d_format == 1 ? launch_image<256, 1>(A, max_blocks, stream)
                              : launch_image<256, 0>(A, max_blocks, stream);
+    case 512:
+      return d_format == 2   ? launch_image<512, 2>(A, max_blocks, stream)
+             : d_format == 1 ? launch_image<512, 1>(A, max_blocks, stream)
+                             : launch_image<512, 0>(A, max_blocks, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

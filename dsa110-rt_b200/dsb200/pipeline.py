@@ -170,12 +170,28 @@ class ImageTables:
     cell_base: np.ndarray   # (G + 1) int32
     c2: np.ndarray          # (n_c2, 2) int32: {k | g << 16, s | conj << 16}
     thr_b: np.ndarray       # (threads + 1) int32: S range of each kernel thread
-    gmeta: np.ndarray       # (max_entries / 8, threads, 8) uint16: w' | n' << 7 | q << 13 | last << 15
+    gmeta: np.ndarray       # (max_entries / epv, threads, epv) entry metadata (see geometry)
     srot: np.ndarray        # (threads,) uint64: 2 bits per entry: packed | parity << 1
     dcols: np.ndarray       # (n_dense,) int32: packed columns with an entry off n' = 0
     dmask: np.ndarray       # (n_dense,) uint64: their occupied n'
     kcols: np.ndarray       # (n_const,) int32: w' | has entries << 16 (constant or zero columns)
     s_mult: int = 1         # most contributions (pattern cells, both targets) to one S entry
+    fold: int = 4           # column passes (N = fold * LC)
+    meta_bits: int = 16     # 16: w' | n' << 7 | q << 13 | last << 15 (uint16);
+    #                         32: w' | n' << 8 | q << 14 | last << 17 | packed << 18 |
+    #                             parity << 19 (uint32, rotation bits in the entry)
+
+
+def image_geometry(N: int) -> dict:
+    """The image kernel's geometry for grid size N (dsb_image_geometry):
+    column passes, threads, S entries per thread, metadata width, and the S
+    capacity of the combine's shared arrays."""
+    import ctypes
+    g = (ctypes.c_int * 5)()
+    rc = int(_lib.lib().dsb_image_geometry(N, g))
+    if rc:
+        raise ValueError(f"dsb_image_fft does not support N={N}")
+    return dict(fold=g[0], threads=g[1], max_entries=g[2], meta_bits=g[3], s_capacity=g[4])
 
 
 def _split_slots(sizes: np.ndarray, n_threads: int, cap: int) -> np.ndarray:
@@ -204,11 +220,8 @@ def build_image_tables(pats, N: int) -> ImageTables:
     chgroup g adds to half cell (u, w) when w <= N/2 and, conjugated, to its
     mirror ((N-u) % N, (N-w) % N) when that column is <= N/2 (both for
     w = 0 and w = N/2): the Hermitian fold of fused_combine_cuda.py:560-620."""
-    L = _lib.lib()
-    fold = int(L.dsb_image_fold(N))
-    if fold <= 0:
-        raise ValueError(f"dsb_image_fft does not support N={N}")
-    n_thr, cap = int(L.dsb_image_threads()), int(L.dsb_image_max_entries())
+    geo = image_geometry(N)
+    fold, n_thr, cap, mbits = geo["fold"], geo["threads"], geo["max_entries"], geo["meta_bits"]
     LC, NC = N // fold, N // 2
     G = len(pats)
     if G > 63:
@@ -240,6 +253,9 @@ def build_image_tables(pats, N: int) -> ImageTables:
     n_s = int(ukey.size)
     if n_s >= 1 << 16:
         raise ValueError("dsb_image_fft needs fewer than 65536 distinct half cells")
+    if n_s > geo["s_capacity"]:
+        raise ValueError(f"dsb_image_fft: {n_s} distinct half cells exceed the kernel's "
+                         f"{geo['s_capacity']} at N={N}")
     s_pk = ukey & 1
     s_q = (ukey >> 1) % fold
     s_slot = (ukey >> 1) // fold          # w' * LC + n'
@@ -253,12 +269,20 @@ def build_image_tables(pats, N: int) -> ImageTables:
     thr_b = _split_slots(np.diff(np.r_[starts, n_s]), n_thr, cap)
     owner = np.repeat(np.arange(n_thr), np.diff(thr_b))
     idx = np.arange(n_s) - thr_b[owner]
-    gmeta = np.zeros((cap // 8, n_thr, 8), np.uint16)
-    gmeta[idx // 8, owner, idx % 8] = (s_wp | (s_n << 7) | (s_q << 13) | (last << 15)
-                                       ).astype(np.uint16)
+    parity = (s_u + s_w) & 1
     srot = np.zeros(n_thr, np.uint64)
-    bits = (s_pk | (((s_u + s_w) & 1) << 1)).astype(np.uint64) << (2 * idx).astype(np.uint64)
-    np.bitwise_or.at(srot, owner, bits)
+    if mbits == 16:
+        epv = 8
+        gmeta = np.zeros((cap // epv, n_thr, epv), np.uint16)
+        gmeta[idx // epv, owner, idx % epv] = (s_wp | (s_n << 7) | (s_q << 13) | (last << 15)
+                                               ).astype(np.uint16)
+        bits = (s_pk | (parity << 1)).astype(np.uint64) << (2 * idx).astype(np.uint64)
+        np.bitwise_or.at(srot, owner, bits)
+    else:
+        epv = 4
+        gmeta = np.zeros((cap // epv, n_thr, epv), np.uint32)
+        gmeta[idx // epv, owner, idx % epv] = (s_wp | (s_n << 8) | (s_q << 14) | (last << 17) |
+                                               (s_pk << 18) | (parity << 19)).astype(np.uint32)
     # columns: dense (an entry off n' = 0) get the LC-point transform; the
     # rest are constant (every entry at n' = 0) or zero
     occ = np.zeros(NC, np.uint64)
@@ -280,7 +304,8 @@ def build_image_tables(pats, N: int) -> ImageTables:
                        c2=np.ascontiguousarray(c2.reshape(-1, 2)),
                        thr_b=thr_b.astype(np.int32), gmeta=gmeta, srot=srot, dcols=dcols,
                        dmask=occ[dcols], kcols=kcols,
-                       s_mult=int(np.bincount(inv, minlength=n_s).max()))
+                       s_mult=int(np.bincount(inv, minlength=n_s).max()), fold=fold,
+                       meta_bits=mbits)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -417,7 +442,8 @@ class SearchPipeline:
         it = T.img
         self.d_img_cmeta = d(it.c_meta.view(np.int32))
         self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
-        self.d_img_thrb, self.d_img_gmeta = d(it.thr_b), d(it.gmeta.view(np.int16))
+        self.d_img_thrb = d(it.thr_b)
+        self.d_img_gmeta = d(it.gmeta.view(np.int16 if it.meta_bits == 16 else np.int32))
         self.d_img_srot = d(it.srot.view(np.int64))
         self.d_img_dcols, self.d_img_dmask = d(it.dcols), d(it.dmask.view(np.int64))
         self.d_img_kcols = d(it.kcols)

@@ -249,20 +249,24 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * Tables (built once per pattern set):
  *   S: the n_s distinct non-zero half cells (u, w), w in [0, N/2], sorted by
  *      (packed column w' = (w == N/2 ? 0 : w), n', u div LC, w == N/2) with
- *      n' = u mod LC, LC = N / dsb_image_fold(N); a slot is one (w', n');
+ *      n' = u mod LC, LC = N / fold; a slot is one (w', n');
  *   c_meta[cell_base[g] + k] = s | conj << 16 | g << 17: pattern cell k <
  *      n_filled[g] of chgroup g adds its value (conjugated if conj) to S
  *      entry s; each chgroup's run is padded with 0xffffffff to a multiple
  *      of 64 entries (cell_base[g] multiples of 64);
  *   c2[i] = {k | g << 16, s | conj << 16}: second targets (cells on w = 0 or
  *      w = N/2 that also land on their mirror);
- *   thr_b: (dsb_image_threads() + 1) S ranges, one per kernel thread, each
- *      made of whole slots and at most dsb_image_max_entries() long;
- *   gmeta: (max_entries / 8, threads, 8) uint16, 16-byte aligned: entry i
- *      of thread t at [i / 8][t][i % 8] = w' | n' << 7 | (u div LC) << 13 |
- *      (last entry of its slot) << 15;
- *   srot: (threads) uint64, 2 bits per entry i at bit 2i: (w == N/2) |
- *      ((u + w) & 1) << 1;
+ *   thr_b: (threads + 1) S ranges, one per kernel thread, each made of whole
+ *      slots and at most max_entries long;
+ *   gmeta, 16-byte aligned, in the form of meta_bits:
+ *      16: (max_entries / 8, threads, 8) uint16, entry i of thread t at
+ *      [i / 8][t][i % 8] = w' | n' << 7 | (u div LC) << 13 | (last entry of
+ *      its slot) << 15;
+ *      32: (max_entries / 4, threads, 4) uint32, entry i of thread t at
+ *      [i / 4][t][i % 4] = w' | n' << 8 | (u div LC) << 14 | last << 17 |
+ *      (w == N/2) << 18 | ((u + w) & 1) << 19;
+ *   srot (16-bit form only; may be null for the 32-bit form): (threads)
+ *      uint64, 2 bits per entry i at bit 2i: (w == N/2) | ((u + w) & 1) << 1;
  *   dcols/dmask: the n_dense packed columns with an entry off n' = 0 and
  *      the bit mask of their occupied n';
  *   kcols: the n_const other packed columns, w' | (has entries) << 16;
@@ -283,15 +287,18 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * read: the caller keeps a row alive while the ring holds its chunk and
  * zeroes it before stage 1 writes a new chunk into it.  A non-finite bound
  * sets DSB_E_ARG in *status.
- * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256; n_s must
- * fit the kernel's shared buffer (N/4 x (N/2 + 2) cells) or DSB_E_CAPACITY
- * is returned.  status: a thread range longer than max_entries or a
- * cell_base[g] that is not a multiple of 64 sets DSB_E_CAPACITY and writes
- * nothing.  Each
- * CTA holds 128 columns of tensor memory while it runs. */
-int dsb_image_fold(int n_grid);
-int dsb_image_threads(void);
-int dsb_image_max_entries(void);
+ * twiddles: (N) complex64 exp(+2 pi i e/N).  Supported N: 64, 256, 512; n_s
+ * must fit the kernel's S capacity (s_capacity of dsb_image_geometry) or
+ * DSB_E_CAPACITY is returned.  status: a thread range longer than
+ * max_entries or a cell_base[g] that is not a multiple of 64 sets
+ * DSB_E_CAPACITY and writes nothing.  Each CTA holds 128 columns of tensor
+ * memory while it runs (all 512 of its SM at N = 512). */
+/* The kernel's geometry at grid size n_grid, for building the tables above:
+ * geom[0] fold (column passes, LC = N / fold), geom[1] threads per CTA,
+ * geom[2] max_entries (S entries per thread), geom[3] meta_bits (16 or 32),
+ * geom[4] s_capacity.  DSB_E_UNSUPPORTED for any other n_grid.  No
+ * counterpart in the reference (a query for the tables of dsb_image_fft). */
+int dsb_image_geometry(int n_grid, int* geom);
 int dsb_image_fft(const void* D, int d_format, const long long* seg_base, const int* seg_depth,
                   const float* scales, const long long* sc_base, const float* amax,
                   const int* shift2, int amax_chunk, int amax_rows, int n_coarse,

@@ -32,6 +32,7 @@ Geometry is parametric (the reference hard-codes 96 antennas and
 
 from __future__ import annotations
 
+import math
 from collections import deque
 from dataclasses import dataclass
 from typing import List, Optional, Sequence, Tuple
@@ -412,22 +413,27 @@ def build_cell_csr(cim: np.ndarray, n_filled: int):
 def stage1_dedisp(vis: np.ndarray, shifts: np.ndarray, cim: np.ndarray,
                   n_filled: int, t_dedisp: int) -> np.ndarray:
     """``out[d, t, cell] = sum_{(b,c) in cell} vis[t + shift[c, d], b, c]``
-    (corr_fast_integration.py:647-700).  ``vis`` ``(T, nbase, C)``, any
-    numeric dtype; ``shifts`` ``(C, n_dm)``.  Sum is exact for integer input.
-    """
+    (corr_fast_integration.py:647-700).  ``vis`` ``(T, nbase, C)`` integers
+    (or any exact type); ``shifts`` ``(C, n_dm)``.  The sum is taken as the
+    reference's gather over each cell's (baseline, channel) sources, grouped
+    by channel: first every channel's baselines are summed into its cells,
+    then each DM adds the channels' rows at their shifted times.  For integer
+    input the result is exact, so the grouping cannot change it."""
+    from scipy.sparse import csr_matrix
     T, nb, nc = vis.shape
     n_dm = shifts.shape[1]
-    offs, sb, sc = build_cell_csr(cim, n_filled)
-    nz = np.diff(offs) > 0
     out = np.zeros((n_dm, t_dedisp, n_filled), dtype=vis.dtype)
-    t = np.arange(t_dedisp)
+    b, c = np.nonzero(cim < n_filled)
+    if b.size == 0:
+        return out
+    cell = cim[b, c].astype(np.int64)
+    M = csr_matrix((np.ones(b.size, vis.dtype), (b * nc + c, c * n_filled + cell)),
+                   shape=(nb * nc, nc * n_filled))
+    Y = np.asarray(vis.reshape(T, nb * nc) @ M).reshape(T, nc, n_filled)
     for d in range(n_dm):
-        if sb.size == 0:
-            break
-        # gather every source at its shifted time, then segment-sum per cell
-        tt = t[:, None] + shifts[sc, d][None, :]            # (t, nsrc)
-        vals = vis[tt, sb[None, :], sc[None, :]]              # (t, nsrc)
-        out[d][:, nz] = np.add.reduceat(vals, offs[:-1][nz], axis=1)
+        for ch in range(nc):
+            sh = int(shifts[ch, d])
+            out[d] += Y[sh:sh + t_dedisp, ch]
     return out
 
 
@@ -635,12 +641,20 @@ def combine_half(streams: np.ndarray, shifts: np.ndarray, t_det: int, t_lo: int 
                  fftshift: bool = True) -> np.ndarray:
     """Hermitian half-spectrum ``0.5 (G[u,w] + conj G[-u,-w])``, ``w <= N/2``
     (fused_combine_cuda.py:560-620)."""
-    full = combine_full(streams, shifts, t_det, t_lo, fftshift=False)
+    return half_from_full(combine_full(streams, shifts, t_det, t_lo, fftshift=False), fftshift)
+
+
+def half_from_full(full: np.ndarray, fftshift: bool = True) -> np.ndarray:
+    """The Hermitian half spectrum of combined grids ``full`` (T, N, N):
+    ``0.5 (G[u,w] + conj G[-u,-w])`` for ``w <= N/2``, times the checkerboard
+    ``(-1)^(u+w)`` when ``fftshift`` (fused_combine_cuda.py:560-620)."""
     N = full.shape[-1]
     u = np.arange(N)
-    um = (N - u) % N
-    h = 0.5 * (full + np.conj(full[:, um][:, :, um]))
-    h = h[:, :, : N // 2 + 1]
+    # G[-u, -w] for w in [0, N/2]: rows reversed and rolled by one (row 0
+    # stays), then column 0 followed by columns N-1 down to N/2
+    rows = np.roll(full[:, ::-1, :], 1, axis=1)
+    mir = np.concatenate([rows[:, :, :1], rows[:, :, N - 1:N // 2 - 1:-1]], axis=2)
+    h = 0.5 * (full[:, :, : N // 2 + 1] + np.conj(mir))
     if fftshift:
         w = np.arange(N // 2 + 1)
         h *= (1 - 2 * ((u[:, None] + w[None, :]) & 1))
@@ -956,7 +970,7 @@ def round_bf16_complex(z: np.ndarray) -> np.ndarray:
 def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block, t_int, csf,
                  n_grid, coarse_dm, fine_dm, fine_to_coarse, log_max_width, threshold, chunk,
                  use_sky=True, sky_window=8, sky_warmup=8, n_top=256, r_t=4, r_f=5, r_lm=3,
-                 l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None):
+                 l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None, keep_images=True):
     """Oracle of the CUDA streaming pipeline; returns candidate tuples
     ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates.
     ``ring_dtype="bf16"`` stores the stage-2 streams in the BF16 form (each
@@ -1033,28 +1047,40 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
         cube = np.zeros((nt, n_fine, N, N), np.float32)
         for f in range(n_fine):
             c = int(fine_to_coarse[f])
-            streams = np.zeros((G, nt, N, N), np.complex128)
-            for g in range(G):
-                r, cc = tb["pats"][g]
-                for t in range(nt):
-                    ts = t0 + t - int(tb["sf"][f, g]) - int(tb["sh2"][g, c])
-                    if 0 <= ts < T1:
-                        streams[g, t, r.astype(np.int64), cc.astype(np.int64)] = D1[g][c][ts]
-            half = combine_half(streams, np.zeros(G, np.int64), nt, 0, fftshift=True)
-            img = image_from_half(half, N)                            # float64 (nt, N, N)
+            img = np.zeros((nt, N, N), np.float64)
+            # the combine of combine_half (sum over chgroups, Hermitian half,
+            # checkerboard) a few times at a time, so that 512^2 cubes stay small
+            for s0 in range(0, nt, 16):
+                s1 = min(nt, s0 + 16)
+                full = np.zeros((s1 - s0, N, N), np.complex128)
+                for g in range(G):
+                    r, cc = tb["pats"][g]
+                    ri, ci = r.astype(np.int64), cc.astype(np.int64)
+                    for t in range(s0, s1):
+                        ts = t0 + t - int(tb["sf"][f, g]) - int(tb["sh2"][g, c])
+                        if 0 <= ts < T1:
+                            full[t - s0, ri, ci] += D1[g][c][ts]
+                half = half_from_full(full, fftshift=True)
+                img[s0:s1] = image_from_half(half, N)                   # float64
             img32 = img.astype(np.float32)
             samp = img32.reshape(nt, N * N)[l1_t][:, l1_pix].reshape(1, -1)
             sig = sigma_clipped_std_batched(samp)[0]
             sig = np.float32(sig if sig > 0 else 1.0)
             mf = (mask / sig).astype(np.float32)
             cube[:, f] = (img32 * mf[None]).astype(np.float32)
-            images.append(img)
-        cs = padded_cumsum(cube, 1 << log_max_width)
-        score, win = multi_boxcar_argmax(cs, widths, offs, sinv, chunk, te)
+            if keep_images:
+                images.append(img)
+        score = np.zeros((chunk, n_fine, N, N), np.float32)
+        win = np.zeros((chunk, n_fine, N, N), np.int16)
+        for r0 in range(0, N, 64):          # pixel-row slabs: the boxcars are per pixel
+            cs = padded_cumsum(cube[:, :, r0:r0 + 64], 1 << log_max_width)
+            score[:, :, r0:r0 + 64], win[:, :, r0:r0 + 64] = multi_boxcar_argmax(
+                cs, widths, offs, sinv, chunk, te)
         for cd in decode_topk(score, win, threshold=threshold, n_top=n_top, r_t=r_t, r_f=r_f,
                               r_lm=r_lm):
             cands.append((jc * chunk - te + cd.t, cd.f, cd.l, cd.m, cd.snr, widths[cd.k]))
-        keep.setdefault("cubes", []).append(cube)
+        if keep_images:
+            keep.setdefault("cubes", []).append(cube)
     keep["images"] = images
     keep["tables"] = tb
     return cands

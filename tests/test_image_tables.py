@@ -34,14 +34,25 @@ def _patterns(N, n_g, seed):
     return pats
 
 
+def _meta_fields(T, m):
+    """(column, n', q, last, rotation bits) of entry metadata m in the table's
+    form: 16-bit w' | n' << 7 | q << 13 | last << 15 with the rotation bits in
+    srot, or 32-bit w' | n' << 8 | q << 14 | last << 17 | rot << 18."""
+    m = np.asarray(m, np.int64)
+    if T.meta_bits == 16:
+        return m & 127, (m >> 7) & 63, (m >> 13) & 3, (m >> 15) & 1, None
+    return m & 255, (m >> 8) & 63, (m >> 14) & 7, (m >> 17) & 1, (m >> 18) & 3
+
+
 def _emulate(T, slices, N, fftshift):
     """The kernel's steps, from its tables: combine into S, per-thread ranges
     with the static rotation, the per-pass fold into slots, dense columns
     transformed from their occupied slots only, constant columns broadcast,
     then the row transforms.  Slots no thread writes in a pass are NaN, so a
     read of one shows up in the result."""
-    fold = 4
+    fold = T.fold
     LC, NC = N // fold, N // 2
+    epv = T.gmeta.shape[2]
     S = np.zeros(T.n_s, np.complex128)
     for g, v in enumerate(slices):
         m = T.c_meta[T.cell_base[g]:T.cell_base[g] + v.size].astype(np.int64)
@@ -52,6 +63,7 @@ def _emulate(T, slices, N, fftshift):
         S[sc & 0xFFFF] += np.conj(v) if (sc >> 16) & 1 else v
     A = np.zeros((N, NC), np.complex128)
     twN = np.exp(2j * np.pi * np.arange(N) / N)
+    wf = np.exp(2j * np.pi * np.arange(fold) / fold)      # W_FOLD^k
     n_thr = T.thr_b.size - 1
     for p in range(fold):
         buf = np.full((LC, NC), np.nan, np.complex128)
@@ -59,12 +71,12 @@ def _emulate(T, slices, N, fftshift):
             b, e = int(T.thr_b[t]), int(T.thr_b[t + 1])
             acc = 0j
             for i in range(e - b):
-                m = int(T.gmeta[i // 8, t, i % 8])
-                sr = (int(T.srot[t]) >> (2 * i)) & 3
-                rot = (sr & 1) + (2 if (sr & 2) and fftshift else 0) + ((m >> 13) & 3) * p
-                acc += S[b + i] * (1j) ** (rot % 4)
-                if m & 0x8000:
-                    buf[(m >> 7) & (LC - 1), m & (NC - 1)] = acc
+                col, npr, q, last, rot = _meta_fields(T, int(T.gmeta[i // epv, t, i % epv]))
+                sr = (int(T.srot[t]) >> (2 * i)) & 3 if rot is None else int(rot)
+                stat = (1j) ** ((sr & 1) + (2 if (sr & 2) and fftshift else 0))
+                acc += S[b + i] * stat * wf[(int(q) * p) % fold]
+                if last:
+                    buf[int(npr), int(col)] = acc
                     acc = 0j
         out = np.full((LC, NC), np.nan, np.complex128)
         for col, occ in zip(T.dcols.tolist(), T.dmask.tolist()):
@@ -97,7 +109,8 @@ def _definition(pats, slices, N, fftshift):
     return np.fft.irfft2(H, s=(N, N))
 
 
-@pytest.mark.parametrize("N,n_g,fftshift", [(64, 3, True), (64, 2, False), (256, 4, True)])
+@pytest.mark.parametrize("N,n_g,fftshift", [(64, 3, True), (64, 2, False), (256, 4, True),
+                                             (512, 4, True)])
 def test_image_tables_restate_irfft2(N, n_g, fftshift):
     pats = _patterns(N, n_g, seed=7 + N)
     T = build_image_tables(pats, N)
@@ -109,28 +122,31 @@ def test_image_tables_restate_irfft2(N, n_g, fftshift):
     assert np.abs(got - want).max() <= 1e-12 * max(1.0, np.abs(want).max())
 
 
-def test_image_tables_layout():
-    from dsb200 import _lib
-    N = 256
+@pytest.mark.parametrize("N", [256, 512])
+def test_image_tables_layout(N):
+    from dsb200.pipeline import image_geometry
     pats = _patterns(N, 3, seed=3)
     T = build_image_tables(pats, N)
-    LC, NC = N // 4, N // 2
-    n_thr, cap = int(_lib.lib().dsb_image_threads()), int(_lib.lib().dsb_image_max_entries())
+    geo = image_geometry(N)
+    assert T.fold == geo["fold"] and T.meta_bits == geo["meta_bits"]
+    LC, NC = N // T.fold, N // 2
+    n_thr, cap = geo["threads"], geo["max_entries"]
+    epv = 8 if T.meta_bits == 16 else 4
     assert T.thr_b.size == n_thr + 1 and T.thr_b[0] == 0 and T.thr_b[-1] == T.n_s
     cnt = np.diff(T.thr_b)
     assert np.all(cnt >= 0) and cnt.max() <= cap
-    assert T.gmeta.shape == (cap // 8, n_thr, 8)
+    assert T.gmeta.shape == (cap // epv, n_thr, epv)
     # entries in S order: slot (w', n') of each, and "last" on its final entry
     owner = np.repeat(np.arange(n_thr), cnt)
     idx = np.arange(T.n_s) - T.thr_b[owner]
-    m = T.gmeta[idx // 8, owner, idx % 8].astype(np.int64)
-    slot = (m & 127) * LC + ((m >> 7) & (LC - 1))
+    col, npr, q, last_bit, _ = _meta_fields(T, T.gmeta[idx // epv, owner, idx % epv])
+    slot = col * LC + npr
     assert np.all(np.diff(slot) >= 0)                    # S is sorted by slot
     last = np.append(slot[1:] != slot[:-1], True)
-    assert np.array_equal((m >> 15).astype(bool), last)
+    assert np.array_equal(last_bit.astype(bool), last)
     # every thread range ends on a slot boundary (whole slots per thread)
     ends = T.thr_b[1:][cnt > 0] - 1
-    assert np.all((m[ends] >> 15) == 1)
+    assert np.all(last_bit[ends] == 1)
     # columns: each packed column once; dense masks are the occupied n'
     cols = np.concatenate([T.dcols, T.kcols & 0xFFFF])
     assert sorted(cols.tolist()) == list(range(NC))
@@ -144,7 +160,7 @@ def test_image_tables_layout():
     assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 64 == 0)
     for g, p in enumerate(pats):                # padding after each chgroup's run
         assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
-    assert T.n_s <= LC * (N // 2 + 2)          # fits the kernel's shared buffer
+    assert T.n_s <= geo["s_capacity"]          # fits the kernel's shared S arrays
     # every S entry is hit by at least one pattern cell
     hit = np.zeros(T.n_s, bool)
     live = T.c_meta != 0xFFFFFFFF

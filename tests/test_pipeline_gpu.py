@@ -28,6 +28,25 @@ def dev():
     return torch.device("cuda", 0)
 
 
+def compare_candidates(got, want, threshold):
+    """Candidate lists of the GPU pipeline and the oracle: identical (time,
+    fine DM, pixel, width) keys, S/N within 1e-5 relative, except a
+    candidate within the epsilon band of the threshold, which may appear in
+    one list only.  Returns the largest S/N relative difference."""
+    key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
+    g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
+    w_map = {key(c): c[4] for c in want}
+    worst = 0.0
+    for k in set(g_map) | set(w_map):
+        if k in g_map and k in w_map:
+            worst = max(worst, abs(g_map[k] - w_map[k]) / abs(w_map[k]))
+            assert abs(g_map[k] - w_map[k]) <= 1e-5 * abs(w_map[k]), (k, g_map[k], w_map[k])
+        else:
+            v = g_map.get(k, w_map.get(k))
+            assert abs(v - threshold) < EPS_BAND * threshold, f"unmatched candidate {k} snr={v}"
+    return worst
+
+
 def _setup(n_blocks=8, amp=1.0):
     from dsb200 import synth
     from dsb200.constants import band_from_edges
@@ -99,20 +118,113 @@ def test_pipeline_matches_oracle(dev, ring, dm_group):
                 else:
                     assert top * (1 - 2.0 ** -8) <= b <= top * (1 + 2.0 ** -8), (g, d, b, top)
 
-    key = lambda c: (c[0], c[1], c[2], c[3], c[5])  # noqa: E731
-    g_map = {key((c.t, c.fdm, c.l, c.m, c.snr, c.width)): c.snr for c in got}
-    w_map = {key(c): c[4] for c in want}
-    worst = 0.0
-    for k in set(g_map) | set(w_map):
-        if k in g_map and k in w_map:
-            worst = max(worst, abs(g_map[k] - w_map[k]) / abs(w_map[k]))
-            assert abs(g_map[k] - w_map[k]) <= 1e-5 * abs(w_map[k]), (k, g_map[k], w_map[k])
-        else:
-            v = g_map.get(k, w_map.get(k))
-            assert abs(v - 6.0) < EPS_BAND * 6.0, f"unmatched candidate {k} snr={v}"
+    worst = compare_candidates(got, want, threshold=6.0)
     print(f"ring {ring}: largest S/N relative difference {worst:.2e}")
     # the injected burst is recovered at its pixel
     assert any(c.l == 32 + 3 and c.m == 32 - 5 for c in got)
+
+
+def test_pipeline_512_grid_boxcars_to_64_matches_oracle(dev):
+    """The imaging and detection of the metric configuration (512^2 grid,
+    boxcars 1..64, bf16 ring) on a small array: a 16-antenna T layout, two
+    chgroups of 32 channels, two coarse x two fine DMs, one dispersed burst
+    at DM 20 with a 96-sample width.  Stage-2 ring bit-exact, candidate
+    lists identical outside the epsilon band, S/N within 1e-5 relative of the
+    oracle (float64 images)."""
+    from dsb200 import synth
+    from dsb200.constants import band_from_edges
+    from dsb200.pipeline import PipelineConfig, SearchPipeline
+    band = band_from_edges(2, 32, 1.49875, 1.31125)
+    ob = O.Band(band.n_chgroup, band.nchan, band.f0_ghz, band.dnu_ghz, band.ch0)
+    nant, npkt, N = 16, 256, 512
+    e, n = synth.t_layout(nant, seed=5)
+    cell = O.top_of_band_cell_lambda(e, n, ob, N)
+    coarse = np.array([15.0, 35.0])
+    fine = (coarse[:, None] + np.array([-5.0, 5.0])[None]).reshape(-1)
+    f2c = np.repeat(np.arange(2), 2)
+    bursts = [synth.Burst(dm=20.0, t0_native=1500, width_native=96, amp=0.6, dl=40,
+                          dm_pix=-70)]
+    blocks = [synth.make_block(band=band, nant=nant, npkt=npkt, block_index=b, seed=9,
+                               antpos_e=e, antpos_n=n, bursts=bursts, cell_lambda=cell,
+                               n_grid=N) for b in range(7)]
+    kw = dict(nant=nant, npkt_block=npkt, t_int=8, csf=4, n_grid=N, coarse_dm=coarse,
+              fine_dm=fine, fine_to_coarse=f2c, log_max_width=6, threshold=6.0)
+    cfg = PipelineConfig(band=band, sky_window=2, sky_warmup=1, chunk_tiles=64, fdm_batch=3,
+                         ring_dtype="bf16", **kw)
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    got = []
+    for b in blocks:
+        got += pipe.process_block(torch.from_numpy(b).to(dev))
+    torch.cuda.synchronize()
+    pipe.check_status()
+    keep = {}
+    want = O.run_pipeline(blocks, ob, e, n, chunk=64, sky_window=2, sky_warmup=1, keep=keep,
+                          keep_images=False, ring_dtype="bf16", **kw)
+    assert len(want) >= 5, "oracle found no burst candidate"
+    T1 = keep["D1"][0][0].shape[0]
+    t1 = np.arange(T1 - 64, T1)
+    for g in range(band.n_chgroup):
+        for d in range(coarse.size):
+            np.testing.assert_array_equal(pipe.ring_values(g, d, t1 + pipe.tab.shift2[g, d]),
+                                          keep["D1"][g][d][t1].astype(np.complex64))
+    worst = compare_candidates(got, want, threshold=6.0)
+    print(f"512^2, boxcars 1..64: largest S/N relative difference {worst:.2e}")
+    best = max(got, key=lambda c: c.snr)
+    assert (best.l, best.m) == (N // 2 + 40, N // 2 - 70) and best.width >= 8
+
+
+def test_config1_small_plain_pipeline_matches_oracle(dev):
+    """The small plain configuration as stated: 16 dual-pol antennas on a
+    seeded T layout (136 baselines with autos), 256 channels over
+    1311.25-1498.75 MHz (two chgroups of 128), 4096-sample blocks of 4-bit
+    Gaussian voltages (sigma 3, clipped), 8-sample correlation, 64^2 grid,
+    32 trial DMs 0-600, boxcars 1..16, threshold 7, one point-source burst at
+    DM 300, 4 samples wide.  At DM 300 the sweep across the band (170 ms) is
+    longer than one block (134 ms), and stage 2 holds the top of the band
+    back by the DM-600 delay (1289 tiles), so the stream runs six blocks and
+    the burst arrives in the third: its band-bottom time falls in the first
+    detector cube that has data from both chgroups at every time.  Ring
+    bit-exact, candidates identical outside the epsilon band, S/N within
+    1e-5 relative of the oracle, the burst recovered at its pixel."""
+    from dsb200 import synth
+    from dsb200.constants import band_from_edges
+    from dsb200.pipeline import PipelineConfig, SearchPipeline
+    band = band_from_edges(2, 128, 1.49875, 1.31125)
+    ob = O.Band(band.n_chgroup, band.nchan, band.f0_ghz, band.dnu_ghz, band.ch0)
+    nant, npkt, N = 16, 2048, 64
+    e, n = synth.t_layout(nant, seed=21)
+    cell = O.top_of_band_cell_lambda(e, n, ob, N)
+    dms = np.linspace(0.0, 600.0, 32)
+    bursts = [synth.Burst(dm=300.0, t0_native=8800, width_native=4, amp=2.0, dl=9,
+                          dm_pix=-13)]
+    blocks = [synth.make_block(band=band, nant=nant, npkt=npkt, block_index=b, seed=31,
+                               antpos_e=e, antpos_n=n, bursts=bursts, cell_lambda=cell,
+                               n_grid=N) for b in range(6)]
+    kw = dict(nant=nant, npkt_block=npkt, t_int=8, csf=1, n_grid=N, coarse_dm=dms, fine_dm=dms,
+              fine_to_coarse=np.arange(32), log_max_width=4, threshold=7.0)
+    cfg = PipelineConfig(band=band, sky_window=2, sky_warmup=1, chunk_tiles=512, fdm_batch=32,
+                         ring_dtype="c64", **kw)
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    got = []
+    for b in blocks:
+        got += pipe.process_block(torch.from_numpy(b).to(dev))
+    torch.cuda.synchronize()
+    pipe.check_status()
+    keep = {}
+    want = O.run_pipeline(blocks, ob, e, n, chunk=512, sky_window=2, sky_warmup=1, keep=keep,
+                          keep_images=False, ring_dtype="c64", **kw)
+    assert len(want) >= 3, "oracle found no burst candidate"
+    T1 = keep["D1"][0][0].shape[0]
+    t1 = np.arange(T1 - 512, T1)
+    for g in range(band.n_chgroup):
+        for d in (0, 15, 31):
+            np.testing.assert_array_equal(pipe.ring_values(g, d, t1 + pipe.tab.shift2[g, d]),
+                                          keep["D1"][g][d][t1].astype(np.complex64))
+    worst = compare_candidates(got, want, threshold=7.0)
+    print(f"config 1: largest S/N relative difference {worst:.2e}")
+    best = max(got, key=lambda c: c.snr)
+    assert (best.l, best.m) == (N // 2 + 9, N // 2 - 13)
+    assert abs(cfg.fine_dm[best.fdm] - 300.0) < 20.0
 
 
 def test_streaming_host_blocks_match_device_blocks(dev):
@@ -149,7 +261,7 @@ def test_pipeline_rejects_wrong_raw_size(dev):
 
 
 @pytest.mark.parametrize("ring", ["c64", "bf16", "cint8"])
-@pytest.mark.parametrize("N", [64, 256])
+@pytest.mark.parametrize("N", [64, 256, 512])
 def test_image_fft_matches_combine_and_irfft2(dev, N, ring):
     """Fused combine + 2-D c2r FFT == dsb_combine_rows + torch.fft.irfft2 on
     the same (random) stage-2 ring, float32 tolerance 2e-6 of the image scale,
