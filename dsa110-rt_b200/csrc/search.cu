@@ -254,25 +254,33 @@ __global__ void padded_cumsum_kernel(const T* __restrict__ x, int n, long long i
   for (int r = 0; r < pr; ++r) cs[(long long)(1 + pl + n + r) * inner + e] = last;
 }
 
-template <bool OUT_F16>
+// CHECK: every prefix row read must lie in [0, cs_rows); an output whose
+// widths / offsets would read outside gets S/N NaN and winner -1 instead
+// (the rows outside belong to no call's data: the shared scratch array of
+// dsb_boxcar_argmax_noalloc).
+template <bool OUT_F16, bool CHECK = false>
 __global__ void multi_boxcar_argmax_kernel(const float* __restrict__ cs, long long inner,
                                            const int* __restrict__ widths,
                                            const int* __restrict__ offsets,
                                            const float* __restrict__ sinv, int K, int n_out,
                                            int t_base, void* __restrict__ out_max,
-                                           int16_t* __restrict__ out_win) {
+                                           int16_t* __restrict__ out_win, long long cs_rows = 0) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n_out * inner) return;
   const int t = (int)(idx / inner);
   const long long e = idx % inner;
   const int ta = t + t_base;
-  float best = (cs[(long long)(ta + offsets[0] + widths[0]) * inner + e] -
-                cs[(long long)(ta + offsets[0]) * inner + e]) * sinv[0];
+  float best = 0.f;
   int win = 0;
-  for (int k = 1; k < K; ++k) {
-    const float s = (cs[(long long)(ta + offsets[k] + widths[k]) * inner + e] -
-                     cs[(long long)(ta + offsets[k]) * inner + e]) * sinv[k];
-    if (s > best) {
+  for (int k = 0; k < K; ++k) {
+    const long long lo = (long long)ta + offsets[k], hi = lo + widths[k];
+    if (CHECK && (lo < 0 || hi < 0 || lo >= cs_rows || hi >= cs_rows)) {
+      best = __int_as_float(0x7fc00000);
+      win = -1;
+      break;
+    }
+    const float s = (cs[hi * inner + e] - cs[lo * inner + e]) * sinv[k];
+    if (k == 0 || s > best) {
       best = s;
       win = k;
     }
@@ -788,33 +796,87 @@ int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, i
 // below, DSB_NOALLOC_SCRATCH_BYTES (16 MiB) long, which every GPU that
 // loads this file's device code holds until the process exits.
 // ===========================================================================
-#include <atomic>
+#include <cuda.h>
+
 #include <mutex>
 
 static __device__ __align__(256) float g_boxcar_cs_scratch[DSB_NOALLOC_SCRATCH_BYTES / 4];
 
 namespace {
 
-constexpr int kNoallocMaxDevices = 64;
-std::atomic<float*> g_boxcar_cs_ptr[kNoallocMaxDevices];
-std::mutex g_boxcar_cs_mu;
+// The scratch array's device address belongs to one CUDA context: after a
+// cudaDeviceReset, or under another context on the same device, it is a
+// different address.  So the cache is keyed on the current context's unique
+// ID (cuCtxGetId, never reused within a process), looked up through the
+// runtime's driver entry points so that the library needs no libcuda link.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of the scratch array on the current device, looked up once
-// per device (on that device's first call) and cached.  Null on failure.
-float* boxcar_cs_scratch(int dev) {
-  float* p = g_boxcar_cs_ptr[dev].load(std::memory_order_acquire);
-  if (p) return p;
-  std::lock_guard<std::mutex> lock(g_boxcar_cs_mu);
-  p = g_boxcar_cs_ptr[dev].load(std::memory_order_relaxed);
-  if (p) return p;
+constexpr int kNoallocCache = 64;
+struct NoallocEntry {
+  unsigned long long ctx_id;
+  float* ptr;
+};
+NoallocEntry g_noalloc_cache[kNoallocCache];
+int g_noalloc_n = 0;
+std::mutex g_noalloc_mu;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+bool load_ctx_fns() {
+  if (g_ctx_get_current && g_ctx_get_id) return true;
+  void* f1 = nullptr;
+  void* f2 = nullptr;
+  cudaDriverEntryPointQueryResult q1{}, q2{};
+  if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+      cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+      q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+    cudaGetLastError();
+    return false;
+  }
+  g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+  g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
+  return true;
+}
+
+// The unique ID of the context current on this thread; 0 when there is none.
+unsigned long long current_ctx_id() {
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the scratch array in the current context (the current
+// device's primary context for a runtime caller), looked up on the first
+// call in that context and cached.  Null on failure.
+float* boxcar_cs_scratch() {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!load_ctx_fns()) return nullptr;
+  unsigned long long id = current_ctx_id();
+  if (id) {
+    for (int i = 0; i < g_noalloc_n; ++i)
+      if (g_noalloc_cache[i].ctx_id == id) return g_noalloc_cache[i].ptr;
+  }
+  // not seen yet (the runtime makes the device's context current here if
+  // no context was)
   void* addr = nullptr;
   if (cudaGetSymbolAddress(&addr, g_boxcar_cs_scratch) != cudaSuccess || !addr) {
     cudaGetLastError();
     return nullptr;
   }
-  p = static_cast<float*>(addr);
-  g_boxcar_cs_ptr[dev].store(p, std::memory_order_release);
-  return p;
+  if (!id) id = current_ctx_id();
+  if (id) {
+    // the oldest entry goes when the table is full (a process that made
+    // more than 64 contexts); its context looks the address up again
+    if (g_noalloc_n == kNoallocCache) {
+      for (int i = 1; i < kNoallocCache; ++i) g_noalloc_cache[i - 1] = g_noalloc_cache[i];
+      --g_noalloc_n;
+    }
+    g_noalloc_cache[g_noalloc_n++] = NoallocEntry{id, static_cast<float*>(addr)};
+  }
+  return static_cast<float*>(addr);
 }
 
 }  // namespace
@@ -828,18 +890,29 @@ extern "C" int dsb_boxcar_argmax_noalloc(const void* x, int x_f16, int n, long l
   if (n <= 0 || inner <= 0 || max_w < 1 || max_w > n || K < 1 || n_out <= 0 || t_base < 0 ||
       (long long)t_base + n_out > n)
     return DSB_E_ARG;
-  if ((long long)(n + max_w) * inner > (long long)(DSB_NOALLOC_SCRATCH_BYTES / 4))
-    return DSB_E_CAPACITY;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return DSB_E_CUDA;
-  if (dev < 0 || dev >= kNoallocMaxDevices) return DSB_E_UNSUPPORTED;
-  float* cs = boxcar_cs_scratch(dev);
+  // (n + max_w) rows of inner floats must fit the array; the sum is formed
+  // in 64 bits and inner is bounded first, so neither the sum nor the
+  // product can overflow
+  constexpr long long kCap = (long long)(DSB_NOALLOC_SCRATCH_BYTES / 4);
+  const long long rows = (long long)n + max_w;
+  if (inner > kCap || rows * inner > kCap) return DSB_E_CAPACITY;
+  float* cs = boxcar_cs_scratch();
   if (!cs) return DSB_E_CUDA;
   // padded_cumsum_kernel writes every one of the (n + max_w) x inner prefix
   // values, its zero padding rows included, so nothing left in the array by
-  // an earlier call is read.
+  // an earlier call is read; the argmax below checks every row it reads
+  // against those (n + max_w) rows.
   const int rc = dsb_padded_cumsum(x, x_f16, n, inner, max_w, cs, stream);
   if (rc != DSB_OK) return rc;
-  return dsb_multi_boxcar_argmax(cs, inner, widths, offsets, sigma_inv, K, n_out, t_base,
-                                 out_max, out_f16, out_win, stream);
+  const long long total = (long long)n_out * inner;
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  if (out_f16)
+    multi_boxcar_argmax_kernel<true, true><<<grid, 256, 0, stream>>>(
+        cs, inner, widths, offsets, sigma_inv, K, n_out, t_base, out_max, (int16_t*)out_win,
+        rows);
+  else
+    multi_boxcar_argmax_kernel<false, true><<<grid, 256, 0, stream>>>(
+        cs, inner, widths, offsets, sigma_inv, K, n_out, t_base, out_max, (int16_t*)out_win,
+        rows);
+  return launch_status();
 }

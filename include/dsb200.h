@@ -338,12 +338,17 @@ int dsb_multi_boxcar_argmax(const float* cs, long long inner, const int* widths,
  * device).  No counterpart in dsa110-rt: it has no such callers.  The prefix
  * sums live in a fixed array inside the library, DSB_NOALLOC_SCRATCH_BYTES
  * long, held on every GPU that loads the library until the process exits;
- * (n + max_w) * inner * 4 bytes beyond it return DSB_E_CAPACITY.  The first
- * call on each device looks up that array's address, so make it before any
- * stream capture.  Every call shares the one array: calls that overlap on
- * the GPU (two streams, or two host threads) race and must be serialised by
- * the caller.  Needs t_base + n_out <= n and the centred offsets
- * max_w/2 - widths[k]/2 with widths[k] <= max_w.  Allocates nothing. */
+ * (n + max_w) * inner * 4 bytes beyond it return DSB_E_CAPACITY (computed in
+ * 64 bits, so no n, max_w or inner can wrap past the check).  The first
+ * call in each CUDA context looks up that array's address (cached per
+ * context ID, so a cudaDeviceReset or another context gets its own lookup),
+ * so make it before any stream capture.  Every call shares the one array:
+ * calls that overlap on the GPU (two streams, or two host threads) race and
+ * must be serialised by the caller.  Needs t_base + n_out <= n and the
+ * centred offsets max_w/2 - widths[k]/2 with widths[k] <= max_w; an output
+ * whose widths / offsets would read a prefix row outside this call's
+ * n + max_w rows gets S/N NaN and winner -1 (nothing outside is read).
+ * Allocates nothing. */
 #define DSB_NOALLOC_SCRATCH_BYTES (16u << 20)
 int dsb_boxcar_argmax_noalloc(const void* x, int x_f16, int n, long long inner, int max_w,
                               const int* widths, const int* offsets, const float* sigma_inv,
