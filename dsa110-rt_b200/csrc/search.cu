@@ -318,6 +318,19 @@ struct DetCand {
 // Element e = f * npix + p of time t is read at x[f*f_stride + t*t_stride + p]
 // and multiplied by mask[f*npix + p] when a mask is given (the per-fine-DM
 // edge mask x 1/sigma), so the detector consumes the FFT output directly.
+// Layer-2 score samples (noise_norm/layer2.py, the streaming detector's
+// per-kernel subsample, detector/forward.py:1425-1530): entries {eg, t, k,
+// slot} sorted by (eg, t), eg = e + pix_off the cell's index over all fine
+// DMs, t the output index (ta - t_base); off[gb] the first entry of global
+// 256-cell block gb.  Each entry's raw boxcar sum of width 2^k (before the
+// 1/sigma_k scale) goes to out[k * m + slot].  out == null: no sampling.
+struct L2Samples {
+  const int* off;
+  const int4* ent;
+  float* out;
+  int m;
+};
+
 template <int LOGW, typename T>
 __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, int n, int npix,
                                                      long long inner, long long f_stride,
@@ -328,13 +341,25 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
                                                      const float* __restrict__ sinv,
                                                      int t_base, int n_out, float thr,
                                                      DetCand* __restrict__ cands, int cap, int pix_off,
-                                                     int* __restrict__ count) {
+                                                     int* __restrict__ count, const L2Samples l2) {
   constexpr int MAXW = 1 << LOGW;
   constexpr int R = MAXW + 1;
   constexpr int K = LOGW + 1;
   constexpr int PL = MAXW / 2;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= inner) return;
+  // this cell's Layer-2 sample entries [s_i, s_end) (a few thousand per
+  // kernel over the whole cube), s_t the output index of the next one
+  int s_i = 0, s_end = 0, s_t = 0x7fffffff;
+  const int eg = (int)e + pix_off;
+  if (l2.out) {
+    const int gb = pix_off / 256 + (int)blockIdx.x;
+    int lo = __ldg(l2.off + gb);
+    s_end = __ldg(l2.off + gb + 1);
+    while (lo < s_end && __ldg(&l2.ent[lo].x) < eg) ++lo;
+    s_i = lo;
+    if (s_i < s_end && __ldg(&l2.ent[s_i].x) == eg) s_t = __ldg(&l2.ent[s_i].y);
+  }
   const long long fidx = e / npix, p = e % npix;
   const T* cube = x + fidx * f_stride + p;
   // x * 1.0f == x exactly, so an absent mask costs one exact multiply
@@ -358,6 +383,25 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   const int total = n + MAXW;  // cs length
   // exact strict-'>' winner of the boxcars ending at ring slot q (the rare
   // path: called only when the max over widths passed the threshold)
+  // the Layer-2 entries of output ta (boxcars ending at ring slot q)
+  auto sample = [&](int q, int ta) {
+    const int t_out = ta - t_base;
+    while (t_out == s_t) {
+      const int4 en = __ldg(&l2.ent[s_i]);
+      float v = 0.f;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int w = 1 << k;
+        const int off = PL - w / 2;
+        const int slo = ((q - MAXW + off) % R + R) % R;
+        const int shi = ((q - MAXW + off + w) % R + R) % R;
+        if (k == en.z) v = ring[shi] - ring[slo];
+      }
+      l2.out[(long long)en.z * l2.m + en.w] = v;
+      ++s_i;
+      s_t = (s_i < s_end && __ldg(&l2.ent[s_i].x) == eg) ? __ldg(&l2.ent[s_i].y) : 0x7fffffff;
+    }
+  };
   auto emit = [&](int q, int ta) {
     float best = 0.f;
     int win = 0;
@@ -403,6 +447,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
           hit |= (ring[shi] - ring[slo]) > tau[k];
         }
         if (hit) emit(q, J0 + q - MAXW);
+        if (J0 + q - MAXW - t_base == s_t) sample(q, J0 + q - MAXW);
       }
       last = ring[R - 1];
       continue;
@@ -428,7 +473,10 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
         }
         ring[q] = v;
         const int ta = J - MAXW;
-        if (ta >= t_base && ta < t_base + n_out) emit(q, ta);
+        if (ta >= t_base && ta < t_base + n_out) {
+          emit(q, ta);
+          if (ta - t_base == s_t) sample(q, ta);
+        }
       }
     }
   }
@@ -727,8 +775,24 @@ int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long lo
                const float* sig_f, int log_maxw, const float* sigma_inv,
                int t_base, int n_out, float threshold, void* cands, int cap, int pix_off,
                int* count, cudaStream_t stream) {
+  return dsb_detect_sampled(cube, cube_f16, n, n_f, npix, f_stride, t_stride, mask,
+                            mask_f_stride, sig_f, log_maxw, sigma_inv, t_base, n_out, threshold,
+                            cands, cap, pix_off, count, nullptr, nullptr, nullptr, 0, stream);
+}
+
+int dsb_detect_sampled(const void* cube, int cube_f16, int n, int n_f, int npix,
+                       long long f_stride, long long t_stride, const float* mask,
+                       long long mask_f_stride, const float* sig_f, int log_maxw,
+                       const float* sigma_inv, int t_base, int n_out, float threshold,
+                       void* cands, int cap, int pix_off, int* count, const int* l2_off,
+                       const void* l2_ent, float* l2_out, int l2_m, cudaStream_t stream) {
   if (!cube || !sigma_inv || !cands || !count || n <= 0 || n_f <= 0 || npix <= 0 || cap < 0)
     return DSB_E_ARG;
+  if (l2_out && (!l2_off || !l2_ent || l2_m <= 0 || pix_off < 0 || (pix_off % 256) != 0 ||
+                 (reinterpret_cast<uintptr_t>(l2_ent) & 15)))
+    return DSB_E_ARG;
+  if ((long long)n_f * npix + pix_off > 0x7fffffffLL) return DSB_E_ARG;
+  const L2Samples l2{l2_off, static_cast<const int4*>(l2_ent), l2_out, l2_m};
   if (log_maxw < 0 || log_maxw > 6 || (1 << log_maxw) > n || t_base < 0 || n_out < 0 ||
       t_base + n_out > n)
     return DSB_E_ARG;
@@ -741,12 +805,12 @@ int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long lo
       detect_kernel<L, __half><<<grid, 256, 0, stream>>>(                                 \
           (const __half*)cube, n, npix, inner, f_stride, t_stride, mask, mask_f_stride,   \
           sig_f, sigma_inv, t_base,                                                       \
-          n_out, threshold, c, cap, pix_off, count);                                      \
+          n_out, threshold, c, cap, pix_off, count, l2);                                   \
     else                                                                                  \
       detect_kernel<L, float><<<grid, 256, 0, stream>>>(                                  \
           (const float*)cube, n, npix, inner, f_stride, t_stride, mask, mask_f_stride,    \
           sig_f, sigma_inv, t_base,                                                       \
-          n_out, threshold, c, cap, pix_off, count);                                      \
+          n_out, threshold, c, cap, pix_off, count, l2);                                   \
   } while (0)
   switch (log_maxw) {
     case 0: DSB_DET(0); break;

@@ -67,6 +67,9 @@ _SIGNATURES = {
                                   _c_int, _c_int, _vp, _c_int, _vp, _vp],
     "dsb_detect": [_vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_ll, _vp, _c_ll, _vp, _c_int,
                    _vp, _c_int, _c_int, _c_float, _vp, _c_int, _c_int, _vp, _vp],
+    "dsb_detect_sampled": [_vp, _c_int, _c_int, _c_int, _c_int, _c_ll, _c_ll, _vp, _c_ll, _vp,
+                           _c_int, _vp, _c_int, _c_int, _c_float, _vp, _c_int, _c_int, _vp,
+                           _vp, _vp, _vp, _c_int, _vp],
     "dsb_clipped_std": [_vp, _c_int, _c_int, _c_float, _c_int, _vp, _vp],
     "dsb_layer1_sigma": [_vp, _c_ll, _c_ll, _c_int, _vp, _c_int, _vp, _c_int, _c_float, _c_int,
                          _vp, _vp],

@@ -43,7 +43,9 @@ from .constants import DSA110_BAND, NATIVE_SAMPLE_US, Band, nbase_of
 from .corr import apply_rfi_mask_to_raw
 from .dedisp import DMPlan, compute_stage2_shifts, compute_time_shift_search
 from .grid import build_pattern, cell_index_map_for, compute_top_of_band_cell_lambda
-from .search import CandidateBuffer, _nms, compute_edge_mask, detect_images, layer1_sigma
+from .noise import Layer2State
+from .search import (CandidateBuffer, Layer2Samples, _nms, compute_edge_mask, detect_images,
+                     layer1_sigma, sigma_clipped_std_batched)
 
 
 def _pow2_at_least(n: int) -> int:
@@ -84,6 +86,16 @@ class PipelineConfig:
     # coarse DMs per stage-1 block: None picks the largest of 32, 16, 8 whose
     # shared time window fits; a value forces that group
     stage1_dm_group: Optional[int] = None
+    # Layer-2 per-kernel noise (noise_norm/layer2.py; the streaming detector,
+    # detector/forward.py:1264): each cube's S/N divides the boxcar sums by
+    # the previous cube's sigma_k (seeded with sqrt(width)); the cube's own
+    # sigma_k estimate (clipped std of layer2_max_samples score samples per
+    # kernel, at most 4096) then updates the state.  Off: the fixed
+    # 1/sqrt(width).
+    layer2: bool = True
+    layer2_max_samples: int = 4096
+    layer2_tau_s: float = 30.0
+    layer2_n_burnin: int = 30
 
     def __post_init__(self):
         if self.ring_dtype not in RING_FORMATS:
@@ -519,6 +531,20 @@ class SearchPipeline:
         widths = [1 << k for k in range(cfg.log_max_width + 1)]
         self.widths = widths
         self.sinv = d((np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32))
+        self.l2 = self.l2_state = None
+        if cfg.layer2:
+            if not 1 <= cfg.layer2_max_samples <= 4096:
+                raise ValueError("layer2_max_samples must be in [1, 4096]")
+            self.l2 = Layer2Samples(n_kernels=len(widths), m=cfg.layer2_max_samples, n_out=C,
+                                    n_fdm=cfg.fine_dm.size, npix=N * N,
+                                    active=T.mask.reshape(-1) != 0, device=self.dev)
+            self.l2_state = Layer2State(len(widths), cube_cadence_s=C * cfg.t_int_us * 1e-6,
+                                        tau_s=cfg.layer2_tau_s, n_burnin=cfg.layer2_n_burnin,
+                                        n_kernel_max_t=1 << cfg.log_max_width, device=self.dev)
+            # the analytic unit-noise value seeds the state (forward.py:746-755)
+            self.l2_state._s_k.copy_(torch.tensor([math.sqrt(w) for w in widths],
+                                                  dtype=torch.float32))
+            self.sinv = torch.reciprocal(torch.clamp(self.l2_state.s_k, min=1e-30))
         self.cands = CandidateBuffer(self.dev, cfg.cand_capacity)
         self.chunk = 0              # next absolute chunk index to correlate
         self.out: List[StreamCandidate] = []
@@ -666,10 +692,19 @@ class SearchPipeline:
             with self._mark("detect"):
                 detect_images(img, self.d_mask, log_max_width=cfg.log_max_width,
                               sigma_inv=self.sinv, t_base=te, n_out=C, threshold=cfg.threshold,
-                              cands=self.cands, pix_offset=f0 * N * N, sigma_f=sig)
+                              cands=self.cands, pix_offset=f0 * N * N, sigma_f=sig,
+                              layer2=self.l2)
             self.launches += 3
             if collect and self.keep_sigma:
                 self.l1_sigma.append(sig.clone())
+        if self.l2 is not None:
+            # this cube's sigma_k from its score samples, folded into the
+            # state that divides the next cube's boxcars
+            with self._mark("layer2"):
+                sig_k = sigma_clipped_std_batched(self.l2.samples)
+                self.launches += 1
+                s_k, _ = self.l2_state.update_and_query(per_kernel_sigma=sig_k)
+                self.sinv = torch.reciprocal(torch.clamp(s_k, min=1e-30))
         if collect:
             got = self.cands.fetch()
             self.last_d2h_bytes += 4 + got.nbytes

@@ -448,10 +448,13 @@ def detect_cube(cube: torch.Tensor, *, log_max_width: int, sigma_inv: torch.Tens
 def detect_images(img: torch.Tensor, mask: torch.Tensor, *, log_max_width: int,
                   sigma_inv: torch.Tensor, t_base: int, n_out: int, threshold: float,
                   cands: CandidateBuffer, pix_offset: int = 0,
-                  sigma_f: Optional[torch.Tensor] = None) -> None:
+                  sigma_f: Optional[torch.Tensor] = None,
+                  layer2: Optional["Layer2Samples"] = None) -> None:
     """Detector on FFT output ``img [F, T, H, W]``, each pixel multiplied while
     reading by ``mask`` (``[F, H, W]`` per fine DM, or one ``[H, W]`` for
-    all) and divided by ``sigma_f[F]`` (the Layer-1 sigma) when given."""
+    all) and divided by ``sigma_f[F]`` (the Layer-1 sigma) when given.  With
+    ``layer2`` the detector also writes that object's per-kernel score
+    samples of these fine DMs (``pix_offset`` = first fine DM x H x W)."""
     _lib.require_cuda(img, "img")
     _lib.require_cuda(mask, "mask")
     F, T, H, W = img.shape
@@ -462,14 +465,54 @@ def detect_images(img: torch.Tensor, mask: torch.Tensor, *, log_max_width: int,
         _lib.require_cuda(sigma_f, "sigma_f")
         if sigma_f.numel() != F or sigma_f.dtype != torch.float32:
             raise ValueError("sigma_f must be float32 [F]")
-    _lib.check(_lib.lib().dsb_detect(_lib.ptr(img), int(img.dtype == torch.float16), T, F, npix,
-                                     T * npix, npix, _lib.ptr(mask),
-                                     npix if mask.numel() == F * npix else 0, _lib.ptr(sigma_f),
-                                     int(log_max_width),
-                                     _lib.ptr(sigma_inv), int(t_base), int(n_out),
-                                     float(threshold), _lib.ptr(cands.buf), cands.capacity,
-                                     int(pix_offset), _lib.ptr(cands.count),
-                                     _lib.stream_of(img.device)), "dsb_detect")
+    l2 = (None, None, None, 0) if layer2 is None else (
+        layer2.d_off, layer2.d_ent, layer2.samples, layer2.m)
+    _lib.check(_lib.lib().dsb_detect_sampled(
+        _lib.ptr(img), int(img.dtype == torch.float16), T, F, npix, T * npix, npix,
+        _lib.ptr(mask), npix if mask.numel() == F * npix else 0, _lib.ptr(sigma_f),
+        int(log_max_width), _lib.ptr(sigma_inv), int(t_base), int(n_out), float(threshold),
+        _lib.ptr(cands.buf), cands.capacity, int(pix_offset), _lib.ptr(cands.count),
+        _lib.ptr(l2[0]), _lib.ptr(l2[1]), _lib.ptr(l2[2]), int(l2[3]),
+        _lib.stream_of(img.device)), "dsb_detect_sampled")
+
+
+class Layer2Samples:
+    """Where the streaming detector samples each kernel's score for the
+    Layer-2 noise estimate (detector/forward.py:1425-1470): ``m`` flat
+    indices per kernel k over the cube's interior ``[n_out, F, H, W]``,
+    drawn by ``torch.randint`` from a generator seeded with k (on the CPU;
+    the reference draws on the cube's device), the ones outside the edge
+    mask left NaN (layer2.py's ``spatial_active``).  ``samples [K, m]`` is
+    filled by the detector, cube by cube."""
+
+    def __init__(self, *, n_kernels: int, m: int, n_out: int, n_fdm: int, npix: int,
+                 active: np.ndarray, device):
+        if npix % 256:
+            raise ValueError("Layer-2 sampling needs H*W a multiple of 256")
+        if n_fdm * npix >= 1 << 31:
+            raise ValueError("Layer-2 sampling needs F*H*W below 2^31")
+        self.m, self.n_kernels = int(m), int(n_kernels)
+        fhw = n_fdm * npix
+        total = n_out * fhw
+        ents = []
+        fill = np.full((n_kernels, m), np.nan, np.float32)
+        for k in range(n_kernels):
+            gen = torch.Generator(device="cpu")
+            gen.manual_seed(int(k))
+            idx = torch.randint(0, total, (m,), generator=gen).numpy()
+            t_in, cell = idx // fhw, idx % fhw
+            act = np.asarray(active, bool).reshape(-1)[cell % npix]
+            slot = np.arange(m)
+            ents.append(np.stack([cell[act], t_in[act], np.full(act.sum(), k), slot[act]], 1))
+        ent = np.concatenate(ents).astype(np.int64)
+        order = np.lexsort((ent[:, 3], ent[:, 2], ent[:, 1], ent[:, 0]))
+        ent = ent[order]
+        n_blk = fhw // 256
+        off = np.searchsorted(ent[:, 0], np.arange(n_blk + 1) * 256).astype(np.int32)
+        self.entries = ent
+        self.d_ent = torch.from_numpy(np.ascontiguousarray(ent.astype(np.int32))).to(device)
+        self.d_off = torch.from_numpy(off).to(device)
+        self.samples = torch.from_numpy(fill).to(device)
 
 
 # ---------------------------------------------------------------------------

@@ -374,6 +374,24 @@ int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long lo
                float threshold, void* cands, int cap, int pix_off, int* count,
                cudaStream_t stream);
 
+/* dsb_detect plus the Layer-2 score subsample of the streaming detector
+ * (DeterministicDetector._streaming_forward, src/dsart/detector/
+ * forward.py:1425-1530; noise_norm/layer2.py:58): while it marches, the
+ * detector writes the raw boxcar sum of width 2^k (before sigma_inv) of
+ * every sampled (cell, output time) to l2_out[k * l2_m + slot].  l2_ent:
+ * 16-byte aligned int4 entries {eg, t, k, slot} sorted by (eg, t), eg =
+ * cell index + pix_off over all fine DMs, t = output time - t_base;
+ * l2_off[gb]: first entry with eg >= 256 gb (one more entry at the end);
+ * pix_off a multiple of 256.  Slots without an entry are not written (the
+ * caller keeps the masked-out ones NaN, which the clipped std drops).  With
+ * l2_out null this is dsb_detect. */
+int dsb_detect_sampled(const void* cube, int cube_f16, int n, int n_f, int npix,
+                       long long f_stride, long long t_stride, const float* mask,
+                       long long mask_f_stride, const float* sig_f, int log_maxw,
+                       const float* sigma_inv, int t_base, int n_out, float threshold,
+                       void* cands, int cap, int pix_off, int* count, const int* l2_off,
+                       const void* l2_ent, float* l2_out, int l2_m, cudaStream_t stream);
+
 /* ---- a18: Layer-1 sigma-clipped std ---------------------------------------------
  * sigma_clipped_std_batched (src/dsart/noise_norm/layer1.py:53): rows of at
  * most 4096 samples; lower median; non-finite samples dropped. */

@@ -967,10 +967,51 @@ def round_bf16_complex(z: np.ndarray) -> np.ndarray:
     return (round_bf16(z.real) + 1j * round_bf16(z.imag)).astype(np.complex64)
 
 
+class Layer2State:
+    """Per-kernel sigma_k of the detector's S/N (noise_norm/layer2.py:113-452)
+    in its default configuration (no floor, no ratio clamp): seeded with
+    sqrt(width) (detector/forward.py:746-755); a zero estimate keeps the
+    previous value; Welford running mean over the first ``n_burnin`` cubes,
+    then the EMA ``gamma * sigma + (1 - gamma) * s`` with gamma = 1 -
+    exp(-cube_cadence_s / tau_s); float32 throughout."""
+
+    def __init__(self, widths, cube_cadence_s: float, tau_s: float = 30.0, n_burnin: int = 30):
+        self.s = np.asarray([math.sqrt(w) for w in widths], np.float32)
+        self.gamma = 1.0 - math.exp(-cube_cadence_s / tau_s)
+        self.n_burnin = int(n_burnin)
+        self.count = 0
+
+    def update(self, sigma: np.ndarray) -> np.ndarray:
+        sig = np.asarray(sigma, np.float32)
+        sig = np.where(sig == 0, self.s, sig).astype(np.float32)
+        if self.count < self.n_burnin:
+            c = np.float32(self.count)
+            self.s = ((c * self.s + sig) / np.float32(self.count + 1.0)).astype(np.float32)
+        else:
+            self.s = (np.float32(self.gamma) * sig
+                      + np.float32(1.0 - self.gamma) * self.s).astype(np.float32)
+        self.count += 1
+        return self.s
+
+
+def layer2_sample_index(n_kernels: int, m: int, total: int) -> np.ndarray:
+    """[K, m] flat indices over a cube interior of ``total`` cells: per kernel
+    k, ``torch.randint(0, total, (m,))`` from a CPU generator seeded k
+    (detector/forward.py:1436-1448)."""
+    import torch
+    out = np.empty((n_kernels, m), np.int64)
+    for k in range(n_kernels):
+        gen = torch.Generator(device="cpu")
+        gen.manual_seed(int(k))
+        out[k] = torch.randint(0, total, (m,), generator=gen).numpy()
+    return out
+
+
 def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block, t_int, csf,
                  n_grid, coarse_dm, fine_dm, fine_to_coarse, log_max_width, threshold, chunk,
                  use_sky=True, sky_window=8, sky_warmup=8, n_top=256, r_t=4, r_f=5, r_lm=3,
-                 l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None, keep_images=True):
+                 l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None, keep_images=True,
+                 layer2=True, layer2_max_samples=4096, layer2_tau_s=30.0, layer2_n_burnin=30):
     """Oracle of the CUDA streaming pipeline; returns candidate tuples
     ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates.
     ``ring_dtype="bf16"`` stores the stage-2 streams in the BF16 form (each
@@ -1039,6 +1080,18 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
     T1 = max(0, n_s1) * chunk
     cands = []
     images = []
+    l2 = None
+    if layer2:
+        # the streaming detector's Layer-2 path: S/N = boxcar / sigma_k of the
+        # previous cube; the cube's score samples update sigma_k afterwards
+        l2 = Layer2State(widths, chunk * t_int * NATIVE_SAMPLE_US * 1e-6, layer2_tau_s,
+                         layer2_n_burnin)
+        l2_idx = layer2_sample_index(len(widths), layer2_max_samples, chunk * n_fine * N * N)
+        l2_t = l2_idx // (n_fine * N * N)
+        l2_cell = l2_idx % (n_fine * N * N)
+        l2_f, l2_p = l2_cell // (N * N), l2_cell % (N * N)
+        l2_act = mask.reshape(-1)[l2_p] != 0
+        keep["layer2_s"] = []
     # first cube whose every time has data from every chgroup (warm-up)
     jc_first = -(-(int(tb["sh2"].max()) + max(0, int(tb["sf"].max())) + 2 * te) // chunk)
     for jc in range(jc_first, max(0, n_s1 - a)):
@@ -1072,10 +1125,26 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
                 images.append(img)
         score = np.zeros((chunk, n_fine, N, N), np.float32)
         win = np.zeros((chunk, n_fine, N, N), np.int16)
+        if l2 is not None:
+            sinv = (np.float32(1.0) / np.maximum(l2.s, np.float32(1e-30))).astype(np.float32)
+            samp = np.full(l2_idx.shape, np.nan, np.float32)
         for r0 in range(0, N, 64):          # pixel-row slabs: the boxcars are per pixel
             cs = padded_cumsum(cube[:, :, r0:r0 + 64], 1 << log_max_width)
             score[:, :, r0:r0 + 64], win[:, :, r0:r0 + 64] = multi_boxcar_argmax(
                 cs, widths, offs, sinv, chunk, te)
+            if l2 is not None:
+                # raw boxcar sums (before 1/sigma_k) at the sampled interior
+                # cells of this slab, inside the edge mask
+                csf = cs.reshape(cs.shape[0], n_fine, -1)
+                for k, (w, off) in enumerate(zip(widths, offs)):
+                    rows = l2_p[k] // N
+                    sel = l2_act[k] & (rows >= r0) & (rows < r0 + 64)
+                    pl = (rows[sel] - r0) * N + l2_p[k][sel] % N
+                    tt = l2_t[k][sel] + te + off
+                    samp[k, sel] = (csf[tt + w, l2_f[k][sel], pl]
+                                    - csf[tt, l2_f[k][sel], pl]).astype(np.float32)
+        if l2 is not None:
+            keep["layer2_s"].append(l2.update(sigma_clipped_std_batched(samp)))
         for cd in decode_topk(score, win, threshold=threshold, n_top=n_top, r_t=r_t, r_f=r_f,
                               r_lm=r_lm):
             cands.append((jc * chunk - te + cd.t, cd.f, cd.l, cd.m, cd.snr, widths[cd.k]))

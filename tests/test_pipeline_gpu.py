@@ -177,9 +177,10 @@ def test_config1_small_plain_pipeline_matches_oracle(dev):
     """The small plain configuration as stated: 16 dual-pol antennas on a
     seeded T layout (136 baselines with autos), 256 channels over
     1311.25-1498.75 MHz (two chgroups of 128), 4096-sample blocks of 4-bit
-    Gaussian voltages (sigma 3, clipped), 8-sample correlation, 64^2 grid,
-    32 trial DMs 0-600, boxcars 1..16, threshold 7, one point-source burst at
-    DM 300, 4 samples wide.  At DM 300 the sweep across the band (170 ms) is
+    Gaussian voltages (sigma 3, clipped), 8-sample correlation, 4 channels
+    summed per subband, 64^2 grid, 32 trial DMs 0-600, boxcars 1..16,
+    threshold 7, one point-source burst at DM 300, 4 samples wide, whose
+    amplitude gives S/N 20 in the oracle.  At DM 300 the sweep across the band (170 ms) is
     longer than one block (134 ms), and stage 2 holds the top of the band
     back by the DM-600 delay (1289 tiles), so the stream runs six blocks and
     the burst arrives in the third: its band-bottom time falls in the first
@@ -200,7 +201,7 @@ def test_config1_small_plain_pipeline_matches_oracle(dev):
     blocks = [synth.make_block(band=band, nant=nant, npkt=npkt, block_index=b, seed=31,
                                antpos_e=e, antpos_n=n, bursts=bursts, cell_lambda=cell,
                                n_grid=N) for b in range(6)]
-    kw = dict(nant=nant, npkt_block=npkt, t_int=8, csf=1, n_grid=N, coarse_dm=dms, fine_dm=dms,
+    kw = dict(nant=nant, npkt_block=npkt, t_int=8, csf=4, n_grid=N, coarse_dm=dms, fine_dm=dms,
               fine_to_coarse=np.arange(32), log_max_width=4, threshold=7.0)
     cfg = PipelineConfig(band=band, sky_window=2, sky_warmup=1, chunk_tiles=512, fdm_batch=32,
                          ring_dtype="c64", **kw)
