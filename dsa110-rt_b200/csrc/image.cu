@@ -803,6 +803,164 @@ int launch_image(const ImgArgs& A, int max_blocks, cudaStream_t stream) {
   return launch_status();
 }
 
+// ===========================================================================
+// Dense inverse real 2-D FFT of Hermitian half spectra, the transform of
+// torch.fft.irfft2(half, s=(N, N)) (norm "backward"): half [n_img][N][N/2+1]
+// complex64 -> out [n_img][N][N] float32.  Used where the combine is dense
+// (GpuImager.process_cube, image/imager_gpu.py:575-605).  Two passes:
+//  1. columns: an N-point inverse complex transform over u of every column
+//     w in place in half (CTA = 16 adjacent columns of one image, staged in
+//     shared memory with a pitch of 17 so that a column's slots fall in
+//     different banks);
+//  2. rows: two rows per complex transform (x_a + i x_b) as in the image
+//     kernel; the imaginary parts of columns 0 and N/2 are dropped (a
+//     Hermitian spectrum makes them zero; numpy and cuFFT drop them too).
+// Both passes use the R1 x R2 factorisation of the image kernel.
+// ===========================================================================
+constexpr int FFT_CW = 16;  // columns per CTA of the column pass
+
+template <int N>
+struct DenseGeom {
+  static constexpr int R1 = (N <= 32) ? 4 : (N <= 128 ? 8 : 16);
+  static constexpr int R2 = N / R1;
+  static constexpr int NH = N / 2 + 1;
+  static constexpr int CP = FFT_CW + 1;         // pitch of the staged columns (float2)
+  static constexpr int COL_THREADS = FFT_CW * R1;
+  static constexpr int ROW_GROUPS = 8;          // row pairs per CTA of the row pass
+  static constexpr int ROW_THREADS = ROW_GROUPS * R1;
+  static_assert(R1 * R2 == N && R2 % R1 == 0, "unsupported size");
+};
+
+// One N-point inverse transform by a group of R1 threads (thread rj) over
+// the N values at slots p(i) of shared memory, in place, natural order out.
+template <int N, typename Slot>
+DSB_DEV void group_idft(Slot p, int rj, unsigned mask, const float2* rtw) {
+  using Dg = DenseGeom<N>;
+  constexpr int R1 = Dg::R1, R2 = Dg::R2, H = R2 / R1;
+  float2 a[R2];
+#pragma unroll
+  for (int k = 0; k < R2; ++k) a[k] = *p(rj + R1 * k);
+  idftR<R2>(a);
+#pragma unroll
+  for (int m2 = 1; m2 < R2; ++m2) a[m2] = cmul(a[m2], rtw[m2 * R1 + rj]);
+  __syncwarp(mask);
+#pragma unroll
+  for (int m2 = 0; m2 < R2; ++m2) *p(m2 * R1 + (rj ^ (m2 & (R1 - 1)))) = a[m2];
+  __syncwarp(mask);
+  float2 b[H][R1];
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    const int m2 = rj + R1 * h;
+#pragma unroll
+    for (int jj = 0; jj < R1; ++jj) b[h][jj] = *p(m2 * R1 + (jj ^ rj));
+  }
+  __syncwarp(mask);
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    idftR<R1>(b[h]);
+#pragma unroll
+    for (int m1 = 0; m1 < R1; ++m1) *p(rj + R1 * h + R2 * m1) = b[h][m1];
+  }
+  __syncwarp(mask);
+}
+
+template <int N>
+__global__ void __launch_bounds__(DenseGeom<N>::COL_THREADS)
+    irfft2_cols_kernel(float2* __restrict__ half, const float2* __restrict__ twn) {
+  using Dg = DenseGeom<N>;
+  constexpr int R1 = Dg::R1, NH = Dg::NH, CP = Dg::CP;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  float2* col = reinterpret_cast<float2*>(smem_raw);   // [N][CP]
+  float2* rtw = col + N * CP;                          // [R2][R1]
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < N; i += blockDim.x) rtw[i] = twn[((i % R1) * (i / R1)) & (N - 1)];
+  const int w0 = blockIdx.x * FFT_CW;
+  const int nw = min(FFT_CW, NH - w0);
+  float2* img = half + (size_t)blockIdx.y * N * NH;
+  for (int i = tid; i < N * FFT_CW; i += blockDim.x) {
+    const int r = i / FFT_CW, c = i % FFT_CW;
+    col[r * CP + c] = c < nw ? img[(size_t)r * NH + w0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int c = tid / R1, rj = tid % R1;
+  const unsigned mask = ((1u << R1) - 1u) << (lane / R1 * R1);
+  group_idft<N>([&](int i) { return col + i * CP + c; }, rj, mask, rtw);
+  __syncthreads();
+  for (int i = tid; i < N * FFT_CW; i += blockDim.x) {
+    const int r = i / FFT_CW, cc = i % FFT_CW;
+    if (cc < nw) img[(size_t)r * NH + w0 + cc] = col[r * CP + cc];
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(DenseGeom<N>::ROW_THREADS)
+    irfft2_rows_kernel(const float2* __restrict__ half, const float2* __restrict__ twn,
+                       float* __restrict__ out) {
+  using Dg = DenseGeom<N>;
+  constexpr int R1 = Dg::R1, NH = Dg::NH;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  float2* rtw = reinterpret_cast<float2*>(smem_raw);   // [R2][R1]
+  float2* reg0 = rtw + N;                              // [ROW_GROUPS][N]
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < N; i += blockDim.x) rtw[i] = twn[((i % R1) * (i / R1)) & (N - 1)];
+  __syncthreads();
+  const int grp = tid / R1, rj = tid % R1;
+  const unsigned mask = ((1u << R1) - 1u) << (lane / R1 * R1);
+  const int pr = blockIdx.x * Dg::ROW_GROUPS + grp;   // row pair (whole groups leave)
+  if (pr >= N / 2) return;
+  const float2* src = half + (size_t)blockIdx.y * N * NH;
+  const float2* ra = src + (size_t)(2 * pr) * NH;
+  const float2* rb = ra + NH;
+  float2* reg = reg0 + grp * N;
+  for (int i = rj; i < N; i += R1) {
+    float2 z;
+    if (i == 0) {
+      z = make_float2(ra[0].x, rb[0].x);
+    } else if (i == N / 2) {
+      z = make_float2(ra[N / 2].x, rb[N / 2].x);
+    } else if (i < N / 2) {
+      const float2 ya = ra[i], yb = rb[i];
+      z = make_float2(ya.x - yb.y, ya.y + yb.x);     // ya + i yb
+    } else {
+      const float2 ya = ra[N - i], yb = rb[N - i];
+      z = make_float2(ya.x + yb.y, -ya.y + yb.x);    // conj(ya) + i conj(yb)
+    }
+    reg[i] = z;
+  }
+  __syncwarp(mask);
+  group_idft<N>([&](int i) { return reg + i; }, rj, mask, rtw);
+  // 1/N^2 (a power of two: exact)
+  constexpr float scale = 1.0f / (float)(N * N);
+  float* oa = out + ((size_t)blockIdx.y * N + 2 * pr) * N;
+  float* ob = oa + N;
+  for (int i = rj; i < N; i += R1) {
+    const float2 v = reg[i];
+    oa[i] = v.x * scale;
+    ob[i] = v.y * scale;
+  }
+}
+
+template <int N>
+int launch_irfft2(float2* half, int n_img, const float2* twn, float* out, cudaStream_t stream) {
+  using Dg = DenseGeom<N>;
+  const size_t smem_c = (size_t)(N * Dg::CP + N) * sizeof(float2);
+  const size_t smem_r = (size_t)(N + Dg::ROW_GROUPS * N) * sizeof(float2);
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(irfft2_cols_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_c) != cudaSuccess ||
+        cudaFuncSetAttribute(irfft2_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_r) != cudaSuccess)
+      return DSB_E_CUDA;
+    attr = true;
+  }
+  const dim3 gc((Dg::NH + FFT_CW - 1) / FFT_CW, n_img);
+  irfft2_cols_kernel<N><<<gc, Dg::COL_THREADS, smem_c, stream>>>(half, twn);
+  const dim3 gr((N / 2 + Dg::ROW_GROUPS - 1) / Dg::ROW_GROUPS, n_img);
+  irfft2_rows_kernel<N><<<gr, Dg::ROW_THREADS, smem_r, stream>>>(half, twn, out);
+  return launch_status();
+}
+
 template <int N>
 int image_geometry(int* g) {
   using Gm = ImgGeom<N>;
@@ -824,6 +982,23 @@ int dsb_image_geometry(int n_grid, int* geom) {
     case 64: return image_geometry<64>(geom);
     case 256: return image_geometry<256>(geom);
     case 512: return image_geometry<512>(geom);
+    default: return DSB_E_UNSUPPORTED;
+  }
+}
+
+int dsb_irfft2(void* half, int n_img, int N, const void* twiddles, float* out,
+               cudaStream_t stream) {
+  if (!half || !twiddles || !out || n_img <= 0 || n_img > 65535) return DSB_E_ARG;
+  if ((reinterpret_cast<uintptr_t>(half) & 7) || (reinterpret_cast<uintptr_t>(out) & 3))
+    return DSB_E_ARG;
+  float2* h = static_cast<float2*>(half);
+  const float2* tw = static_cast<const float2*>(twiddles);
+  switch (N) {
+    case 32: return launch_irfft2<32>(h, n_img, tw, out, stream);
+    case 64: return launch_irfft2<64>(h, n_img, tw, out, stream);
+    case 128: return launch_irfft2<128>(h, n_img, tw, out, stream);
+    case 256: return launch_irfft2<256>(h, n_img, tw, out, stream);
+    case 512: return launch_irfft2<512>(h, n_img, tw, out, stream);
     default: return DSB_E_UNSUPPORTED;
   }
 }

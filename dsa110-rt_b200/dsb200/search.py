@@ -117,10 +117,43 @@ def compute_edge_mask(*, n_grid: int, kernel_support: int = 5, sigma_l_pix=None,
     return mask
 
 
-def irfft2_image(half: torch.Tensor, n_grid: int) -> torch.Tensor:
+_TWIDDLES: dict = {}
+
+
+def twiddles(n_grid: int, device) -> torch.Tensor:
+    """(N,) complex64 exp(+2 pi i e / N) on ``device`` (cached)."""
+    key = (int(n_grid), str(device))
+    if key not in _TWIDDLES:
+        e = np.arange(n_grid)
+        _TWIDDLES[key] = torch.from_numpy(
+            np.exp(2j * np.pi * e / n_grid).astype(np.complex64)).to(device)
+    return _TWIDDLES[key]
+
+
+def irfft2_image(half: torch.Tensor, n_grid: int, out: Optional[torch.Tensor] = None
+                 ) -> torch.Tensor:
     """Real image from the (fftshift-folded) Hermitian half spectrum
-    ``[..., N, N/2+1]`` complex64 -> ``[..., N, N]`` float32."""
-    return torch.fft.irfft2(half, s=(n_grid, n_grid))
+    ``[..., N, N/2+1]`` complex64 -> ``[..., N, N]`` float32: the inverse
+    real 2-D FFT of torch.fft.irfft2 (image/imager_gpu.py:590) on this
+    library's own kernels (``dsb_irfft2``).  ``half`` is the kernel's work
+    buffer: it is overwritten."""
+    _lib.require_cuda(half, "half")
+    N = int(n_grid)
+    if half.dtype != torch.complex64 or tuple(half.shape[-2:]) != (N, N // 2 + 1):
+        raise ValueError(f"half must be complex64 [..., {N}, {N // 2 + 1}]")
+    if not half.is_contiguous():
+        raise ValueError("half must be contiguous")
+    lead = tuple(half.shape[:-2])
+    n_img = int(np.prod(lead)) if lead else 1
+    if out is None:
+        out = torch.empty(lead + (N, N), dtype=torch.float32, device=half.device)
+    elif out.dtype != torch.float32 or tuple(out.shape) != lead + (N, N) or \
+            not out.is_contiguous():
+        raise ValueError(f"out must be contiguous float32 {lead + (N, N)}")
+    _lib.check(_lib.lib().dsb_irfft2(_lib.ptr(half), n_img, N,
+                                     _lib.ptr(twiddles(N, half.device)), _lib.ptr(out),
+                                     _lib.stream_of(half.device)), "dsb_irfft2")
+    return out
 
 
 def mask_into_cube(img: torch.Tensor, mask: torch.Tensor, cube: torch.Tensor, f0: int) -> None:
@@ -165,7 +198,8 @@ class GpuImager:
     inverse real FFT, and the edge mask (or the per-fine-DM mask of
     ``set_edge_mask_per_fdm``) into ``output_cube [t_det, n_fdm, N, N]``;
     two output cubes alternate, so a returned cube stays valid until the
-    next-but-one call.  The streaming pipeline itself uses the fused
+    next-but-one call.  Combine, transform (``dsb_irfft2``) and mask are this
+    library's kernels.  The streaming pipeline itself uses the fused
     ``dsb_image_fft`` path instead."""
 
     def __init__(self, config: GpuImagerConfig, device: torch.device, edge_mask_real, output_cube,
@@ -196,6 +230,14 @@ class GpuImager:
         out_alt = torch.empty(shape, dtype=config.cube_dtype, device=dev)
         uv = torch.empty((config.t_det, N, N // 2 + 1), dtype=torch.complex64, device=dev)
         return cls(config, dev, edge_t, out, out_alt, uv)
+
+    def _img_buffer(self, n_t: int) -> torch.Tensor:
+        N = self.config.n_grid
+        buf = getattr(self, "_img", None)
+        if buf is None or buf.shape[0] < n_t:
+            buf = self._img = torch.empty((self.config.t_det, N, N), dtype=torch.float32,
+                                          device=self.device)
+        return buf[:n_t]
 
     def set_edge_mask_per_fdm(self, sigma_inv: Optional[torch.Tensor]) -> None:
         """``edge_mask * sigma_inv[f]`` per fine DM (the Layer-1 divide fused
@@ -240,7 +282,7 @@ class GpuImager:
                                                fftshift=True)
             if cfg.imager_uv_prescale != 1.0:
                 uv.mul_(cfg.imager_uv_prescale)
-            img = irfft2_image(uv, N)[None]                    # (1, n_t, N, N)
+            img = irfft2_image(uv, N, out=self._img_buffer(n_t))[None]   # (1, n_t, N, N)
             mask = (self.edge_mask_real if self.edge_mask_per_fdm is None
                     else self.edge_mask_per_fdm[f:f + 1])
             mask_into_cube(img.contiguous(), mask, cube[t_lo:] if t_lo else cube, f)

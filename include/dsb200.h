@@ -293,6 +293,16 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  * max_entries or a cell_base[g] that is not a multiple of 64 sets
  * DSB_E_CAPACITY and writes nothing.  Each CTA holds 128 columns of tensor
  * memory while it runs (all 512 of its SM at N = 512). */
+/* Dense inverse real 2-D FFT, the torch.fft.irfft2(half, s=(N, N)) that
+ * GpuImager.process_cube runs after its dense combine
+ * (src/dsart/image/imager_gpu.py:590): half [n_img][N][N/2+1] complex64 ->
+ * out [n_img][N][N] float32, 1/N^2 normalisation, the imaginary parts of
+ * columns 0 and N/2 dropped after the column transforms (as numpy and cuFFT
+ * do).  half is used as the work buffer and is overwritten.  twiddles: (N)
+ * complex64 exp(+2 pi i e/N).  N in {32, 64, 128, 256, 512}; n_img <= 65535. */
+int dsb_irfft2(void* half, int n_img, int N, const void* twiddles, float* out,
+               cudaStream_t stream);
+
 /* The kernel's geometry at grid size n_grid, for building the tables above:
  * geom[0] fold (column passes, LC = N / fold), geom[1] threads per CTA,
  * geom[2] max_entries (S entries per thread), geom[3] meta_bits (16 or 32),
