@@ -80,6 +80,15 @@ def workload_config(name: str):
                               n_grid=256, coarse_dm=np.linspace(0.0, 2000.0, 32),
                               fine_per_coarse=16, log_max_width=4, threshold=7.0,
                               chunk_tiles=512, fdm_batch=8)
+    if name == "medium5":
+        # the per-image work of the metric configuration (96 antennas, 512^2,
+        # boxcars 1..64, t_int 32) on 4 chgroups and short rings: a few GB on
+        # the device, for profiling the per-image kernels
+        from dsb200.constants import Band
+        return PipelineConfig(nant=96, band=Band(n_chgroup=4), npkt_block=2048, t_int=32,
+                              csf=16, n_grid=512, coarse_dm=np.linspace(0.0, 300.0, 8),
+                              fine_per_coarse=4, log_max_width=6, threshold=7.0,
+                              chunk_tiles=128, fdm_batch=8)
     if name == "medium":
         # the full per-image work (96 antennas, 16 chgroups, 256^2) on short
         # rings: a few GB on the device, for profiling the per-image kernels
