@@ -331,6 +331,57 @@ struct L2Samples {
   int m;
 };
 
+// The K boxcar sums (widths 1, 2, ..., 2^(K-1)) of one output, before the
+// 1/sigma_k scale.
+template <int K>
+struct BoxSums {
+  float v[K];
+};
+
+// Exact strict-'>' winner over the widths (the lowest k wins ties) and, when
+// its S/N passes thr, one appended candidate.  Out of line: called only for
+// outputs the screen lets through.
+template <int K>
+__device__ __noinline__ void det_emit(const BoxSums<K> d, const float* __restrict__ sinv,
+                                      float thr, int t_out, int pix,
+                                      DetCand* __restrict__ cands, int cap,
+                                      int* __restrict__ count) {
+  float best = 0.f;
+  int win = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const float s = d.v[k] * __ldg(sinv + k);
+    if (k == 0 || s > best) {
+      best = s;
+      win = k;
+    }
+  }
+  if (best > thr) {
+    const int slot = atomicAdd(count, 1);
+    if (slot < cap) cands[slot] = DetCand{t_out, pix, best, win};
+  }
+}
+
+// Every Layer-2 entry of (cell eg, output t_out) from entry s_i on: the raw
+// boxcar of its width into its slot.  Returns the next entry and its output
+// time (0x7fffffff when this cell has no more).
+template <int K>
+__device__ __noinline__ int2 det_sample(const BoxSums<K> d, const L2Samples l2, int s_i,
+                                        int s_end, int eg, int t_out) {
+  int s_t = t_out;
+  while (s_t == t_out) {
+    const int4 en = __ldg(&l2.ent[s_i]);
+    float v = 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k == en.z) v = d.v[k];
+    l2.out[(long long)en.z * l2.m + en.w] = v;
+    ++s_i;
+    s_t = (s_i < s_end && __ldg(&l2.ent[s_i].x) == eg) ? __ldg(&l2.ent[s_i].y) : 0x7fffffff;
+  }
+  return make_int2(s_i, s_t);
+}
+
 template <int LOGW, typename T>
 __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, int n, int npix,
                                                      long long inner, long long f_stride,
@@ -365,14 +416,13 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   // x * 1.0f == x exactly, so an absent mask costs one exact multiply
   float mval = mask ? mask[fidx * mask_f_stride + p] : 1.0f;
   if (sig_f) mval = mval / sig_f[fidx];
-  float si[K], tau[K];
+  float tau[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    si[k] = sinv[k];
     // screen level of width k: a boxcar sum d can give fl(d * si) > thr only
     // if d > thr / si up to two roundings (2^-23 relative), so a level
     // lowered by 2^-20 of its magnitude never misses one
-    const float lv = thr / si[k];
+    const float lv = thr / sinv[k];
     tau[k] = lv - fabsf(lv) * 0x1p-20f;
   }
   float ring[R];
@@ -381,45 +431,34 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
   double run = 0.0;
   float last = 0.f;
   const int total = n + MAXW;  // cs length
-  // exact strict-'>' winner of the boxcars ending at ring slot q (the rare
-  // path: called only when the max over widths passed the threshold)
-  // the Layer-2 entries of output ta (boxcars ending at ring slot q)
-  auto sample = [&](int q, int ta) {
-    const int t_out = ta - t_base;
-    while (t_out == s_t) {
-      const int4 en = __ldg(&l2.ent[s_i]);
-      float v = 0.f;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int w = 1 << k;
-        const int off = PL - w / 2;
-        const int slo = ((q - MAXW + off) % R + R) % R;
-        const int shi = ((q - MAXW + off + w) % R + R) % R;
-        if (k == en.z) v = ring[shi] - ring[slo];
-      }
-      l2.out[(long long)en.z * l2.m + en.w] = v;
-      ++s_i;
-      s_t = (s_i < s_end && __ldg(&l2.ent[s_i].x) == eg) ? __ldg(&l2.ent[s_i].y) : 0x7fffffff;
-    }
-  };
-  auto emit = [&](int q, int ta) {
-    float best = 0.f;
-    int win = 0;
+  // the boxcar sums of the output whose newest prefix sits in ring slot q
+  // (the one MAXW/2 + 1 past its centre), widths 1, 2, ..., MAXW
+  auto boxcars = [&](int q, BoxSums<K>& d) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int w = 1 << k;
       const int off = PL - w / 2;
       const int slo = ((q - MAXW + off) % R + R) % R;
       const int shi = ((q - MAXW + off + w) % R + R) % R;
-      const float s = (ring[shi] - ring[slo]) * si[k];
-      if (k == 0 || s > best) {
-        best = s;
-        win = k;
-      }
+      d.v[k] = ring[shi] - ring[slo];
     }
-    if (best > thr) {
-      const int slot = atomicAdd(count, 1);
-      if (slot < cap) cands[slot] = DetCand{ta - t_base, (int)e + pix_off, best, win};
+  };
+  // One output: the screen compares each boxcar sum with its lowered level
+  // (a superset of what the exact strict-'>' chain of det_emit reports,
+  // which decides); the threshold hits and the Layer-2 samples are rare, so
+  // both are calls out of this loop, which keeps the unrolled loop (R steps)
+  // small enough for the instruction cache.
+  auto output = [&](int q, int ta) {
+    BoxSums<K> d;
+    boxcars(q, d);
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) hit |= d.v[k] > tau[k];
+    if (hit) det_emit<K>(d, sinv, thr, ta - t_base, (int)e + pix_off, cands, cap, count);
+    if (ta - t_base == s_t) {
+      const int2 r = det_sample<K>(d, l2, s_i, s_end, eg, ta - t_base);
+      s_i = r.x;
+      s_t = r.y;
     }
   };
   for (int J0 = 0; J0 < total; J0 += R) {
@@ -428,26 +467,14 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
                           J0 + R - 1 - MAXW < t_base + n_out;
     float xin[R];
     if (interior) {
-      // steady state: every sample loaded, every time an output; the screen
-      // compares each boxcar sum with its lowered level (a superset of what
-      // the exact strict-'>' chain of emit() reports, which decides)
+      // steady state: every sample loaded, every time an output
 #pragma unroll
       for (int q = 0; q < R; ++q) xin[q] = ldf<T>(cube, (long long)(J0 + q - 1 - PL) * t_stride);
 #pragma unroll
       for (int q = 0; q < R; ++q) {
         run += (double)(xin[q] * mval);
         ring[q] = (float)run;
-        bool hit = false;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int w = 1 << k;
-          const int off = PL - w / 2;
-          const int slo = ((q - MAXW + off) % R + R) % R;
-          const int shi = ((q - MAXW + off + w) % R + R) % R;
-          hit |= (ring[shi] - ring[slo]) > tau[k];
-        }
-        if (hit) emit(q, J0 + q - MAXW);
-        if (J0 + q - MAXW - t_base == s_t) sample(q, J0 + q - MAXW);
+        output(q, J0 + q - MAXW);
       }
       last = ring[R - 1];
       continue;
@@ -473,10 +500,7 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
         }
         ring[q] = v;
         const int ta = J - MAXW;
-        if (ta >= t_base && ta < t_base + n_out) {
-          emit(q, ta);
-          if (ta - t_base == s_t) sample(q, ta);
-        }
+        if (ta >= t_base && ta < t_base + n_out) output(q, ta);
       }
     }
   }
