@@ -214,6 +214,64 @@ def stage_work(pipe):
     }
 
 
+def measure_int8_peak(dev) -> float:
+    """Dense int8 tensor throughput of this GPU (TOP/s): cuBLASLt's int8 GEMM
+    (torch._int_mm) on 8192^3, best of 10 -- the denominator of the
+    correlator's roofline (2 x 8192^3 ops per call)."""
+    import torch
+    n = 8192
+    a = torch.randint(-8, 8, (n, n), dtype=torch.int8, device=dev)
+    b = torch.randint(-8, 8, (n, n), dtype=torch.int8, device=dev)
+    for _ in range(3):
+        torch._int_mm(a, b)
+    best = float("inf")
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+# DRAM bytes per unit of work of the 512^2 kernels (bf16 ring), from the ncu
+# captures of the medium5 workload (profiles/): image_kernel<512, 1> wrote
+# 1550.277 MB for 1536 images and read 28.840 MB for 2 coarse DMs x 192
+# times x 4 chgroups; detect_kernel<6> read 1619.558 MB for 1536 images
+IMAGE512_DRAM_WRITE_PER_IMAGE = 1550.277e6 / 1536
+IMAGE512_DRAM_READ_PER_SLICE_TIME_CHGROUP = 28.840e6 / (2 * 192 * 4)
+DETECT64_DRAM_READ_PER_IMAGE = 1619.558e6 / 1536
+
+
+def stage_traffic(pipe) -> dict:
+    """Measured DRAM bytes per launch (ncu, scaled from a capture of the same
+    kernel on a smaller case by its units of work) where one was taken."""
+    cfg = pipe.cfg
+    out = {}
+    nt = cfg.chunk_tiles + 2 * cfg.t_edge
+    nb = cfg.fdm_batch
+    if cfg.n_grid == 512 and cfg.ring_dtype == "bf16":
+        cpb = max(1, nb // cfg.fine_per_coarse)
+        out["image"] = (IMAGE512_DRAM_WRITE_PER_IMAGE * nb * nt +
+                        IMAGE512_DRAM_READ_PER_SLICE_TIME_CHGROUP * cpb * nt * cfg.band.n_chgroup,
+                        "ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel<512> on "
+                        "medium5 (1536 images), scaled by images written and ring slices read")
+    if cfg.log_max_width == 6:
+        out["detect"] = (DETECT64_DRAM_READ_PER_IMAGE * nb * nt * (cfg.n_grid / 512) ** 2,
+                         "ncu dram__bytes_read.sum of detect_kernel<6> on medium5 (1536 images of "
+                         "512^2), scaled by image bytes read")
+    if cfg.n_grid == 256 and cfg.ring_dtype != "cint8":
+        cpb = max(1, nb // cfg.fine_per_coarse)
+        rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_C64_RATIO
+                                                if cfg.ring_dtype == "c64" else 1.0)
+        out["image"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt,
+                        "ncu dram bytes of image_kernel<256> on the medium workload (1152 "
+                        "images), scaled to this launch")
+    return out
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -702,44 +760,34 @@ def main():
                                                  "block_ms": cfg.block_seconds * 1e3}}
         del host
 
-    # roofline of the dominant kernel
+    # roofline of every kernel (stage), the dominant one as "roofline"
     hbm, bf16, peak_src = load_peaks()
+    i8 = measure_int8_peak(dev)
     work = stage_work(pipe)
-    dom = max(stages, key=lambda k: stages[k]["total_ms"])
-    kind, flops, nbytes = work[dom]
-    mean_s = stages[dom]["mean_ms"] / 1e3
-    if kind == "tensor":
-        achieved = flops / mean_s / 1e12
-        peak = 2.0 * bf16
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None, "kernel": dom,
-                "peak_note": f"int8 dense = 2 x {peak_src} bf16"}
-    else:
-        achieved = nbytes / mean_s / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "kernel": dom,
-                "peak_note": f"{peak_src} copy bandwidth"}
-    roof["algorithmic_bytes_per_launch"] = nbytes
-    roof["mean_launch_ms"] = stages[dom]["mean_ms"]
-    if dom == "image" and cfg.n_grid == 256:
-        # DRAM bytes of one image_kernel launch from an ncu capture of the same
-        # kernel on the medium workload (same per-image shape), scaled to this
-        # launch: writes by images, reads by coarse-DM slice-times
-        cfg_ = pipe.cfg
-        nt = cfg_.chunk_tiles + 2 * cfg_.t_edge
-        nb = cfg_.fdm_batch
-        cpb = max(1, nb // cfg_.fine_per_coarse)
-        rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_C64_RATIO
-                                                if cfg.ring_dtype == "c64" else 1.0)
-        roof["traffic"] = (IMAGE_DRAM_WRITE_PER_IMAGE * nb * nt + rd * cpb * nt
-                           if cfg.ring_dtype != "cint8" else None)
-        roof["traffic_note"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel on "
-                                "the medium workload (1152 images, bf16 ring), scaled to this "
-                                "launch"
-                                + ("; ring reads x 2.005, the complex64/bf16 read ratio of a "
-                                   "paired capture" if cfg.ring_dtype == "c64" else "")
-                                + ("; not captured for the cint8 ring"
-                                   if cfg.ring_dtype == "cint8" else ""))
+    traffic = stage_traffic(pipe)
+    roofs = {}
+    for st, tm in stages.items():
+        if st not in work:
+            continue
+        kind, flops, nbytes = work[st]
+        mean_s = tm["mean_ms"] / 1e3
+        if kind == "tensor":
+            achieved = flops / mean_s / 1e12
+            r = {"bound": "tensor", "achieved": achieved, "peak": i8, "unit": "TOP/s",
+                 "frac": achieved / i8, "algorithmic_ops_per_launch": flops,
+                 "peak_note": "dense int8 (cuBLASLt torch._int_mm 8192^3, best of 10, measured "
+                              "in this run)",
+                 "raw_input_gbs": nbytes / mean_s / 1e9}
+        else:
+            achieved = nbytes / mean_s / 1e9
+            r = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                 "frac": achieved / hbm, "algorithmic_bytes_per_launch": nbytes,
+                 "peak_note": f"{peak_src} copy bandwidth"}
+        r["mean_launch_ms"] = tm["mean_ms"]
+        r["traffic"], r["traffic_note"] = traffic.get(st, (None, None))
+        roofs[st] = r
+    dom = max((k for k in stages if k in roofs), key=lambda k: stages[k]["total_ms"])
+    roof = dict(roofs[dom], kernel=dom)
 
     if rank == 0:
         cb = None
@@ -754,6 +802,7 @@ def main():
                           else "int8 (correlator) / f32"), "data": "synthetic (seeded 4-bit Gaussian "
                 "voltages, sigma 3, T-layout antennas)", "config": workload_desc(a.workload, cfg),
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+                "rooflines_per_kernel": roofs,
                 "cpu_baseline": cb,
                 "stages_ms_per_step": {k: round(v["total_ms"] / a.steps, 3)
                                        for k, v in stages.items()}}

@@ -382,8 +382,21 @@ __device__ __noinline__ int2 det_sample(const BoxSums<K> d, const L2Samples l2, 
   return make_int2(s_i, s_t);
 }
 
+// One thread per cell; it marches the cell's time series once, keeping its
+// last MAXW + 1 prefix sums in a register ring.  Time is walked in blocks of
+// DB steps (unrolled; det_db): step j of a block writes its prefix to ring slot
+// MAXW + j, and the block ends by moving the newest MAXW prefixes down to
+// slots 0 .. MAXW-1 (MAXW register moves per DB steps), so the ring indices
+// are compile-time constants while the unrolled code stays DB steps long.
+// The inputs are prefetched DB steps ahead, one load per step.
+// DB = 16 steps per block; inputs are prefetched DP = 8 steps ahead (a
+// rolling set of DP registers), so that ring and prefetch fit 128 registers
+// at MAXW 64: two CTAs per SM.
+constexpr int DET_DB = 16;
+constexpr int DET_DP = 8;
+
 template <int LOGW, typename T>
-__global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, int n, int npix,
+__global__ void __launch_bounds__(256, 2) detect_kernel(const T* __restrict__ x, int n, int npix,
                                                      long long inner, long long f_stride,
                                                      long long t_stride,
                                                      const float* __restrict__ mask,
@@ -394,9 +407,11 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
                                                      DetCand* __restrict__ cands, int cap, int pix_off,
                                                      int* __restrict__ count, const L2Samples l2) {
   constexpr int MAXW = 1 << LOGW;
-  constexpr int R = MAXW + 1;
   constexpr int K = LOGW + 1;
   constexpr int PL = MAXW / 2;
+  constexpr int DB = DET_DB, DP = DET_DP;
+  constexpr int RS = MAXW + DB;  // ring registers
+  static_assert(DB % DP == 0, "the prefetch set cycles within a block");
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= inner) return;
   // this cell's Layer-2 sample entries [s_i, s_end) (a few thousand per
@@ -425,84 +440,108 @@ __global__ void __launch_bounds__(256) detect_kernel(const T* __restrict__ x, in
     const float lv = thr / sinv[k];
     tau[k] = lv - fabsf(lv) * 0x1p-20f;
   }
-  float ring[R];
+  // ring[i] holds prefix J0 - MAXW + i at the start of the block of steps
+  // J0 .. J0 + DB - 1 (prefix index J: 0 for J <= PL, the running sum of
+  // inputs 0 .. J-PL-1 up to J = PL + n, then the last sum: the padded
+  // cumsum); the output of step J is ta = J - MAXW and reads ring slots
+  // j .. j + MAXW
+  float ring[RS];
 #pragma unroll
-  for (int q = 0; q < R; ++q) ring[q] = 0.f;
+  for (int q = 0; q < RS; ++q) ring[q] = 0.f;
   double run = 0.0;
   float last = 0.f;
   const int total = n + MAXW;  // cs length
-  // the boxcar sums of the output whose newest prefix sits in ring slot q
-  // (the one MAXW/2 + 1 past its centre), widths 1, 2, ..., MAXW
-  auto boxcars = [&](int q, BoxSums<K>& d) {
+  // One output: the screen compares each boxcar sum with its lowered level
+  // (a superset of what the exact strict-'>' chain of det_emit reports,
+  // which decides); the threshold hits and the Layer-2 samples are rare, so
+  // both are calls out of the unrolled loop.
+  auto output = [&](int j, int ta, auto with_samples) {
+    BoxSums<K> d;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int w = 1 << k;
       const int off = PL - w / 2;
-      const int slo = ((q - MAXW + off) % R + R) % R;
-      const int shi = ((q - MAXW + off + w) % R + R) % R;
-      d.v[k] = ring[shi] - ring[slo];
+      d.v[k] = ring[j + off + w] - ring[j + off];
     }
-  };
-  // One output: the screen compares each boxcar sum with its lowered level
-  // (a superset of what the exact strict-'>' chain of det_emit reports,
-  // which decides); the threshold hits and the Layer-2 samples are rare, so
-  // both are calls out of this loop, which keeps the unrolled loop (R steps)
-  // small enough for the instruction cache.
-  auto output = [&](int q, int ta) {
-    BoxSums<K> d;
-    boxcars(q, d);
     bool hit = false;
 #pragma unroll
     for (int k = 0; k < K; ++k) hit |= d.v[k] > tau[k];
     if (hit) det_emit<K>(d, sinv, thr, ta - t_base, (int)e + pix_off, cands, cap, count);
-    if (ta - t_base == s_t) {
+    if (decltype(with_samples)::value && ta - t_base == s_t) {
       const int2 r = det_sample<K>(d, l2, s_i, s_end, eg, ta - t_base);
       s_i = r.x;
       s_t = r.y;
     }
   };
-  for (int J0 = 0; J0 < total; J0 += R) {
-    // issue this block's R loads before any of them is consumed
-    const bool interior = J0 >= PL + 1 && J0 + R - 1 <= PL + n && J0 - MAXW >= t_base &&
-                          J0 + R - 1 - MAXW < t_base + n_out;
-    float xin[R];
-    if (interior) {
-      // steady state: every sample loaded, every time an output
+  // input of step J: x[J - 1 - PL] (for PL < J <= PL + n); xin[j % DP]
+  // holds the input of step J0 + j, loaded DP steps earlier
+  auto input = [&](int J) -> float {
+    const int i = J - 1 - PL;
+    return (i >= 0 && i < n) ? ldf<T>(cube, (long long)i * t_stride) : 0.f;
+  };
+  float xin[DP];
 #pragma unroll
-      for (int q = 0; q < R; ++q) xin[q] = ldf<T>(cube, (long long)(J0 + q - 1 - PL) * t_stride);
+  for (int j = 0; j < DP; ++j) xin[j] = input(j);
+  // the first steps produce no output (ta < t_base): prefixes only
+  const int warm_end = t_base + MAXW;
+  for (int J0 = 0; J0 < total; J0 += DB) {
+    if (J0 + DB <= warm_end && J0 + DB + DP - 1 - PL <= n) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) {
-        run += (double)(xin[q] * mval);
-        ring[q] = (float)run;
-        output(q, J0 + q - MAXW);
-      }
-      last = ring[R - 1];
-      continue;
-    }
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int i = J0 + q - 1 - PL;
-      xin[q] = (i >= 0 && i < n) ? ldf<T>(cube, (long long)i * t_stride) : 0.f;
-    }
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int J = J0 + q;
-      if (J < total) {
-        float v;
-        if (J <= PL) {
-          v = 0.f;
-        } else if (J <= PL + n) {
-          run += (double)(xin[q] * mval);
-          last = (float)run;
-          v = last;
-        } else {
-          v = last;
+      for (int j = 0; j < DB; ++j) {
+        const int J = J0 + j;
+        float v = 0.f;
+        if (J > PL) {
+          run += (double)(xin[j % DP] * mval);
+          v = (float)run;
         }
-        ring[q] = v;
-        const int ta = J - MAXW;
-        if (ta >= t_base && ta < t_base + n_out) output(q, ta);
+        ring[MAXW + j] = v;
+        xin[j % DP] = input(J + DP);
+      }
+      last = ring[MAXW + DB - 1];
+    } else if (J0 >= PL + 1 && J0 + DB - 1 <= PL + n && J0 - MAXW >= t_base &&
+               J0 + DB - 1 - MAXW < t_base + n_out && J0 + DB - 1 + DP - 1 - PL < n) {
+      // steady state: every step an input, a prefix and an output, and the
+      // prefetched input in range; the Layer-2 test only in the (rare)
+      // blocks that hold this cell's next sample
+      const T* nxt = cube + (long long)(J0 + DP - 1 - PL) * t_stride;
+      auto steady = [&](auto with_samples) {
+#pragma unroll
+        for (int j = 0; j < DB; ++j) {
+          run += (double)(xin[j % DP] * mval);
+          ring[MAXW + j] = (float)run;
+          xin[j % DP] = ldf<T>(nxt, (long long)j * t_stride);
+          output(j, J0 + j - MAXW, with_samples);
+        }
+      };
+      if ((unsigned)(s_t - (J0 - MAXW - t_base)) < (unsigned)DB)
+        steady(std::true_type{});
+      else
+        steady(std::false_type{});
+      last = ring[MAXW + DB - 1];
+    } else {
+#pragma unroll
+      for (int j = 0; j < DB; ++j) {
+        const int J = J0 + j;
+        if (J < total) {
+          float v;
+          if (J <= PL) {
+            v = 0.f;
+          } else if (J <= PL + n) {
+            run += (double)(xin[j % DP] * mval);
+            last = (float)run;
+            v = last;
+          } else {
+            v = last;
+          }
+          ring[MAXW + j] = v;
+          const int ta = J - MAXW;
+          if (ta >= t_base && ta < t_base + n_out) output(j, ta, std::true_type{});
+        }
+        xin[j % DP] = input(J + DP);
       }
     }
+#pragma unroll
+    for (int q = 0; q < MAXW; ++q) ring[q] = ring[q + DB];
   }
 }
 
