@@ -226,6 +226,89 @@ __global__ void mask_to_cube_kernel(const float* __restrict__ img, const float* 
 }
 
 // ===========================================================================
+// Compact-layout combine (combine_sparse_v4 + build_sparse_cell_csr,
+// image/tiled_combine_cuda.py:966-1060, 1092-1240): streams in the
+// time-minor compact layout dense[g][k][t][re, im] int8 (k a pattern cell of
+// stream g), a CSR over the active half cells (u, w <= N/2) listing every
+// stream g that carries the cell (k) or its mirror (km), -1 where absent.
+// out[f][out_row0 + t][u][w] = 0.5 (sum_g q(k) + conj q(km)) at stream time
+// t + t_lo - shift[f][g] (zero outside [0, t_rows)), times (-1)^(u+w) when
+// fftshift; int32 sums, so exact; fp16 pairs or complex64.  Only active
+// cells are written.
+// One CTA per (active cell, tile of CS_T output times): the cell's entries
+// go to shared memory, then each thread takes (fine DM, time) pairs; a
+// warp's consecutive times read consecutive 2-byte stream words.
+// ===========================================================================
+constexpr int CS_T = 64;
+constexpr int CS_MAXE = 64;
+
+template <bool OUT_F16>
+__global__ void __launch_bounds__(256) combine_sparse_kernel(
+    const int16_t* __restrict__ dense, const int* __restrict__ cell_uw,
+    const int* __restrict__ cell_ptr, const int* __restrict__ ent_g,
+    const int* __restrict__ ent_k, const int* __restrict__ ent_km,
+    const int* __restrict__ shifts, void* __restrict__ out, int n_sb, int t_rows, int t_pad,
+    int nfm, int N, int n_fdm, int t_out_len, int t_lo, int fftshift, int out_rows,
+    int out_row0, int* __restrict__ status) {
+  __shared__ int s_g[CS_MAXE], s_k[CS_MAXE], s_km[CS_MAXE];
+  const int a = blockIdx.x;
+  const int nh = N / 2 + 1;
+  const int uw = cell_uw[a];
+  const int u = uw / nh, w = uw % nh;
+  const int e0 = cell_ptr[a];
+  const int ne = cell_ptr[a + 1] - e0;
+  if (ne > CS_MAXE || ne < 0) {
+    if (threadIdx.x == 0) dsb_flag(status, DSB_E_CAPACITY);
+    return;
+  }
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    const int g = ent_g[e0 + e], k = ent_k[e0 + e], km = ent_km[e0 + e];
+    const bool ok = g >= 0 && g < n_sb && k < nfm && km < nfm;
+    s_g[e] = ok ? g : -1;
+    s_k[e] = k;
+    s_km[e] = km;
+    if (!ok) dsb_flag(status, DSB_E_ARG);
+  }
+  __syncthreads();
+  const bool flip = fftshift && ((u + w) & 1);
+  const int t0 = blockIdx.y * CS_T;
+  const int nt = min(CS_T, t_out_len - t0);
+  for (int idx = threadIdx.x; idx < n_fdm * CS_T; idx += blockDim.x) {
+    const int f = idx / CS_T, tl = idx % CS_T;
+    if (tl >= nt) continue;
+    const int t = t0 + tl;
+    int re = 0, im = 0;
+    for (int e = 0; e < ne; ++e) {
+      const int g = s_g[e];
+      if (g < 0) continue;
+      const int ts = t + t_lo - shifts[f * n_sb + g];
+      if (ts < 0 || ts >= t_rows) continue;
+      const long long row = (long long)g * nfm;
+      if (s_k[e] >= 0) {
+        const int16_t v = __ldg(dense + (row + s_k[e]) * t_pad + ts);
+        re += (int)(int8_t)(v & 0xff);
+        im += (int)(int8_t)((v >> 8) & 0xff);
+      }
+      if (s_km[e] >= 0) {
+        const int16_t v = __ldg(dense + (row + s_km[e]) * t_pad + ts);
+        re += (int)(int8_t)(v & 0xff);
+        im -= (int)(int8_t)((v >> 8) & 0xff);
+      }
+    }
+    float o_re = 0.5f * (float)re, o_im = 0.5f * (float)im;
+    if (flip) {
+      o_re = -o_re;
+      o_im = -o_im;
+    }
+    const long long o = ((long long)f * out_rows + out_row0 + t) * N * nh + (long long)u * nh + w;
+    if (OUT_F16)
+      reinterpret_cast<__half2*>(out)[o] = __floats2half2_rn(o_re, o_im);
+    else
+      reinterpret_cast<float2*>(out)[o] = make_float2(o_re, o_im);
+  }
+}
+
+// ===========================================================================
 // padded cumsum / boxcars (detector/forward.py:250-455,
 // detector/triton_boxcar.py:47-360).  Each prefix is accumulated in float64
 // and rounded once to float32.
@@ -748,6 +831,35 @@ int dsb_combine_rows(const void* D, int d_format, const long long* seg_base, con
     combine_rows_kernel<1><<<grid, 128, 0, stream>>>(A);
   else
     combine_rows_kernel<0><<<grid, 128, 0, stream>>>(A);
+  return launch_status();
+}
+
+int dsb_combine_sparse(const void* dense, const int* cell_uw, const int* cell_ptr,
+                       const int* ent_g, const int* ent_k, const int* ent_km, int n_act,
+                       const int* shifts, void* out, int out_f16, int n_sb, int t_rows,
+                       int t_pad, int n_filled_max, int N, int n_fdm, int t_out_len, int t_lo,
+                       int fftshift, int out_rows, int out_row0, int* status,
+                       cudaStream_t stream) {
+  if (!dense || !cell_uw || !cell_ptr || !shifts || !out || !status || n_act < 0 ||
+      n_sb <= 0 || t_rows < 0 || t_pad < t_rows || n_filled_max <= 0 || N <= 0 || (N & 1) ||
+      n_fdm <= 0 || t_out_len < 0 || out_row0 < 0 || out_row0 + t_out_len > out_rows)
+    return DSB_E_ARG;
+  if (n_act > 0 && (!ent_g || !ent_k || !ent_km)) return DSB_E_ARG;
+  if ((reinterpret_cast<uintptr_t>(dense) & 1) || (reinterpret_cast<uintptr_t>(out) & 3))
+    return DSB_E_ARG;
+  if (n_act == 0 || t_out_len == 0) return DSB_OK;
+  if ((t_out_len + CS_T - 1) / CS_T > 65535) return DSB_E_ARG;
+  const dim3 grid(n_act, (t_out_len + CS_T - 1) / CS_T);
+  if (out_f16)
+    combine_sparse_kernel<true><<<grid, 256, 0, stream>>>(
+        static_cast<const int16_t*>(dense), cell_uw, cell_ptr, ent_g, ent_k, ent_km, shifts, out,
+        n_sb, t_rows, t_pad, n_filled_max, N, n_fdm, t_out_len, t_lo, fftshift, out_rows,
+        out_row0, status);
+  else
+    combine_sparse_kernel<false><<<grid, 256, 0, stream>>>(
+        static_cast<const int16_t*>(dense), cell_uw, cell_ptr, ent_g, ent_k, ent_km, shifts, out,
+        n_sb, t_rows, t_pad, n_filled_max, N, n_fdm, t_out_len, t_lo, fftshift, out_rows,
+        out_row0, status);
   return launch_status();
 }
 

@@ -51,6 +51,9 @@ _SIGNATURES = {
                          _c_int, _c_int, _c_ll, _c_int, _c_int, _vp, _vp],
     "dsb_combine_dense": [_vp, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                           _c_int, _c_int, _c_int, _c_int, _vp],
+    "dsb_combine_sparse": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _c_int, _c_int,
+                           _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                           _c_int, _c_int, _vp, _vp],
     "dsb_encode_rows": [_vp, _c_ll, _c_int, _c_int, _c_int, _vp, _vp, _vp],
     "dsb_cluster_mst": [_vp, _c_int, _c_int, _c_int, _vp, _vp],
     "dsb_cal_apply": [_vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,

@@ -79,6 +79,134 @@ def fused_dequant_combine_per_fdm_half(streams_cint8, shifts, output, *, scales=
 
 
 # ---------------------------------------------------------------------------
+# combine (compact time-minor layout; tiled_combine_cuda.py:1080-1240)
+# ---------------------------------------------------------------------------
+
+# per-cell stream-count buckets, the reference's launch grouping (:1069)
+_V4_BUCKETS = (8, 16, 32, 64)
+
+
+@dataclass
+class SparseCellCsr:
+    """Per-half-cell list of the streams carrying the cell or its mirror
+    (tiled_combine_cuda.py:1069-1090): active cells ``cell_uw = u * (N/2+1)
+    + w`` grouped by entry-count bucket (<= 8, 16, 32, 64) and ascending
+    inside a bucket, entries [cell_ptr[a], cell_ptr[a+1]) with stream
+    ``ent_g`` (ascending) and compact indices ``ent_k`` / ``ent_km`` of the
+    cell and its mirror (-1 where absent); ``buckets`` (start, end, max
+    entries) per non-empty bucket."""
+    n_sb: int
+    n_grid: int
+    cell_uw: torch.Tensor
+    cell_ptr: torch.Tensor
+    ent_g: torch.Tensor
+    ent_k: torch.Tensor
+    ent_km: torch.Tensor
+    buckets: tuple
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cell_uw.shape[0])
+
+    @property
+    def n_entries(self) -> int:
+        return int(self.ent_g.shape[0])
+
+
+def build_sparse_cell_csr(inv_lut: torch.Tensor, *, n_grid: int) -> SparseCellCsr:
+    """The tables of ``combine_sparse_v4`` from the inverse LUT ``[n_sb,
+    N*N]`` (compact index of each grid cell in each stream, -1 if absent):
+    tiled_combine_cuda.py:1092.  Built once per pattern set (host)."""
+    n_sb = int(inv_lut.shape[0])
+    N = int(n_grid)
+    if tuple(inv_lut.shape) != (n_sb, N * N):
+        raise ValueError(f"inv_lut must be (n_sb, {N * N}); got {tuple(inv_lut.shape)}")
+    if n_sb > 64:
+        raise ValueError(f"v4 supports n_sb <= 64; got {n_sb}")
+    dev = inv_lut.device
+    lut = inv_lut.detach().to("cpu").numpy().astype(np.int64)
+    nh = N // 2 + 1
+    u = np.repeat(np.arange(N), nh)
+    w = np.tile(np.arange(nh), N)
+    lin = u * N + w
+    linm = ((N - u) % N) * N + ((N - w) % N)
+    k_lin = lut[:, lin].T                   # [n_half_cells, n_sb]
+    k_linm = lut[:, linm].T
+    present = (k_lin >= 0) | (k_linm >= 0)
+    ne = present.sum(1)
+    uw = u * nh + w
+    order_parts, buckets, lo, start = [], [], 0, 0
+    for hi in _V4_BUCKETS:
+        sel = np.flatnonzero((ne > lo) & (ne <= hi))
+        if sel.size:
+            order_parts.append(sel)
+            buckets.append((start, start + int(sel.size), int(ne[sel].max())))
+            start += int(sel.size)
+        lo = hi
+    order = np.concatenate(order_parts) if order_parts else np.zeros(0, np.int64)
+    cell_ptr = np.zeros(order.size + 1, np.int32)
+    cell_ptr[1:] = np.cumsum(ne[order])
+    rows, g = np.nonzero(present[order])    # cell-major, g ascending
+    cells = order[rows]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.int32)).to(dev)  # noqa: E731
+    return SparseCellCsr(n_sb=n_sb, n_grid=N, cell_uw=t(uw[order]), cell_ptr=t(cell_ptr),
+                         ent_g=t(g), ent_k=t(k_lin[cells, g]), ent_km=t(k_linm[cells, g]),
+                         buckets=tuple(buckets))
+
+
+def combine_sparse_v4(dense: torch.Tensor, csr: SparseCellCsr, shifts: torch.Tensor, *,
+                      t_rows: int, t_out_len: int, t_lo: int = 0, fftshift: bool = True,
+                      threads: int = 512, out: torch.Tensor, out_row0: int = 0,
+                      shift_min: int, shift_max: int) -> torch.Tensor:
+    """Compact-layout half-spectrum combine (tiled_combine_cuda.py:1142):
+    ``dense [n_sb, n_filled_max, t_pad, 2]`` int8 time-minor streams and the
+    ``csr`` of ``build_sparse_cell_csr``; writes ONLY the active cells of
+    ``out [>= n_fdm, rows, N, N/2+1]`` (complex32, float16 [.., 2] or, here
+    also, complex64) at rows ``out_row0 ..``: the caller zeroes the rest.
+    ``threads`` and the shift bounds are accepted for the reference's
+    signature; this kernel needs neither."""
+    n_sb, nfm, t_pad, two = dense.shape
+    if two != 2 or n_sb != csr.n_sb:
+        raise ValueError(f"dense {tuple(dense.shape)} does not match csr n_sb={csr.n_sb}")
+    if dense.dtype != torch.int8 or not dense.is_contiguous():
+        raise ValueError("dense must be contiguous int8")
+    N = csr.n_grid
+    nh = N // 2 + 1
+    n_fdm = int(shifts.shape[0])
+    if shifts.ndim != 2 or shifts.shape[1] != n_sb:
+        raise ValueError(f"shifts must be [n_fdm, n_sb={n_sb}]; got {tuple(shifts.shape)}")
+    if not out.is_contiguous():
+        raise ValueError("out must be contiguous (pass the parent buffer + out_row0)")
+    if out.dtype == torch.complex32:
+        tail, f16 = (N, nh), 1
+    elif out.dtype == torch.float16:
+        tail, f16 = (N, nh, 2), 1
+    elif out.dtype == torch.complex64:
+        tail, f16 = (N, nh), 0
+    else:
+        raise ValueError(f"out dtype {out.dtype} not complex32/float16/complex64")
+    if int(out.shape[0]) < n_fdm or tuple(out.shape[2:]) != tail:
+        raise ValueError(f"out shape {tuple(out.shape)} incompatible with n_fdm={n_fdm} N={N}")
+    out_rows = int(out.shape[1])
+    if out_row0 < 0 or out_row0 + t_out_len > out_rows:
+        raise ValueError(f"out_row0={out_row0} + t_out_len={t_out_len} > rows={out_rows}")
+    if t_rows > t_pad:
+        raise ValueError(f"t_rows={t_rows} > t_pad={t_pad}")
+    for x, nm in ((dense, "dense"), (shifts, "shifts"), (out, "out")):
+        _lib.require_cuda(x, nm)
+    sh = shifts.to(torch.int32).contiguous()
+    st = _lib.status_word(out.device)
+    _lib.check(_lib.lib().dsb_combine_sparse(
+        _lib.ptr(dense), _lib.ptr(csr.cell_uw), _lib.ptr(csr.cell_ptr), _lib.ptr(csr.ent_g),
+        _lib.ptr(csr.ent_k), _lib.ptr(csr.ent_km), csr.n_cells, _lib.ptr(sh), _lib.ptr(out),
+        f16, n_sb, int(t_rows), int(t_pad), int(nfm), N, n_fdm, int(t_out_len), int(t_lo),
+        int(bool(fftshift)), out_rows, int(out_row0), _lib.ptr(st),
+        _lib.stream_of(out.device)), "dsb_combine_sparse")
+    _lib.check_status(st, "dsb_combine_sparse")
+    return out
+
+
+# ---------------------------------------------------------------------------
 # imaging
 # ---------------------------------------------------------------------------
 
@@ -261,10 +389,10 @@ class GpuImager:
                      compact_shift_bounds: Optional[tuple] = None) -> torch.Tensor:
         """One cube: ``streams_cint8 [G, T_stream, 2, N, N]`` int8 and
         ``time_shifts_gpu [n_fdm, G]`` int32 -> ``[t_det, n_fdm, N, N]``
-        (imager_gpu.py:217-657).  The compact-layout combine is not built."""
+        (imager_gpu.py:217-657); with ``compact_inv_lut`` the streams are the
+        compact time-minor ``[G, n_filled_max, t_pad, 2]`` and the combine is
+        ``combine_sparse_v4``."""
         cfg = self.config
-        if compact_inv_lut is not None:
-            raise NotImplementedError("the compact-layout combine is not built; pass dense streams")
         if time_shifts_gpu.shape != (cfg.n_fdm, streams_cint8.shape[0]):
             raise ValueError(f"time_shifts_gpu shape {tuple(time_shifts_gpu.shape)}, expected "
                              f"({cfg.n_fdm}, {streams_cint8.shape[0]})")
@@ -274,6 +402,10 @@ class GpuImager:
         cube = self.output_cube_alt if self._flip else self.output_cube
         self._flip = not self._flip
         shifts = time_shifts_gpu.to(torch.int32).contiguous()
+        if compact_inv_lut is not None:
+            return self._process_compact(streams_cint8, shifts, compact_inv_lut,
+                                         int(compact_t_stream), t_lo, cube,
+                                         (chgroup_scales, chgroup_offsets_re, chgroup_offsets_im))
         for f in range(cfg.n_fdm):
             fused_dequant_combine_per_fdm_half(streams_cint8, shifts[f], uv,
                                                scales=chgroup_scales,
@@ -283,6 +415,48 @@ class GpuImager:
             if cfg.imager_uv_prescale != 1.0:
                 uv.mul_(cfg.imager_uv_prescale)
             img = irfft2_image(uv, N, out=self._img_buffer(n_t))[None]   # (1, n_t, N, N)
+            mask = (self.edge_mask_real if self.edge_mask_per_fdm is None
+                    else self.edge_mask_per_fdm[f:f + 1])
+            mask_into_cube(img.contiguous(), mask, cube[t_lo:] if t_lo else cube, f)
+        return cube
+
+
+    def _process_compact(self, streams, shifts, inv_lut, t_stream, t_lo, cube, calib):
+        """The compact path of process_cube (imager_gpu.py:300-330, 487-520):
+        ``streams [N_chg, n_filled_max, t_pad, 2]`` int8 time-minor, every
+        fine DM combined in one launch (combine_sparse_v4) into a zeroed
+        half-spectrum buffer, then the transform and mask per fine DM."""
+        cfg = self.config
+        N = cfg.n_grid
+        if streams.ndim != 4 or streams.shape[3] != 2:
+            raise ValueError("compact combine expects [N_chg, n_filled_max, t_pad, 2]; "
+                             f"got {tuple(streams.shape)}")
+        if int(streams.shape[0]) != cfg.n_chgroup:
+            raise ValueError(f"compact N_chg={streams.shape[0]} != config "
+                             f"N_chgroup={cfg.n_chgroup}")
+        if any(x is not None for x in calib):
+            raise ValueError("compact combine is the unit-scale path only; per-chgroup "
+                             "calibration needs the dense combine")
+        if t_stream < cfg.t_det:
+            raise ValueError(f"compact_t_stream={t_stream} < T_det={cfg.t_det}")
+        key = (int(inv_lut.data_ptr()), tuple(inv_lut.shape), N)
+        if getattr(self, "_csr_key", None) != key:
+            self._csr = build_sparse_cell_csr(inv_lut, n_grid=N)
+            self._csr_key = key
+        full = getattr(self, "_uv_full", None)
+        if full is None:
+            full = self._uv_full = torch.empty((cfg.n_fdm, cfg.t_det, N, N // 2 + 1),
+                                               dtype=torch.complex64, device=self.device)
+        full[:, t_lo:cfg.t_det].zero_()
+        combine_sparse_v4(streams, self._csr, shifts, t_rows=t_stream,
+                          t_out_len=cfg.t_det - t_lo, t_lo=t_lo, fftshift=True, out=full,
+                          out_row0=t_lo, shift_min=0, shift_max=0)
+        n_t = cfg.t_det - t_lo
+        for f in range(cfg.n_fdm):
+            uv = full[f, t_lo:cfg.t_det]
+            if cfg.imager_uv_prescale != 1.0:
+                uv.mul_(cfg.imager_uv_prescale)
+            img = irfft2_image(uv.contiguous(), N, out=self._img_buffer(n_t))[None]
             mask = (self.edge_mask_real if self.edge_mask_per_fdm is None
                     else self.edge_mask_per_fdm[f:f + 1])
             mask_into_cube(img.contiguous(), mask, cube[t_lo:] if t_lo else cube, f)

@@ -231,6 +231,26 @@ int dsb_ring_encode_cint8(const void* X, const long long* x_base, int n_t, const
                           void* D, const long long* seg_base, const int* seg_depth,
                           float* scales, const long long* sc_base, int* status,
                           cudaStream_t stream);
+/* ---- a12: compact-layout combine -----------------------------------------------
+ * combine_sparse_v4 (src/dsart/image/tiled_combine_cuda.py:1142; kernel :966)
+ * with build_sparse_cell_csr's tables (:1092): dense [n_sb][n_filled_max]
+ * [t_pad][re, im] int8 (time-minor compact streams, 2-byte aligned); the
+ * n_act active half cells cell_uw = u * (N/2+1) + w with their entries
+ * [cell_ptr[a], cell_ptr[a+1]) (at most 64 per cell) of stream ent_g
+ * carrying the cell at compact index ent_k and / or its mirror at ent_km
+ * (-1 where absent).  out[f][out_row0 + t][u][w] for t < t_out_len =
+ * 0.5 (sum q(k) + conj q(km)) over the entries at stream time
+ * t + t_lo - shifts[f * n_sb + g] (absent outside [0, t_rows)), times
+ * (-1)^(u+w) if fftshift; int32 sums (exact), then half2 (out_f16) or
+ * complex64.  Writes only the active cells: the caller zeroes the rest.
+ * out is [n_fdm][out_rows][N][N/2+1].  A cell with more than 64 entries
+ * sets DSB_E_CAPACITY in *status, an entry outside the tables DSB_E_ARG. */
+int dsb_combine_sparse(const void* dense, const int* cell_uw, const int* cell_ptr,
+                       const int* ent_g, const int* ent_k, const int* ent_km, int n_act,
+                       const int* shifts, void* out, int out_f16, int n_sb, int t_rows,
+                       int t_pad, int n_filled_max, int N, int n_fdm, int t_out_len, int t_lo,
+                       int fftshift, int out_rows, int out_row0, int* status,
+                       cudaStream_t stream);
 int dsb_combine_dense(const void* streams, const int* shifts, const float* scales,
                       const float* off_re, const float* off_im, int per_t, void* out,
                       int out_f16, int half,

@@ -661,6 +661,29 @@ def half_from_full(full: np.ndarray, fftshift: bool = True) -> np.ndarray:
     return h
 
 
+def combine_sparse(dense: np.ndarray, inv_lut: np.ndarray, shifts: np.ndarray, *,
+                   t_rows: int, t_out_len: int, t_lo: int = 0,
+                   fftshift: bool = True) -> np.ndarray:
+    """The compact-layout combine (image/tiled_combine_cuda.py:966-1060):
+    ``dense [n_sb, n_filled_max, t_pad, 2]`` int8 time-minor streams,
+    ``inv_lut [n_sb, N*N]`` the compact index of each grid cell per stream
+    (-1 absent), ``shifts [n_fdm, n_sb]``.  Each stream is scattered back to
+    its dense grid and combined as ``combine_half`` does (stream time
+    t + t_lo - shift, zero outside [0, t_rows)); returns complex128
+    ``[n_fdm, t_out_len, N, N/2+1]`` (exact: the sums are of integers)."""
+    n_sb, nfm, t_pad, _ = dense.shape
+    N = int(round(np.sqrt(inv_lut.shape[1])))
+    streams = np.zeros((n_sb, t_rows, N * N), np.complex128)
+    for g in range(n_sb):
+        cells = np.flatnonzero(inv_lut[g] >= 0)
+        k = inv_lut[g, cells]
+        v = dense[g, k, :t_rows].astype(np.float64)            # (cells, t, 2)
+        streams[g][:, cells] = (v[..., 0] + 1j * v[..., 1]).T
+    streams = streams.reshape(n_sb, t_rows, N, N)
+    return np.stack([combine_half(streams, shifts[f], t_lo + t_out_len, t_lo, fftshift=fftshift)
+                     for f in range(shifts.shape[0])])
+
+
 def _fma32(a, b, c):
     """float32 fma: a*b + c rounded once (a*b is exact in float64 for the
     float32 x int8 products used here, and so is the sum at these ranges)."""

@@ -625,6 +625,39 @@ def make_cluster():
     np.savez_compressed(os.path.join(HERE, "cluster.npz"), **out)
 
 
+SPARSE_SEED = 808
+
+
+def sparse_inv_lut(seed: int = SPARSE_SEED, n_sb: int = 5, N: int = 32, n_filled: int = 60):
+    """Seeded inverse LUTs [n_sb, N*N]: each stream's n_filled cells (compact
+    index 0..n_filled-1 in ascending cell order), -1 elsewhere; some cells
+    shared by several streams, some by their mirrors."""
+    rng = np.random.default_rng(seed)
+    lut = np.full((n_sb, N * N), -1, np.int64)
+    for g in range(n_sb):
+        cells = np.sort(rng.choice(N * N, n_filled, replace=False))
+        lut[g, cells] = np.arange(n_filled)
+    return lut
+
+
+def make_sparse_csr():
+    """build_sparse_cell_csr (image/tiled_combine_cuda.py:1092) on torch CPU:
+    the combine_sparse_v4 tables, pinned field by field."""
+    import torch
+    from dsart.image.tiled_combine_cuda import build_sparse_cell_csr
+    out = {}
+    for name, kw in (("a", dict(n_sb=5, N=32, n_filled=60)),
+                     ("b", dict(n_sb=16, N=16, n_filled=100))):
+        lut = sparse_inv_lut(**kw)
+        csr = build_sparse_cell_csr(torch.from_numpy(lut), n_grid=kw["N"])
+        out[f"{name}_lut"] = lut.astype(np.int32)
+        out[f"{name}_n_grid"] = kw["N"]
+        for f in ("cell_uw", "cell_ptr", "ent_g", "ent_k", "ent_km"):
+            out[f"{name}_{f}"] = getattr(csr, f).numpy().astype(np.int32)
+        out[f"{name}_buckets"] = np.asarray(csr.buckets, np.int64).reshape(-1, 3)
+    np.savez_compressed(os.path.join(HERE, "sparse_csr.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DSART_REFERENCE", ""))
@@ -635,7 +668,7 @@ def main():
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
             make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
-            make_cluster, make_cal, make_layer2, make_layer1_state]
+            make_cluster, make_cal, make_layer2, make_layer1_state, make_sparse_csr]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
