@@ -658,6 +658,21 @@ def make_sparse_csr():
     np.savez_compressed(os.path.join(HERE, "sparse_csr.npz"), **out)
 
 
+def make_kernel_bank():
+    """build_kernel_bank (detector/kernels.py:191): ids, widths and order of
+    the default bank and of the production (unit, d1, b1..b64) bank."""
+    from dsart.detector.kernels import build_kernel_bank
+    out = {}
+    for name, kw in (("full", {}), ("prod", dict(image_tokens=("unit",), dm_tokens=("d1",),
+                                                 time_tokens=("b1", "b2", "b4", "b8", "b16",
+                                                              "b32", "b64")))):
+        bank = build_kernel_bank(**kw)
+        out[f"{name}_ids"] = np.asarray([k.kernel_id for k in bank])
+        out[f"{name}_w"] = np.asarray([[k.k_dm_width, k.k_time_width, k.image_kernel_size]
+                                       for k in bank], np.int64)
+    np.savez_compressed(os.path.join(HERE, "kernel_bank.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DSART_REFERENCE", ""))
@@ -668,7 +683,8 @@ def main():
     sys.path.insert(0, a.reference)
     todo = [make_unpack, make_corr, make_grid_and_plan, make_stage1, make_fifos_and_sky,
             make_image_detector, make_transport, make_rfi, make_slow_corr, make_postproc,
-            make_cluster, make_cal, make_layer2, make_layer1_state, make_sparse_csr]
+            make_cluster, make_cal, make_layer2, make_layer1_state, make_sparse_csr,
+            make_kernel_bank]
     for fn in todo:
         if a.only and a.only not in fn.__name__:
             continue
