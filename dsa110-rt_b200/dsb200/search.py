@@ -552,6 +552,7 @@ class Candidate:
     width_samples: int
     kernel_id: str
     snr: float
+    flags: int = 0
 
 
 def _nms(items, *, threshold, n_top, shape, r_t, r_f, r_lm):
