@@ -77,7 +77,7 @@ def test_gpu_imager_compact_equals_dense():
     full = np.zeros((G, t_rows, 2, N * N), np.int8)
     for g in range(G):
         cells = np.flatnonzero(lut[g] >= 0)
-        full[g, :, :, cells] = dense[g, lut[g, cells], :t_rows].transpose(1, 0, 2)
+        full[g, :, :, cells] = dense[g, lut[g, cells], :t_rows]     # (cells, t, 2)
     full = full.reshape(G, t_rows, 2, N, N)
     cfg = GpuImagerConfig(n_grid=N, t_det=16, n_fdm=3, n_chgroup=G, kernel_support=1,
                           cube_dtype=torch.float32, device=dev)
