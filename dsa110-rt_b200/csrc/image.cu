@@ -722,27 +722,46 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
 #pragma unroll
           for (int jj = 0; jj < R1; ++jj) b[h][jj] = reg[m2 * R1 + (jj ^ rj)];
         }
-        __syncwarp(rmask);
-        float* stage = reinterpret_cast<float*>(reg);
-#pragma unroll
-        for (int h = 0; h < H; ++h) {
-          idftR<R1>(b[h]);
-#pragma unroll
-          for (int m1 = 0; m1 < R1; ++m1) {
-            const int x = rj + R1 * h + R2 * m1;
-            stage[x] = b[h][m1].x;
-            stage[N + x] = b[h][m1].y;
-          }
-        }
-        __syncwarp(rmask);
         const size_t ibase = ((size_t)fl * A.n_t + t) * N;
-        float4* oa = reinterpret_cast<float4*>(A.out + (ibase + FOLD * (2 * pr) + p) * N);
-        float4* ob = reinterpret_cast<float4*>(A.out + (ibase + FOLD * (2 * pr + 1) + p) * N);
-        const float4* s4 = reinterpret_cast<const float4*>(stage);
+        float* ra_out = A.out + (ibase + FOLD * (2 * pr) + p) * N;
+        float* rb_out = A.out + (ibase + FOLD * (2 * pr + 1) + p) * N;
+        if constexpr (N == 512) {
+          // outputs straight from registers: for each (h, m1) the group's
+          // 16 lanes hold 16 consecutive pixels of each row (64 bytes), so
+          // no staging through shared memory (whose pipe the transposes
+          // already keep busy)
 #pragma unroll
-        for (int q = rj; q < N / 4; q += R1) {
-          oa[q] = s4[q];
-          ob[q] = s4[N / 4 + q];
+          for (int h = 0; h < H; ++h) {
+            idftR<R1>(b[h]);
+#pragma unroll
+            for (int m1 = 0; m1 < R1; ++m1) {
+              const int x = rj + R1 * h + R2 * m1;
+              ra_out[x] = b[h][m1].x;
+              rb_out[x] = b[h][m1].y;
+            }
+          }
+        } else {
+          __syncwarp(rmask);
+          float* stage = reinterpret_cast<float*>(reg);
+#pragma unroll
+          for (int h = 0; h < H; ++h) {
+            idftR<R1>(b[h]);
+#pragma unroll
+            for (int m1 = 0; m1 < R1; ++m1) {
+              const int x = rj + R1 * h + R2 * m1;
+              stage[x] = b[h][m1].x;
+              stage[N + x] = b[h][m1].y;
+            }
+          }
+          __syncwarp(rmask);
+          float4* oa = reinterpret_cast<float4*>(ra_out);
+          float4* ob = reinterpret_cast<float4*>(rb_out);
+          const float4* s4 = reinterpret_cast<const float4*>(stage);
+#pragma unroll
+          for (int q = rj; q < N / 4; q += R1) {
+            oa[q] = s4[q];
+            ob[q] = s4[N / 4 + q];
+          }
         }
       }
       __syncthreads();
