@@ -477,6 +477,11 @@ __device__ __noinline__ int2 det_sample(const BoxSums<K> d, const L2Samples l2, 
 // at MAXW 64: two CTAs per SM.
 constexpr int DET_DB = 16;
 constexpr int DET_DP = 8;
+constexpr int DET_PF = 32;  // L2 prefetch distance (steps)
+
+DSB_DEV void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 
 template <int LOGW, typename T>
 __global__ void __launch_bounds__(256, 2) detect_kernel(const T* __restrict__ x, int n, int npix,
@@ -587,12 +592,17 @@ __global__ void __launch_bounds__(256, 2) detect_kernel(const T* __restrict__ x,
       // prefetched input in range; the Layer-2 test only in the (rare)
       // blocks that hold this cell's next sample
       const T* nxt = cube + (long long)(J0 + DP - 1 - PL) * t_stride;
+      // L2 prefetch DET_PF steps ahead by one lane per warp (the warp's 32
+      // cells of a time are one 128-byte line), where still inside the cube
+      const bool pf = (threadIdx.x & 31) == 0 && J0 + DB - 1 + DET_PF - 1 - PL < n;
+      const T* pfp = cube + (long long)(J0 + DET_PF - 1 - PL) * t_stride;
       auto steady = [&](auto with_samples) {
 #pragma unroll
         for (int j = 0; j < DB; ++j) {
           run += (double)(xin[j % DP] * mval);
           ring[MAXW + j] = (float)run;
           xin[j % DP] = ldf<T>(nxt, (long long)j * t_stride);
+          if (pf) prefetch_l2(pfp + (long long)j * t_stride);
           output(j, J0 + j - MAXW, with_samples);
         }
       };
