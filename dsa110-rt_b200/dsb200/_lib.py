@@ -42,6 +42,9 @@ _SIGNATURES = {
     "dsb_stage1_dm_group": [],
     "dsb_stage1_smem_bytes": [_c_int, _c_int, _c_int],
     "dsb_image_geometry": [_c_int, _vp],
+    "dsb_graph_begin": [_vp],
+    "dsb_graph_end_launch": [_vp, _vp],
+    "dsb_graph_destroy": [_vp],
     "dsb_irfft2": [_vp, _c_int, _c_int, _vp, _vp, _vp],
     "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int,
                       _c_int, _vp,

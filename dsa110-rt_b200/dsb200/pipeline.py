@@ -545,6 +545,7 @@ class SearchPipeline:
             self.l2_state._s_k.copy_(torch.tensor([math.sqrt(w) for w in widths],
                                                   dtype=torch.float32))
             self.sinv = torch.reciprocal(torch.clamp(self.l2_state.s_k, min=1e-30))
+            self.l2_sig = torch.empty(len(widths), dtype=torch.float32, device=self.dev)
         self.cands = CandidateBuffer(self.dev, cfg.cand_capacity)
         self.chunk = 0              # next absolute chunk index to correlate
         self.out: List[StreamCandidate] = []
@@ -676,7 +677,15 @@ class SearchPipeline:
             max_blocks, _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_image_fft")
 
     def _search(self, jc: int, collect: bool = True) -> None:
-        cfg, T = self.cfg, self.tab
+        self._search_device(jc)
+        self._search_host(jc, collect)
+
+    def _search_device(self, jc: int) -> None:
+        """The detector cube ending with chunk jc on the device: images,
+        Layer-1, detector (candidates and Layer-2 samples), the cube's
+        per-kernel sigma into ``l2_sig``.  Launches only: no host sync and no
+        allocation, so it can be captured in a CUDA graph."""
+        cfg = self.cfg
         C, te, N = cfg.chunk_tiles, cfg.t_edge, cfg.n_grid
         t0 = jc * C - 2 * te
         nt = C + 2 * te
@@ -695,16 +704,24 @@ class SearchPipeline:
                               cands=self.cands, pix_offset=f0 * N * N, sigma_f=sig,
                               layer2=self.l2)
             self.launches += 3
-            if collect and self.keep_sigma:
+            if self.keep_sigma:
                 self.l1_sigma.append(sig.clone())
         if self.l2 is not None:
-            # this cube's sigma_k from its score samples, folded into the
-            # state that divides the next cube's boxcars
             with self._mark("layer2"):
-                sig_k = sigma_clipped_std_batched(self.l2.samples)
+                sigma_clipped_std_batched(self.l2.samples, out=self.l2_sig)
                 self.launches += 1
-                s_k, _ = self.l2_state.update_and_query(per_kernel_sigma=sig_k)
-                self.sinv = torch.reciprocal(torch.clamp(s_k, min=1e-30))
+
+    def _search_host(self, jc: int, collect: bool = True) -> None:
+        """The host side of cube jc, after its device work: the Layer-2
+        update (this cube's sigma_k folded into the state that divides the
+        next cube's boxcars, written into the same divisor buffer) and the
+        candidates' read-back and decode."""
+        cfg = self.cfg
+        C, te, N = cfg.chunk_tiles, cfg.t_edge, cfg.n_grid
+        nfine = cfg.fine_dm.size
+        if self.l2 is not None:
+            s_k, _ = self.l2_state.update_and_query(per_kernel_sigma=self.l2_sig)
+            self.sinv.copy_(torch.reciprocal(torch.clamp(s_k, min=1e-30)))
         if collect:
             got = self.cands.fetch()
             self.last_d2h_bytes += 4 + got.nbytes
@@ -763,6 +780,42 @@ class SearchPipeline:
                 if jc >= self.jc_first:
                     self._search(jc, collect)
             self.chunk += 1
+        return self.out
+
+    def device_block(self, raw: torch.Tensor) -> List[int]:
+        """The device work of one block ``raw`` (on this pipeline's device):
+        every chunk's correlator and stage 1 and the detector cube it
+        completes, launches only (see ``_search_device``).  Returns the cubes
+        (chunk indices) whose host work ``host_block`` must then do.  At most
+        one cube per block: its candidate and Layer-2 buffers are single."""
+        npkt = self.block_packets(raw)
+        if raw.device != self.dev:
+            raise ValueError("device_block needs the block on the pipeline's device")
+        cfg = self.cfg
+        C, ppfv = cfg.chunk_tiles, cfg.t_int // 2
+        cubes = []
+        for ci in range(npkt // (C * ppfv)):
+            self._corr(raw, ci * C * ppfv, npkt)
+            j = self.chunk - self.depth1
+            if j >= 0:
+                self._stage1(j)
+                jc = j - self.a
+                if jc >= self.jc_first:
+                    if cubes:
+                        raise ValueError("device_block: a block may complete one detector "
+                                         "cube (chunk_tiles = the block's tiles)")
+                    self._search_device(jc)
+                    cubes.append(jc)
+            self.chunk += 1
+        return cubes
+
+    def host_block(self, cubes: List[int], *, collect: bool = True) -> List[StreamCandidate]:
+        """The host work of the cubes ``device_block`` returned, once their
+        device work has run: Layer-2 update, candidate read-back, decode."""
+        self.out = []
+        self.last_d2h_bytes = 0
+        for jc in cubes:
+            self._search_host(jc, collect)
         return self.out
 
     def process_blocks(self, blocks: Iterable[torch.Tensor], *,

@@ -761,8 +761,10 @@ def layer1_sigma(img: torch.Tensor, times: torch.Tensor, pix: torch.Tensor, *,
 
 
 def sigma_clipped_std_batched(samples: torch.Tensor, *, n_sigma: float = 3.0,
-                              n_iterations: int = 3) -> torch.Tensor:
-    """Row-wise sigma-clipped std, lower median (noise_norm/layer1.py:53)."""
+                              n_iterations: int = 3,
+                              out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Row-wise sigma-clipped std, lower median (noise_norm/layer1.py:53);
+    into ``out`` (float32 [B]) when given."""
     if samples.dim() != 2:
         raise ValueError(f"samples.dim()={samples.dim()}, expected 2 [B, M]")
     B, M = samples.shape
@@ -770,7 +772,10 @@ def sigma_clipped_std_batched(samples: torch.Tensor, *, n_sigma: float = 3.0,
     if B == 0 or M == 0:
         return torch.zeros((B,), dtype=torch.float32, device=samples.device)
     s = samples.to(torch.float32).contiguous()
-    out = torch.empty(B, dtype=torch.float32, device=s.device)
+    if out is None:
+        out = torch.empty(B, dtype=torch.float32, device=s.device)
+    elif out.dtype != torch.float32 or out.numel() != B or not out.is_contiguous():
+        raise ValueError(f"out must be contiguous float32 [{B}]")
     _lib.check(_lib.lib().dsb_clipped_std(_lib.ptr(s), B, M, float(n_sigma), int(n_iterations),
                                           _lib.ptr(out), _lib.stream_of(s.device)),
                "dsb_clipped_std")

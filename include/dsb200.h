@@ -437,6 +437,19 @@ int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, i
                      const int* times, int n_times, const int* pix, int n_pix, float n_sigma,
                      int n_iter, float* sigma, cudaStream_t stream);
 
+/* ---- the batched form: one block's launch sequence as a CUDA graph -------------
+ * No counterpart in the reference (its per-group plain runs are Python
+ * loops of launches).  dsb_graph_begin(stream) starts capturing (relaxed
+ * mode) on a non-default stream; the launches made on it are recorded, not
+ * run.  dsb_graph_end_launch(stream, &exec) ends the capture, instantiates
+ * the graph into *exec the first time (exec null) or updates *exec in place
+ * with the new graph's arguments (cudaGraphExecUpdate; a changed topology
+ * is instantiated afresh), and launches it on the stream.
+ * dsb_graph_destroy(exec) frees it. */
+int dsb_graph_begin(cudaStream_t stream);
+int dsb_graph_end_launch(cudaStream_t stream, void** exec);
+int dsb_graph_destroy(void* exec);
+
 /* ---- a3: per-antenna complex gains on split voltages ---------------------------
  * Replaces apply_cal_split (src/dsart/services/slow_corr_kernel.py:459-528,
  * eager form :417-423): out_re = re*g_re - im*g_im, out_im = re*g_im + im*g_re
