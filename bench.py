@@ -600,6 +600,96 @@ def serve_main(a, cfg):
         "data": "synthetic (seeded 4-bit Gaussian voltages)"}))
 
 
+def batched_main(a):
+    """Batched form: six channel groups of uneven size (512-1536 channels),
+    sub-arrays of 96, 64 and 48 antennas and DM plans of 128-1024 trials
+    (``dsb200.batched.config3_groups``) advanced together, one CUDA graph of
+    every group's launches per 16384-sample block.  With ``--autotune`` each
+    group's tile shapes are chosen by ``dsb200.batched.autotune`` first.
+    Times K blocks with the graph and K without (the same launches issued
+    one by one), and an end-to-end pass with every group's block copied
+    from pinned host memory inside the timed region.  Prints its own JSON
+    line."""
+    import torch
+    from dsb200 import synth
+    from dsb200.batched import BatchedSearch, autotune, config3_groups
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    groups = config3_groups()
+    tuned = []
+    if a.autotune:
+        new = []
+        for cfg, e, n in groups:
+            best, table = autotune(cfg, e, n, device=dev, blocks=2)
+            tuned.append({"fdm_batch": best.fdm_batch, "stage1_dm_group": best.stage1_dm_group,
+                          "ms_per_block": {f"{k[0]}x{k[1]}": v for k, v in table.items()}})
+            new.append((best, e, n))
+        groups = new
+    blocks = [synth.random_block_device(band=c.band, nant=c.nant, npkt=c.npkt_block, device=dev,
+                                        seed=100 + i) for i, (c, _, _) in enumerate(groups)]
+    block_s = groups[0][0].block_seconds
+    out = {}
+    for graph in (True, False):
+        bs = BatchedSearch(groups, device=dev, use_graph=graph)
+        bs.skip_warmup()
+        for _ in range(a.warmup):
+            bs.process_block(blocks)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(a.steps):
+            bs.process_block(blocks)
+        ev1.record()
+        torch.cuda.synchronize()
+        bs.check_status()
+        out[graph] = ev0.elapsed_time(ev1) / a.steps
+        launches = sum(p.launches for p in bs.pipes)
+        if graph:
+            n_launch = launches // (a.warmup + a.steps)
+            host = [torch.empty(b.shape, dtype=torch.uint8, pin_memory=True).copy_(b)
+                    for b in blocks]
+            dbuf = blocks
+            ev0.record()
+            for _ in range(a.steps):
+                for h, d in zip(host, dbuf):
+                    d.copy_(h, non_blocking=True)
+                bs.process_block(dbuf)
+            ev1.record()
+            torch.cuda.synchronize()
+            bs.check_status()
+            ms_e2e = ev0.elapsed_time(ev1) / a.steps
+            h2d = sum(b.numel() for b in blocks)
+            d2h = sum(p.last_d2h_bytes for p in bs.pipes)
+            del host
+        bs.close()
+        del bs
+        torch.cuda.empty_cache()
+    print(json.dumps({
+        "metric": "batched form: real-time factor (data-seconds of the whole band per "
+                  "device-second)", "value": block_s / (out[True] / 1e3),
+        "unit": "data-seconds/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": out[True], "ms_per_step_without_graph": out[False],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "gpu_launches": n_launch, "graph_launches_per_step": 1,
+        "e2e": {"value": block_s / (ms_e2e / 1e3), "unit": "data-seconds/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "autotune": tuned or None,
+        "config": {"workload": "batched: 6 channel groups (512, 768, 1024, 1024, 1280, 1536 ch "
+                               "as 256-channel chgroups, csf 16), sub-arrays 96/96/64/64/48/48 "
+                               "ant, DM plans 128/256/512/512/768/1024 trials to 500-3000, "
+                               "16384-sample blocks, t_int 8, 256^2 grid, boxcars 1..16",
+                   "groups": [{"nant": c.nant, "chans": c.band.n_chgroup * c.band.nchan,
+                               "n_dm": int(c.fine_dm.size), "max_dm": float(c.coarse_dm.max()),
+                               "fdm_batch": c.fdm_batch, "stage1_dm_group": c.stage1_dm_group}
+                              for c, _, _ in groups],
+                   "l2": "inputs larger than L2 (every group's block resident, "
+                         f"{sum(b.numel() for b in blocks) / 1e9:.1f} GB)"},
+        "dtype": "int8 (correlator) / bf16 ring, f32 accumulate",
+        "data": "synthetic (seeded 4-bit Gaussian voltages, sigma 3, T-layout antennas)"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -618,6 +708,12 @@ def main():
                     help="served streaming form instead: S voltage streams, seeded uneven "
                          "blocks, Poisson arrivals; prints its own JSON line")
     ap.add_argument("--serve-blocks", type=int, default=4, help="blocks per served stream")
+    ap.add_argument("--batched", action="store_true",
+                    help="batched form instead: six uneven channel groups with their own "
+                         "sub-arrays and DM plans, one CUDA graph per block; prints its own "
+                         "JSON line")
+    ap.add_argument("--autotune", action="store_true",
+                    help="with --batched: choose each group's tile shapes by timing first")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
 
@@ -630,6 +726,10 @@ def main():
     if a.serve:
         if rank == 0:
             serve_main(a, cfg)
+        return
+    if a.batched:
+        if rank == 0:
+            batched_main(a)
         return
 
     if a.impl == "reference":

@@ -49,6 +49,16 @@ int dsb_graph_end_launch(cudaStream_t stream, void** exec) {
   return cudaGraphLaunch(ge, stream) == cudaSuccess ? DSB_OK : DSB_E_CUDA;
 }
 
+int dsb_graph_abort(cudaStream_t stream) {
+  // ends a capture whose host side failed part-way; nothing is launched
+  if (!stream) return DSB_E_ARG;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(stream, &graph);
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  return e == cudaSuccess ? DSB_OK : DSB_E_CUDA;
+}
+
 int dsb_graph_destroy(void* exec) {
   if (!exec) return DSB_OK;
   return cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(exec)) == cudaSuccess ? DSB_OK

@@ -24,7 +24,8 @@ _c_int, _c_ll, _c_float, _vp = ctypes.c_int, ctypes.c_longlong, ctypes.c_float, 
 _SIGNATURES = {
     "dsb_version": [],
     "dsb_unpack_int4": [_vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp, _vp],
-    "dsb_corr_split": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp],
+    "dsb_corr_split": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp,
+                       _vp],
     "dsb_corr_tc": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp,
                     _c_ll, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
     "dsb_corr_tc_grid": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp,
@@ -44,6 +45,7 @@ _SIGNATURES = {
     "dsb_image_geometry": [_c_int, _vp],
     "dsb_graph_begin": [_vp],
     "dsb_graph_end_launch": [_vp, _vp],
+    "dsb_graph_abort": [_vp],
     "dsb_graph_destroy": [_vp],
     "dsb_irfft2": [_vp, _c_int, _c_int, _vp, _vp, _vp],
     "dsb_image_fft": [_vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _c_int,

@@ -51,9 +51,16 @@ int dsb_unpack_int4(const void* raw, int npkt, int nant, int nchan, int out_dtyp
  * (src/dsart/services/corr_fast_kernel.py:364-413, CPU path :698-755).
  * re/im: (nchan, 2t, 2p, npkt, nant) of in_dtype.  out (complex64):
  * fuse_stokes_i -> (n_fv, nbase, nchan/csf); else (n_fv, nbase, nchan, 2).
- * V[bls(a,b)] = sum conj(E_b) E_a, b <= a (F18). */
+ * V[bls(a,b)] = sum conj(E_b) E_a, b <= a (F18).  On the tcgen05 tensor
+ * cores, float32 accumulators in tensor memory, as the reference's fp16
+ * HMMA correlator (src/dsart/services/triton_corr_fused.py:135-138): int8
+ * codes and float16 voltages as kind::f16 (int8 -> f16 is exact, so integer
+ * codes correlate exactly below 2^24), float32 voltages as kind::tf32 (each
+ * part rounded to tf32, nearest, ties away).  nant <= 128.  status (device
+ * int, may be null) receives DSB_E_TIMEOUT if a bounded wait gave up. */
 int dsb_corr_split(const void* re, const void* im, int in_dtype, int nchan, int npkt, int nant,
-                   int t_int, int fuse_stokes_i, int csf, void* out, cudaStream_t stream);
+                   int t_int, int fuse_stokes_i, int csf, void* out, int* status,
+                   cudaStream_t stream);
 
 /* ---- a4/a5: fused unpack + correlate on tcgen05 tensor cores -------------
  * Replaces the unpack -> cal -> fused HMMA correlator chain
@@ -445,9 +452,11 @@ int dsb_layer1_sigma(const float* img, long long f_stride, long long t_stride, i
  * the graph into *exec the first time (exec null) or updates *exec in place
  * with the new graph's arguments (cudaGraphExecUpdate; a changed topology
  * is instantiated afresh), and launches it on the stream.
- * dsb_graph_destroy(exec) frees it. */
+ * dsb_graph_abort(stream) ends a capture whose host side failed part-way
+ * and discards it (nothing runs).  dsb_graph_destroy(exec) frees *exec. */
 int dsb_graph_begin(cudaStream_t stream);
 int dsb_graph_end_launch(cudaStream_t stream, void** exec);
+int dsb_graph_abort(cudaStream_t stream);
 int dsb_graph_destroy(void* exec);
 
 /* ---- a3: per-antenna complex gains on split voltages ---------------------------
