@@ -65,114 +65,6 @@ __global__ void unpack_kernel(const uint32_t* __restrict__ raw, int rows, int nc
 }
 
 // ===========================================================================
-// generic (CUDA-core) correlator on GEMM-layout voltages
-// ===========================================================================
-DSB_DEV void bls_to_ab(int j, int& a, int& b) {
-  int aa = (int)((sqrtf(8.f * (float)j + 1.f) - 1.f) * 0.5f);
-  while (aa * (aa + 1) / 2 > j) --aa;
-  while ((aa + 1) * (aa + 2) / 2 <= j) ++aa;
-  a = aa;
-  b = j - aa * (aa + 1) / 2;
-}
-
-template <typename T>
-DSB_DEV float to_f(T v);
-template <>
-DSB_DEV float to_f<int8_t>(int8_t v) { return (float)v; }
-template <>
-DSB_DEV float to_f<__half>(__half v) { return __half2float(v); }
-template <>
-DSB_DEV float to_f<float>(float v) { return v; }
-
-constexpr int GEN_THREADS = 256;
-constexpr int GEN_KCH = 32;   // samples staged per pass
-constexpr int GEN_MAXB = 24;  // baselines per thread (nbase <= 6144)
-
-// One block per output unit. Stokes-I unit = (fv, summed channel): K runs
-// over (ch in group, pol, t-sub, packet). 2-pol unit = (fv, ch, pol).
-template <typename T, typename Acc>
-__global__ void __launch_bounds__(GEN_THREADS) corr_generic_kernel(
-    const T* __restrict__ re, const T* __restrict__ im, int nchan, int npkt, int nant,
-    int ppfv, int fuse, int csf, float2* __restrict__ out) {
-  __shared__ float sR[GEN_KCH][128];
-  __shared__ float sI[GEN_KCH][128];
-  const int nbase = nant * (nant + 1) / 2;
-  const int n_fv = npkt / ppfv;
-  const int unit = blockIdx.x;
-  int fv, ch0, nch_u, pol0, npol_u;
-  if (fuse) {
-    const int ceff = nchan / csf;
-    fv = unit / ceff;
-    ch0 = (unit % ceff) * csf;
-    nch_u = csf;
-    pol0 = 0;
-    npol_u = 2;
-  } else {
-    fv = unit / (nchan * 2);
-    ch0 = (unit / 2) % nchan;
-    nch_u = 1;
-    pol0 = unit % 2;
-    npol_u = 1;
-  }
-  if (fv >= n_fv) return;
-  const int ksz = nch_u * npol_u * 2 * ppfv;  // samples per antenna
-  Acc accr[GEN_MAXB], acci[GEN_MAXB];
-  int aa[GEN_MAXB], bb[GEN_MAXB];
-  int nmine = 0;
-  for (int j = threadIdx.x; j < nbase && nmine < GEN_MAXB; j += GEN_THREADS) {
-    bls_to_ab(j, aa[nmine], bb[nmine]);
-    accr[nmine] = 0;
-    acci[nmine] = 0;
-    ++nmine;
-  }
-  const size_t plane = (size_t)npkt * nant;
-  for (int k0 = 0; k0 < ksz; k0 += GEN_KCH) {
-    const int kn = min(GEN_KCH, ksz - k0);
-    for (int idx = threadIdx.x; idx < kn * nant; idx += GEN_THREADS) {
-      const int kk = idx / nant, a = idx % nant;
-      int k = k0 + kk;
-      // k -> (ch, pol, t, p)
-      const int p = k % ppfv;
-      k /= ppfv;
-      const int t = k % 2;
-      k /= 2;
-      const int pol = pol0 + (k % npol_u);
-      const int ch = ch0 + k / npol_u;
-      const size_t o = (((size_t)ch * 2 + t) * 2 + pol) * plane + (size_t)(fv * ppfv + p) * nant + a;
-      sR[kk][a] = to_f<T>(re[o]);
-      sI[kk][a] = to_f<T>(im[o]);
-    }
-    __syncthreads();
-    for (int m = 0; m < nmine; ++m) {
-      const int a = aa[m], b = bb[m];
-      Acc sr = 0, si = 0;
-      for (int kk = 0; kk < kn; ++kk) {
-        const float rb = sR[kk][b], ib = sI[kk][b], ra = sR[kk][a], ia = sI[kk][a];
-        if constexpr (std::is_integral<Acc>::value) {
-          sr += (int)rb * (int)ra + (int)ib * (int)ia;
-          si += (int)rb * (int)ia - (int)ib * (int)ra;
-        } else {
-          sr = fmaf(rb, ra, fmaf(ib, ia, sr));
-          si = fmaf(rb, ia, fmaf(-ib, ra, si));
-        }
-      }
-      accr[m] += sr;
-      acci[m] += si;
-    }
-    __syncthreads();
-  }
-  for (int m = 0; m < nmine; ++m) {
-    const int j = upper_bls(aa[m], bb[m]);
-    size_t o;
-    if (fuse)
-      o = ((size_t)fv * nbase + j) * (nchan / csf) + ch0 / csf;
-    else
-      o = (((size_t)fv * nbase + j) * nchan + ch0) * 2 + pol0;
-    out[o] = make_float2((float)accr[m], (float)acci[m]);
-  }
-}
-
-// ===========================================================================
 // tensor-core correlator (tcgen05, kind::i8)
 // ===========================================================================
 constexpr int TC_THREADS = 256;
@@ -599,6 +491,236 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   }
 }
 
+// ===========================================================================
+// tensor-core correlator on split (GEMM-layout) voltages: tcgen05 kind::f16
+// (int8 codes and float16 voltages, exact conversion to f16) or kind::tf32
+// (float32 voltages, rounded to tf32 as a float32 tensor-core product does),
+// float32 accumulators in TMEM.
+// ===========================================================================
+struct SplitTcArgs {
+  const void* re;
+  const void* im;
+  int dtype;                 // DSB_DT_INT8 / DSB_DT_F16 / DSB_DT_F32
+  int nchan, npkt, nant, nant_p, ppfv, fuse, csf, ceff;
+  int n_fv, n_units, kprime, n_chunks, rows, nstage, stage_bytes;
+  float2* out;
+  int* status;
+};
+
+// Output unit u -> the fast-vis tile, its channel range and pols, and the
+// output column: Stokes-I unit = (fv, summed channel s), K over (channel of
+// the group, pol, t-sub, packet); 2-pol unit = (fv, ch, pol), K over
+// (t-sub, packet).
+DSB_DEV void split_unit(const SplitTcArgs& A, int u, int& fv, int& ch0, int& pol0, int& npol_u) {
+  if (A.fuse) {
+    fv = u / A.ceff;
+    ch0 = (u % A.ceff) * A.csf;
+    pol0 = 0;
+    npol_u = 2;
+  } else {
+    fv = u / (A.nchan * 2);
+    ch0 = (u / 2) % A.nchan;
+    pol0 = u % 2;
+    npol_u = 1;
+  }
+}
+
+template <int ELEM>
+DSB_DEV uint32_t split_load_bits(const SplitTcArgs& A, const void* p, size_t o) {
+  if constexpr (ELEM == 2) {
+    if (A.dtype == DSB_DT_INT8)
+      return (uint32_t)__half_as_ushort(__int2half_rn((int)static_cast<const int8_t*>(p)[o]));
+    return (uint32_t)__half_as_ushort(static_cast<const __half*>(p)[o]);
+  } else {
+    // round the float32 to tf32 (10 mantissa bits), nearest with ties away
+    // from zero: add half of the dropped range to the magnitude bits (a
+    // carry moves into the exponent correctly), clear the dropped bits;
+    // infinities and NaNs pass unchanged
+    const uint32_t u = __float_as_uint(static_cast<const float*>(p)[o]);
+    if ((u & 0x7F800000u) == 0x7F800000u) return u;
+    return (u + 0x1000u) & 0xFFFFE000u;
+  }
+}
+
+// One K chunk (KC complex samples) of unit u into an operand stage:
+// rows [0, nant_p) = [R | I], rows [nant_p, 2 nant_p) = [I | -R] (K-major,
+// SW128, one 128-byte row per operand row); samples past the unit's K and
+// antennas past nant are zero.
+template <int ELEM>
+DSB_DEV void split_fill(const SplitTcArgs& A, uint8_t* st, int u, int q) {
+  constexpr int KC = 64 / ELEM;    // complex samples per chunk
+  constexpr int G = 16 / ELEM;     // samples per 16-byte group
+  constexpr int NG = KC / G;       // groups per half row (4)
+  int fv, ch0, pol0, npol_u;
+  split_unit(A, u, fv, ch0, pol0, npol_u);
+  const size_t plane = (size_t)A.npkt * A.nant;
+  for (int idx = threadIdx.x; idx < A.nant_p * NG; idx += TC_THREADS) {
+    const int a = idx % A.nant_p, j = idx / A.nant_p;
+    uint32_t r[G], m[G];
+#pragma unroll
+    for (int i = 0; i < G; ++i) {
+      int k = q * KC + j * G + i;
+      r[i] = 0u;
+      m[i] = 0u;
+      if (a < A.nant && k < A.kprime) {
+        const int p = k % A.ppfv;
+        k /= A.ppfv;
+        const int t = k & 1;
+        k >>= 1;
+        const int pol = pol0 + k % npol_u;
+        const int ch = ch0 + k / npol_u;
+        const size_t o = (((size_t)ch * 2 + t) * 2 + pol) * plane +
+                         (size_t)(fv * A.ppfv + p) * A.nant + a;
+        r[i] = split_load_bits<ELEM>(A, A.re, o);
+        m[i] = split_load_bits<ELEM>(A, A.im, o);
+      }
+    }
+    uint4 R, I, N;
+    if constexpr (ELEM == 2) {
+      R = make_uint4(r[0] | (r[1] << 16), r[2] | (r[3] << 16), r[4] | (r[5] << 16),
+                     r[6] | (r[7] << 16));
+      I = make_uint4(m[0] | (m[1] << 16), m[2] | (m[3] << 16), m[4] | (m[5] << 16),
+                     m[6] | (m[7] << 16));
+      N = make_uint4(R.x ^ 0x80008000u, R.y ^ 0x80008000u, R.z ^ 0x80008000u,
+                     R.w ^ 0x80008000u);
+    } else {
+      R = make_uint4(r[0], r[1], r[2], r[3]);
+      I = make_uint4(m[0], m[1], m[2], m[3]);
+      N = make_uint4(r[0] ^ 0x80000000u, r[1] ^ 0x80000000u, r[2] ^ 0x80000000u,
+                     r[3] ^ 0x80000000u);
+    }
+    const uint32_t kr = (uint32_t)j * 16u, ki = 64u + (uint32_t)j * 16u;
+    const uint32_t ra = (uint32_t)a, rb = (uint32_t)(A.nant_p + a);
+    *reinterpret_cast<uint4*>(st + sw128_offset(ra, kr)) = R;
+    *reinterpret_cast<uint4*>(st + sw128_offset(ra, ki)) = I;
+    *reinterpret_cast<uint4*>(st + sw128_offset(rb, kr)) = I;
+    *reinterpret_cast<uint4*>(st + sw128_offset(rb, ki)) = N;
+  }
+}
+
+// Accumulator `buf` of unit u: rows b < nant, columns a (Re) and nant_p + a
+// (Im); the upper triangle b <= a goes to bls(a, b) (conj(E_b) E_a).
+DSB_DEV void split_epilogue(const SplitTcArgs& A, uint32_t tmem_base, int buf, int u) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quarter = warp & 3, half = warp >> 2;
+  const int nant = A.nant, nbase = nant * (nant + 1) / 2;
+  const int b = quarter * 32 + lane;
+  int fv, ch0, pol0, npol_u;
+  split_unit(A, u, fv, ch0, pol0, npol_u);
+  if (quarter * 32 < nant) {
+    const uint32_t lane_base =
+        tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * 256);
+    for (int c0 = half * 16; c0 < nant; c0 += 32) {
+      if (c0 + 15 < quarter * 32) continue;  // whole chunk below this warp's rows
+      uint32_t vr[16], vi[16];
+      tmem_ld16(lane_base + (uint32_t)c0, vr);
+      tmem_ld16(lane_base + (uint32_t)(A.nant_p + c0), vi);
+      tmem_ld_wait();
+      if (b < nant) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int a = c0 + j;
+          if (a < b || a >= nant) continue;
+          const size_t bls = (size_t)upper_bls(a, b);
+          const size_t o = A.fuse ? ((size_t)fv * nbase + bls) * A.ceff + ch0 / A.csf
+                                  : (((size_t)fv * nbase + bls) * A.nchan + ch0) * 2 + pol0;
+          A.out[o] = make_float2(__uint_as_float(vr[j]), __uint_as_float(vi[j]));
+        }
+      }
+    }
+  }
+}
+
+template <int ELEM>
+__global__ void __launch_bounds__(TC_THREADS, 1) corr_split_tc_kernel(const SplitTcArgs A) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* stages = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bar_mma = reinterpret_cast<uint64_t*>(stages + (size_t)A.nstage * A.stage_bytes);
+  uint64_t* bar_acc = bar_mma + A.nstage;
+  uint64_t* bar_drain = bar_acc + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_drain + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, TC_TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < A.nstage; ++i) mbar_init(&bar_mma[i], 1);
+    mbar_init(&bar_acc[0], 1);
+    mbar_init(&bar_acc[1], 1);
+    mbar_init(bar_drain, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int per_cta = (A.n_units + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int u_begin = (int)blockIdx.x * per_cta;
+  const int my_units = max(0, min(per_cta, A.n_units - u_begin));
+  const int n_items = my_units * A.n_chunks;
+  // c_format F32; a/b format F16 (0) or TF32 (2); K-major; N = 2 nant_p; M = 128
+  constexpr uint32_t fmt = ELEM == 2 ? 0u : 2u;
+  const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
+                         (((uint32_t)(2 * A.nant_p) >> 3) << 17) | ((128u >> 4) << 24);
+  bool ok = true;
+  for (int it = 0; it < n_items; ++it) {
+    const int lu = it / A.n_chunks, q = it % A.n_chunks;
+    const int slot = it % A.nstage;
+    bool w_ok = true;
+    if (it >= A.nstage) w_ok = mbar_wait(&bar_mma[slot], (uint32_t)((it / A.nstage - 1) & 1));
+    if (!__syncthreads_and(w_ok)) { ok = false; break; }
+    uint8_t* st = stages + (size_t)slot * A.stage_bytes;
+    split_fill<ELEM>(A, st, u_begin + lu, q);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t d = tmem_base + (uint32_t)((lu & 1) * 256);
+      const uint32_t sbase = smem_u32(st);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {   // 4 MMAs of 32 bytes of K each
+        const uint64_t desc = sdesc_k_sw128(sbase + (uint32_t)m * 32u);
+        if constexpr (ELEM == 2) umma_f16_ss(d, desc, desc, idesc, (q > 0 || m > 0) ? 1u : 0u);
+        else umma_tf32_ss(d, desc, desc, idesc, (q > 0 || m > 0) ? 1u : 0u);
+      }
+      umma_commit(&bar_mma[slot]);
+      if (q == A.n_chunks - 1) umma_commit(&bar_acc[lu & 1]);
+    }
+    if (q == A.n_chunks - 1 && lu >= 1) {
+      const int pl = lu - 1;
+      const bool a_ok = mbar_wait(&bar_acc[pl & 1], (uint32_t)((pl >> 1) & 1));
+      if (!__syncthreads_and(a_ok)) { ok = false; break; }
+      tc_fence_after();
+      split_epilogue(A, tmem_base, pl & 1, u_begin + pl);
+      tc_fence_before();
+    }
+  }
+  if (ok && my_units > 0) {
+    const int pl = my_units - 1;
+    const bool a_ok = mbar_wait(&bar_acc[pl & 1], (uint32_t)((pl >> 1) & 1));
+    if (__syncthreads_and(a_ok)) {
+      tc_fence_after();
+      split_epilogue(A, tmem_base, pl & 1, u_begin + pl);
+    } else {
+      ok = false;
+    }
+  }
+  if (!ok && tid == 0) {
+    dsb_flag(A.status, DSB_E_TIMEOUT);
+    // drain every MMA this CTA issued before tensor memory is released
+    umma_commit(bar_drain);
+    mbar_wait(bar_drain, 0u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TC_TMEM_COLS);
+  }
+}
+
 int g_num_sms = 0;
 int num_sms() {
   if (g_num_sms == 0) {
@@ -693,34 +815,49 @@ int dsb_unpack_int4(const void* raw, int npkt, int nant, int nchan, int out_dtyp
 }
 
 int dsb_corr_split(const void* re, const void* im, int in_dtype, int nchan, int npkt, int nant,
-                   int t_int, int fuse_stokes_i, int csf, void* out, cudaStream_t stream) {
+                   int t_int, int fuse_stokes_i, int csf, void* out, int* status,
+                   cudaStream_t stream) {
   if (!re || !im || !out || nchan <= 0 || npkt <= 0 || nant <= 0) return DSB_E_ARG;
-  if (nant > 128 || t_int <= 0 || t_int % 2 || npkt % (t_int / 2)) return DSB_E_ARG;
-  const int nbase = nant * (nant + 1) / 2;
-  if (nbase > GEN_THREADS * GEN_MAXB) return DSB_E_UNSUPPORTED;
-  const int ppfv = t_int / 2, n_fv = npkt / ppfv;
-  int units;
-  if (fuse_stokes_i) {
+  if (t_int <= 0 || t_int % 2 || npkt % (t_int / 2)) return DSB_E_ARG;
+  if (nant > 128) return DSB_E_UNSUPPORTED;
+  if (in_dtype != DSB_DT_INT8 && in_dtype != DSB_DT_F16 && in_dtype != DSB_DT_F32)
+    return DSB_E_ARG;
+  SplitTcArgs A{};
+  A.re = re; A.im = im; A.dtype = in_dtype;
+  A.nchan = nchan; A.npkt = npkt; A.nant = nant;
+  A.nant_p = (nant + 7) & ~7;
+  A.ppfv = t_int / 2;
+  A.n_fv = npkt / A.ppfv;
+  A.fuse = fuse_stokes_i ? 1 : 0;
+  if (A.fuse) {
     if (csf <= 0 || nchan % csf) return DSB_E_ARG;
-    units = n_fv * (nchan / csf);
+    A.csf = csf;
+    A.ceff = nchan / csf;
+    A.n_units = A.n_fv * A.ceff;
+    A.kprime = 2 * csf * t_int;     // (channel, pol, t-sub, packet)
   } else {
-    units = n_fv * nchan * 2;
+    A.csf = 1;
+    A.ceff = nchan;
+    A.n_units = A.n_fv * nchan * 2;
+    A.kprime = t_int;               // (t-sub, packet)
   }
-  float2* o = static_cast<float2*>(out);
-  switch (in_dtype) {
-    case DSB_DT_INT8:
-      corr_generic_kernel<int8_t, int><<<units, GEN_THREADS, 0, stream>>>(
-          (const int8_t*)re, (const int8_t*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
-      break;
-    case DSB_DT_F16:
-      corr_generic_kernel<__half, float><<<units, GEN_THREADS, 0, stream>>>(
-          (const __half*)re, (const __half*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
-      break;
-    case DSB_DT_F32:
-      corr_generic_kernel<float, float><<<units, GEN_THREADS, 0, stream>>>(
-          (const float*)re, (const float*)im, nchan, npkt, nant, ppfv, fuse_stokes_i, csf, o);
-      break;
-    default: return DSB_E_ARG;
+  const int kc = in_dtype == DSB_DT_F32 ? 16 : 32;
+  A.n_chunks = (A.kprime + kc - 1) / kc;
+  A.rows = std::max(128, 2 * A.nant_p);
+  A.stage_bytes = A.rows * 128;
+  A.nstage = 4;
+  A.out = static_cast<float2*>(out);
+  A.status = status;
+  const int smem = A.nstage * A.stage_bytes + 1024 + (A.nstage + 3) * 8 + 16;
+  const int grid = std::min(A.n_units, num_sms());
+  if (in_dtype == DSB_DT_F32) {
+    cudaFuncSetAttribute(corr_split_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
+    corr_split_tc_kernel<4><<<grid, TC_THREADS, smem, stream>>>(A);
+  } else {
+    cudaFuncSetAttribute(corr_split_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
+    corr_split_tc_kernel<2><<<grid, TC_THREADS, smem, stream>>>(A);
   }
   return launch_status();
 }

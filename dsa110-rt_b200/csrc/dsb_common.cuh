@@ -138,6 +138,35 @@ DSB_DEV void umma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint3
       : "memory");
 }
 
+// D[tmem] (+)= A[smem] * B[smem]^T, float16 inputs (kind::f16; the
+// instruction descriptor says f16 for both), float32 accumulate.
+DSB_DEV void umma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                         uint32_t accumulate) {
+  uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2),
+      "r"(m3)
+      : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, tf32 inputs (kind::tf32), float32 accumulate.
+DSB_DEV void umma_tf32_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                          uint32_t accumulate) {
+  uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2),
+      "r"(m3)
+      : "memory");
+}
+
 // Arrive on an mbarrier once every tcgen05.mma issued so far by this thread
 // has completed.
 DSB_DEV void umma_commit(uint64_t* bar) {

@@ -240,10 +240,15 @@ def validate_fast_voltage_shape(real_v, imag_v, *, t_int_fast_native: int, nants
 
 @dataclass
 class FastCorrKernel:
-    """Fast X-engine (corr_fast_kernel.py:290).  ``compute_split`` takes the
-    reference's GEMM-layout voltages (int8 codes, fp16 or fp32);
-    ``compute_raw`` correlates on-wire bytes directly on the tcgen05 tensor
-    cores (Stokes-I + channel sum, integer exact)."""
+    """Fast X-engine (corr_fast_kernel.py:290), both entry points on the
+    tcgen05 tensor cores.  ``compute_split`` takes the reference's
+    GEMM-layout voltages: int8 codes and fp16 voltages (calibrated ones
+    included) as kind::f16 with float32 accumulation, as the reference's
+    fp16 HMMA correlator (triton_corr_fused.py:135-138), integer codes
+    exact; fp32 voltages as kind::tf32.  ``compute_raw`` correlates
+    on-wire bytes directly (kind::i8; Stokes-I + channel sum, integer
+    exact).  ``check_status`` raises if the last launch's bounded waits
+    gave up."""
 
     device: torch.device
     t_int_fast_native: int = 8
@@ -271,6 +276,11 @@ class FastCorrKernel:
     def nbase(self) -> int:
         return self._nbase
 
+    def check_status(self) -> None:
+        st = getattr(self, "_last_status", None)
+        if st is not None:
+            _lib.check_status(st, "FastCorrKernel")
+
     def compute_split(self, real_v: torch.Tensor, imag_v: torch.Tensor, *,
                       n_fv_chunk: Optional[int] = None, fuse_stokes_i: bool = False,
                       chan_sum_factor: int = 1) -> torch.Tensor:
@@ -296,10 +306,12 @@ class FastCorrKernel:
         else:
             out = torch.empty((n_fv, self._nbase, self.nchan, 2), dtype=torch.complex64,
                               device=self.device)
+        st = _lib.status_word(self.device)
         _lib.check(_lib.lib().dsb_corr_split(
             _lib.ptr(re), _lib.ptr(im), _DT[re.dtype], self.nchan, re.shape[3], self.nants,
             self.t_int_fast_native, int(bool(fuse_stokes_i)), int(chan_sum_factor),
-            _lib.ptr(out), _lib.stream_of(self.device)), "dsb_corr_split")
+            _lib.ptr(out), _lib.ptr(st), _lib.stream_of(self.device)), "dsb_corr_split")
+        self._last_status = st
         return out
 
     def compute_raw(self, raw: torch.Tensor, *, chan_sum_factor: int, npkt: Optional[int] = None,

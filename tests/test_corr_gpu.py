@@ -46,10 +46,14 @@ def test_unpack_rejects_wrong_size(dev):
         unpack_int4_split(np.zeros(100, np.uint8), device=dev, npkt=2, nant=4, nchan=8)
 
 
-@pytest.mark.parametrize("fuse,csf", [(True, 4), (True, 1), (False, 1)])
-def test_corr_split_int8_exact(dev, fuse, csf):
+@pytest.mark.parametrize("fuse,csf,nant", [(True, 4, 24), (True, 1, 24), (False, 1, 24),
+                                           (True, 2, 21), (False, 1, 128), (True, 8, 128)])
+def test_corr_split_int8_exact(dev, fuse, csf, nant):
+    """The tensor-core split correlator (kind::f16 on int8 codes) equals
+    the oracle's integer sums exactly, including antenna counts that are not
+    a multiple of 8 (padded rows) and the largest supported (128)."""
     from dsb200.corr import FastCorrKernel, unpack_int4_split
-    npkt, nant, nchan, t_int = 16, 24, 8, 8
+    npkt, nchan, t_int = 16, 8, 8
     raw = _raw(npkt, nant, nchan, 5)
     re, im = unpack_int4_split(raw, device=dev, out_dtype=torch.int8, npkt=npkt, nant=nant,
                                nchan=nchan)
@@ -59,6 +63,43 @@ def test_corr_split_int8_exact(dev, fuse, csf):
     vr, vi = O.corr_fast(ore, oim, t_int=t_int, csf=csf, fuse_stokes_i=fuse)
     np.testing.assert_array_equal(vis.real.astype(np.int64), vr)
     np.testing.assert_array_equal(vis.imag.astype(np.int64), vi)
+
+
+@pytest.mark.parametrize("fuse", [True, False])
+def test_corr_split_fp32_on_tf32(dev, fuse):
+    """float32 voltages run as kind::tf32: integer-valued voltages (the
+    codes) correlate exactly; Gaussian voltages agree with the float64
+    correlation within the tf32 rounding of the parts (2e-3 of the largest
+    visibility)."""
+    from dsb200.corr import FastCorrKernel, unpack_int4_split
+    npkt, nant, nchan, t_int, csf = 32, 40, 8, 16, 2
+    raw = _raw(npkt, nant, nchan, 9)
+    re, im = unpack_int4_split(raw, device=dev, out_dtype=torch.float32, scale=1.0, npkt=npkt,
+                               nant=nant, nchan=nchan)
+    k = FastCorrKernel(dev, t_int_fast_native=t_int, nants=nant, nchan=nchan)
+    c = csf if fuse else 1
+    vis = k.compute_split(re, im, fuse_stokes_i=fuse, chan_sum_factor=c).cpu().numpy()
+    k.check_status()
+    ore, oim = O.unpack_int4_gemm_layout(raw, npkt, nant, nchan)
+    vr, vi = O.corr_fast(ore, oim, t_int=t_int, csf=c, fuse_stokes_i=fuse)
+    np.testing.assert_array_equal(vis.real.astype(np.int64), vr)
+    np.testing.assert_array_equal(vis.imag.astype(np.int64), vi)
+    rng = np.random.default_rng(4)
+    gr = rng.standard_normal(ore.shape).astype(np.float32)
+    gi = rng.standard_normal(ore.shape).astype(np.float32)
+    vis = k.compute_split(torch.from_numpy(gr).to(dev), torch.from_numpy(gi).to(dev),
+                          fuse_stokes_i=fuse, chan_sum_factor=c).cpu().numpy()
+    E = (gr.astype(np.float64) + 1j * gi).reshape(nchan, 2, 2, npkt // (t_int // 2),
+                                                   t_int // 2, nant)
+    V = np.einsum("ctpfkb,ctpfka->fcpba", np.conj(E), E)    # (fv, ch, pol, b, a)
+    a_idx, b_idx = O.upper_tri_indices(nant)
+    want = V[:, :, :, b_idx, a_idx]                           # (fv, ch, pol, bls)
+    if fuse:
+        want = want.sum(axis=2).reshape(want.shape[0], nchan // c, c, -1).sum(axis=2)
+        want = want.transpose(0, 2, 1)                        # (fv, bls, ch/csf)
+    else:
+        want = want.transpose(0, 3, 1, 2)                     # (fv, bls, ch, pol)
+    assert np.abs(vis - want).max() <= 2e-3 * np.abs(want).max()
 
 
 def test_corr_split_fp16_within_reference_tolerance(dev):
