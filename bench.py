@@ -600,6 +600,124 @@ def serve_main(a, cfg):
         "data": "synthetic (seeded 4-bit Gaussian voltages)"}))
 
 
+def stress_main(a):
+    """Stress/recovery sweep of the metric configuration: 200 bursts on an
+    S/N grid 6-50 x width grid 1-32 search samples x DM grid 100-2900,
+    arriving 0.3 s apart over a 60-data-second stream of seeded noise, at
+    seeded random pixels.  The amplitude for each (S/N, width) follows from
+    one reference burst measured first in a stream of its own
+    (``dsb200.synth.amp_for_snr``: S/N ~ amp^2 sqrt(width)).  Blocks are
+    replayed back to back (as fast as the GPU takes them); each is a copy of
+    one of three resident noise blocks with the bursts that cover it drawn
+    in (``inject_bursts_device``).  Reports the fraction of bursts
+    recovered (a candidate at the burst's pixel +-2, DM +-10 % (at least 30)
+    and time, ``match_bursts``), by S/N, width and DM, and the measured S/N
+    against the injected.  The candidate lists of a reduced sweep are checked
+    against the oracle on the same seeds in the test suite; at this size
+    the oracle does not run.  Prints its own JSON line."""
+    import torch
+    from dsb200 import synth
+    from dsb200.pipeline import SearchPipeline
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = workload_config(a.workload)
+    cfg.ring_dtype = a.ring
+    e, n = synth.t_layout(cfg.nant, seed=11)
+    npkt = cfg.npkt_block
+    blk = 2 * npkt                                       # native samples per block
+    noise = [synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=npkt, device=dev,
+                                       seed=900 + i) for i in range(3)]
+    work = torch.empty_like(noise[0])
+    nu = cfg.band.freq_table()
+    k_bot = 4.148808 * (1.0 / float(nu.min()) ** 2 - 1.0 / float(nu[0, 0]) ** 2) * 1e3 / 32.768
+    warm = 4 * blk                                       # rings full before the first burst
+
+    def stream(bursts, n_blocks, seed):
+        pipe = SearchPipeline(cfg, e, n, device=dev)
+        cell = pipe.tab.cell_lambda
+        cands, dev_ms = [], 0.0
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        for k in range(n_blocks):
+            s0 = k * blk
+            work.copy_(noise[k % len(noise)])
+            mine = [b for b in bursts if b.t0_native < s0 + blk and
+                    b.t0_native + k_bot * b.dm + b.width_native + 8 > s0]
+            synth.inject_bursts_device(work, band=cfg.band, nant=cfg.nant, s0=s0, bursts=mine,
+                                       antpos_e=e, antpos_n=n, cell_lambda=cell,
+                                       n_grid=cfg.n_grid, seed=seed)
+            ev0.record()
+            got = pipe.process_block(work)
+            ev1.record()
+            torch.cuda.synchronize()
+            dev_ms += ev0.elapsed_time(ev1)
+            cands += got
+        pipe.check_status()
+        fine = pipe.cfg.fine_dm
+        del pipe
+        torch.cuda.empty_cache()
+        return cands, dev_ms, fine
+
+    def blocks_for(t_last, dm_max, w_max):
+        return int(np.ceil((t_last + k_bot * dm_max + w_max) / blk)) + 3
+
+    # reference burst: width 4 search samples, DM 1000, its own stream
+    ti = cfg.t_int
+    ref = (0.0, 4 * ti, 1000.0, warm + blk // 3, 40, -60)
+    amp_ref = 0.06
+    rb = [synth.Burst(dm=ref[2], t0_native=ref[3], width_native=ref[1], amp=amp_ref,
+                      dl=ref[4], dm_pix=ref[5])]
+    rc, _, fine = stream(rb, blocks_for(ref[3], ref[2], ref[1]), seed=77)
+    m = synth.match_bursts([ref], rc, band=cfg.band, fine_dm=fine, n_grid=cfg.n_grid, t_int=ti)
+    if m[0] is None:
+        raise SystemExit("stress: the reference burst was not detected")
+    snr_ref = float(m[0].snr)
+
+    snrs = [6, 7, 8, 10, 12, 15, 20, 30, 40, 50]
+    widths = [1, 4, 16, 32]                              # search samples
+    dms = [100.0, 800.0, 1500.0, 2200.0, 2900.0]
+    spacing = int(round(0.3 / (32.768e-6)))
+    grid = synth.burst_grid(snrs=snrs, widths=[w * ti for w in widths], dms=dms,
+                            t_first_native=warm, spacing_native=spacing, n_grid=cfg.n_grid,
+                            seed=2024)
+    amps = [synth.amp_for_snr(s, w, amp_ref=amp_ref, snr_ref=snr_ref, width_ref=ref[1])
+            for s, w, *_ in grid]
+    bursts = [synth.Burst(dm=d, t0_native=t0, width_native=w, amp=am, dl=dl, dm_pix=dp)
+              for (s, w, d, t0, dl, dp), am in zip(grid, amps)]
+    n_blocks = blocks_for(max(g[3] for g in grid), max(dms),
+                          max(widths) * ti)
+    cands, dev_ms, fine = stream(bursts, n_blocks, seed=2024)
+    got = synth.match_bursts(grid, cands, band=cfg.band, fine_dm=fine, n_grid=cfg.n_grid,
+                             t_int=ti)
+
+    def frac(sel):
+        idx = [i for i, g in enumerate(grid) if sel(g)]
+        return {"n": len(idx), "recovered": float(np.mean([got[i] is not None for i in idx]))}
+    ratio = [float(q.snr) / g[0] for g, q in zip(grid, got) if q is not None]
+    data_s = n_blocks * cfg.block_seconds
+    print(json.dumps({
+        "metric": "stress/recovery sweep: fraction of injected bursts recovered",
+        "value": float(np.mean([q is not None for q in got])), "unit": "fraction",
+        "higher_is_better": True, "n_gpus": 1, "n_bursts": len(grid),
+        "recovered_at_or_above_snr_8": frac(lambda g: g[0] >= 8)["recovered"],
+        "by_snr": {str(s): frac(lambda g, s=s: g[0] == s) for s in snrs},
+        "by_width_search_samples": {str(w): frac(lambda g, w=w: g[1] == w * ti) for w in widths},
+        "by_dm": {str(d): frac(lambda g, d=d: g[2] == d) for d in dms},
+        "measured_over_injected_snr": {"median": float(np.median(ratio)),
+                                       "p10": float(np.percentile(ratio, 10)),
+                                       "p90": float(np.percentile(ratio, 90))},
+        "reference_burst": {"amp": amp_ref, "width_native": ref[1], "dm": ref[2],
+                            "snr": snr_ref},
+        "candidates": len(cands), "blocks": n_blocks, "data_seconds": data_s,
+        "device_seconds": dev_ms / 1e3, "real_time_factor": data_s / (dev_ms / 1e3),
+        "config": dict(workload_desc(a.workload, cfg),
+                       sweep="S/N {6..50} x width {1,4,16,32} search samples x DM {100..2900}, "
+                             "200 bursts 0.3 s apart, seeded pixels; blocks replayed back to "
+                             "back"),
+        "data": "synthetic (seeded 4-bit Gaussian noise blocks, sigma 3, bursts drawn in)"}))
+
+
 def batched_main(a):
     """Batched form: six channel groups of uneven size (512-1536 channels),
     sub-arrays of 96, 64 and 48 antennas and DM plans of 128-1024 trials
@@ -712,6 +830,9 @@ def main():
                     help="batched form instead: six uneven channel groups with their own "
                          "sub-arrays and DM plans, one CUDA graph per block; prints its own "
                          "JSON line")
+    ap.add_argument("--stress", action="store_true",
+                    help="stress/recovery sweep of the workload instead: 200 bursts on an "
+                         "S/N x width x DM grid over 60 data-seconds; prints its own JSON line")
     ap.add_argument("--autotune", action="store_true",
                     help="with --batched: choose each group's tile shapes by timing first")
     a = ap.parse_args()
@@ -730,6 +851,10 @@ def main():
     if a.batched:
         if rank == 0:
             batched_main(a)
+        return
+    if a.stress:
+        if rank == 0:
+            stress_main(a)
         return
 
     if a.impl == "reference":
