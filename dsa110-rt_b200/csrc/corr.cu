@@ -94,6 +94,9 @@ struct TcArgs {
   long long y_t_stride;
   long long t_base;
   long long t_mask;
+  // (n_chgroup, ceff, nant) complex gains or null: every visibility is
+  // multiplied by g_a conj(g_b) of its subband before it is gridded
+  const float2* gains;
   int* status;
 };
 
@@ -303,6 +306,17 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
           if constexpr (MODE == 0) {
             A.out[(size_t)g * A.o_g + (size_t)f * A.o_f + (size_t)bls * A.o_b + (size_t)s * A.o_s] =
                 make_float2((float)re, (float)im);
+          } else if (A.gains) {
+            // calibrated: V' = g_a conj(g_b) V (V = conj(E_b) E_a), every
+            // product and sum rounded on its own (no contraction)
+            const float2* gs = A.gains + ((size_t)g * A.ceff + s) * nant;
+            const float2 ga = gs[a], gb = gs[b];
+            const float pr = __fadd_rn(__fmul_rn(ga.x, gb.x), __fmul_rn(ga.y, gb.y));
+            const float pi = __fsub_rn(__fmul_rn(ga.y, gb.x), __fmul_rn(ga.x, gb.y));
+            const float fr = (float)re, fi = (float)im;
+            reinterpret_cast<float2*>(vbuf)[bls] =
+                make_float2(__fsub_rn(__fmul_rn(fr, pr), __fmul_rn(fi, pi)),
+                            __fadd_rn(__fmul_rn(fr, pi), __fmul_rn(fi, pr)));
           } else {
             vbuf[bls] = make_int2(re, im);
           }
@@ -330,11 +344,31 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
     if (reload && threadIdx.x == 0) *tab.cached = gs;
     const long long tp = (A.t_base + f) & A.t_mask;
     float2* yrow = A.yout + tp * A.y_t_stride + row0;
-    if (use_tab) {
+    if (cnt > 0 && !(DSB_INB(row0, A.y_t_stride, A.status) &&
+                     DSB_INB(row0 + cnt - 1, A.y_t_stride, A.status)))
+      return;
+    if (A.gains) {
+      // calibrated visibilities: float sums in CSR order
+      const float2* fbuf = reinterpret_cast<const float2*>(vbuf);
+      for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
+        const long long r = row0 + k;
+        float sr = 0.f, si = 0.f;
+        const int j0 = use_tab ? tab.roff[k] + e0 : A.row_off[r];
+        const int j1 = use_tab ? tab.roff[k + 1] + e0 : A.row_off[r + 1];
+        for (int j = j0; j < j1; ++j) {
+          const int bl = use_tab ? (int)tab.bls[j - e0] : A.row_bls[j];
+          if (!DSB_INB(bl, A.nant * (A.nant + 1) / 2, A.status)) continue;
+          sr = __fadd_rn(sr, fbuf[bl].x);
+          si = __fadd_rn(si, fbuf[bl].y);
+        }
+        yrow[k] = make_float2(sr, si);
+      }
+    } else if (use_tab) {
       for (int k = threadIdx.x; k < cnt; k += TC_THREADS) {
         int sr = 0, si = 0;
         const int j1 = tab.roff[k + 1];
         for (int j = tab.roff[k]; j < j1; ++j) {
+          if (!DSB_INB(tab.bls[j], A.nant * (A.nant + 1) / 2, A.status)) continue;
           const int2 v = vbuf[tab.bls[j]];
           sr += v.x;
           si += v.y;
@@ -346,6 +380,7 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
         const long long r = row0 + k;
         int sr = 0, si = 0;
         for (int j = A.row_off[r]; j < A.row_off[r + 1]; ++j) {
+          if (!DSB_INB(A.row_bls[j], A.nant * (A.nant + 1) / 2, A.status)) continue;
           const int2 v = vbuf[A.row_bls[j]];
           sr += v.x;
           si += v.y;
@@ -786,6 +821,7 @@ const char* dsb_strerror(int code) {
     case DSB_E_UNSUPPORTED: return "unsupported geometry";
     case DSB_E_TIMEOUT: return "device-side bounded wait ran out";
     case DSB_E_CAPACITY: return "size exceeds a fixed capacity";
+    case DSB_E_BOUNDS: return "index out of range (bounds-checked build)";
     default: return "unknown error";
   }
 }
@@ -889,8 +925,8 @@ int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt
 int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
                      int nchan, int t_int, int csf, const int* yoff, const int* ycnt,
                      const int* row_off, const int* row_bls, void* yout, long long y_t_stride,
-                     long long t_base, long long t_mask, int max_ctas, int* status,
-                     cudaStream_t stream) {
+                     long long t_base, long long t_mask, int max_ctas, const void* gains,
+                     int* status, cudaStream_t stream) {
   if (!raw || !yout || !yoff || !ycnt || !row_off || !row_bls) return DSB_E_ARG;
   if (((uintptr_t)raw & 15) || (raw_g_stride & 15)) return DSB_E_ARG;
   TcArgs A{};
@@ -901,6 +937,7 @@ int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int
   A.yoff = yoff; A.ycnt = ycnt; A.row_off = row_off; A.row_bls = row_bls;
   A.yout = static_cast<float2*>(yout);
   A.y_t_stride = y_t_stride; A.t_base = t_base; A.t_mask = t_mask;
+  A.gains = static_cast<const float2*>(gains);
   A.status = status;
   int rc = tc_plan(A, 1);
   if (rc) return rc;

@@ -260,9 +260,11 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
             if (tau < s_len[sb]) {
               const long long r2 = ((((A.t0 + tt + s_lo[sb] + tau) & A.y_mask) * A.y_rows) +
                                     ycol + (long long)sb * pitch) / 2;
-              v0[q] = Y4[r2];
-              v1[q] = Y4[r2 + 1];
-              ei[q] = e;
+              if (DSB_INB(r2 + 1, (A.y_mask + 1) * A.y_rows / 2, A.status)) {
+                v0[q] = Y4[r2];
+                v1[q] = Y4[r2 + 1];
+                ei[q] = e;
+              }
             }
           }
         }
@@ -302,6 +304,7 @@ __global__ void __launch_bounds__(S1_THREADS) stage1_rows_kernel(const S1Args A)
       amax = fmaxf(amax, fmaxf(fmaxf(fabsf(o0.x), fabsf(o0.y)), fmaxf(fabsf(o0.z), fabsf(o0.w))));
       amax = fmaxf(amax, fmaxf(fmaxf(fabsf(o1.x), fabsf(o1.y)), fmaxf(fabsf(o1.z), fabsf(o1.w))));
       const long long o = seg + slot * pitch;  // element of cell c0, a multiple of 4
+      if (!(DSB_INB(slot, dep, A.status) && DSB_INB(c0 + 3, pitch, A.status))) continue;
       if constexpr (BF16) {
         reinterpret_cast<uint4*>(A.D)[o / 4] =
             make_uint4(bf16_pair(o0.x, o0.y), bf16_pair(o0.z, o0.w), bf16_pair(o1.x, o1.y),

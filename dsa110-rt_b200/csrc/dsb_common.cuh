@@ -70,6 +70,22 @@ DSB_DEV void dsb_flag(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
+// Bounds-checked build (-DDSB_CHECK): DSB_INB(i, n, status) is true when
+// 0 <= i < n; otherwise it records DSB_E_BOUNDS in *status and is false, and
+// the access it guards is skipped (no trap).  The normal build compiles it
+// to true.  It guards the indices that come from host-built tables: ring
+// slots and cells, gridding rows and baselines, combine targets.
+#ifdef DSB_CHECK
+DSB_DEV bool dsb_inb(long long i, long long n, int* status) {
+  if (i >= 0 && i < n) return true;
+  dsb_flag(status, DSB_E_BOUNDS);
+  return false;
+}
+#define DSB_INB(i, n, st) dsb_inb((long long)(i), (long long)(n), (st))
+#else
+#define DSB_INB(i, n, st) true
+#endif
+
 // ---------------------------------------------------------------------------
 // mbarrier
 // ---------------------------------------------------------------------------

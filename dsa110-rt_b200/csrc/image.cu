@@ -468,6 +468,7 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       float* s_im = s_re + A.s_stride;
       auto add = [&](unsigned m, float2 v) {
         const unsigned t = m & 0xffffu;
+        if (!DSB_INB(t, A.s_stride, A.status)) return;
         // v is already scaled by 2^k: integer atomics (native, no
         // compare-and-swap loop) and a sum that does not depend on order
         const int re = __float2int_rn(v.x), im = __float2int_rn(v.y);
@@ -514,7 +515,7 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
             // cells e, e + 1 (e even): both inside the row's pitch whenever
             // e is a pattern cell (the pitch is n_filled rounded up to 4)
             const int e = 64 * ch + 2 * lane;
-            if (e < g_end) {
+            if (e < g_end && DSB_INB(e - g_lo + 1, A.d_pitch[g], A.status)) {
               m[q] = __ldg(cm2 + (e >> 1));
               v[q] = *reinterpret_cast<const Elem2*>(src + (e - g_lo));
               sc[q] = g_sc;
@@ -530,6 +531,8 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       }
       for (int i = tid; i < A.n_c2; i += THREADS) {
         const int2 cm = __ldg(A.c2 + i);
+        if (!DSB_INB(cm.x & 0xffff, A.d_pitch[(cm.x >> 16) & (IMG_MAX_G - 1)], A.status))
+          continue;
         add((unsigned)cm.y,
             RingElem<FMT>::get(s_slice[(cm.x >> 16) & (IMG_MAX_G - 1)] + (cm.x & 0xffff),
                                s_scale[(cm.x >> 16) & (IMG_MAX_G - 1)]));

@@ -441,7 +441,10 @@ __device__ __noinline__ void det_emit(const BoxSums<K> d, const float* __restric
   }
   if (best > thr) {
     const int slot = atomicAdd(count, 1);
-    if (slot < cap) cands[slot] = DetCand{t_out, pix, best, win};
+    if (slot < cap)
+      cands[slot] = DetCand{t_out, pix, best, win};
+    else  // the largest S/N that did not fit (positive floats order as ints)
+      atomicMax(count + 1, __float_as_int(best));
   }
 }
 

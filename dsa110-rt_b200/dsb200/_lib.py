@@ -14,7 +14,10 @@ from typing import Optional
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-SO_PATH = os.path.join(_HERE, "_native", "libdsb200.so")
+# DSB200_CHECK=1 loads the bounds-checked build (table indices range-checked
+# on the device, violations reported as DSB_E_BOUNDS in the status words)
+CHECKED = os.environ.get("DSB200_CHECK", "") == "1"
+SO_PATH = os.path.join(_HERE, "_native", "libdsb200_check.so" if CHECKED else "libdsb200.so")
 
 DT_INT8, DT_F16, DT_F32 = 0, 1, 2
 
@@ -29,7 +32,7 @@ _SIGNATURES = {
     "dsb_corr_tc": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp,
                     _c_ll, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
     "dsb_corr_tc_grid": [_vp, _c_ll, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp,
-                         _vp, _vp, _vp, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp],
+                         _vp, _vp, _vp, _c_ll, _c_ll, _c_ll, _c_int, _vp, _vp, _vp],
     "dsb_uv_cells": [_vp, _vp, _c_int, _vp, _c_int, ctypes.c_double, _c_int, _vp, _vp, _vp],
     "dsb_grid_vis": [_vp, _c_int, _c_ll, _vp, _vp, _c_int, _vp, _vp],
     "dsb_dedisp_vis": [_vp, _vp, _c_int, _c_ll, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_int,
@@ -99,7 +102,8 @@ def lib() -> ctypes.CDLL:
         if not os.path.exists(SO_PATH):
             raise RuntimeError(
                 f"dsb200 native library missing ({SO_PATH}); build it with "
-                "`python -c 'import __graft_entry__ as g; g.build()'` — there is no CPU fallback")
+                "`python -c 'import __graft_entry__ as g; g.build()'` (check=True for the "
+                "bounds-checked one) — there is no CPU fallback")
         L = ctypes.CDLL(SO_PATH)
         for name, args in _SIGNATURES.items():
             fn = getattr(L, name)

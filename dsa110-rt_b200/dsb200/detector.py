@@ -206,11 +206,11 @@ class DeterministicDetector:
             _lib.ptr(self._cands.buf), self._cands.capacity, 0, _lib.ptr(self._cands.count),
             _lib.ptr(l2.d_off), _lib.ptr(l2.d_ent), _lib.ptr(l2.samples), l2.m,
             _lib.stream_of(self.device)), "dsb_detect_sampled")
-        got = self._cands.fetch()
         # decoder_n_top grows with the cube / interior ratio (forward.py:1383-1399)
         n_top = self._n_top
         if t_base > 0 and n_out < T:
             n_top = max(n_top, int(math.ceil(n_top * float(T) / float(n_out))))
+        got = self._cands.fetch_top(n_top * K)
         items = [(float(c["snr"]), int(c["t"]) * (F * npix) + int(c["pix"]), int(c["k"]))
                  for c in got]
         r_lm, r_f, r_t = self._r

@@ -71,13 +71,17 @@ class PipelineConfig:
     sky_warmup: int = 8
     chunk_tiles: int = 512
     fdm_batch: int = 8
-    n_top: int = 256
+    # cells decoded per cube (top by S/N, then merge-radius suppression).
+    # None: the reference's streaming rule (detector/forward.py:1383-1399,
+    # :1607), 64 per kernel scaled by the cube / interior ratio:
+    # max(64, ceil(64 (C + 2 t_edge) / C)) x the number of boxcar widths
+    n_top: Optional[int] = None
     merge_radius_t: int = 4
     merge_radius_fdm: int = 5
     merge_radius_lm: int = 3
     l1_times: int = 16
     l1_pixels: int = 256
-    cand_capacity: int = 1 << 22
+    cand_capacity: int = 1 << 24     # above-threshold cells one cube may hold
     # stage-2 ring element: "c64" (complex64), "bf16" (the BF16 storage form:
     # each part rounded to nearest-even bf16, accumulated in float32 on read)
     # or "cint8" (the reference's cint8 wire form: every (chgroup, coarse DM,
@@ -94,6 +98,14 @@ class PipelineConfig:
     # 1/sqrt(width).
     layer2: bool = True
     layer2_max_samples: int = 4096
+    # calibration on the fast path: complex gain of every antenna in every
+    # summed channel, (n_chgroup, nchan // csf, nant) or anything that
+    # broadcasts to it ((nant,): one gain per antenna).  The correlator's
+    # gridding epilogue multiplies each visibility by g_a conj(g_b), which is
+    # what calibrated voltages give (apply_cal_split) when a gain is the same
+    # on the summed channels and both pols.  None: uncalibrated (integer
+    # exact).
+    gains: Optional[np.ndarray] = None
     layer2_tau_s: float = 30.0
     layer2_n_burnin: int = 30
 
@@ -114,6 +126,13 @@ class PipelineConfig:
             self.fine_to_coarse = np.repeat(np.arange(nc), K)
         self.fine_dm = np.asarray(self.fine_dm, np.float64)
         self.fine_to_coarse = np.asarray(self.fine_to_coarse, np.int64)
+
+    @property
+    def decoder_n_top(self) -> int:
+        if self.n_top is not None:
+            return int(self.n_top)
+        C, te = self.chunk_tiles, self.t_edge
+        return max(64, math.ceil(64 * (C + 2 * te) / C)) * (self.log_max_width + 1)
 
     @property
     def t_int_us(self) -> float:
@@ -524,6 +543,11 @@ class SearchPipeline:
                                 device=self.dev) if cfg.use_sky else None)
         self.sky_count = self.sky_head = self.sky_seen = 0
         self.status = _lib.status_word(self.dev)
+        self.d_gains = None
+        if cfg.gains is not None:
+            gq = np.broadcast_to(np.asarray(cfg.gains, np.complex64),
+                                 (cfg.band.n_chgroup, cfg.ceff, cfg.nant))
+            self.d_gains = torch.from_numpy(np.ascontiguousarray(gq)).to(self.dev)
         nt_cube = C + 2 * te
         nb = cfg.fdm_batch
         N = cfg.n_grid
@@ -610,8 +634,8 @@ class SearchPipeline:
                 _lib.ctypes.c_void_p(base), page, cfg.band.n_chgroup, C * ppfv, cfg.nant,
                 cfg.band.nchan, cfg.t_int, cfg.csf, _lib.ptr(self.d_yoff), _lib.ptr(self.d_ycnt),
                 _lib.ptr(self.d_row_off), _lib.ptr(self.d_row_bls), _lib.ptr(self.Y),
-                self.tab.n_rows_y, self.chunk * C, self.TY - 1, 0, _lib.ptr(self.status),
-                _lib.stream_of(self.dev)), "dsb_corr_tc_grid")
+                self.tab.n_rows_y, self.chunk * C, self.TY - 1, 0, _lib.ptr(self.d_gains),
+                _lib.ptr(self.status), _lib.stream_of(self.dev)), "dsb_corr_tc_grid")
         self.launches += 1
 
     def _stage1(self, j: int) -> None:
@@ -723,11 +747,11 @@ class SearchPipeline:
             s_k, _ = self.l2_state.update_and_query(per_kernel_sigma=self.l2_sig)
             self.sinv.copy_(torch.reciprocal(torch.clamp(s_k, min=1e-30)))
         if collect:
-            got = self.cands.fetch()
-            self.last_d2h_bytes += 4 + got.nbytes
+            got = self.cands.fetch_top(cfg.decoder_n_top)
+            self.last_d2h_bytes += 8 + got.nbytes
             self._pending = [(float(c["snr"]), int(c["t"]) * (nfine * N * N) + int(c["pix"]),
                               int(c["k"])) for c in got]
-            res = _nms(self._pending, threshold=cfg.threshold, n_top=cfg.n_top,
+            res = _nms(self._pending, threshold=cfg.threshold, n_top=cfg.decoder_n_top,
                        shape=(C, nfine, N, N), r_t=cfg.merge_radius_t, r_f=cfg.merge_radius_fdm,
                        r_lm=cfg.merge_radius_lm)
             t_first = jc * C - te

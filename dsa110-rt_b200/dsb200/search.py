@@ -626,23 +626,47 @@ DET_CAND_DTYPE = np.dtype([("t", np.int32), ("pix", np.int32), ("snr", np.float3
 
 
 class CandidateBuffer:
-    """Device buffer the fused detector appends above-threshold cells to."""
+    """Device buffer the fused detector appends above-threshold cells to.
+    ``count`` holds the number of cells found (which may pass the capacity)
+    and the bits of the largest S/N among those that did not fit."""
 
     def __init__(self, device, capacity: int = 1 << 20):
         self.device = device
         self.capacity = int(capacity)
         self.buf = torch.empty(self.capacity * 4, dtype=torch.int32, device=device)
-        self.count = torch.zeros(1, dtype=torch.int32, device=device)
+        self.count = torch.zeros(2, dtype=torch.int32, device=device)
 
     def reset(self):
         self.count.zero_()
 
     def fetch(self) -> np.ndarray:
-        n = int(self.count.item())
+        n = int(self.count[0].item())
         if n > self.capacity:
             raise _lib.DsbError(f"detector candidate buffer overflow ({n} > {self.capacity})")
         raw = self.buf[: 4 * n].cpu().numpy()
         return raw.view(DET_CAND_DTYPE)
+
+    def fetch_top(self, n_top: int) -> np.ndarray:
+        """The entries that can be among the ``n_top`` largest S/N (the only
+        ones a top-n_top decode reads): all of them when there are at most
+        ``n_top``, else, selected on the device, every entry whose S/N is at
+        least the ``n_top``-th largest (ties included, so that the decode's
+        flat-index order among equal values still decides).  When cells did
+        not fit the buffer, the selection is exact as long as the largest
+        S/N among them lies below the selected ones; otherwise DsbError."""
+        cnt = self.count.cpu()
+        n, dropped = int(cnt[0]), int(cnt[1])
+        m = min(n, self.capacity)
+        rec = self.buf[: 4 * m].view(m, 4)
+        if n <= max(n_top, 0) or m == 0:
+            return rec.cpu().numpy().reshape(-1).view(DET_CAND_DTYPE)
+        snr = rec[:, 2].contiguous().view(torch.float32)
+        vk = float(torch.topk(snr, min(n_top, m)).values[-1])
+        out = rec[snr >= vk].cpu().numpy().reshape(-1).view(DET_CAND_DTYPE)
+        if n > self.capacity and not float(np.int32(dropped).view(np.float32)) < vk:
+            raise _lib.DsbError(f"detector candidate buffer overflow ({n} > {self.capacity}) "
+                                "reaches the top entries")
+        return out
 
 
 def detect_cube(cube: torch.Tensor, *, log_max_width: int, sigma_inv: torch.Tensor,

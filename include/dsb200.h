@@ -29,6 +29,8 @@ extern "C" {
 #define DSB_E_UNSUPPORTED 3  /* geometry outside what the kernel supports   */
 #define DSB_E_TIMEOUT 4      /* device-side bounded wait ran out (status)   */
 #define DSB_E_CAPACITY 5     /* a size exceeds a fixed capacity             */
+#define DSB_E_BOUNDS 6       /* bounds-checked build: a table index out of  */
+                             /* range (status; the access was skipped)      */
 
 #define DSB_DT_INT8 0
 #define DSB_DT_F16 1
@@ -82,12 +84,18 @@ int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt
  * channel.  Group (g, s) owns rows [yoff[g*ceff+s], + ycnt[...]); row r sums
  * the baselines row_bls[row_off[r] .. row_off[r+1]) (exact int32).
  * Output row r, tile f -> yout[((t_base + f) & t_mask)*y_t_stride + r]
- * (time-major ring; y_t_stride >= number of rows). */
+ * (time-major ring; y_t_stride >= number of rows).
+ * gains (may be null): (n_chgroup, ceff, nant) complex64, the gain of each
+ * antenna in each summed channel; every visibility is multiplied by
+ * g_a conj(g_b) before it is gridded (each product and sum rounded in
+ * float32, rows summed in CSR order), the identity calibrated voltages
+ * give (apply_cal_split, src/dsart/services/slow_corr_kernel.py:459)
+ * when a gain is the same on the summed channels and both pols. */
 int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
                      int nchan, int t_int, int csf, const int* yoff, const int* ycnt,
                      const int* row_off, const int* row_bls, void* yout, long long y_t_stride,
-                     long long t_base, long long t_mask, int max_ctas, int* status,
-                     cudaStream_t stream);
+                     long long t_base, long long t_mask, int max_ctas, const void* gains,
+                     int* status, cudaStream_t stream);
 
 /* ---- a6: uv cells in FP64 -------------------------------------------------
  * Replaces the (u, v) -> cell arithmetic of build_pattern / from_pattern
@@ -403,8 +411,12 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
  * mask[f*mask_f_stride + p] (the edge mask; mask_f_stride 0 shares one mask
  * over the fine DMs), divided by sig_f[f] (the Layer-1 sigma) when sig_f is
  * non-null.  Every output cell with max S/N > threshold is appended to
- * cands (struct {int t, pix; float snr; int k;}, pix = e + pix_off); *count
- * counts them (entries past cap are counted, not written). */
+ * cands (struct {int t, pix; float snr; int k;}, pix = e + pix_off); count[0]
+ * counts them (entries past cap are counted, not written) and count[1]
+ * keeps the bits of the largest S/N that was not written (0 when every entry
+ * fit): a caller selecting the top entries knows its selection is exact
+ * when that S/N lies below them.  count points at two ints, zeroed before
+ * the launch. */
 int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
                long long t_stride, const float* mask, long long mask_f_stride,
                const float* sig_f, int log_maxw, const float* sigma_inv, int t_base, int n_out,

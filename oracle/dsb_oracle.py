@@ -1032,9 +1032,10 @@ def layer2_sample_index(n_kernels: int, m: int, total: int) -> np.ndarray:
 
 def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block, t_int, csf,
                  n_grid, coarse_dm, fine_dm, fine_to_coarse, log_max_width, threshold, chunk,
-                 use_sky=True, sky_window=8, sky_warmup=8, n_top=256, r_t=4, r_f=5, r_lm=3,
+                 use_sky=True, sky_window=8, sky_warmup=8, n_top=None, r_t=4, r_f=5, r_lm=3,
                  l1_times=16, l1_pixels=256, ring_dtype="c64", keep=None, keep_images=True,
-                 layer2=True, layer2_max_samples=4096, layer2_tau_s=30.0, layer2_n_burnin=30):
+                 layer2=True, layer2_max_samples=4096, layer2_tau_s=30.0, layer2_n_burnin=30,
+                 gains=None):
     """Oracle of the CUDA streaming pipeline; returns candidate tuples
     ``(t_abs, fdm, l, m, snr, width)`` and (optionally) intermediates.
     ``ring_dtype="bf16"`` stores the stage-2 streams in the BF16 form (each
@@ -1059,6 +1060,15 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
                                         nchan=band.nchan, t_int=t_int, csf=csf)
             vis[g].append(vr + 1j * vi)
     vis = [np.concatenate(v, axis=0) for v in vis]
+    if gains is not None:
+        # calibration as the voltages would carry it (apply_cal_split,
+        # slow_corr_kernel.py:459) with one gain per antenna and summed
+        # channel: V_ab -> g_a conj(g_b) V_ab, in float64
+        ceff = band.nchan // csf
+        gq = np.broadcast_to(np.asarray(gains, np.complex64), (G, ceff, nant)).astype(np.complex128)
+        a_idx, b_idx = upper_tri_indices(nant)
+        for g in range(G):
+            vis[g] = vis[g] * (gq[g][:, a_idx] * np.conj(gq[g][:, b_idx])).T[None]
     T_total = vis[0].shape[0]
     max_sh1 = int(tb["sh1"].max())
     depth1 = -(-max_sh1 // chunk)
@@ -1075,10 +1085,9 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
             pad = (j + 1) * chunk + max_sh1 - j * chunk - win.shape[0]
             if pad > 0:
                 win = np.concatenate([win, np.zeros((pad,) + win.shape[1:], win.dtype)])
-            o_re = stage1_dedisp(np.rint(win.real).astype(np.int64), tb["sh1"][g],
-                                 tb["cims"][g], r.size, chunk)
-            o_im = stage1_dedisp(np.rint(win.imag).astype(np.int64), tb["sh1"][g],
-                                 tb["cims"][g], r.size, chunk)
+            exact = (lambda x: np.rint(x).astype(np.int64)) if gains is None else (lambda x: x)
+            o_re = stage1_dedisp(exact(win.real), tb["sh1"][g], tb["cims"][g], r.size, chunk)
+            o_im = stage1_dedisp(exact(win.imag), tb["sh1"][g], tb["cims"][g], r.size, chunk)
             for d in range(n_coarse):
                 x = (o_re[d] + 1j * o_im[d]).astype(np.complex64)
                 if sky is not None:
@@ -1094,6 +1103,9 @@ def run_pipeline(raw_blocks, band: Band, antpos_e, antpos_n, *, nant, npkt_block
     a = -(-L // chunk)
     te = (1 << log_max_width) // 2
     widths = [1 << k for k in range(log_max_width + 1)]
+    if n_top is None:
+        # the streaming decoder's rule (detector/forward.py:1383-1399, :1607)
+        n_top = max(64, math.ceil(64 * (chunk + 2 * te) / chunk)) * len(widths)
     sinv = (np.float32(1.0) / np.sqrt(np.asarray(widths, np.float32))).astype(np.float32)
     offs = boxcar_offsets(widths, 1 << log_max_width)
     mask = edge_mask(N, kernel_support=1)

@@ -199,7 +199,7 @@ def test_cumsum_boxcars_argmax_vs_reference(dev, golden_dir):
 
 @pytest.mark.parametrize("log_w", [2, 4])
 @pytest.mark.parametrize("f16", [False, True])
-@pytest.mark.parametrize("hw", [(12, 10), (11, 9)])
+@pytest.mark.parametrize("hw", [(12, 10), (11, 9), (16, 16)])
 def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16, hw):
     """Candidates of the streaming detector == every cell above threshold of
     the padded cumsum + boxcar argmax, bit for bit, for even and odd pixel
@@ -226,6 +226,42 @@ def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16, hw):
     want = sorted((int(i // inner), int(i % inner), float(mx.reshape(-1)[i]), int(win.reshape(-1)[i]))
                   for i in sel)
     have = sorted((int(c["t"]), int(c["pix"]), float(c["snr"]), int(c["k"])) for c in got)
+    assert have == want
+
+
+@pytest.mark.parametrize("cap", [1 << 16, 600, 300])
+def test_candidate_buffer_top_selection_is_exact_or_raises(dev, cap):
+    """fetch_top(n) returns every entry whose S/N is at least the n-th
+    largest of all cells above threshold (ties included).  With a buffer too
+    small for every cell, it returns that same set whenever the cells that
+    did not fit rank below it, and raises otherwise -- never a wrong set."""
+    from dsb200 import _lib
+    from dsb200.search import CandidateBuffer, detect_cube
+    rng = np.random.default_rng(21)
+    T, F, H, W = 40, 2, 16, 16
+    x = rng.normal(size=(T, F, H, W)).astype(np.float32)
+    x[10:14, 1, 3, 4] += 9.0
+    x[25:27, 0, 8, 8] += 7.0
+    sinv = torch.ones(3, dtype=torch.float32, device=dev)
+    full = CandidateBuffer(dev, 1 << 16)
+    detect_cube(torch.from_numpy(x).to(dev), log_max_width=2, sigma_inv=sinv, t_base=2,
+                n_out=T - 4, threshold=1.0, cands=full)
+    every = full.fetch()
+    assert len(every) > 1000
+    n_top = 64
+    vk = np.sort(every["snr"])[::-1][n_top - 1]
+    want = sorted(tuple(int(v) if k != "snr" else float(v) for k, v in zip(e.dtype.names, e))
+                  for e in every[every["snr"] >= vk])
+    buf = CandidateBuffer(dev, cap)
+    detect_cube(torch.from_numpy(x).to(dev), log_max_width=2, sigma_inv=sinv, t_base=2,
+                n_out=T - 4, threshold=1.0, cands=buf)
+    try:
+        got = buf.fetch_top(n_top)
+    except _lib.DsbError:
+        assert cap < len(every)
+        return
+    have = sorted(tuple(int(v) if k != "snr" else float(v) for k, v in zip(e.dtype.names, e))
+                  for e in got)
     assert have == want
 
 
