@@ -499,7 +499,7 @@ def reference_cpu_chain(cfg, threads: int):
                               kernel_ids=[f"unit_d1_b{w}" for w in widths],
                               kernel_time_widths=widths, merge_radius_lm=cfg.merge_radius_lm,
                               merge_radius_fdm=cfg.merge_radius_fdm,
-                              merge_radius_t=cfg.merge_radius_t, n_top=cfg.n_top)
+                              merge_radius_t=cfg.merge_radius_t, n_top=cfg.decoder_n_top)
     sec["detect"] = (clock() - t0) * n_fine * tiles_per_s / n_out
     total = sum(sec.values())
     return {"value": 1.0 / total, "unit": "data-seconds/s", "cores": threads,
@@ -521,12 +521,18 @@ def reference_cpu_chain(cfg, threads: int):
 def serve_main(a, cfg):
     """Served streaming form: ``a.serve`` independent voltage streams on one
     GPU through ``dsb200.serve.StreamServer``.  Stream i delivers
-    ``a.serve_blocks`` blocks of a seeded uneven length of 1-4 chunks
-    (4096-16384 samples) with Poisson arrivals at (i mod 4 + 1) x real time;
+    ``a.serve_blocks`` blocks of a seeded uneven length of 1-8 chunks
+    (4096-32768 samples) with Poisson arrivals at (i mod 4 + 1) x real time;
     block copies are admitted under a device budget of two of the largest
-    blocks.  Reports the sustained real-time factor (data-seconds of all
-    streams per wall-second, first arrival to last candidate) and the p50/p99
-    arrival-to-candidate latency."""
+    blocks, or what HBM holds beside the resident pipelines.  Bursts arrive
+    in every stream at 0.5 per data-second (Poisson),
+    DM uniform 50-2000, S/N uniform 7-40, 4 search samples wide, at seeded
+    pixels; each block's bursts are drawn into its device copy before the
+    search (the server's ``prepare`` hook), with amplitudes set from one
+    reference burst measured first.  Reports the sustained real-time factor
+    (data-seconds of all streams per wall-second, first arrival to last
+    candidate), the p50/p99 arrival-to-candidate latency, and the fraction of
+    bursts recovered."""
     import threading
     import torch
     from dsb200 import synth
@@ -537,13 +543,23 @@ def serve_main(a, cfg):
     torch.cuda.set_device(dev)
     S = a.serve
     e, n = synth.t_layout(cfg.nant, seed=11)
+    ti = cfg.t_int
+    # amplitude scale from one reference burst in a stream of its own
+    noise = [synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=cfg.npkt_block,
+                                       device=dev, seed=900 + i) for i in range(2)]
+    ref = _reference_burst(cfg, e, n, noise, torch.empty_like(noise[0]), amp_ref=0.09)
+    del noise
+    torch.cuda.empty_cache()
+
     pipes = [SearchPipeline(cfg, e, n, device=dev) for _ in range(S)]
     for p in pipes:
         p.skip_warmup()
+    k0 = pipes[0].chunk
     C = cfg.chunk_tiles
     per_chunk = C * cfg.t_int // 2                     # packets per chunk
-    chunk_s = per_chunk * 2 * 32.768e-6                # data-seconds per chunk
-    max_k = 4
+    chunk_samp = 2 * per_chunk
+    chunk_s = chunk_samp * 32.768e-6                   # data-seconds per chunk
+    max_k = 8
     # one pinned host source of the largest block, shared (read-only) by all
     # streams; a k-chunk block is its contiguous prefix viewed as k-chunk pages
     src = synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=max_k * per_chunk,
@@ -556,16 +572,63 @@ def serve_main(a, cfg):
         return src[:G * npkt * cfg.nant * cfg.band.nchan * 4].view(G, npkt, *page_shape)
     rng = np.random.default_rng(2024)
     plan = []                                          # (arrival s, stream, chunks)
+    offsets = [[] for _ in range(S)]                   # first native sample of each block
     for i in range(S):
         rate = i % 4 + 1
-        t = 0.0
+        t, s0 = 0.0, 0
         for _ in range(a.serve_blocks):
             k = int(rng.integers(1, max_k + 1))
             t += rng.exponential(k * chunk_s / rate)
             plan.append((t, i, k))
+            offsets[i].append(s0)
+            s0 += k * chunk_samp
+        offsets[i].append(s0)
     plan.sort()
-    budget = 2 * src.numel()
-    srv = StreamServer(pipes, budget).start()
+    # bursts: Poisson at 0.5 per data-second of each stream, after the rings fill
+    k_bot = _delay_per_dm(cfg.band)
+    lat_chunks = pipes[0].depth1 + pipes[0].a + 2
+    warm = int(k_bot * float(cfg.coarse_dm.max())) + chunk_samp
+    bursts, grid = [], []
+    for i in range(S):
+        total = offsets[i][-1]
+        tb = warm + rng.exponential(1.0 / 0.5) / 32.768e-6
+        bi, gi = [], []
+        while True:
+            dm = float(rng.uniform(50.0, 2000.0))
+            snr = float(rng.uniform(7.0, 40.0))
+            w = 4 * ti
+            end_chunk = (tb + k_bot * dm + w) / chunk_samp + lat_chunks
+            if end_chunk >= total / chunk_samp:
+                break
+            dl, dmp = (int(v) for v in rng.integers(-(cfg.n_grid // 2 - 8), cfg.n_grid // 2 - 7, 2))
+            amp = synth.amp_for_snr(snr, w, amp_ref=ref["amp"], snr_ref=ref["snr"],
+                                    width_ref=ref["width_native"])
+            bi.append(synth.Burst(dm=dm, t0_native=int(tb), width_native=w, amp=amp, dl=dl,
+                                  dm_pix=dmp))
+            gi.append((snr, w, dm, int(tb), dl, dmp))
+            tb += rng.exponential(1.0 / 0.5) / 32.768e-6
+        bursts.append(bi)
+        grid.append(gi)
+
+    def prepare(i, k, blk):
+        s0 = offsets[i][k]
+        n_samp = 2 * blk.shape[1]
+        mine = [b for b in bursts[i] if b.t0_native < s0 + n_samp and
+                b.t0_native + k_bot * b.dm + b.width_native + 8 > s0]
+        if mine:
+            synth.inject_bursts_device(blk, band=cfg.band, nant=cfg.nant, s0=s0, bursts=mine,
+                                       antpos_e=e, antpos_n=n,
+                                       cell_lambda=pipes[i].tab.cell_lambda, n_grid=cfg.n_grid,
+                                       seed=31 + i)
+
+    # two of the largest blocks, or what the device has left beside the
+    # resident pipelines (less 8 GB of working room), at least one block
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = min(2 * src.numel(), free - (8 << 30))
+    if budget < src.numel():
+        raise SystemExit(f"serve: {free / 1e9:.1f} GB free cannot hold one "
+                         f"{src.numel() / 1e9:.1f} GB block beside the pipelines")
+    srv = StreamServer(pipes, budget, prepare=prepare).start()
     t0 = time.perf_counter()
 
     def feed():
@@ -585,6 +648,15 @@ def serve_main(a, cfg):
         p.check_status()
     data_s = sum(k for _, _, k in plan) * chunk_s
     lat = np.asarray(srv.latencies_s()) * 1e3
+    found = []
+    for i in range(S):
+        cands = [c for r in srv.results[i] for c in r.candidates]
+        # the streams started in steady state (skip_warmup): their first
+        # sample is search sample k0 * C of the pipeline's clock
+        off = k0 * C * ti
+        found += synth.match_bursts([(a_, w_, d_, t_ + off, l_, m_)
+                                     for a_, w_, d_, t_, l_, m_ in grid[i]], cands,
+                                    band=cfg.band, fine_dm=cfg.fine_dm, n_grid=cfg.n_grid, t_int=ti)
     print(json.dumps({
         "metric": "served streaming: sustained real-time factor (data-seconds of all streams "
                   "per wall-second) and arrival-to-candidate latency",
@@ -594,10 +666,78 @@ def serve_main(a, cfg):
                                        "p99": float(np.percentile(lat, 99))},
         "offered_load_x_realtime": float(sum(i % 4 + 1 for i in range(S))),
         "device_budget_bytes": budget, "budget_peak_bytes": srv.budget.peak,
+        "bursts": {"injected": len(found), "recovered": int(sum(q is not None for q in found)),
+                   "reference_burst": ref},
         "config": dict(workload_desc(a.workload, cfg),
-                       blocks="seeded 1-4 chunks (4096-16384 samples), Poisson arrivals at "
-                              "1-4x real time per stream"),
-        "data": "synthetic (seeded 4-bit Gaussian voltages)"}))
+                       blocks="seeded 1-8 chunks (4096-32768 samples), Poisson arrivals at "
+                              "1-4x real time per stream",
+                       bursts="0.5 per data-second per stream, DM U(50, 2000), S/N U(7, 40), "
+                              "4 search samples wide"),
+        "data": "synthetic (seeded 4-bit Gaussian voltages, bursts drawn in on the device)"}))
+
+
+def _delay_per_dm(band) -> float:
+    """Native samples of dispersion delay per unit DM between the top and the
+    bottom of the band."""
+    nu = band.freq_table()
+    return 4.148808 * (1.0 / float(nu.min()) ** 2 - 1.0 / float(nu[0, 0]) ** 2) * 1e3 / 32.768
+
+
+def _injected_stream(cfg, e, n, noise, work, bursts, n_blocks, seed):
+    """A fresh ``SearchPipeline`` over ``n_blocks`` blocks, block k a copy of
+    ``noise[k % len(noise)]`` with the bursts that cover it drawn in
+    (``inject_bursts_device``).  Returns (candidates, device ms in
+    ``process_block``, fine DMs)."""
+    import torch
+    from dsb200 import synth
+    from dsb200.pipeline import SearchPipeline
+    dev = work.device
+    blk = 2 * cfg.npkt_block
+    k_bot = _delay_per_dm(cfg.band)
+    pipe = SearchPipeline(cfg, e, n, device=dev)
+    cell = pipe.tab.cell_lambda
+    cands, dev_ms = [], 0.0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for k in range(n_blocks):
+        s0 = k * blk
+        work.copy_(noise[k % len(noise)])
+        mine = [b for b in bursts if b.t0_native < s0 + blk and
+                b.t0_native + k_bot * b.dm + b.width_native + 8 > s0]
+        synth.inject_bursts_device(work, band=cfg.band, nant=cfg.nant, s0=s0, bursts=mine,
+                                   antpos_e=e, antpos_n=n, cell_lambda=cell,
+                                   n_grid=cfg.n_grid, seed=seed)
+        ev0.record()
+        got = pipe.process_block(work)
+        ev1.record()
+        torch.cuda.synchronize()
+        dev_ms += ev0.elapsed_time(ev1)
+        cands += got
+    pipe.check_status()
+    fine = pipe.cfg.fine_dm
+    del pipe
+    torch.cuda.empty_cache()
+    return cands, dev_ms, fine
+
+
+def _reference_burst(cfg, e, n, noise, work, amp_ref, dm=1000.0, width_search=4):
+    """Measure the S/N of one burst of amplitude ``amp_ref`` (``width_search``
+    search samples, DM ``dm``) in a stream of its own: the scale from which
+    ``synth.amp_for_snr`` sets every injected burst's amplitude."""
+    from dsb200 import synth
+    blk = 2 * cfg.npkt_block
+    ti = cfg.t_int
+    warm = max(4 * blk, int(_delay_per_dm(cfg.band) * float(cfg.coarse_dm.max())) + blk)
+    ref = (0.0, width_search * ti, float(dm), warm + blk // 3, 40 % (cfg.n_grid // 4),
+           -(60 % (cfg.n_grid // 4)))
+    rb = [synth.Burst(dm=ref[2], t0_native=ref[3], width_native=ref[1], amp=amp_ref,
+                      dl=ref[4], dm_pix=ref[5])]
+    n_blocks = int(np.ceil((ref[3] + _delay_per_dm(cfg.band) * dm + ref[1]) / blk)) + 3
+    rc, _, fine = _injected_stream(cfg, e, n, noise, work, rb, n_blocks, seed=77)
+    m = synth.match_bursts([ref], rc, band=cfg.band, fine_dm=fine, n_grid=cfg.n_grid, t_int=ti)
+    if m[0] is None:
+        raise SystemExit("the reference burst was not detected")
+    return {"amp": amp_ref, "width_native": ref[1], "dm": float(dm), "snr": float(m[0].snr)}
 
 
 def stress_main(a):
@@ -617,7 +757,6 @@ def stress_main(a):
     the oracle does not run.  Prints its own JSON line."""
     import torch
     from dsb200 import synth
-    from dsb200.pipeline import SearchPipeline
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -629,50 +768,14 @@ def stress_main(a):
     noise = [synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=npkt, device=dev,
                                        seed=900 + i) for i in range(3)]
     work = torch.empty_like(noise[0])
-    nu = cfg.band.freq_table()
-    k_bot = 4.148808 * (1.0 / float(nu.min()) ** 2 - 1.0 / float(nu[0, 0]) ** 2) * 1e3 / 32.768
+    k_bot = _delay_per_dm(cfg.band)
     warm = 4 * blk                                       # rings full before the first burst
-
-    def stream(bursts, n_blocks, seed):
-        pipe = SearchPipeline(cfg, e, n, device=dev)
-        cell = pipe.tab.cell_lambda
-        cands, dev_ms = [], 0.0
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        for k in range(n_blocks):
-            s0 = k * blk
-            work.copy_(noise[k % len(noise)])
-            mine = [b for b in bursts if b.t0_native < s0 + blk and
-                    b.t0_native + k_bot * b.dm + b.width_native + 8 > s0]
-            synth.inject_bursts_device(work, band=cfg.band, nant=cfg.nant, s0=s0, bursts=mine,
-                                       antpos_e=e, antpos_n=n, cell_lambda=cell,
-                                       n_grid=cfg.n_grid, seed=seed)
-            ev0.record()
-            got = pipe.process_block(work)
-            ev1.record()
-            torch.cuda.synchronize()
-            dev_ms += ev0.elapsed_time(ev1)
-            cands += got
-        pipe.check_status()
-        fine = pipe.cfg.fine_dm
-        del pipe
-        torch.cuda.empty_cache()
-        return cands, dev_ms, fine
 
     def blocks_for(t_last, dm_max, w_max):
         return int(np.ceil((t_last + k_bot * dm_max + w_max) / blk)) + 3
 
-    # reference burst: width 4 search samples, DM 1000, its own stream
     ti = cfg.t_int
-    ref = (0.0, 4 * ti, 1000.0, warm + blk // 3, 40, -60)
-    amp_ref = 0.06
-    rb = [synth.Burst(dm=ref[2], t0_native=ref[3], width_native=ref[1], amp=amp_ref,
-                      dl=ref[4], dm_pix=ref[5])]
-    rc, _, fine = stream(rb, blocks_for(ref[3], ref[2], ref[1]), seed=77)
-    m = synth.match_bursts([ref], rc, band=cfg.band, fine_dm=fine, n_grid=cfg.n_grid, t_int=ti)
-    if m[0] is None:
-        raise SystemExit("stress: the reference burst was not detected")
-    snr_ref = float(m[0].snr)
+    ref = _reference_burst(cfg, e, n, noise, work, amp_ref=0.06)
 
     snrs = [6, 7, 8, 10, 12, 15, 20, 30, 40, 50]
     widths = [1, 4, 16, 32]                              # search samples
@@ -681,13 +784,13 @@ def stress_main(a):
     grid = synth.burst_grid(snrs=snrs, widths=[w * ti for w in widths], dms=dms,
                             t_first_native=warm, spacing_native=spacing, n_grid=cfg.n_grid,
                             seed=2024)
-    amps = [synth.amp_for_snr(s, w, amp_ref=amp_ref, snr_ref=snr_ref, width_ref=ref[1])
-            for s, w, *_ in grid]
+    amps = [synth.amp_for_snr(s, w, amp_ref=ref["amp"], snr_ref=ref["snr"],
+                              width_ref=ref["width_native"]) for s, w, *_ in grid]
     bursts = [synth.Burst(dm=d, t0_native=t0, width_native=w, amp=am, dl=dl, dm_pix=dp)
               for (s, w, d, t0, dl, dp), am in zip(grid, amps)]
     n_blocks = blocks_for(max(g[3] for g in grid), max(dms),
                           max(widths) * ti)
-    cands, dev_ms, fine = stream(bursts, n_blocks, seed=2024)
+    cands, dev_ms, fine = _injected_stream(cfg, e, n, noise, work, bursts, n_blocks, seed=2024)
     got = synth.match_bursts(grid, cands, band=cfg.band, fine_dm=fine, n_grid=cfg.n_grid,
                              t_int=ti)
 
@@ -696,6 +799,13 @@ def stress_main(a):
         return {"n": len(idx), "recovered": float(np.mean([got[i] is not None for i in idx]))}
     ratio = [float(q.snr) / g[0] for g, q in zip(grid, got) if q is not None]
     data_s = n_blocks * cfg.block_seconds
+    # a cube decodes its top cells before merging them (the reference's
+    # decoder), so a bright burst can take every decoded cell of a cube that
+    # a fainter one shares: count the misses that share a cube with a
+    # stronger burst
+    cube = [int((g[3] + k_bot * g[2]) / ti // cfg.chunk_tiles) for g in grid]
+    crowded = sum(1 for i, q in enumerate(got) if q is None and any(
+        cube[j] == cube[i] and grid[j][0] > grid[i][0] for j in range(len(grid))))
     print(json.dumps({
         "metric": "stress/recovery sweep: fraction of injected bursts recovered",
         "value": float(np.mean([q is not None for q in got])), "unit": "fraction",
@@ -707,8 +817,10 @@ def stress_main(a):
         "measured_over_injected_snr": {"median": float(np.median(ratio)),
                                        "p10": float(np.percentile(ratio, 10)),
                                        "p90": float(np.percentile(ratio, 90))},
-        "reference_burst": {"amp": amp_ref, "width_native": ref[1], "dm": ref[2],
-                            "snr": snr_ref},
+        "reference_burst": ref,
+        "missed": int(sum(q is None for q in got)),
+        "missed_sharing_a_cube_with_a_stronger_burst": int(crowded),
+        "decoder_n_top": cfg.decoder_n_top,
         "candidates": len(cands), "blocks": n_blocks, "data_seconds": data_s,
         "device_seconds": dev_ms / 1e3, "real_time_factor": data_s / (dev_ms / 1e3),
         "config": dict(workload_desc(a.workload, cfg),
@@ -825,7 +937,7 @@ def main():
     ap.add_argument("--serve", type=int, default=0, metavar="S",
                     help="served streaming form instead: S voltage streams, seeded uneven "
                          "blocks, Poisson arrivals; prints its own JSON line")
-    ap.add_argument("--serve-blocks", type=int, default=4, help="blocks per served stream")
+    ap.add_argument("--serve-blocks", type=int, default=12, help="blocks per served stream")
     ap.add_argument("--batched", action="store_true",
                     help="batched form instead: six uneven channel groups with their own "
                          "sub-arrays and DM plans, one CUDA graph per block; prints its own "

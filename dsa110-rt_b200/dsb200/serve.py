@@ -18,6 +18,9 @@ detector buffers stay resident on the device for the life of the stream.
 * Blocks may hold any whole number of chunks (uneven lengths).
 * Each result records the block's arrival and completion times, for
   arrival-to-candidate latency.
+* An optional ``prepare(stream, block_index, device_block)`` runs on the
+  block's device copy, on the stream's CUDA stream, before the search (the
+  served benchmark draws its injected bursts in there).
 
 A stream's candidates do not depend on what runs beside it: pipelines share
 no state, only the GPU.
@@ -30,7 +33,7 @@ import queue
 import threading
 import time
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence
+from typing import Callable, List, Optional, Sequence
 
 import torch
 
@@ -87,9 +90,11 @@ class StreamServer:
     ``close()`` ends every stream after its queued blocks; ``join()`` waits
     and re-raises the first error of any worker."""
 
-    def __init__(self, pipelines: Sequence, budget_bytes: int):
+    def __init__(self, pipelines: Sequence, budget_bytes: int,
+                 prepare: Optional[Callable[[int, int, torch.Tensor], None]] = None):
         self.pipes = list(pipelines)
         self.budget = DeviceBudget(budget_bytes)
+        self.prepare = prepare
         self._queues: List[queue.Queue] = [queue.Queue() for _ in self.pipes]
         self.results: List[List[BlockResult]] = [[] for _ in self.pipes]
         self._errors: List[BaseException] = []
@@ -144,6 +149,10 @@ class StreamServer:
                     t_admit = time.perf_counter()
                     try:
                         dev_raw = raw.to(pipe.dev, non_blocking=True)
+                        if self.prepare is not None:
+                            if dev_raw.data_ptr() == raw.data_ptr():
+                                dev_raw = raw.clone()   # never change the caller's block
+                            self.prepare(i, k, dev_raw)
                         cands = pipe.process_block(dev_raw)
                         if getattr(pipe.dev, "type", None) == "cuda":
                             # the block's copy is released only once nothing reads it

@@ -89,6 +89,37 @@ def test_streams_alone_and_mixed_agree():
     assert srv.budget.peak <= budget and srv.budget.used == 0
 
 
+def test_prepare_hook_sees_each_block_once_in_order():
+    """prepare(stream, block index, device block) runs before the search on
+    a private copy: the caller's blocks stay unchanged, and the pipeline sees
+    the prepared block."""
+    streams = [_blocks(s, 4) for s in range(2)]
+    orig = [[x.clone() for x in bl] for bl in streams]
+    seen = []
+
+    def prepare(i, k, blk):
+        seen.append((i, k))
+        blk.view(-1)[0] = 7
+    pipes = [_FakePipe(delay=0.0) for _ in streams]
+    srv = StreamServer(pipes, 1 << 20, prepare=prepare).start()
+    for k in range(4):
+        for i, bl in enumerate(streams):
+            srv.submit(i, bl[k])
+    srv.close()
+    srv.join(30)
+    assert sorted(seen) == [(i, k) for i in range(2) for k in range(4)]
+    for i in range(2):
+        assert [k for j, k in seen if j == i] == list(range(4))
+        assert all(torch.equal(a, b) for a, b in zip(streams[i], orig[i]))
+        want = _FakePipe()
+        exp = []
+        for x in orig[i]:
+            y = x.clone()
+            y.view(-1)[0] = 7
+            exp.append(want.process_block(y))
+        assert [r.candidates for r in srv.results[i]] == exp
+
+
 def test_stream_error_is_reported():
     pipes = [_FakePipe(), _FakePipe(fail_at=1)]
     srv = StreamServer(pipes, 1 << 20).start()
