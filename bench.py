@@ -804,8 +804,10 @@ def stress_main(a):
     # a fainter one shares: count the misses that share a cube with a
     # stronger burst
     cube = [int((g[3] + k_bot * g[2]) / ti // cfg.chunk_tiles) for g in grid]
-    crowded = sum(1 for i, q in enumerate(got) if q is None and any(
-        cube[j] == cube[i] and grid[j][0] > grid[i][0] for j in range(len(grid))))
+    shaded = [any(cube[j] == cube[i] and grid[j][0] > grid[i][0] for j in range(len(grid)))
+              for i in range(len(grid))]
+    crowded = sum(1 for i, q in enumerate(got) if q is None and shaded[i])
+    alone = [i for i in range(len(grid)) if not shaded[i]]
     print(json.dumps({
         "metric": "stress/recovery sweep: fraction of injected bursts recovered",
         "value": float(np.mean([q is not None for q in got])), "unit": "fraction",
@@ -820,6 +822,11 @@ def stress_main(a):
         "reference_burst": ref,
         "missed": int(sum(q is None for q in got)),
         "missed_sharing_a_cube_with_a_stronger_burst": int(crowded),
+        "without_a_stronger_burst_in_their_cube": {
+            "n": len(alone),
+            "recovered": float(np.mean([got[i] is not None for i in alone])) if alone else None,
+            "recovered_at_or_above_snr_8": float(np.mean(
+                [got[i] is not None for i in alone if grid[i][0] >= 8])) if alone else None},
         "decoder_n_top": cfg.decoder_n_top,
         "candidates": len(cands), "blocks": n_blocks, "data_seconds": data_s,
         "device_seconds": dev_ms / 1e3, "real_time_factor": data_s / (dev_ms / 1e3),

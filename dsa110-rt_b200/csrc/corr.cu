@@ -12,8 +12,12 @@
 //                        grids them per subband into time-major rows.
 #include "dsb_common.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <type_traits>
 
 namespace {
@@ -97,6 +101,10 @@ struct TcArgs {
   // (n_chgroup, ceff, nant) complex gains or null: every visibility is
   // multiplied by g_a conj(g_b) of its subband before it is gridded
   const float2* gains;
+  // raw staging by TMA (tma != 0): each item's raw bytes, ppk packets x nant
+  // antennas x csf channels x 4 bytes, arrive by one 4-D tensor copy into one
+  // of nraw shared-memory stages of raw_stage bytes, nraw - 1 items ahead
+  int tma, ppk, raw_stage, nraw;
   int* status;
 };
 
@@ -138,6 +146,7 @@ DSB_DEV void tc_load(const TcArgs& A, int g, int f, int s, int q, uint4 (&w)[TC_
 // chunk 0 moved by q * (kc/4/csf) packets.
 struct TcFillPlan {
   int ld[TC_PRE];
+  int lds[TC_PRE];    // the same word in a TMA raw stage [ppk][nant][csf * 4 bytes]
   uint32_t st[TC_PRE][4];
   long long q_step;   // bytes between chunks
   long long f_step;   // bytes between fast-vis tiles
@@ -154,6 +163,7 @@ DSB_DEV void tc_fill_plan(const TcArgs& A, TcFillPlan& P) {
     const int a = idx / nv, v = idx % nv;
     const int p = (v * 4) / A.csf, c = (v * 4) % A.csf;
     P.ld[r] = (int)(((long long)p * A.nant + a) * A.nchan * 4 + (long long)c * 4);
+    P.lds[r] = ((p * A.nant + a) * A.csf + c) * 4;
     const uint32_t kr = (uint32_t)v * 16u, ki = (uint32_t)A.kc + (uint32_t)v * 16u;
     const uint32_t ra = (uint32_t)a, rb = (uint32_t)(A.nant + a);
     P.st[r][0] = (kr >> 7) * region + sw128_offset(ra, kr & 127u);
@@ -391,15 +401,20 @@ DSB_DEV void tc_epilogue(const TcArgs& A, uint32_t tmem_base, int buf, int g, in
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) {
+template <int MODE, bool TMA>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    corr_tc_kernel(const TcArgs A, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stages = smem;
-  uint64_t* bar_mma = reinterpret_cast<uint64_t*>(stages + (size_t)A.nstage * A.stage_bytes);
+  // TMA: nraw raw stages after the operand stages (both 1024-byte multiples)
+  uint8_t* raw_st = stages + (size_t)A.nstage * A.stage_bytes;
+  uint64_t* bar_mma =
+      reinterpret_cast<uint64_t*>(raw_st + (TMA ? (size_t)A.nraw * A.raw_stage : 0));
   uint64_t* bar_acc = bar_mma + A.nstage;
   uint64_t* bar_drain = bar_acc + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_drain + 1);
+  uint64_t* bar_raw = bar_drain + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_raw + (TMA ? A.nraw : 0));
   int2* vbuf = reinterpret_cast<int2*>(tmem_slot + 4);
   TcTab tab{};
   if constexpr (MODE == 1) {
@@ -419,6 +434,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     mbar_init(&bar_acc[0], 1);
     mbar_init(&bar_acc[1], 1);
     mbar_init(bar_drain, 1);
+    if constexpr (TMA)
+      for (int i = 0; i < A.nraw; ++i) mbar_init(&bar_raw[i], 1);
     fence_mbar_init();
   }
   tc_fence_before();
@@ -439,9 +456,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   TcFillPlan plan{};
   if (planned) tc_fill_plan(A, plan);
   bool ok = true;
+  // TMA: item `item`'s raw bytes (ppk packets x nant x csf channels x 4 bytes
+  // of one chgroup page) into raw stage item % nraw, by thread 0
+  int issued = 0, it_stop = n_items;
+  auto issue_raw = [&](int item) {
+    const int lu = item / A.n_chunks, q = item % A.n_chunks;
+    int g, f, s;
+    tc_unit_coords(A, u_begin + lu, g, f, s);
+    const int r = item % A.nraw;
+    mbar_arrive_expect_tx(&bar_raw[r], (uint32_t)(A.ppk * A.nant * A.csf * 4));
+    tma_load_4d(raw_st + (size_t)r * A.raw_stage, &tmap, s * A.csf * 4, 0,
+                f * A.ppfv + q * A.ppk, g, &bar_raw[r]);
+  };
+  if constexpr (TMA) {
+    if (tid == 0)
+      for (; issued < A.nraw - 1 && issued < n_items; ++issued) issue_raw(issued);
+  }
   // the raw words of the next item are loaded while this one is unpacked
   uint4 pre[TC_PRE];
-  if (vec && n_items > 0) {
+  if (!TMA && vec && n_items > 0) {
     int g0, f0, s0;
     tc_unit_coords(A, u_begin, g0, f0, s0);
     if (planned) tc_load_planned(A, plan, g0, f0, s0, 0, pre);
@@ -456,9 +489,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     const int slot = it % A.nstage;
     bool w_ok = true;
     if (it >= A.nstage) w_ok = mbar_wait(&bar_mma[slot], (uint32_t)((it / A.nstage - 1) & 1));
-    if (!__syncthreads_and(w_ok)) { ok = false; break; }
+    if constexpr (TMA)
+      w_ok = w_ok && mbar_wait(&bar_raw[it % A.nraw], (uint32_t)((it / A.nraw) & 1));
+    if (!__syncthreads_and(w_ok)) { ok = false; it_stop = it; break; }
     uint8_t* st = stages + (size_t)slot * A.stage_bytes;
-    if (vec) {
+    if constexpr (TMA) {
+      // every thread is done with item it - 1: its raw stage takes item
+      // it + nraw - 1
+      if (tid == 0 && issued < n_items) issue_raw(issued++);
+      const uint8_t* rs = raw_st + (size_t)(it % A.nraw) * A.raw_stage;
+      const int n_w = A.nant * (A.kc / 16);
+      uint4 cur[TC_PRE];
+#pragma unroll
+      for (int r = 0; r < TC_PRE; ++r)
+        if (tid + r * TC_THREADS < n_w) cur[r] = *reinterpret_cast<const uint4*>(rs + plan.lds[r]);
+      tc_store_planned(A, plan, st, cur);
+    } else if (vec) {
       uint4 cur[TC_PRE];
 #pragma unroll
       for (int r = 0; r < TC_PRE; ++r) cur[r] = pre[r];
@@ -491,7 +537,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
     if (q == A.n_chunks - 1 && lu >= 1) {
       const int pl = lu - 1;
       const bool a_ok = mbar_wait(&bar_acc[pl & 1], (uint32_t)((pl >> 1) & 1));
-      if (!__syncthreads_and(a_ok)) { ok = false; break; }
+      if (!__syncthreads_and(a_ok)) { ok = false; it_stop = it; break; }
       tc_fence_after();
       int pg, pf, ps;
       tc_unit_coords(A, u_begin + pl, pg, pf, ps);
@@ -512,10 +558,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) corr_tc_kernel(const TcArgs A) 
   }
   if (!ok) {
     if (tid == 0) dsb_flag(A.status, DSB_E_TIMEOUT);
-    // Drain every MMA this CTA issued before releasing tensor memory.
+    // Drain every MMA this CTA issued before releasing tensor memory, and
+    // every tensor copy still writing into its shared memory.
     if (tid == 0) {
       umma_commit(bar_drain);
       mbar_wait(bar_drain, 0u);
+      if constexpr (TMA)
+        for (int i = it_stop; i < issued; ++i)
+          mbar_wait(&bar_raw[i % A.nraw], (uint32_t)((i / A.nraw) & 1));
     }
   }
   tc_fence_before();
@@ -801,7 +851,78 @@ int tc_plan(TcArgs& A, int mode) {
   const int budget = TC_SMEM_BUDGET - extra - 1024 - 256;
   A.nstage = std::min(4, budget / A.stage_bytes);
   if (A.nstage < 2) return DSB_E_UNSUPPORTED;
+  // raw staging by TMA when a chunk is whole packets of 16-byte channel runs
+  // and four raw stages still leave two operand stages
+  A.tma = 0;
+  if ((A.csf % 4) == 0 && (A.nchan % 4) == 0 && ((A.kc / 4) % A.csf) == 0 && A.nant <= 256) {
+    A.ppk = (A.kc / 4) / A.csf;
+    A.raw_stage = (A.ppk * A.nant * A.csf * 4 + 1023) & ~1023;
+    A.nraw = 4;
+    const int ns = std::min(4, (budget - A.nraw * A.raw_stage) / A.stage_bytes);
+    if (ns >= 2) {
+      A.tma = 1;
+      A.nstage = ns;
+    }
+  }
   return DSB_OK;
+}
+
+// The driver's tensor-map encoder, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// The raw pages as a 4-D uint8 tensor (channel bytes, antenna, packet,
+// chgroup) with one item's box (csf channels x 4 bytes, every antenna, ppk
+// packets, one chgroup).  False if it cannot be encoded (the kernel then
+// loads the raw words itself).
+bool tc_raw_tmap(const TcArgs& A, CUtensorMap* m) {
+  auto fn = tmap_encoder();
+  if (!fn) return false;
+  const cuuint64_t row = (cuuint64_t)A.nchan * 4;
+  const cuuint64_t pkt = row * (cuuint64_t)A.nant;
+  const cuuint64_t gs = A.n_chgroup > 1 ? (cuuint64_t)A.raw_g_stride : pkt * (cuuint64_t)A.npkt;
+  const cuuint64_t dims[4] = {row, (cuuint64_t)A.nant, (cuuint64_t)A.npkt,
+                              (cuuint64_t)A.n_chgroup};
+  const cuuint64_t strides[3] = {row, pkt, gs};
+  const cuuint32_t box[4] = {(cuuint32_t)(A.csf * 4), (cuuint32_t)A.nant, (cuuint32_t)A.ppk, 1u};
+  const cuuint32_t es[4] = {1u, 1u, 1u, 1u};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(A.raw), dims, strides, box,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launch corr_tc_kernel<MODE, TMA> on the planned geometry.
+template <int MODE>
+int tc_launch(TcArgs& A, int grid, cudaStream_t stream) {
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  if (A.tma && !tc_raw_tmap(A, &tmap)) A.tma = 0;
+  const int raw = A.tma ? A.nraw * A.raw_stage : 0;
+  const int smem = std::max(A.nstage * A.stage_bytes + raw + 1024 + 256 + tc_extra_bytes(A, MODE),
+                            TC_MIN_SMEM);
+  if (A.tma) {
+    cudaFuncSetAttribute(corr_tc_kernel<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
+    corr_tc_kernel<MODE, true><<<grid, TC_THREADS, smem, stream>>>(A, tmap);
+  } else {
+    cudaFuncSetAttribute(corr_tc_kernel<MODE, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    corr_tc_kernel<MODE, false><<<grid, TC_THREADS, smem, stream>>>(A, tmap);
+  }
+  return launch_status();
 }
 
 }  // namespace
@@ -914,12 +1035,8 @@ int dsb_corr_tc(const void* raw, long long raw_g_stride, int n_chgroup, int npkt
   A.status = status;
   int rc = tc_plan(A, 0);
   if (rc) return rc;
-  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256, TC_MIN_SMEM);
-  cudaFuncSetAttribute(corr_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int n_units = n_chgroup * A.n_fv * A.ceff;
-  int grid = std::min(n_units, max_ctas > 0 ? max_ctas : num_sms());
-  corr_tc_kernel<0><<<grid, TC_THREADS, smem, stream>>>(A);
-  return launch_status();
+  return tc_launch<0>(A, std::min(n_units, max_ctas > 0 ? max_ctas : num_sms()), stream);
 }
 
 int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int npkt, int nant,
@@ -941,13 +1058,8 @@ int dsb_corr_tc_grid(const void* raw, long long raw_g_stride, int n_chgroup, int
   A.status = status;
   int rc = tc_plan(A, 1);
   if (rc) return rc;
-  const int smem = std::max(A.nstage * A.stage_bytes + 1024 + 256 + tc_extra_bytes(A, 1),
-                           TC_MIN_SMEM);
-  cudaFuncSetAttribute(corr_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int n_units = n_chgroup * A.n_fv * A.ceff;
-  int grid = std::min(n_units, max_ctas > 0 ? max_ctas : num_sms());
-  corr_tc_kernel<1><<<grid, TC_THREADS, smem, stream>>>(A);
-  return launch_status();
+  return tc_launch<1>(A, std::min(n_units, max_ctas > 0 ? max_ctas : num_sms()), stream);
 }
 
 }  // extern "C"

@@ -113,6 +113,24 @@ DSB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// Arrive on `bar` expecting `bytes` of asynchronous copies in this phase.
+DSB_DEV void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// One 4-D tile of a tensor map (this GPU's global memory; no multicast) into
+// this CTA's shared memory, completing on `bar`.  The innermost coordinate
+// times the element size must be a multiple of 16 bytes.
+DSB_DEV void tma_load_4d(void* dst, const void* tmap, int x, int y, int z, int w,
+                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // tcgen05 (5th-generation tensor core, accumulators in tensor memory)
 // ---------------------------------------------------------------------------
