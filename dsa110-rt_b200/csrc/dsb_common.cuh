@@ -280,14 +280,21 @@ DSB_DEV void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: 
 // ---------------------------------------------------------------------------
 // int4 helpers: four packed (real | imag << 4) complex samples per 32-bit word
 // ---------------------------------------------------------------------------
+// Four two's-complement nibbles sign-extended to int8 bytes without byte
+// SIMD: a nibble's bit 3 times 0x1E fills bits 4-7 of its own byte (0x08 *
+// 0x1E = 0xF0, no carry into the next byte), and as those bits are clear in
+// the nibble, adding is or-ing: one multiply-add after two masks.
 DSB_DEV uint32_t nib_lo_s8x4(uint32_t w) {
-  uint32_t lo = w & 0x0F0F0F0Fu;
-  return __vsub4(lo ^ 0x08080808u, 0x08080808u);
+  return (w & 0x08080808u) * 0x1Eu + (w & 0x0F0F0F0Fu);
 }
 DSB_DEV uint32_t nib_hi_s8x4(uint32_t w) {
-  uint32_t hi = (w >> 4) & 0x0F0F0F0Fu;
-  return __vsub4(hi ^ 0x08080808u, 0x08080808u);
+  const uint32_t h = (w >> 4) & 0x0F0F0F0Fu;
+  return (h & 0x08080808u) * 0x1Eu + h;
 }
-DSB_DEV uint32_t neg_s8x4(uint32_t v) { return __vsub4(0u, v); }
+// Byte-wise 0 - v (v in -8..7 per byte): 0x80 - (v & 0x7F) cannot borrow
+// across bytes, and xor-ing the complement of v's top bit restores the sign.
+DSB_DEV uint32_t neg_s8x4(uint32_t v) {
+  return (0x80808080u - (v & 0x7F7F7F7Fu)) ^ (~v & 0x80808080u);
+}
 
 DSB_DEV int upper_bls(int a, int b) { return a * (a + 1) / 2 + b; }
