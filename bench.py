@@ -1020,6 +1020,7 @@ def main():
     torch.cuda.set_device(dev)
     e, n = synth.t_layout(cfg.nant, seed=11)
     pipe = SearchPipeline(cfg, e, n, device=dev)
+    resident_bytes = torch.cuda.memory_allocated(dev)
     pipe.skip_warmup()
     # one device-resident block (19.3 GB, larger than L2) for the timed run
     blocks = [synth.random_block_device(band=cfg.band, nant=cfg.nant, npkt=cfg.npkt_block,
@@ -1146,6 +1147,7 @@ def main():
                           else "int8 (correlator) / f32"), "data": "synthetic (seeded 4-bit Gaussian "
                 "voltages, sigma 3, T-layout antennas)", "config": workload_desc(a.workload, cfg),
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+                "pipeline_resident_bytes": int(resident_bytes),
                 "rooflines_per_kernel": roofs,
                 "cpu_baseline": cb,
                 "stages_ms_per_step": {k: round(v["total_ms"] / a.steps, 3)
