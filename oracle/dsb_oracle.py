@@ -243,6 +243,23 @@ def corr_fast(re: np.ndarray, im: np.ndarray, *, t_int: int, csf: int = 1,
     I = im.astype(np.float64).reshape(nchan, nt, npol, n_fv, ppfv, nant)
     R = R.transpose(3, 0, 2, 1, 4, 5).reshape(n_fv, nchan, npol, nt * ppfv, nant)
     I = I.transpose(3, 0, 2, 1, 4, 5).reshape(n_fv, nchan, npol, nt * ppfv, nant)
+    if fuse_stokes_i:
+        # Stokes I and the channel sum folded into the contraction: the
+        # products of a subband's channels and both pols summed by one matmul
+        # over K = csf * 2p * 2t * ppfv (exact: integer sums far below 2**53)
+        ceff = nchan // csf
+        Rk = R.reshape(n_fv, ceff, csf * npol * nt * ppfv, nant)
+        Ik = I.reshape(n_fv, ceff, csf * npol * nt * ppfv, nant)
+        step = max(1, 4096 // max(1, ceff))
+        for f0 in range(0, n_fv, step):
+            f1 = min(n_fv, f0 + step)
+            r, i = Rk[f0:f1], Ik[f0:f1]
+            rt, it = np.swapaxes(r, -1, -2), np.swapaxes(i, -1, -2)
+            vre = rt @ r + it @ i            # (f, ceff, nant, nant): [m, n]
+            vim = rt @ i - it @ r
+            out_re[f0:f1] = np.rint(vre[..., b_idx, a_idx]).astype(np.int64).transpose(0, 2, 1)
+            out_im[f0:f1] = np.rint(vim[..., b_idx, a_idx]).astype(np.int64).transpose(0, 2, 1)
+        return out_re, out_im
     step = max(1, 64 // max(1, nchan // 16))
     for f0 in range(0, n_fv, step):
         f1 = min(n_fv, f0 + step)
