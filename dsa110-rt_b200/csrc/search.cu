@@ -475,11 +475,20 @@ __device__ __noinline__ int2 det_sample(const BoxSums<K> d, const L2Samples l2, 
 // slots 0 .. MAXW-1 (MAXW register moves per DB steps), so the ring indices
 // are compile-time constants while the unrolled code stays DB steps long.
 // The inputs are prefetched DB steps ahead, one load per step.
-// DB = 16 steps per block; inputs are prefetched DP = 8 steps ahead (a
-// rolling set of DP registers), so that ring and prefetch fit 128 registers
-// at MAXW 64: two CTAs per SM.
-constexpr int DET_DB = 16;
-constexpr int DET_DP = 8;
+// Boxcars to 32 or 64 (MAXW 32, 64): DB = 16 steps per block, inputs
+// prefetched DP = 8 steps ahead (a rolling set of DP registers), so that ring
+// and prefetch fit 128 registers: two CTAs per SM.  Narrower boxcars keep a
+// short ring and run more CTAs per SM (three at 16: 80 registers, 16 steps
+// per block; four below: 64 registers, 8 steps per block, 4 ahead), whose
+// occupancy hides load latency better (at b16: 116 -> 96 ms per block of the
+// 512-DM 256^2 workload against two CTAs per SM).
+template <int LOGW>
+struct DetCfg {
+  // steps per block, prefetch depth, CTAs per SM (64 / 80 / 128 registers)
+  static constexpr int DB = LOGW >= 4 ? 16 : 8;
+  static constexpr int DP = LOGW >= 4 ? 8 : 4;
+  static constexpr int MINB = LOGW >= 5 ? 2 : (LOGW == 4 ? 3 : 4);
+};
 constexpr int DET_PF = 32;  // L2 prefetch distance (steps)
 
 DSB_DEV void prefetch_l2(const void* p) {
@@ -487,7 +496,7 @@ DSB_DEV void prefetch_l2(const void* p) {
 }
 
 template <int LOGW, typename T>
-__global__ void __launch_bounds__(256, 2) detect_kernel(const T* __restrict__ x, int n, int npix,
+__global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB) detect_kernel(const T* __restrict__ x, int n, int npix,
                                                      long long inner, long long f_stride,
                                                      long long t_stride,
                                                      const float* __restrict__ mask,
@@ -500,7 +509,7 @@ __global__ void __launch_bounds__(256, 2) detect_kernel(const T* __restrict__ x,
   constexpr int MAXW = 1 << LOGW;
   constexpr int K = LOGW + 1;
   constexpr int PL = MAXW / 2;
-  constexpr int DB = DET_DB, DP = DET_DP;
+  constexpr int DB = DetCfg<LOGW>::DB, DP = DetCfg<LOGW>::DP;
   constexpr int RS = MAXW + DB;  // ring registers
   static_assert(DB % DP == 0, "the prefetch set cycles within a block");
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
