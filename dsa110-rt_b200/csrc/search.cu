@@ -584,7 +584,10 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB) detect_kernel(const T
   for (int j = 0; j < DP; ++j) xin[j] = input(j);
   // the first steps produce no output (ta < t_base): prefixes only
   const int warm_end = t_base + MAXW;
-  for (int J0 = 0; J0 < total; J0 += DB) {
+  // blocks after the last output step (J = t_base + n_out - 1 + MAXW) feed
+  // nothing: the cell is done
+  const int out_end = t_base + n_out + MAXW;
+  for (int J0 = 0; J0 < total && J0 < out_end; J0 += DB) {
     if (J0 + DB <= warm_end && J0 + DB + DP - 1 - PL <= n) {
 #pragma unroll
       for (int j = 0; j < DB; ++j) {
@@ -604,17 +607,26 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB) detect_kernel(const T
       // prefetched input in range; the Layer-2 test only in the (rare)
       // blocks that hold this cell's next sample
       const T* nxt = cube + (long long)(J0 + DP - 1 - PL) * t_stride;
-      // L2 prefetch DET_PF steps ahead by one lane per warp (the warp's 32
-      // cells of a time are one 128-byte line), where still inside the cube
-      const bool pf = (threadIdx.x & 31) == 0 && J0 + DB - 1 + DET_PF - 1 - PL < n;
-      const T* pfp = cube + (long long)(J0 + DET_PF - 1 - PL) * t_stride;
+      // L2 prefetch DET_PF steps ahead, the block's DB lines in one
+      // instruction: lane j < DB takes step J0 + j's line of the warp (lane
+      // 0's cell), where still inside the cube
+      // (lane 0's cell is always active when any lane of its warp is; the
+      // branch is warp-uniform, so the warp's live lanes are all here)
+      {
+        const unsigned lane = threadIdx.x & 31;
+        const long long n_live = inner - (e - lane);  // lanes of this warp with a cell
+        const unsigned live = n_live >= 32 ? 0xffffffffu : ((1u << n_live) - 1u);
+        const T* cube0 = reinterpret_cast<const T*>(
+            __shfl_sync(live, reinterpret_cast<unsigned long long>(cube), 0));
+        const int ipf = J0 + (int)lane + DET_PF - 1 - PL;
+        if (lane < (unsigned)DB && ipf < n) prefetch_l2(cube0 + (long long)ipf * t_stride);
+      }
       auto steady = [&](auto with_samples) {
 #pragma unroll
         for (int j = 0; j < DB; ++j) {
           run += (double)(xin[j % DP] * mval);
           ring[MAXW + j] = (float)run;
           xin[j % DP] = ldf<T>(nxt, (long long)j * t_stride);
-          if (pf) prefetch_l2(pfp + (long long)j * t_stride);
           output(j, J0 + j - MAXW, with_samples);
         }
       };
