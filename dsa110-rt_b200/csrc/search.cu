@@ -2,6 +2,10 @@
 // noise estimate, and the FP64 uv-cell geometry kernel (sm_100a).
 #include "dsb_common.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
 #include <type_traits>
 
 #include <algorithm>
@@ -662,6 +666,188 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB) detect_kernel(const T
   }
 }
 
+// The same detector with the cube staged in shared memory by TMA (float
+// cubes whose fine DMs are whole warps of cells: npix a multiple of 32).
+// Each warp owns 32 consecutive cells of one fine DM and a ring of DET_NST
+// shared-memory stages, each one block of DB times x 32 cells (one 3-D tile
+// of the cube's tensor map, completing on the stage's mbarrier).  Lane 0
+// issues block b + DET_NST - 1 when the warp starts block b, so the copies
+// run DET_NST - 1 blocks ahead with no registers held for them and no barrier
+// wider than the warp; times outside [0, n) arrive as zeros.  The marching,
+// the screen and the rare paths are detect_kernel's, so the outputs are the
+// same bits.  A wait that does not complete within DSB_SPIN_LIMIT polls sets
+// count[1] to a quiet NaN (DET_TIMEOUT_BITS) and ends the warp after waiting,
+// again bounded, for its copies in flight.
+constexpr int DET_NST = 4;
+constexpr int DET_TIMEOUT_BITS = 0x7fc00000;
+
+template <int LOGW>
+constexpr int det_tma_smem() {
+  return 8 * DET_NST * DetCfg<LOGW>::DB * 32 * 4 + 8 * DET_NST * 8;
+}
+
+template <int LOGW>
+__global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
+    detect_tma_kernel(const __grid_constant__ CUtensorMap tmap, int n, int npix, long long inner,
+                      const float* __restrict__ mask, long long mask_f_stride,
+                      const float* __restrict__ sig_f, const float* __restrict__ sinv,
+                      int t_base, int n_out, float thr, DetCand* __restrict__ cands, int cap,
+                      int pix_off, int* __restrict__ count, const L2Samples l2) {
+  constexpr int MAXW = 1 << LOGW;
+  constexpr int K = LOGW + 1;
+  constexpr int PL = MAXW / 2;
+  constexpr int DB = DetCfg<LOGW>::DB;
+  constexpr int RS = MAXW + DB;  // ring registers
+  constexpr int SB = DB * 32;    // floats per stage
+  extern __shared__ __align__(128) uint8_t det_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* stages = reinterpret_cast<float*>(det_smem) + warp * DET_NST * SB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(det_smem + 8 * DET_NST * SB * 4) + warp * DET_NST;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // npix % 32 == 0, so inner is whole warps: a warp is in or out as a whole
+  if (e >= inner) return;
+  int s_i = 0, s_end = 0, s_t = 0x7fffffff;
+  const int eg = (int)e + pix_off;
+  if (l2.out) {
+    const int gb = pix_off / 256 + (int)blockIdx.x;
+    int lo = __ldg(l2.off + gb);
+    s_end = __ldg(l2.off + gb + 1);
+    while (lo < s_end && __ldg(&l2.ent[lo].x) < eg) ++lo;
+    s_i = lo;
+    if (s_i < s_end && __ldg(&l2.ent[s_i].x) == eg) s_t = __ldg(&l2.ent[s_i].y);
+  }
+  const long long fidx = e / npix, p = e % npix;
+  const int p0 = (int)(p - lane);  // the warp's first cell (a multiple of 32)
+  float mval = mask ? mask[fidx * mask_f_stride + p] : 1.0f;
+  if (sig_f) mval = mval / sig_f[fidx];
+  float tau[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const float lv = thr / sinv[k];
+    tau[k] = lv - fabsf(lv) * 0x1p-20f;
+  }
+  float ring[RS];
+#pragma unroll
+  for (int q = 0; q < RS; ++q) ring[q] = 0.f;
+  double run = 0.0;
+  float last = 0.f;
+  const int total = n + MAXW;
+  const int warm_end = t_base + MAXW;
+  const int out_end = t_base + n_out + MAXW;
+  const int n_blk = (min(total, out_end) + DB - 1) / DB;
+  // block b holds inputs x[b DB - 1 - PL .. b DB + DB - 2 - PL]; a block with
+  // none inside the cube completes its phase with no copy (its inputs are
+  // never read)
+  auto issue = [&](int b) {
+    uint64_t* bar = bars + b % DET_NST;
+    const int y0 = b * DB - 1 - PL;
+    if (y0 < n && y0 + DB > 0) {
+      mbar_arrive_expect_tx(bar, SB * 4);
+      tma_load_3d(stages + (b % DET_NST) * SB, &tmap, p0, y0, (int)fidx, bar);
+    } else {
+      mbar_arrive(bar);
+    }
+  };
+  if (lane == 0) {
+    for (int s = 0; s < DET_NST; ++s) mbar_init(bars + s, 1);
+    fence_mbar_init();
+    for (int b = 0; b < min(DET_NST - 1, n_blk); ++b) issue(b);
+  }
+  __syncwarp();
+  auto output = [&](int j, int ta, auto with_samples) {
+    BoxSums<K> d;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int w = 1 << k;
+      const int off = PL - w / 2;
+      d.v[k] = ring[j + off + w] - ring[j + off];
+    }
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) hit |= d.v[k] > tau[k];
+    if (hit) det_emit<K>(d, sinv, thr, ta - t_base, (int)e + pix_off, cands, cap, count);
+    if (decltype(with_samples)::value && ta - t_base == s_t) {
+      const int2 r = det_sample<K>(d, l2, s_i, s_end, eg, ta - t_base);
+      s_i = r.x;
+      s_t = r.y;
+    }
+  };
+  int b = 0;
+  bool ok = true;
+  for (; b < n_blk; ++b) {
+    const int J0 = b * DB;
+    // every lane is done with block b - 1, whose stage takes block
+    // b + DET_NST - 1 (generic-proxy reads before the async-proxy write)
+    __syncwarp();
+    if (lane == 0 && b + DET_NST - 1 < n_blk) {
+      fence_proxy_async_smem();
+      issue(b + DET_NST - 1);
+    }
+    if (!__all_sync(0xffffffffu,
+                    mbar_wait(bars + b % DET_NST, (uint32_t)((b / DET_NST) & 1)))) {
+      ok = false;
+      break;
+    }
+    // input of step J0 + j (x[J0 + j - 1 - PL]) at sx[32 j]
+    const float* sx = stages + (b % DET_NST) * SB + lane;
+    if (J0 + DB <= warm_end && J0 + DB - 2 - PL < n) {
+#pragma unroll
+      for (int j = 0; j < DB; ++j) {
+        const int J = J0 + j;
+        float v = 0.f;
+        if (J > PL) {
+          run += (double)(sx[32 * j] * mval);
+          v = (float)run;
+        }
+        ring[MAXW + j] = v;
+      }
+      last = ring[MAXW + DB - 1];
+    } else if (J0 >= PL + 1 && J0 + DB - 1 <= PL + n && J0 - MAXW >= t_base &&
+               J0 + DB - 1 - MAXW < t_base + n_out) {
+      auto steady = [&](auto with_samples) {
+#pragma unroll
+        for (int j = 0; j < DB; ++j) {
+          run += (double)(sx[32 * j] * mval);
+          ring[MAXW + j] = (float)run;
+          output(j, J0 + j - MAXW, with_samples);
+        }
+      };
+      if ((unsigned)(s_t - (J0 - MAXW - t_base)) < (unsigned)DB)
+        steady(std::true_type{});
+      else
+        steady(std::false_type{});
+      last = ring[MAXW + DB - 1];
+    } else {
+#pragma unroll
+      for (int j = 0; j < DB; ++j) {
+        const int J = J0 + j;
+        if (J < total) {
+          float v;
+          if (J <= PL) {
+            v = 0.f;
+          } else if (J <= PL + n) {
+            run += (double)(sx[32 * j] * mval);
+            last = (float)run;
+            v = last;
+          } else {
+            v = last;
+          }
+          ring[MAXW + j] = v;
+          const int ta = J - MAXW;
+          if (ta >= t_base && ta < t_base + n_out) output(j, ta, std::true_type{});
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < MAXW; ++q) ring[q] = ring[q + DB];
+  }
+  if (!ok && lane == 0) {
+    atomicMax(count + 1, DET_TIMEOUT_BITS);
+    for (int c = b; c < min(n_blk, b + DET_NST - 1); ++c)
+      mbar_wait(bars + c % DET_NST, (uint32_t)((c / DET_NST) & 1));
+  }
+}
+
 // ===========================================================================
 // Layer-1 sigma-clipped std (noise_norm/layer1.py:53-125): one block per
 // row, rows of at most L1_MAX samples; bitonic sort, then the clipping
@@ -827,6 +1013,67 @@ __global__ void __launch_bounds__(L1_THREADS) clipped_std_kernel(const L1Src src
     if (src.nonpos_to_one && !(o > 0.f)) o = 1.f;
     out[blockIdx.x] = o;
   }
+}
+
+// The driver's tensor-map encoder, looked up once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 det_tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* q = nullptr;
+    cudaDriverEntryPointQueryResult r;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &r) ==
+            cudaSuccess &&
+        r == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(q);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// The float cube as a 3-D tensor (cell, time, fine DM) with one detector
+// block's box (32 cells x db times x 1).  False when the layout does not
+// allow it (the caller then runs detect_kernel): npix a multiple of 32, the
+// base 16-byte aligned, the strides whole 16-byte units.
+bool det_cube_tmap(const float* x, int n, int n_f, int npix, long long f_stride,
+                   long long t_stride, int db, CUtensorMap* m) {
+  if (npix % 32 || (reinterpret_cast<uintptr_t>(x) & 15) || t_stride % 4 || t_stride < npix ||
+      (n_f > 1 && (f_stride % 4 || f_stride < (long long)n * t_stride)))
+    return false;
+  auto fn = det_tmap_encoder();
+  if (!fn) return false;
+  const long long fs = n_f > 1 ? f_stride : (long long)n * t_stride;
+  const cuuint64_t dims[3] = {(cuuint64_t)npix, (cuuint64_t)n, (cuuint64_t)n_f};
+  const cuuint64_t strides[2] = {(cuuint64_t)t_stride * 4, (cuuint64_t)fs * 4};
+  const cuuint32_t box[3] = {32u, (cuuint32_t)db, 1u};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(x), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int LOGW>
+int det_tma_launch(const float* x, int n, int n_f, int npix, long long f_stride,
+                   long long t_stride, const float* mask, long long mask_f_stride,
+                   const float* sig_f, const float* sinv, int t_base, int n_out, float thr,
+                   DetCand* c, int cap, int pix_off, int* count, const L2Samples& l2,
+                   cudaStream_t stream, bool* done) {
+  *done = false;
+  CUtensorMap tm;
+  memset(&tm, 0, sizeof(tm));
+  if (!det_cube_tmap(x, n, n_f, npix, f_stride, t_stride, DetCfg<LOGW>::DB, &tm)) return DSB_OK;
+  constexpr int smem = det_tma_smem<LOGW>();
+  if (cudaFuncSetAttribute(detect_tma_kernel<LOGW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem) != cudaSuccess)
+    return DSB_E_CUDA;
+  const long long inner = (long long)n_f * npix;
+  const unsigned grid = (unsigned)((inner + 255) / 256);
+  detect_tma_kernel<LOGW><<<grid, 256, smem, stream>>>(tm, n, npix, inner, mask, mask_f_stride,
+                                                       sig_f, sinv, t_base, n_out, thr, c, cap,
+                                                       pix_off, count, l2);
+  *done = true;
+  return launch_status();
 }
 
 }  // namespace
@@ -1008,6 +1255,26 @@ int dsb_detect_sampled(const void* cube, int cube_f16, int n, int n_f, int npix,
   const long long inner = (long long)n_f * npix;
   const unsigned grid = (unsigned)((inner + 255) / 256);
   DetCand* c = (DetCand*)cands;
+  if (!cube_f16) {
+    // float cubes of whole-warp fine DMs: the TMA-staged form
+    bool done = false;
+    int rc = DSB_OK;
+#define DSB_DET_TMA(L)                                                                      \
+  rc = det_tma_launch<L>((const float*)cube, n, n_f, npix, f_stride, t_stride, mask,         \
+                         mask_f_stride, sig_f, sigma_inv, t_base, n_out, threshold, c, cap,  \
+                         pix_off, count, l2, stream, &done)
+    switch (log_maxw) {
+      case 0: DSB_DET_TMA(0); break;
+      case 1: DSB_DET_TMA(1); break;
+      case 2: DSB_DET_TMA(2); break;
+      case 3: DSB_DET_TMA(3); break;
+      case 4: DSB_DET_TMA(4); break;
+      case 5: DSB_DET_TMA(5); break;
+      case 6: DSB_DET_TMA(6); break;
+    }
+#undef DSB_DET_TMA
+    if (done || rc != DSB_OK) return rc;
+  }
 #define DSB_DET(L)                                                                        \
   do {                                                                                    \
     if (cube_f16)                                                                         \

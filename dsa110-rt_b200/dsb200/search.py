@@ -639,8 +639,18 @@ class CandidateBuffer:
     def reset(self):
         self.count.zero_()
 
+    # count[1] as the detector leaves it when one of its shared-memory
+    # staging copies did not complete within its bounded wait
+    TIMEOUT_BITS = 0x7fc00000
+
+    def _check_timeout(self, dropped: int) -> None:
+        if dropped == self.TIMEOUT_BITS:
+            raise _lib.DsbError("detector: a staging copy wait timed out (DSB_E_TIMEOUT)")
+
     def fetch(self) -> np.ndarray:
-        n = int(self.count[0].item())
+        cnt = self.count.cpu()
+        self._check_timeout(int(cnt[1]))
+        n = int(cnt[0])
         if n > self.capacity:
             raise _lib.DsbError(f"detector candidate buffer overflow ({n} > {self.capacity})")
         raw = self.buf[: 4 * n].cpu().numpy()
@@ -656,6 +666,7 @@ class CandidateBuffer:
         S/N among them lies below the selected ones; otherwise DsbError."""
         cnt = self.count.cpu()
         n, dropped = int(cnt[0]), int(cnt[1])
+        self._check_timeout(dropped)
         m = min(n, self.capacity)
         rec = self.buf[: 4 * m].view(m, 4)
         if n <= max(n_top, 0) or m == 0:

@@ -416,7 +416,10 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
  * keeps the bits of the largest S/N that was not written (0 when every entry
  * fit): a caller selecting the top entries knows its selection is exact
  * when that S/N lies below them.  count points at two ints, zeroed before
- * the launch. */
+ * the launch.  Float cubes whose npix is a multiple of 32 (16-byte aligned,
+ * strides in whole 16-byte units) are staged into shared memory by TMA with
+ * bounded waits: a wait that runs out leaves count[1] = 0x7fc00000 (a quiet
+ * NaN, above any S/N's bits), which the caller reads as DSB_E_TIMEOUT. */
 int dsb_detect(const void* cube, int cube_f16, int n, int n_f, int npix, long long f_stride,
                long long t_stride, const float* mask, long long mask_f_stride,
                const float* sig_f, int log_maxw, const float* sigma_inv, int t_base, int n_out,

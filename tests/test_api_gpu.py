@@ -197,13 +197,14 @@ def test_cumsum_boxcars_argmax_vs_reference(dev, golden_dir):
     np.testing.assert_array_equal(win.cpu().numpy(), owin)
 
 
-@pytest.mark.parametrize("log_w", [2, 4])
+@pytest.mark.parametrize("log_w", [2, 4, 6])
 @pytest.mark.parametrize("f16", [False, True])
 @pytest.mark.parametrize("hw", [(12, 10), (11, 9), (16, 16)])
 def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16, hw):
     """Candidates of the streaming detector == every cell above threshold of
     the padded cumsum + boxcar argmax, bit for bit, for even and odd pixel
-    counts and float or half cubes."""
+    counts and float or half cubes (float cubes of 16 x 16 x 3 = 768 cells
+    take the TMA-staged kernel, the others the register-prefetch one)."""
     from dsb200.search import CandidateBuffer, detect_cube
     rng = np.random.default_rng(10 + log_w)
     T, F = 70, 3
