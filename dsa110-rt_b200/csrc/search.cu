@@ -425,6 +425,9 @@ struct BoxSums {
   float v[K];
 };
 
+// Saturation level of the detector's candidate count (capacities are below it).
+constexpr int DET_COUNT_MAX = 1 << 30;
+
 // Exact strict-'>' winner over the widths (the lowest k wins ties) and, when
 // its S/N passes thr, one appended candidate.  Out of line: called only for
 // outputs the screen lets through.
@@ -444,7 +447,16 @@ __device__ __noinline__ void det_emit(const BoxSums<K> d, const float* __restric
     }
   }
   if (best > thr) {
-    const int slot = atomicAdd(count, 1);
+    // count[0] stops growing near DET_COUNT_MAX (above any capacity) instead
+    // of wrapping to negative slots when nearly every cell passes: once the
+    // buffer is full only the count's current value is read, and it is
+    // raised while below the saturation level (concurrent raises overshoot
+    // it by at most the resident threads)
+    int slot = __ldcg(count);
+    if (slot < cap)
+      slot = atomicAdd(count, 1);
+    else if (slot < DET_COUNT_MAX)
+      atomicAdd(count, 1);
     if (slot < cap)
       cands[slot] = DetCand{t_out, pix, best, win};
     else  // the largest S/N that did not fit (positive floats order as ints)
@@ -1242,7 +1254,8 @@ int dsb_detect_sampled(const void* cube, int cube_f16, int n, int n_f, int npix,
                        const float* sigma_inv, int t_base, int n_out, float threshold,
                        void* cands, int cap, int pix_off, int* count, const int* l2_off,
                        const void* l2_ent, float* l2_out, int l2_m, cudaStream_t stream) {
-  if (!cube || !sigma_inv || !cands || !count || n <= 0 || n_f <= 0 || npix <= 0 || cap < 0)
+  if (!cube || !sigma_inv || !cands || !count || n <= 0 || n_f <= 0 || npix <= 0 || cap < 0 ||
+      cap > DET_COUNT_MAX)
     return DSB_E_ARG;
   if (l2_out && (!l2_off || !l2_ent || l2_m <= 0 || pix_off < 0 || (pix_off % 256) != 0 ||
                  (reinterpret_cast<uintptr_t>(l2_ent) & 15)))

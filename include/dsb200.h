@@ -412,7 +412,9 @@ int dsb_boxcar_from_cs(const float* cs, long long inner, int width, int start, i
  * over the fine DMs), divided by sig_f[f] (the Layer-1 sigma) when sig_f is
  * non-null.  Every output cell with max S/N > threshold is appended to
  * cands (struct {int t, pix; float snr; int k;}, pix = e + pix_off); count[0]
- * counts them (entries past cap are counted, not written) and count[1]
+ * counts them (entries past cap are counted, not written; the count stops
+ * growing a little above 2^30, so it never wraps, and cap may not exceed
+ * 2^30) and count[1]
  * keeps the bits of the largest S/N that was not written (0 when every entry
  * fit): a caller selecting the top entries knows its selection is exact
  * when that S/N lies below them.  count points at two ints, zeroed before

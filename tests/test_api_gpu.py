@@ -230,6 +230,29 @@ def test_fused_detector_matches_cumsum_argmax(dev, log_w, f16, hw):
     assert have == want
 
 
+@pytest.mark.parametrize("hw", [(16, 16), (12, 10)])
+def test_detector_count_saturates_instead_of_wrapping(dev, hw):
+    """When nearly every cell passes the threshold the candidate count stops
+    near 2^30 instead of wrapping to negative slots: started just below the
+    saturation level, a launch with thousands of hits writes nothing and
+    leaves the count between 2^30 and 2^31 (both detector forms)."""
+    from dsb200.search import CandidateBuffer, detect_cube
+    rng = np.random.default_rng(5)
+    T, F = 24, 2
+    H, W = hw
+    x = (5.0 + rng.random(size=(T, F, H, W))).astype(np.float32)
+    sinv = torch.ones(3, dtype=torch.float32, device=dev)
+    buf = CandidateBuffer(dev, 64)
+    buf.buf.fill_(-7)
+    buf.count[0] = (1 << 30) - 3
+    detect_cube(torch.from_numpy(x).to(dev), log_max_width=2, sigma_inv=sinv, t_base=2,
+                n_out=T - 4, threshold=1.0, cands=buf)
+    cnt = buf.count.cpu().numpy()
+    assert (1 << 30) <= int(cnt[0]) < (1 << 31) - 1
+    assert bool((buf.buf == -7).all())
+    assert np.int32(cnt[1]).view(np.float32) > 1.0
+
+
 @pytest.mark.parametrize("cap", [1 << 16, 600, 300])
 def test_candidate_buffer_top_selection_is_exact_or_raises(dev, cap):
     """fetch_top(n) returns every entry whose S/N is at least the n-th
