@@ -305,6 +305,15 @@ struct ImgGeom {
   // S entries the combine's split int32 arrays hold
   static constexpr int SCAP = (N == 512) ? 24576 : BUF;
   static constexpr size_t BUFB = (size_t)(BUF > SCAP ? BUF : SCAP) * 8;
+  // 32-bit form: the fold reads compact tables that follow gmeta in its
+  // buffer (a nibble q | last << 3 per entry, [chunk][thread]; the first slot
+  // of each thread; the slots' column-buffer offsets n' P + w' as uint16),
+  // copied per image into the part of buf the column buffer leaves free
+  static constexpr int MAXC = MAXE / 8;                         // 8-entry chunks
+  static constexpr size_t GM_BYTES = (size_t)(MAXE / 4) * THREADS * 16;
+  static constexpr size_t FC_BYTES = (size_t)MAXC * THREADS * 4;
+  static constexpr size_t TS_BYTES = (size_t)((THREADS + 1 + 3) / 4) * 16;
+  static constexpr int MAX_SLOTS = LC * NC;
   static_assert(C1 * C1 == LC && R1 * R2 == N && R2 % R1 == 0, "unsupported size");
   static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
   static_assert((2 * P * 8) % 16 == 0, "row-pair regions must stay 16-byte aligned");
@@ -318,6 +327,8 @@ struct ImgGeom {
   static constexpr size_t SMEM = BUFB + (size_t)(N + R1 * R2 + C1 * C1) * 8 + IMG_MAX_G * 8 +
                                  (IMG_MAX_G + 1) * 4 + IMG_MAX_G * 4 + IMG_MAX_G * 4 + 16;
   static_assert(SMEM <= 227 * 1024, "shared memory of one CTA");
+  static_assert(!META32 || (size_t)BUF * 8 + FC_BYTES + (size_t)MAX_SLOTS * 2 <= BUFB,
+                "the fold's tables fit beside the column buffer");
 };
 
 // The 8 metadata entries of chunk c of this thread (entries 8c .. 8c + 7).
@@ -371,7 +382,17 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
   // this thread's S entries [sb, sb + sn), whole slots
   const int sb = __ldg(A.thr_b + tid);
   const int sn = __ldg(A.thr_b + tid + 1) - sb;
-  const bool bad_range = sn < 0 || sn > MAXE || sb < 0 || sb + sn > A.n_s;
+  // 32-bit form: this thread's first slot and the number of slots (the
+  // fold's compact tables after gmeta)
+  int sl0 = 0, n_sl = 0;
+  if constexpr (Gm::META32) {
+    const int* ts = reinterpret_cast<const int*>(reinterpret_cast<const uint8_t*>(A.gmeta) +
+                                                 Gm::GM_BYTES + Gm::FC_BYTES);
+    sl0 = __ldg(ts + tid);
+    n_sl = __ldg(ts + THREADS);
+  }
+  const bool bad_range = sn < 0 || sn > MAXE || sb < 0 || sb + sn > A.n_s ||
+                         n_sl < 0 || n_sl > Gm::MAX_SLOTS || sl0 < 0 || sl0 > n_sl;
   bool bad_base = false;  // each chgroup's run: whole 64-entry pairs of chunks
   for (int g = tid; g <= A.G; g += THREADS) bad_base |= (A.cell_base[g] & 63) != 0;
   if (__syncthreads_or(bad_range || bad_base)) {
@@ -570,6 +591,19 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       tmem_st_wait();
     }
     __syncthreads();  // S is read: buf is free for the passes
+    if constexpr (Gm::META32) {
+      // the fold's compact tables into the part of buf past the column buffer
+      // (the combine's S arrays overlapped it): this thread's nibble words,
+      // and every slot's offset (16-byte copies; slot_off is padded to 8)
+      uint32_t* s_code = reinterpret_cast<uint32_t*>(buf + Gm::BUF);
+      const uint8_t* gt = reinterpret_cast<const uint8_t*>(A.gmeta) + Gm::GM_BYTES;
+      const uint32_t* g_code = reinterpret_cast<const uint32_t*>(gt);
+      for (int c = 0; c < nch; ++c) s_code[c * THREADS + tid] = __ldg(g_code + c * THREADS + tid);
+      const uint4* g_slot = reinterpret_cast<const uint4*>(gt + Gm::FC_BYTES + Gm::TS_BYTES);
+      uint4* s_slot4 = reinterpret_cast<uint4*>(s_code + Gm::MAXC * THREADS);
+      for (int i = tid; i < (n_sl + 7) / 8; i += THREADS) s_slot4[i] = __ldg(g_slot + i);
+      __syncthreads();
+    }
 
     for (int p = 0; p < FOLD; ++p) {
       // ---- 2a. fold S into the occupied slots (n', col) of buf: each slot's
@@ -582,6 +616,40 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       auto fold = [&](auto pass) {
         constexpr unsigned PP = decltype(pass)::value;
         float2 acc = make_float2(0.f, 0.f);
+        if constexpr (Gm::META32) {
+          // compact tables in shared memory: one nibble word per chunk, and
+          // the offset of each of this thread's slots, in order
+          const uint32_t* s_code = reinterpret_cast<const uint32_t*>(buf + Gm::BUF);
+          const uint16_t* s_soff = reinterpret_cast<const uint16_t*>(s_code + Gm::MAXC * THREADS);
+          int si = sl0;
+          for (int c = 0; c < nch; ++c) {
+            const uint32_t cw = s_code[c * THREADS + tid];
+            uint32_t r[16];
+            tmem_ld16_wait(tbase + 16 * c, r);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              if (8 * c + j < sn) {
+                const unsigned code = (cw >> (4 * j)) & 15u;
+                float2 v = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
+                if constexpr (PP != 0) {
+                  // W_8^k = i^(k >> 1) x (W_8 if k is odd), k = q p mod 8
+                  const unsigned k = ((code & 7u) * PP) & 7u;
+                  if constexpr (PP & 1u) {
+                    if (k & 1u) v = cmul_w8(v);
+                  }
+                  v = crot_rt(v, k >> 1);
+                }
+                acc = cadd(acc, v);
+                if (code & 8u) {
+                  const unsigned off = s_soff[si++];
+                  if (DSB_INB(off, Gm::BUF, A.status)) buf[off] = acc;
+                  acc = make_float2(0.f, 0.f);
+                }
+              }
+            }
+          }
+          return;
+        }
         unsigned md_next[8];
         load_meta8<N>(gmeta, 0, tid, md_next);
         for (int c = 0; c < nch; ++c) {

@@ -211,6 +211,23 @@ class ImageTables:
     meta_bits: int = 16     # 16: w' | n' << 7 | q << 13 | last << 15 (uint16);
     #                         32: w' | n' << 8 | q << 14 | last << 17 | packed << 18 |
     #                             parity << 19 (uint32, rotation bits in the entry)
+    # 32-bit form only: the fold's compact tables, which the device buffer of
+    # gmeta carries right after gmeta itself (see fold_bytes)
+    fold_code: Optional[np.ndarray] = None   # (max_entries / 8, threads) uint32: entry i's
+    #                                          nibble q | last << 3 at bits 4 (i % 8)
+    thr_slot: Optional[np.ndarray] = None    # (threads + 1) int32: first slot of each thread
+    slot_off: Optional[np.ndarray] = None    # (slots, padded to 8) uint16: n' * (N/2 + 2) + w'
+
+    def gmeta_device_bytes(self) -> np.ndarray:
+        """The bytes of the kernel's gmeta buffer: gmeta, then (32-bit form)
+        fold_code, thr_slot padded to 16 bytes and slot_off."""
+        parts = [np.ascontiguousarray(self.gmeta).view(np.uint8).reshape(-1)]
+        if self.fold_code is not None:
+            ts = np.zeros(-(-self.thr_slot.size // 4) * 4, np.int32)
+            ts[:self.thr_slot.size] = self.thr_slot
+            parts += [self.fold_code.view(np.uint8).reshape(-1), ts.view(np.uint8),
+                      self.slot_off.view(np.uint8)]
+        return np.concatenate(parts)
 
 
 def image_geometry(N: int) -> dict:
@@ -302,6 +319,7 @@ def build_image_tables(pats, N: int) -> ImageTables:
     idx = np.arange(n_s) - thr_b[owner]
     parity = (s_u + s_w) & 1
     srot = np.zeros(n_thr, np.uint64)
+    fold_code = thr_slot = slot_off = None
     if mbits == 16:
         epv = 8
         gmeta = np.zeros((cap // epv, n_thr, epv), np.uint16)
@@ -314,6 +332,16 @@ def build_image_tables(pats, N: int) -> ImageTables:
         gmeta = np.zeros((cap // epv, n_thr, epv), np.uint32)
         gmeta[idx // epv, owner, idx % epv] = (s_wp | (s_n << 8) | (s_q << 14) | (last << 17) |
                                                (s_pk << 18) | (parity << 19)).astype(np.uint32)
+        # the fold's compact form: a nibble per entry (q | last << 3), and the
+        # slots in S order with their column-buffer offsets (each thread's
+        # slots are consecutive, from thr_slot[t])
+        fold_code = np.zeros((cap // 8, n_thr), np.uint32)
+        np.bitwise_or.at(fold_code, (idx // 8, owner),
+                         ((s_q | (last << 3)) << (4 * (idx % 8))).astype(np.uint32))
+        thr_slot = np.searchsorted(starts, thr_b).astype(np.int32)
+        offs = s_n[starts] * (NC + 2) + s_wp[starts]
+        slot_off = np.zeros(-(-starts.size // 8) * 8, np.uint16)
+        slot_off[:starts.size] = offs.astype(np.uint16)
     # columns: dense (an entry off n' = 0) get the LC-point transform; the
     # rest are constant (every entry at n' = 0) or zero
     occ = np.zeros(NC, np.uint64)
@@ -336,7 +364,8 @@ def build_image_tables(pats, N: int) -> ImageTables:
                        thr_b=thr_b.astype(np.int32), gmeta=gmeta, srot=srot, dcols=dcols,
                        dmask=occ[dcols], kcols=kcols,
                        s_mult=int(np.bincount(inv, minlength=n_s).max()), fold=fold,
-                       meta_bits=mbits)
+                       meta_bits=mbits, fold_code=fold_code, thr_slot=thr_slot,
+                       slot_off=slot_off)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:
@@ -474,7 +503,8 @@ class SearchPipeline:
         self.d_img_cmeta = d(it.c_meta.view(np.int32))
         self.d_img_cbase, self.d_img_c2 = d(it.cell_base), d(it.c2)
         self.d_img_thrb = d(it.thr_b)
-        self.d_img_gmeta = d(it.gmeta.view(np.int16 if it.meta_bits == 16 else np.int32))
+        self.d_img_gmeta = d(it.gmeta_device_bytes().view(np.int16 if it.meta_bits == 16
+                                                          else np.int32))
         self.d_img_srot = d(it.srot.view(np.int64))
         self.d_img_dcols, self.d_img_dmask = d(it.dcols), d(it.dmask.view(np.int64))
         self.d_img_kcols = d(it.kcols)

@@ -65,19 +65,34 @@ def _emulate(T, slices, N, fftshift):
     twN = np.exp(2j * np.pi * np.arange(N) / N)
     wf = np.exp(2j * np.pi * np.arange(fold) / fold)      # W_FOLD^k
     n_thr = T.thr_b.size - 1
+    compact = T.fold_code is not None
     for p in range(fold):
-        buf = np.full((LC, NC), np.nan, np.complex128)
+        # the column buffer with its row pitch NC + 2 (the compact tables of
+        # the 32-bit form address it as n' * (NC + 2) + w')
+        bufp = np.full((LC, NC + 2), np.nan, np.complex128)
         for t in range(n_thr):
             b, e = int(T.thr_b[t]), int(T.thr_b[t + 1])
             acc = 0j
+            si = int(T.thr_slot[t]) if compact else 0
             for i in range(e - b):
                 col, npr, q, last, rot = _meta_fields(T, int(T.gmeta[i // epv, t, i % epv]))
+                if compact:   # the fold reads q and last from the nibble table
+                    code = (int(T.fold_code[i // 8, t]) >> (4 * (i % 8))) & 15
+                    q, last = code & 7, code >> 3
                 sr = (int(T.srot[t]) >> (2 * i)) & 3 if rot is None else int(rot)
                 stat = (1j) ** ((sr & 1) + (2 if (sr & 2) and fftshift else 0))
                 acc += S[b + i] * stat * wf[(int(q) * p) % fold]
                 if last:
-                    buf[int(npr), int(col)] = acc
+                    if compact:
+                        off = int(T.slot_off[si])
+                        si += 1
+                        bufp.reshape(-1)[off] = acc
+                    else:
+                        bufp[int(npr), int(col)] = acc
                     acc = 0j
+            if compact:
+                assert si == int(T.thr_slot[t + 1])
+        buf = bufp[:, :NC]
         out = np.full((LC, NC), np.nan, np.complex128)
         for col, occ in zip(T.dcols.tolist(), T.dmask.tolist()):
             y = np.array([buf[n, col] if (occ >> n) & 1 else 0j for n in range(LC)])
@@ -158,6 +173,21 @@ def test_image_tables_layout(N):
     for kc in T.kcols.tolist():
         assert occ.get(kc & 0xFFFF, 0) == (1 if kc >> 16 else 0)
     assert T.cell_base[-1] == T.c_meta.size and np.all(T.cell_base % 64 == 0)
+    if T.meta_bits == 32:
+        # the fold's compact tables: nibbles q | last << 3, slots in S order
+        code = (T.fold_code[idx // 8, owner].astype(np.int64) >> (4 * (idx % 8))) & 15
+        assert np.array_equal(code & 7, q) and np.array_equal(code >> 3, last_bit)
+        starts = np.flatnonzero(np.r_[True, slot[1:] != slot[:-1]])
+        n_sl = starts.size
+        assert T.thr_slot.size == n_thr + 1 and T.thr_slot[-1] == n_sl
+        assert np.all(np.diff(T.thr_slot) >= 0)
+        assert np.array_equal(T.thr_slot[:-1], np.searchsorted(starts, T.thr_b[:-1]))
+        assert np.array_equal(T.slot_off[:n_sl], npr[starts] * (NC + 2) + col[starts])
+        assert T.slot_off.size % 8 == 0 and n_sl <= LC * NC
+        # device bytes: gmeta, nibbles, thr_slot padded to 16 bytes, slot_off
+        nb = T.gmeta_device_bytes().size
+        assert nb == (T.gmeta.nbytes + T.fold_code.nbytes + -(-(n_thr + 1) // 4) * 16 +
+                      T.slot_off.nbytes)
     for g, p in enumerate(pats):                # padding after each chgroup's run
         assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
     assert T.n_s <= geo["s_capacity"]          # fits the kernel's shared S arrays
