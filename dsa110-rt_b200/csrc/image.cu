@@ -313,6 +313,7 @@ struct ImgGeom {
   static constexpr size_t GM_BYTES = (size_t)(MAXE / 4) * THREADS * 16;
   static constexpr size_t FC_BYTES = (size_t)MAXC * THREADS * 4;
   static constexpr size_t TS_BYTES = (size_t)((THREADS + 1 + 3) / 4) * 16;
+  static constexpr size_t ROT_BYTES = (size_t)THREADS * 16;  // 2 bits x 64 entries
   static constexpr int MAX_SLOTS = LC * NC;
   static_assert(C1 * C1 == LC && R1 * R2 == N && R2 % R1 == 0, "unsupported size");
   static_assert(2 * P >= N, "a row pair's slots must hold the transpose and two output rows");
@@ -399,8 +400,15 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
     if (tid == 0) dsb_flag(A.status, DSB_E_CAPACITY);
     return;  // every thread leaves, before any TMEM is taken
   }
-  // rotation bits of the 16-bit form: 2 per entry (packed | parity << 1)
+  // rotation bits: 2 per entry (packed | parity << 1); the 16-bit form's in
+  // srot, the 32-bit form's in the compact tables after gmeta (entry i at
+  // bits 2 (i % 16) of word i / 16)
   const unsigned long long srot = Gm::META32 ? 0ull : __ldg(A.srot + tid);
+  uint4 rot32 = make_uint4(0u, 0u, 0u, 0u);
+  if constexpr (Gm::META32)
+    rot32 = __ldg(reinterpret_cast<const uint4*>(reinterpret_cast<const uint8_t*>(A.gmeta) +
+                                                 Gm::GM_BYTES + Gm::FC_BYTES + Gm::TS_BYTES) +
+                  tid);
   const int nch = (__reduce_max_sync(0xffffffffu, sn) + 7) >> 3;  // 8-entry chunks, per warp
   if (warp == 0) {
     tmem_alloc(s_tmem, Gm::TMEM_COLS);
@@ -568,8 +576,12 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       const float* s_im = s_re + A.s_stride;
       const float unfix = ldexpf(scale, -*s_fixk);  // 2^-k x 0.5 / N^2
       for (int c = 0; c < nch; ++c) {
-        unsigned md[8];
-        if constexpr (Gm::META32) load_meta8<N>(gmeta, c, tid, md);
+        // this chunk's 16 rotation bits (32-bit form)
+        unsigned rw = 0u;
+        if constexpr (Gm::META32) {
+          const unsigned w2 = (c & 2) ? ((c & 4) ? rot32.w : rot32.y) : ((c & 4) ? rot32.z : rot32.x);
+          rw = (c & 1) ? (w2 >> 16) : w2;
+        }
         uint32_t r[16];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -577,7 +589,7 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
           float2 v = make_float2(0.f, 0.f);
           if (i < sn) {
             unsigned b;
-            if constexpr (Gm::META32) b = (md[j] >> Gm::ROT_SH) & 3u;
+            if constexpr (Gm::META32) b = (rw >> (2 * j)) & 3u;
             else b = (unsigned)(srot >> (2 * i)) & 3u;
             const float2 x = make_float2(__int2float_rn(__float_as_int(s_re[sb + i])) * unfix,
                                          __int2float_rn(__float_as_int(s_im[sb + i])) * unfix);
@@ -599,7 +611,8 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
       const uint8_t* gt = reinterpret_cast<const uint8_t*>(A.gmeta) + Gm::GM_BYTES;
       const uint32_t* g_code = reinterpret_cast<const uint32_t*>(gt);
       for (int c = 0; c < nch; ++c) s_code[c * THREADS + tid] = __ldg(g_code + c * THREADS + tid);
-      const uint4* g_slot = reinterpret_cast<const uint4*>(gt + Gm::FC_BYTES + Gm::TS_BYTES);
+      const uint4* g_slot =
+          reinterpret_cast<const uint4*>(gt + Gm::FC_BYTES + Gm::TS_BYTES + Gm::ROT_BYTES);
       uint4* s_slot4 = reinterpret_cast<uint4*>(s_code + Gm::MAXC * THREADS);
       for (int i = tid; i < (n_sl + 7) / 8; i += THREADS) s_slot4[i] = __ldg(g_slot + i);
       __syncthreads();

@@ -217,16 +217,18 @@ class ImageTables:
     #                                          nibble q | last << 3 at bits 4 (i % 8)
     thr_slot: Optional[np.ndarray] = None    # (threads + 1) int32: first slot of each thread
     slot_off: Optional[np.ndarray] = None    # (slots, padded to 8) uint16: n' * (N/2 + 2) + w'
+    fold_rot: Optional[np.ndarray] = None    # (threads, 4) uint32: entry i's rotation bits
+    #                                          packed | parity << 1 at bits 2 (i % 16) of word i / 16
 
     def gmeta_device_bytes(self) -> np.ndarray:
         """The bytes of the kernel's gmeta buffer: gmeta, then (32-bit form)
-        fold_code, thr_slot padded to 16 bytes and slot_off."""
+        fold_code, thr_slot padded to 16 bytes, fold_rot and slot_off."""
         parts = [np.ascontiguousarray(self.gmeta).view(np.uint8).reshape(-1)]
         if self.fold_code is not None:
             ts = np.zeros(-(-self.thr_slot.size // 4) * 4, np.int32)
             ts[:self.thr_slot.size] = self.thr_slot
             parts += [self.fold_code.view(np.uint8).reshape(-1), ts.view(np.uint8),
-                      self.slot_off.view(np.uint8)]
+                      self.fold_rot.view(np.uint8).reshape(-1), self.slot_off.view(np.uint8)]
         return np.concatenate(parts)
 
 
@@ -319,7 +321,7 @@ def build_image_tables(pats, N: int) -> ImageTables:
     idx = np.arange(n_s) - thr_b[owner]
     parity = (s_u + s_w) & 1
     srot = np.zeros(n_thr, np.uint64)
-    fold_code = thr_slot = slot_off = None
+    fold_code = thr_slot = slot_off = fold_rot = None
     if mbits == 16:
         epv = 8
         gmeta = np.zeros((cap // epv, n_thr, epv), np.uint16)
@@ -342,6 +344,9 @@ def build_image_tables(pats, N: int) -> ImageTables:
         offs = s_n[starts] * (NC + 2) + s_wp[starts]
         slot_off = np.zeros(-(-starts.size // 8) * 8, np.uint16)
         slot_off[:starts.size] = offs.astype(np.uint16)
+        fold_rot = np.zeros((n_thr, 4), np.uint32)
+        np.bitwise_or.at(fold_rot, (owner, idx // 16),
+                         ((s_pk | (parity << 1)) << (2 * (idx % 16))).astype(np.uint32))
     # columns: dense (an entry off n' = 0) get the LC-point transform; the
     # rest are constant (every entry at n' = 0) or zero
     occ = np.zeros(NC, np.uint64)
@@ -365,7 +370,7 @@ def build_image_tables(pats, N: int) -> ImageTables:
                        dmask=occ[dcols], kcols=kcols,
                        s_mult=int(np.bincount(inv, minlength=n_s).max()), fold=fold,
                        meta_bits=mbits, fold_code=fold_code, thr_slot=thr_slot,
-                       slot_off=slot_off)
+                       slot_off=slot_off, fold_rot=fold_rot)
 
 
 def build_tables(cfg: PipelineConfig, antpos_e, antpos_n, device, core_mask=None) -> Tables:

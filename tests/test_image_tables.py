@@ -79,6 +79,8 @@ def _emulate(T, slices, N, fftshift):
                 if compact:   # the fold reads q and last from the nibble table
                     code = (int(T.fold_code[i // 8, t]) >> (4 * (i % 8))) & 15
                     q, last = code & 7, code >> 3
+                if compact:   # the copy into TMEM reads the rotation table
+                    rot = (int(T.fold_rot[t, i // 16]) >> (2 * (i % 16))) & 3
                 sr = (int(T.srot[t]) >> (2 * i)) & 3 if rot is None else int(rot)
                 stat = (1j) ** ((sr & 1) + (2 if (sr & 2) and fftshift else 0))
                 acc += S[b + i] * stat * wf[(int(q) * p) % fold]
@@ -187,7 +189,10 @@ def test_image_tables_layout(N):
         # device bytes: gmeta, nibbles, thr_slot padded to 16 bytes, slot_off
         nb = T.gmeta_device_bytes().size
         assert nb == (T.gmeta.nbytes + T.fold_code.nbytes + -(-(n_thr + 1) // 4) * 16 +
-                      T.slot_off.nbytes)
+                      T.fold_rot.nbytes + T.slot_off.nbytes)
+        _, _, _, _, rot = _meta_fields(T, T.gmeta[idx // epv, owner, idx % epv])
+        rot_c = (T.fold_rot[owner, idx // 16].astype(np.int64) >> (2 * (idx % 16))) & 3
+        assert np.array_equal(rot_c, rot)
     for g, p in enumerate(pats):                # padding after each chgroup's run
         assert np.all(T.c_meta[T.cell_base[g] + p.ix_row.size:T.cell_base[g + 1]] == 0xFFFFFFFF)
     assert T.n_s <= geo["s_capacity"]          # fits the kernel's shared S arrays
