@@ -299,7 +299,13 @@ int dsb_combine_dense(const void* streams, const int* shifts, const float* scale
  *      its slot) << 15;
  *      32: (max_entries / 4, threads, 4) uint32, entry i of thread t at
  *      [i / 4][t][i % 4] = w' | n' << 8 | (u div LC) << 14 | last << 17 |
- *      (w == N/2) << 18 | ((u + w) & 1) << 19;
+ *      (w == N/2) << 18 | ((u + w) & 1) << 19; then, in the same buffer,
+ *      the fold's compact tables: (max_entries / 8, threads) uint32 with
+ *      entry i's nibble (u div LC) | last << 3 at bits 4 (i % 8) of word
+ *      [i / 8][t]; (threads + 1) int32 first slot of each thread (the slots
+ *      in S order), padded to 16 bytes; (threads, 4) uint32 with entry i's
+ *      (w == N/2) | ((u + w) & 1) << 1 at bits 2 (i % 16) of word [t][i / 16];
+ *      one uint16 per slot, n' * (N/2 + 2) + w', padded to 8 entries;
  *   srot (16-bit form only; may be null for the 32-bit form): (threads)
  *      uint64, 2 bits per entry i at bit 2i: (w == N/2) | ((u + w) & 1) << 1;
  *   dcols/dmask: the n_dense packed columns with an entry off n' = 0 and
