@@ -680,22 +680,31 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB) detect_kernel(const T
 
 // The same detector with the cube staged in shared memory by TMA (float
 // cubes whose fine DMs are whole warps of cells: npix a multiple of 32).
-// Each warp owns 32 consecutive cells of one fine DM and a ring of DET_NST
+// Each warp owns 32 consecutive cells of one fine DM and a ring of NST
 // shared-memory stages, each one block of DB times x 32 cells (one 3-D tile
 // of the cube's tensor map, completing on the stage's mbarrier).  Lane 0
-// issues block b + DET_NST - 1 when the warp starts block b, so the copies
-// run DET_NST - 1 blocks ahead with no registers held for them and no barrier
+// issues block b + NST - 1 when the warp starts block b, so the copies
+// run NST - 1 blocks ahead with no registers held for them and no barrier
 // wider than the warp; times outside [0, n) arrive as zeros.  The marching,
 // the screen and the rare paths are detect_kernel's, so the outputs are the
 // same bits.  A wait that does not complete within DSB_SPIN_LIMIT polls sets
 // count[1] to a quiet NaN (DET_TIMEOUT_BITS) and ends the warp after waiting,
 // again bounded, for its copies in flight.
-constexpr int DET_NST = 4;
 constexpr int DET_TIMEOUT_BITS = 0x7fc00000;
+
+// Steps per block and stages of the TMA form: with the inputs out of the
+// registers, boxcars to 64 afford 32-step blocks (96 ring registers, half
+// the ring moves per step) in three stages of 4 KB per warp; the narrower
+// widths keep detect_kernel's blocks in four stages.
+template <int LOGW>
+struct DetTmaCfg {
+  static constexpr int DB = LOGW == 6 ? 32 : DetCfg<LOGW>::DB;
+  static constexpr int NST = LOGW == 6 ? 3 : 4;
+};
 
 template <int LOGW>
 constexpr int det_tma_smem() {
-  return 8 * DET_NST * DetCfg<LOGW>::DB * 32 * 4 + 8 * DET_NST * 8;
+  return 8 * DetTmaCfg<LOGW>::NST * DetTmaCfg<LOGW>::DB * 32 * 4 + 8 * DetTmaCfg<LOGW>::NST * 8;
 }
 
 template <int LOGW>
@@ -708,7 +717,8 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
   constexpr int MAXW = 1 << LOGW;
   constexpr int K = LOGW + 1;
   constexpr int PL = MAXW / 2;
-  constexpr int DB = DetCfg<LOGW>::DB;
+  constexpr int DB = DetTmaCfg<LOGW>::DB;
+  constexpr int DET_NST = DetTmaCfg<LOGW>::NST;
   constexpr int RS = MAXW + DB;  // ring registers
   constexpr int SB = DB * 32;    // floats per stage
   extern __shared__ __align__(128) uint8_t det_smem[];
@@ -855,7 +865,7 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
   }
   if (!ok && lane == 0) {
     atomicMax(count + 1, DET_TIMEOUT_BITS);
-    for (int c = b; c < min(n_blk, b + DET_NST - 1); ++c)
+    for (int c = b; c < min(n_blk, b + DET_NST); ++c)
       mbar_wait(bars + c % DET_NST, (uint32_t)((c / DET_NST) & 1));
   }
 }
@@ -1074,7 +1084,8 @@ int det_tma_launch(const float* x, int n, int n_f, int npix, long long f_stride,
   *done = false;
   CUtensorMap tm;
   memset(&tm, 0, sizeof(tm));
-  if (!det_cube_tmap(x, n, n_f, npix, f_stride, t_stride, DetCfg<LOGW>::DB, &tm)) return DSB_OK;
+  if (!det_cube_tmap(x, n, n_f, npix, f_stride, t_stride, DetTmaCfg<LOGW>::DB, &tm))
+    return DSB_OK;
   constexpr int smem = det_tma_smem<LOGW>();
   if (cudaFuncSetAttribute(detect_tma_kernel<LOGW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem) != cudaSuccess)
