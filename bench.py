@@ -238,11 +238,12 @@ def measure_int8_peak(dev) -> float:
 
 # DRAM bytes per unit of work of the 512^2 kernels (bf16 ring), from the ncu
 # captures of the medium5 workload (profiles/): image_kernel<512, 1> wrote
-# 1550.277 MB for 1536 images and read 28.840 MB for 2 coarse DMs x 192
-# times x 4 chgroups; detect_kernel<6> read 1619.558 MB for 1536 images
-IMAGE512_DRAM_WRITE_PER_IMAGE = 1550.277e6 / 1536
-IMAGE512_DRAM_READ_PER_SLICE_TIME_CHGROUP = 28.840e6 / (2 * 192 * 4)
-DETECT64_DRAM_READ_PER_IMAGE = 1619.558e6 / 1536
+# 1558.412 MB for 1536 images and read 28.509 MB for 2 coarse DMs x 192
+# times x 4 chgroups; detect_tma_kernel<6> read 1611.367 MB and wrote
+# 16.182 MB (candidates, Layer-2 samples, register spills) for 1536 images
+IMAGE512_DRAM_WRITE_PER_IMAGE = 1558.412e6 / 1536
+IMAGE512_DRAM_READ_PER_SLICE_TIME_CHGROUP = 28.509e6 / (2 * 192 * 4)
+DETECT64_DRAM_PER_IMAGE = (1611.367e6 + 16.182e6) / 1536
 
 
 def stage_traffic(pipe) -> dict:
@@ -259,9 +260,9 @@ def stage_traffic(pipe) -> dict:
                         "ncu dram__bytes_read.sum + dram__bytes_write.sum of image_kernel<512> on "
                         "medium5 (1536 images), scaled by images written and ring slices read")
     if cfg.log_max_width == 6:
-        out["detect"] = (DETECT64_DRAM_READ_PER_IMAGE * nb * nt * (cfg.n_grid / 512) ** 2,
-                         "ncu dram__bytes_read.sum of detect_kernel<6> on medium5 (1536 images of "
-                         "512^2), scaled by image bytes read")
+        out["detect"] = (DETECT64_DRAM_PER_IMAGE * nb * nt * (cfg.n_grid / 512) ** 2,
+                         "ncu dram__bytes_read.sum + dram__bytes_write.sum of detect_tma_kernel<6> "
+                         "on medium5 (1536 images of 512^2), scaled by image bytes read")
     if cfg.n_grid == 256 and cfg.ring_dtype != "cint8":
         cpb = max(1, nb // cfg.fine_per_coarse)
         rd = IMAGE_DRAM_READ_PER_SLICE_TIME * (IMAGE_DRAM_READ_C64_RATIO
