@@ -748,9 +748,13 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
     const float lv = thr / sinv[k];
     tau[k] = lv - fabsf(lv) * 0x1p-20f;
   }
-  float ring[RS];
+  // the ring as float32 pairs (slot i in rg[i / 2], .x even, .y odd), so
+  // that two consecutive steps' boxcars of one width are one packed
+  // float32x2 subtraction where their slots align (widths 4 and up)
+  float2 rg[(RS + 1) / 2];
 #pragma unroll
-  for (int q = 0; q < RS; ++q) ring[q] = 0.f;
+  for (int q = 0; q < (RS + 1) / 2; ++q) rg[q] = make_float2(0.f, 0.f);
+  auto ring = [&](int i) -> float& { return (i & 1) ? rg[i >> 1].y : rg[i >> 1].x; };
   double run = 0.0;
   float last = 0.f;
   const int total = n + MAXW;
@@ -776,14 +780,9 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
     for (int b = 0; b < min(DET_NST - 1, n_blk); ++b) issue(b);
   }
   __syncwarp();
-  auto output = [&](int j, int ta, auto with_samples) {
-    BoxSums<K> d;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int w = 1 << k;
-      const int off = PL - w / 2;
-      d.v[k] = ring[j + off + w] - ring[j + off];
-    }
+  // the screen, the threshold hits and the Layer-2 samples of one output
+  // from its boxcar sums
+  auto decide = [&](const BoxSums<K>& d, int ta, auto with_samples) {
     bool hit = false;
 #pragma unroll
     for (int k = 0; k < K; ++k) hit |= d.v[k] > tau[k];
@@ -793,6 +792,40 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
       s_i = r.x;
       s_t = r.y;
     }
+  };
+  auto output = [&](int j, int ta, auto with_samples) {
+    BoxSums<K> d;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int w = 1 << k;
+      const int off = PL - w / 2;
+      d.v[k] = ring(j + off + w) - ring(j + off);
+    }
+    decide(d, ta, with_samples);
+  };
+  // the screens of steps j and j + 1 (j even): widths 1 and 2 one by one,
+  // the wider ones (both slots even) as packed pairs, with the same
+  // roundings; an output that passes a screen or holds a Layer-2 sample
+  // (rare) recomputes its sums from the ring and decides as output does
+  auto output2 = [&](int j, int ta, auto with_samples) {
+    bool hit0 = false, hit1 = false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int w = 1 << k;
+      const int off = PL - w / 2;
+      if (w >= 4 && PL % 2 == 0) {
+        const float2 dd = f2_sub(rg[(j + off + w) >> 1], rg[(j + off) >> 1]);
+        hit0 |= dd.x > tau[k];
+        hit1 |= dd.y > tau[k];
+      } else {
+        hit0 |= ring(j + off + w) - ring(j + off) > tau[k];
+        hit1 |= ring(j + 1 + off + w) - ring(j + 1 + off) > tau[k];
+      }
+    }
+    if (hit0 || (decltype(with_samples)::value && ta - t_base == s_t))
+      output(j, ta, with_samples);
+    if (hit1 || (decltype(with_samples)::value && ta + 1 - t_base == s_t))
+      output(j + 1, ta + 1, with_samples);
   };
   int b = 0;
   bool ok = true;
@@ -821,24 +854,26 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
           run += (double)(sx[32 * j] * mval);
           v = (float)run;
         }
-        ring[MAXW + j] = v;
+        ring(MAXW + j) = v;
       }
-      last = ring[MAXW + DB - 1];
+      last = ring(MAXW + DB - 1);
     } else if (J0 >= PL + 1 && J0 + DB - 1 <= PL + n && J0 - MAXW >= t_base &&
                J0 + DB - 1 - MAXW < t_base + n_out) {
       auto steady = [&](auto with_samples) {
 #pragma unroll
-        for (int j = 0; j < DB; ++j) {
+        for (int j = 0; j < DB; j += 2) {
           run += (double)(sx[32 * j] * mval);
-          ring[MAXW + j] = (float)run;
-          output(j, J0 + j - MAXW, with_samples);
+          ring(MAXW + j) = (float)run;
+          run += (double)(sx[32 * (j + 1)] * mval);
+          ring(MAXW + j + 1) = (float)run;
+          output2(j, J0 + j - MAXW, with_samples);
         }
       };
       if ((unsigned)(s_t - (J0 - MAXW - t_base)) < (unsigned)DB)
         steady(std::true_type{});
       else
         steady(std::false_type{});
-      last = ring[MAXW + DB - 1];
+      last = ring(MAXW + DB - 1);
     } else {
 #pragma unroll
       for (int j = 0; j < DB; ++j) {
@@ -854,14 +889,15 @@ __global__ void __launch_bounds__(256, DetCfg<LOGW>::MINB)
           } else {
             v = last;
           }
-          ring[MAXW + j] = v;
+          ring(MAXW + j) = v;
           const int ta = J - MAXW;
           if (ta >= t_base && ta < t_base + n_out) output(j, ta, std::true_type{});
         }
       }
     }
+    static_assert(DB % 2 == 0, "blocks of whole slot pairs");
 #pragma unroll
-    for (int q = 0; q < MAXW; ++q) ring[q] = ring[q + DB];
+    for (int q = 0; q < (MAXW + 1) / 2; ++q) rg[q] = rg[q + DB / 2];
   }
   if (!ok && lane == 0) {
     atomicMax(count + 1, DET_TIMEOUT_BITS);
