@@ -654,8 +654,11 @@ __global__ void __launch_bounds__(ImgGeom<N>::THREADS, ImgGeom<N>::CTAS)
                 }
                 acc = cadd(acc, v);
                 if (code & 8u) {
-                  const unsigned off = s_soff[si++];
-                  if (DSB_INB(off, Gm::BUF, A.status)) buf[off] = acc;
+                  if (DSB_INB(si, n_sl, A.status)) {
+                    const unsigned off = s_soff[si];
+                    if (DSB_INB(off, Gm::BUF, A.status)) buf[off] = acc;
+                  }
+                  ++si;
                   acc = make_float2(0.f, 0.f);
                 }
               }
