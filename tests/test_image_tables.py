@@ -202,3 +202,31 @@ def test_image_tables_layout(N):
     hit[T.c_meta[live] & 0xFFFF] = True
     hit[T.c2[:, 1] & 0xFFFF] = True
     assert hit.all()
+
+
+def test_metric_configuration_tables_fit_and_restate_irfft2():
+    """The 512^2 tables of the metric configuration's array (96 antennas on
+    the bench's seeded T layout, 16 x 384 channels summed 16 to a subband)
+    fit the kernel (S capacity, entries per thread, slots of the compact fold
+    tables), and the kernel's steps restated from them give irfft2."""
+    from dsb200 import synth
+    from dsb200.pipeline import image_geometry
+    N, csf = 512, 16
+    e, n = synth.t_layout(96, seed=11)
+    band = O.REFERENCE_BAND
+    cell = O.top_of_band_cell_lambda(e, n, band, N)
+    pats = []
+    for g in range(band.n_chgroup):
+        r, c = O.build_pattern(e, n, band, g, n_grid=N, csf=csf, cell_lambda=cell)
+        pats.append(types.SimpleNamespace(ix_row=r, ix_col=c))
+    T = build_image_tables(pats, N)
+    geo = image_geometry(N)
+    assert 20000 < T.n_s <= geo["s_capacity"]
+    assert np.diff(T.thr_b).max() <= geo["max_entries"]
+    assert int(T.thr_slot[-1]) <= (N // T.fold) * (N // 2)
+    rng = np.random.default_rng(96)
+    slices = [rng.standard_normal(p.ix_row.size) + 1j * rng.standard_normal(p.ix_row.size)
+              for p in pats]
+    got = _emulate(T, slices, N, True)
+    want = _definition(pats, slices, N, True)
+    assert np.abs(got - want).max() <= 1e-12 * max(1.0, np.abs(want).max())
