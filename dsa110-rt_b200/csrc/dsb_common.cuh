@@ -124,7 +124,7 @@ DSB_DEV void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
 DSB_DEV void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// One 3-D tile of a tensor map (this GPU's global memory; no multicast) into
+// One 3-D tile of a tensor map (this GPU's global memory, one CTA) into
 // this CTA's shared memory, completing on `bar`.  The innermost coordinate
 // times the element size must be a multiple of 16 bytes.
 DSB_DEV void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
@@ -134,7 +134,7 @@ DSB_DEV void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint6
       "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
-// One 4-D tile of a tensor map (this GPU's global memory; no multicast) into
+// One 4-D tile of a tensor map (this GPU's global memory, one CTA) into
 // this CTA's shared memory, completing on `bar`.  The innermost coordinate
 // times the element size must be a multiple of 16 bytes.
 DSB_DEV void tma_load_4d(void* dst, const void* tmap, int x, int y, int z, int w,
