@@ -330,6 +330,11 @@ struct ImgGeom {
   static_assert(SMEM <= 227 * 1024, "shared memory of one CTA");
   static_assert(!META32 || (size_t)BUF * 8 + FC_BYTES + (size_t)MAX_SLOTS * 2 <= BUFB,
                 "the fold's tables fit beside the column buffer");
+  static_assert(GM_BYTES % 16 == 0 && FC_BYTES % 16 == 0 && TS_BYTES % 16 == 0 &&
+                    ROT_BYTES % 16 == 0,
+                "every table after gmeta starts 16-byte aligned");
+  static_assert(!META32 || ROT_SH == LAST_SH + 1,
+                "the 32-bit entry's rotation bits follow its last bit");
 };
 
 // The 8 metadata entries of chunk c of this thread (entries 8c .. 8c + 7).
